@@ -1,0 +1,374 @@
+#!/usr/bin/env python
+"""Benchmark: Mpaths/s at 1080p for the B200 progressive path tracer.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--config terrain|box_sphere]
+
+A *step* renders one batch of the workload: 64 samples per pixel of the
+1920x1080 terrain configuration (2,420,738 triangles: a 1024^2 fBm
+heightfield + 256 instanced icospheres, 2048x1024 procedural sky, up to 12
+bounces), accumulated into the FP64 buffer by the path-tracing kernel.
+
+`value` is paths per second over the K timed steps with the scene resident
+in HBM, timed with CUDA events; `e2e` is the same metric through the C ABI a
+caller uses (mrtUpdateMesh + mrtSetEnvironment + mrtCommitScene + 64 x
+mrtRenderFrame + mrtReadFramebuffer(RGBA32F) into host memory), wall-clock
+timed, host<->device copies included. With N > 1 GPUs (torchrun, one process
+per GPU) each rank renders its own sample stream (frame index = rank + N * s)
+and one NCCL reduce per step sums the FP64 accumulation buffers on rank 0
+(weak scaling). `--impl reference` times the CPU restatement of the reference
+path tracer (the oracle) on all host cores, on bounded samples of the same
+workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "Mpaths/s at 1080p"
+UNIT = "Mpaths/s"
+# algorithmic bytes per counted unit: one BVH node record, one
+# triangle test's vertices, one surface gather, one pixel's FP64 accumulation RMW
+NODE_BYTES, TRI_BYTES, HIT_BYTES, ACCUM_BYTES = 32, 48, 312, 64
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--config", choices=["terrain", "box_sphere"], default="terrain")
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def make_scene(name):
+    from miniraytrace_b200 import scenes
+    if name == "terrain":
+        return scenes.terrain()
+    return scenes.box_sphere(1920, 1080, spp=16)
+
+
+def workload_desc(scene):
+    st = scene.settings
+    if scene.name == "terrain":
+        return (f"terrain {st['width']}x{st['height']}, {scene.spp} spp/step, max bounces {st['max_bounces']}, "
+                f"{scene.triangle_count:,} triangles (1024^2 fBm heightfield + 256 x 1280-triangle icosphere "
+                f"instances), 2048x1024 procedural sky, env importance sampling + MIS")
+    return f"box_sphere {st['width']}x{st['height']}, {scene.spp} spp/step, sun light"
+
+
+# ---- clocks ---------------------------------------------------------------------------
+
+class ClockSampler:
+    """nvidia-smi sampling during the timed region (200 ms period)."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.gpu)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(smax)), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---- roofline inputs --------------------------------------------------------------------
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic_per_launch(config):
+    """DRAM bytes (read + write) per path-tracing launch of this workload from
+    the committed ncu summary (profiles/pathtrace_<config>.md), or None."""
+    p = ROOT / "profiles" / f"pathtrace_{config}.md"
+    if not p.exists():
+        return None
+    m = re.search(r"dram bytes per full launch:\s*([0-9.eE+]+)", p.read_text())
+    return float(m.group(1)) if m else None
+
+
+# ---- CPU side (oracle) ------------------------------------------------------------------
+
+def cpu_sample_rate(scene, seconds, threads, label):
+    """Paths/s of the oracle (FP32 restatement of the reference shaders) on a
+    bounded pixel sample of `scene` at 1 spp, using `threads` host threads."""
+    import oracle
+    from oracle import build_oracle
+    build_oracle.build()
+    o = oracle.OracleScene(scene.settings["width"], scene.settings["height"])
+    scene.apply(o)
+    o.commit()
+    npix = scene.settings["width"] * scene.settings["height"]
+    rng = np.random.default_rng(12345)
+    pilot = rng.choice(npix, size=min(npix, 4000), replace=False).astype(np.uint32)
+    t0 = time.perf_counter()
+    o.render_f32(0, 1, pixels=pilot, threads=threads)
+    rate = pilot.size / max(time.perf_counter() - t0, 1e-6)
+    n = int(min(npix, max(2000, rate * seconds)))
+    return o, rng, n, label
+
+
+def run_cpu_sample(o, rng, n, npix, threads, frame):
+    pix = rng.choice(npix, size=n, replace=False).astype(np.uint32)
+    t0 = time.perf_counter()
+    o.render_f32(frame, 1, pixels=pix, threads=threads)
+    return n / (time.perf_counter() - t0)
+
+
+# ---- arms ----------------------------------------------------------------------------
+
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    scene = make_scene(args.config)
+    threads = os.cpu_count() or 1
+    npix = scene.settings["width"] * scene.settings["height"]
+    o, rng, n, _ = cpu_sample_rate(scene, max(2.0, args.cpu_seconds / 3), threads, "reference")
+    for w in range(args.warmup):
+        run_cpu_sample(o, rng, max(1000, n // 4), npix, threads, 1000 + w)
+    rates = [run_cpu_sample(o, rng, n, npix, threads, s) for s in range(args.steps)]
+    value = float(np.mean(rates)) / 1e6
+    sample = (f"{n} uniformly drawn pixels x 1 spp per step of the {args.config} workload "
+              f"(full frame = {npix} pixels x {scene.spp} spp)")
+    out = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": float(n / (value * 1e6) * 1e3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": workload_desc(scene), "triangles": scene.triangle_count},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out), flush=True)
+    return 0
+
+
+def ours_arm(args):
+    import miniraytrace_b200 as mrt
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    import torch
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    else:
+        torch.cuda.set_device(0)
+
+    scene = make_scene(args.config)
+    W, H, spp = scene.settings["width"], scene.settings["height"], scene.spp
+    paths_per_step = W * H * spp
+
+    mrt.build.build()
+    eng = mrt.Engine(W, H, gpu_index1=local + 1)
+    ids = scene.apply(eng)
+    commit = eng.commit()
+    st0 = eng.stats()
+    eng.set_sample_stream(rank, world)
+
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")  # > 126 MB L2
+    red = torch.empty((H, W, 4), dtype=torch.float64, device="cuda") if world > 1 else None
+
+    def step():
+        eng.render_frames(spp)
+        if world > 1:
+            # every rank's buffer holds its own cumulative samples; their sum on
+            # rank 0 is the combined image of all ranks' sample streams
+            eng.copy_accumulation_device(red.data_ptr(), red.numel() * 8, False)
+            dist.reduce(red, dst=0)
+
+    for _ in range(args.warmup):
+        flush.fill_(1)
+        step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    kernel_ms, counters = [], []
+    launches = 0
+    for k in range(args.steps):
+        flush.fill_(k & 0xFF)  # evict the previous step's scene lines from L2
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        ev[k][0].record()
+        step()
+        ev[k][1].record()
+        torch.cuda.synchronize()
+        s = eng.stats()
+        kernel_ms.append(s["lastRenderMs"])
+        counters.append(s)
+        launches += s["kernelLaunches"]
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    total = torch.tensor([sum(step_ms)], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(total, op=dist.ReduceOp.MAX)
+    total_ms = float(total.item())
+    value = world * paths_per_step * args.steps / (total_ms / 1e3) / 1e6
+
+    # roofline of the dominant kernel (path tracing), per launch
+    c = counters[-1]
+    algo_bytes = (c["nodeFetches"] * NODE_BYTES + c["triTests"] * TRI_BYTES + c["surfaceHits"] * HIT_BYTES
+                  + W * H * ACCUM_BYTES)
+    launch_s = float(np.mean(kernel_ms)) / 1e3
+    achieved = algo_bytes / launch_s / 1e9
+    peak, peak_kind = measured_peaks()
+    traffic = ncu_traffic_per_launch(args.config)
+    rays = c["raysClosest"] + c["raysShadow"]
+
+    # end to end through the C ABI with host buffers (rank-local)
+    e2e = None
+    if args.e2e_steps > 0:
+        hf = scene.meshes[0]
+        host_img = np.empty((H, W, 4), np.float32)
+        e2e_times, h2d = [], []
+        for k in range(args.e2e_steps + 1):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            eng.update_mesh(ids["meshes"][0], hf.positions, hf.indices, hf.normals, hf.uvs)
+            eng.set_environment(scene.environment, scene.env_rotation, scene.env_intensity)
+            eng.commit()
+            h2d.append(eng.stats()["commitH2DBytes"])
+            for _ in range(spp):
+                eng.render_frame()
+            eng.read_framebuffer(mrt.MRT_PIXEL_RGBA32F_LINEAR, out=host_img)
+            dt = time.perf_counter() - t0
+            if k > 0:  # first one warms the host-side allocations
+                e2e_times.append(dt)
+        e2e_t = torch.tensor([float(np.mean(e2e_times))], dtype=torch.float64, device="cuda")
+        if dist:
+            dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
+        e2e = {"value": world * paths_per_step / float(e2e_t.item()) / 1e6, "unit": UNIT,
+               "h2d_bytes_per_step": int(np.mean(h2d)), "d2h_bytes_per_step": W * H * 16,
+               "seconds_per_step": float(e2e_t.item()),
+               "breakdown": "mrtUpdateMesh(heightfield) + mrtSetEnvironment + mrtCommitScene (BVH rebuild, "
+                            "packing, env CDF kernel, uploads) + 64 x mrtRenderFrame + RGBA32F readback"}
+
+    out = None
+    if rank == 0:
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            threads = os.cpu_count() or 1
+            o, rng, n, _ = cpu_sample_rate(scene, args.cpu_seconds, threads, "port")
+            r = run_cpu_sample(o, rng, n, W * H, threads, 7)
+            cpu = {"value": r / 1e6, "unit": UNIT, "cores": threads, "kind": "port",
+                   "sample": f"{n} uniformly drawn pixels x 1 spp of the same workload (oracle FP32, "
+                             f"{threads} threads)"}
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": workload_desc(scene), "width": W, "height": H, "spp_per_step": spp,
+                       "max_bounces": scene.settings["max_bounces"], "triangles": scene.triangle_count,
+                       "l2": "scene arrays (%.0f MB) exceed the 126 MB L2; a 256 MiB buffer is also written "
+                             "between timed steps" % (st0["deviceBytes"] / 1e6),
+                       "parallelism": ("single GPU" if world == 1 else
+                                       f"{world} sample-striped replicas + 1 NCCL reduce of the FP64 "
+                                       f"accumulation per step"),
+                       "accumulation": "fp64"},
+            "gpu_launches": launches,
+            "kernel_ms_per_launch": float(np.mean(kernel_ms)),
+            "mrays_per_s": world * rays / launch_s / 1e6,
+            "rays_per_path": rays / paths_per_step,
+            "commit_ms": commit["commitMs"],
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "peak_source": peak_kind,
+                         "algorithmic_bytes_per_launch": algo_bytes,
+                         "note": "algorithmic bytes = node records x 32 B + triangle tests x 48 B + hits x 312 B "
+                                 "+ pixels x 64 B, counted in the same launch; most are served by L2"},
+            "clocks": clocks,
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(out), flush=True)
+    eng.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        return reference_arm(args)
+    return ours_arm(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

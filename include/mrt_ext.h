@@ -1,0 +1,106 @@
+/*
+ * mrt_ext.h -- extensions of the MiniRaytrace C ABI exported by libmrt.so.
+ *
+ * The reference ABI versions its structs by `structSize >= sizeof(T)`
+ * (reference capi/src/capi.cpp:23-24), so appending a field to any v1 struct
+ * would make every existing caller fail with MRT_ERROR_INVALID_ARGUMENT. Every
+ * new capability is therefore a new exported function with its own structs.
+ * None of these functions has a counterpart in the reference ABI; each one
+ * names the reference behaviour it builds on.
+ */
+#ifndef MRT_EXT_H
+#define MRT_EXT_H
+
+#include "mini_raytrace.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Equivalent to `count` consecutive mrtRenderFrame calls (reference
+ * Renderer.cpp:773-843: one sample per pixel per frame, stop at sppLimit),
+ * issued as one device submission. outInfo reports the state after the last
+ * sample. */
+MRT_API mrtResult mrtxRenderFrames(mrtEngine*, uint32_t count, mrtFrameInfo* outInfo);
+
+/* One ray of a trace query: world space, t in (1e-4, tMax). */
+typedef struct mrtxRay {
+    float origin[3];
+    float tMax;
+    float dir[3];
+    float pad;
+} mrtxRay;
+
+/* Closest hit of one ray. instance = the mrtInstanceId that was hit (0 on a
+ * miss); prim = triangle index in the mesh's own index buffer order (the
+ * reference's "original" triangle order before the BVH leaf reordering,
+ * reference Renderer.cpp:403-411); u, v = barycentrics of vertices 1 and 2. */
+typedef struct mrtxHit {
+    float t;
+    uint32_t instance;
+    uint32_t prim;
+    uint32_t hit;
+    float u, v;
+    uint32_t pad[2];
+} mrtxHit;
+
+/* Closest-hit traversal of the committed scene (reference intersect.glsl:
+ * 88-125 `traceRay`) for `count` rays; commits pending scene changes first. */
+MRT_API mrtResult mrtxTraceRays(mrtEngine*, const mrtxRay* rays, uint32_t count, mrtxHit* hits);
+
+/* Any-hit traversal (reference intersect.glsl:128-178 `traceShadowRay`):
+ * occluded[i] = 1 when ray i hits anything in (1e-4, tMax), else 0. */
+MRT_API mrtResult mrtxTraceShadowRays(mrtEngine*, const mrtxRay* rays, uint32_t count,
+                                      uint32_t* occluded);
+
+/* The FP64 accumulation buffer: 4 doubles per pixel (sum r, g, b, and the
+ * sample count), row-major, top row first. dstSize >= width*height*32. */
+MRT_API mrtResult mrtxReadAccumulation(mrtEngine*, double* dst, size_t dstSize,
+                                       uint32_t* outSpp);
+
+/* Device timings and counters. All times are CUDA-event times in ms. */
+typedef struct mrtxStats {
+    size_t structSize;
+    float lastRenderMs;    /* device time of the last render call's kernels */
+    uint32_t lastRenderSpp; /* samples per pixel rendered by that call */
+    float commitBvhMs;     /* last commit: acceleration structure build */
+    float commitEnvCdfMs;  /* last commit: environment CDF kernel */
+    float commitUploadMs;  /* last commit: host-to-device copies */
+    float commitTotalMs;   /* last commit: host wall time */
+    uint32_t bvhNodes;     /* total nodes (all BLAS + TLAS) */
+    uint32_t triangles;    /* total triangles */
+    uint32_t instances;    /* total instances */
+    uint32_t kernelLaunches; /* kernels launched by the last render call */
+    uint64_t deviceBytes;  /* device memory held by the engine */
+    /* counters of the last render call (all samples of all pixels) */
+    uint64_t raysClosest;  /* closest-hit rays traced */
+    uint64_t raysShadow;   /* shadow (any-hit) rays traced */
+    uint64_t nodeFetches;  /* 32-byte BVH node records read */
+    uint64_t triTests;     /* ray/triangle tests (48 bytes of vertices each) */
+    uint64_t surfaceHits;  /* hits shaded (one surface gather each) */
+    uint64_t commitH2DBytes; /* bytes copied host-to-device by the last commit */
+} mrtxStats;
+MRT_API mrtResult mrtxGetStats(mrtEngine*, mrtxStats* out);
+
+/* The environment CDF exactly as the commit builds it (reference
+ * Renderer.cpp:620-655), computed by the device kernel on this engine's GPU:
+ * rgba = w*h RGBA32F texels; cdfOut receives w*h + h floats (conditional rows,
+ * then the marginal); *integralOut receives the float integral. */
+MRT_API mrtResult mrtxBuildEnvCdf(mrtEngine*, const float* rgba, uint32_t w, uint32_t h,
+                                  float* cdfOut, float* integralOut);
+
+/* Sample-stream striping for replicas: sample s of this engine uses the
+ * random stream of frame index (s * stride + offset). stride = 1, offset = 0
+ * is the reference stream (reference pathtrace.comp:105). Resets accumulation. */
+MRT_API mrtResult mrtxSetSampleStream(mrtEngine*, uint32_t offset, uint32_t stride);
+
+/* Copy the FP64 accumulation buffer (layout as mrtxReadAccumulation) to a
+ * device pointer on this engine's GPU, or add a device buffer of the same
+ * layout into it (accumulate != 0). Used to reduce replicas' samples. */
+MRT_API mrtResult mrtxCopyAccumulationDevice(mrtEngine*, void* devPtr, size_t bytes,
+                                             int32_t accumulate);
+
+#ifdef __cplusplus
+} /* extern "C" */
+#endif
+#endif /* MRT_EXT_H */

@@ -1,0 +1,142 @@
+// Plain-old-data layouts shared by the host engine (C++) and the sm_100a
+// kernels (CUDA). Nothing here is a C++ class: these cross the seam between
+// the host translation units and the .cu translation units as raw bytes.
+//
+// HBM layout of one committed scene (all arrays 16-byte aligned, read-only
+// during a frame, fetched with 128-bit non-coherent loads):
+//
+//   nodes      MrtNode[]     BVH2 nodes, 32 B each. Per mesh a BLAS, then the
+//                            TLAS. Children of an internal node are adjacent
+//                            (left, left + 1), so one 64-byte fetch yields
+//                            both child boxes.
+//   triVerts   float4[3*T]   the three vertex positions of every triangle,
+//                            in BLAS leaf order (48 B per triangle test;
+//                            w of vertex 0 holds the original triangle index
+//                            as bits, w of vertex 1 the global triangle slot).
+//   triIndex   uint4[T]      global vertex indices (i0, i1, i2, original
+//                            index) in the same order, read once per hit.
+//   normals    float4[V]     shading normals (xyz), per global vertex.
+//   uvs        float2[V]
+//   tangents   float4[V]     xyz + handedness.
+//   instances  MrtInstance[] 112 B each, in TLAS leaf order.
+//   materials  MrtMaterial[] 80 B each, index 0 = default material.
+//   lights     MrtLight[]    80 B each, environment at slot 0 when present.
+//   envTexels  float4[w*h]   RGBA32F equirect map.
+//   envCdf     float[w*h+h]  conditional rows, then the marginal.
+//   textures   MrtTexture[64]
+//
+//   accum      double4[W*H]  FP64 running sums (r, g, b, sample count).
+#pragma once
+
+#include <stdint.h>
+#include <vector_types.h>
+
+#ifdef __CUDACC__
+#define MRT_HD __host__ __device__
+#else
+#define MRT_HD
+#endif
+
+#define MRT_MAX_TEXTURES 64
+#define MRT_MAX_BOUNCES_CAP 16
+
+// Reference BVH node semantics (core/src/accel/Bvh.hpp:15-26): count == 0
+// marks an internal node whose children are (leftOrPrim, leftOrPrim + 1);
+// otherwise leftOrPrim is the first triangle (or instance, in the TLAS).
+typedef struct MrtNode {
+    float lo[3];
+    uint32_t leftOrPrim;
+    float hi[3];
+    uint32_t packed;  // (count << 2) | split axis
+} MrtNode;
+
+// Instance: row-major 3x4 transforms (rows of [R | t]).
+typedef struct MrtInstance {
+    float w2o[12];
+    float o2w[12];
+    uint32_t blasRoot;
+    uint32_t materialIndex;
+    uint32_t userId;  // mrtInstanceId
+    uint32_t meshId;
+} MrtInstance;
+
+// Reference GpuMaterial (core/src/render/GpuTypes.hpp:55-61), 80 bytes.
+typedef struct MrtMaterial {
+    float baseColorOpacity[4];
+    float emissionRoughness[4];
+    float params[4];  // metallic, transmission, ior, unused
+    int32_t tex[8];   // baseColor, roughness, metallic, normal, emission, -, -, -
+} MrtMaterial;
+
+// Reference GpuLight (GpuTypes.hpp:69-75), 80 bytes.
+enum { MRT_DLIGHT_ENV = 0, MRT_DLIGHT_SUN = 1, MRT_DLIGHT_POINT = 2, MRT_DLIGHT_RECT = 3 };
+typedef struct MrtLight {
+    float p0[4];  // sun: dir + cos(angular radius) | point: pos | rect: corner + area
+    float p1[4];  // sun: radiance | point: intensity | rect: edge0
+    float p2[4];  // rect: edge1
+    float p3[4];  // rect: radiance + twoSided
+    int32_t type;
+    int32_t pad[3];
+} MrtLight;
+
+enum { MRT_DTEX_RGBA8_SRGB = 0, MRT_DTEX_RGBA8_UNORM = 1, MRT_DTEX_RGBA32F = 2 };
+typedef struct MrtTexture {
+    const void* texels;  // NULL = white 1x1 placeholder
+    uint32_t width, height;
+    uint32_t format;
+    uint32_t pad;
+} MrtTexture;
+
+enum { MRT_FLAG_HAS_ENV = 1u, MRT_FLAG_ORTHO = 4u };
+
+// Everything one path-tracing launch reads; passed by value as the kernel
+// parameter block (no constant-memory update, so launches stay
+// graph-capturable with new parameters).
+typedef struct MrtFrameParams {
+    // camera (reference Renderer.cpp:711-764 fillGlobals)
+    float camPos[3], camRight[3], camUp[3], camForward[3];
+    float frustum[4];  // left, right, bottom, top
+    uint32_t width, height;
+    uint32_t maxBounces, lightCount;
+    uint32_t envW, envH, flags, tlasRoot;
+    float envRotation, envIntensity, envIntegral, fireflyClamp;
+    // Sample streams: the n-th sample since the last reset uses the pcg4d
+    // frame index streamOffset + n * streamStride (reference stream:
+    // offset 0, stride 1, pathtrace.comp:105).
+    uint32_t streamOffset, streamStride;
+    uint32_t nodeCount, instanceCount;
+    // scene arrays (device pointers)
+    const MrtNode* nodes;
+    const float4* triVerts;
+    const uint4* triIndex;
+    const float4* normals;
+    const float2* uvs;
+    const float4* tangents;
+    const MrtInstance* instances;
+    const MrtMaterial* materials;
+    const MrtLight* lights;
+    const float4* envTexels;
+    const float* envCdf;
+    const MrtTexture* textures;
+    // frame buffers
+    double* accum;           // 4 doubles per pixel
+    uint32_t* errorFlags;    // bit 0: traversal stack overflow, bit 1: bad index
+    unsigned long long* rayCounters;  // [closest, shadow], NULL = not counted
+} MrtFrameParams;
+
+// One query ray of mrtxTraceRays (same layout as mrtxRay) and its hit.
+typedef struct MrtQueryRay {
+    float origin[3];
+    float tMax;
+    float dir[3];
+    float pad;
+} MrtQueryRay;
+
+typedef struct MrtQueryHit {
+    float t;
+    uint32_t instance;
+    uint32_t prim;
+    uint32_t hit;
+    float u, v;
+    uint32_t pad[2];
+} MrtQueryHit;

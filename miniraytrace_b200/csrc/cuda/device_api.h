@@ -1,0 +1,50 @@
+// The seam between the host engine (C++, g++) and the sm_100a kernels
+// (CUDA, nvcc): extern "C" launch functions taking plain pointers, sizes and
+// a stream, returning cudaError_t. No C++ type crosses this boundary.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#include "../common/device_types.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+// Path tracing: samples [sampleBase, sampleBase + sampleCount) of every pixel;
+// sampleBase == 0 overwrites the accumulation, otherwise it adds.
+cudaError_t mrtcu_pathtrace(const MrtFrameParams* p, uint32_t sampleBase, uint32_t sampleCount,
+                            cudaStream_t stream);
+
+// Trace queries (closest hit / any hit) for n device-resident rays.
+cudaError_t mrtcu_trace_closest(const MrtFrameParams* p, const MrtQueryRay* rays, uint32_t n, MrtQueryHit* hits,
+                                cudaStream_t stream);
+cudaError_t mrtcu_trace_any(const MrtFrameParams* p, const MrtQueryRay* rays, uint32_t n, uint32_t* occluded,
+                            cudaStream_t stream);
+
+// Environment CDF (reference Renderer.cpp:620-655): texels = w*h float4,
+// sinTheta = h floats (sin((y + 0.5) * pi / h) as evaluated on the host),
+// cdf = w*h + h floats out, rowSums = h doubles of scratch, integral = one
+// float out (device memory).
+cudaError_t mrtcu_env_cdf(const float4* texels, const float* sinTheta, uint32_t w, uint32_t h, float* cdf,
+                          double* rowSums, float* integral, cudaStream_t stream);
+
+// RGBA32F readback conversion: out[i] = (sum / count, 1) with the pixel's
+// own sample count; spp == 0 (nothing accumulated since the last reset)
+// gives (0, 0, 0, 1) as the reference does (Renderer.cpp:904).
+cudaError_t mrtcu_readback_rgba32f(const double* accum, size_t npix, uint32_t spp, float4* out,
+                                   cudaStream_t stream);
+
+// RGBA8 resolve (reference resolve.comp:24-56): mean = sum / count,
+// exposure, optional ACES, sRGB encode, UNORM8 store, alpha 255.
+cudaError_t mrtcu_resolve_rgba8(const double* accum, size_t npix, float exposure, uint32_t tonemap,
+                                uchar4* out, cudaStream_t stream);
+
+// dst[i] += src[i] for n doubles (combining replicas' accumulations).
+cudaError_t mrtcu_add_f64(double* dst, const double* src, size_t n, cudaStream_t stream);
+
+#ifdef __cplusplus
+}
+#endif

@@ -1,0 +1,264 @@
+// The exported C ABI (include/mini_raytrace.h, include/mrt_ext.h).
+//
+// Argument handling mirrors the reference translation layer
+// (capi/src/capi.cpp:10-316): structs shorter than the version compiled
+// here are rejected, a NULL engine yields MRT_ERROR_INVALID_HANDLE for
+// commit/render and MRT_ERROR_INVALID_ARGUMENT for readback/settings, void
+// scene calls ignore bad handles, add-calls return MRT_INVALID_ID, and no C++
+// exception crosses the boundary (std::bad_alloc -> MRT_ERROR_OUT_OF_MEMORY,
+// anything else -> MRT_ERROR_UNKNOWN).
+#include <cstring>
+#include <new>
+
+#include "../../../include/mrt_ext.h"
+#include "engine.h"
+
+namespace {
+
+mrt::Engine* unwrap(mrtEngine* e) { return reinterpret_cast<mrt::Engine*>(e); }
+
+template <class T> bool validStruct(const T* s) { return s && s->structSize >= sizeof(T); }
+
+template <class Fn> mrtResult guarded(Fn fn) {
+    try {
+        return fn();
+    } catch (const std::bad_alloc&) {
+        return mrt::fail(MRT_ERROR_OUT_OF_MEMORY, "host allocation failed");
+    } catch (...) {
+        return mrt::fail(MRT_ERROR_UNKNOWN, "unexpected exception in libmrt");
+    }
+}
+
+template <class Fn> uint32_t guardedId(Fn fn) {
+    try {
+        return fn();
+    } catch (...) {
+        mrt::setLastError("allocation failed while copying scene data");
+        return MRT_INVALID_ID;
+    }
+}
+
+template <class Fn> void guardedVoid(Fn fn) {
+    try {
+        fn();
+    } catch (...) {
+        mrt::setLastError("allocation failed while copying scene data");
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+MRT_API mrtResult mrtCreateEngine(const mrtEngineDesc* desc, mrtEngine** outEngine) {
+    if (!validStruct(desc) || !outEngine) return MRT_ERROR_INVALID_ARGUMENT;
+    return guarded([&] {
+        mrt::Engine* e = nullptr;
+        const mrtResult r = mrt::Engine::create(*desc, &e);
+        if (r == MRT_SUCCESS) *outEngine = reinterpret_cast<mrtEngine*>(e);
+        return r;
+    });
+}
+
+MRT_API void mrtDestroyEngine(mrtEngine* engine) { delete unwrap(engine); }
+
+MRT_API mrtMeshId mrtAddMesh(mrtEngine* e, const mrtMeshDesc* d) {
+    mrt::Engine* eng = unwrap(e);
+    if (!eng || !validStruct(d)) return MRT_INVALID_ID;
+    return guardedId([&] { return eng->scene().addMesh(*d); });
+}
+
+MRT_API void mrtUpdateMesh(mrtEngine* e, mrtMeshId id, const mrtMeshDesc* d) {
+    mrt::Engine* eng = unwrap(e);
+    if (eng && validStruct(d)) guardedVoid([&] { eng->scene().updateMesh(id, *d); });
+}
+
+MRT_API void mrtRemoveMesh(mrtEngine* e, mrtMeshId id) {
+    if (mrt::Engine* eng = unwrap(e)) eng->scene().removeMesh(id);
+}
+
+MRT_API mrtInstanceId mrtAddInstance(mrtEngine* e, mrtMeshId mesh, const float* xform3x4, mrtMaterialId mat) {
+    mrt::Engine* eng = unwrap(e);
+    if (!eng) return MRT_INVALID_ID;
+    return guardedId([&] { return eng->scene().addInstance(mesh, xform3x4, mat); });
+}
+
+MRT_API void mrtSetInstanceTransform(mrtEngine* e, mrtInstanceId id, const float* xform3x4) {
+    if (mrt::Engine* eng = unwrap(e)) eng->scene().setInstanceTransform(id, xform3x4);
+}
+
+MRT_API void mrtRemoveInstance(mrtEngine* e, mrtInstanceId id) {
+    if (mrt::Engine* eng = unwrap(e)) eng->scene().removeInstance(id);
+}
+
+MRT_API mrtMaterialId mrtAddMaterial(mrtEngine* e, const mrtMaterialDesc* d) {
+    mrt::Engine* eng = unwrap(e);
+    if (!eng || !validStruct(d)) return MRT_INVALID_ID;
+    return guardedId([&] { return eng->scene().addMaterial(*d); });
+}
+
+MRT_API void mrtUpdateMaterial(mrtEngine* e, mrtMaterialId id, const mrtMaterialDesc* d) {
+    mrt::Engine* eng = unwrap(e);
+    if (eng && validStruct(d)) eng->scene().updateMaterial(id, *d);
+}
+
+MRT_API void mrtRemoveMaterial(mrtEngine* e, mrtMaterialId id) {
+    if (mrt::Engine* eng = unwrap(e)) eng->scene().removeMaterial(id);
+}
+
+MRT_API mrtTextureId mrtAddTexture(mrtEngine* e, const mrtTextureDesc* d) {
+    mrt::Engine* eng = unwrap(e);
+    if (!eng || !validStruct(d)) return MRT_INVALID_ID;
+    return guardedId([&] { return eng->scene().addTexture(*d); });
+}
+
+MRT_API void mrtRemoveTexture(mrtEngine* e, mrtTextureId id) {
+    if (mrt::Engine* eng = unwrap(e)) eng->scene().removeTexture(id);
+}
+
+MRT_API mrtLightId mrtAddLight(mrtEngine* e, const mrtLightDesc* d) {
+    mrt::Engine* eng = unwrap(e);
+    if (!eng || !validStruct(d)) return MRT_INVALID_ID;
+    return guardedId([&] { return eng->scene().addLight(*d); });
+}
+
+MRT_API void mrtUpdateLight(mrtEngine* e, mrtLightId id, const mrtLightDesc* d) {
+    mrt::Engine* eng = unwrap(e);
+    if (eng && validStruct(d)) eng->scene().updateLight(id, *d);
+}
+
+MRT_API void mrtRemoveLight(mrtEngine* e, mrtLightId id) {
+    if (mrt::Engine* eng = unwrap(e)) eng->scene().removeLight(id);
+}
+
+MRT_API void mrtSetEnvironment(mrtEngine* e, const mrtTextureDesc* hdri, float rotationRad, float intensity) {
+    mrt::Engine* eng = unwrap(e);
+    if (!eng) return;
+    if (!hdri) {
+        eng->scene().clearEnvironment();
+        return;
+    }
+    if (validStruct(hdri)) guardedVoid([&] { eng->scene().setEnvironment(*hdri, rotationRad, intensity); });
+}
+
+MRT_API void mrtSetCamera(mrtEngine* e, const mrtCameraDesc* d) {
+    mrt::Engine* eng = unwrap(e);
+    if (!eng || !validStruct(d)) return;
+    eng->scene().setCamera(*d);
+}
+
+MRT_API void mrtSetCameraEx(mrtEngine* e, const mrtCameraDescEx* d) {
+    mrt::Engine* eng = unwrap(e);
+    if (!eng || !validStruct(d)) return;
+    eng->scene().setCameraEx(*d);
+}
+
+MRT_API mrtResult mrtCommitScene(mrtEngine* e, mrtCommitStats* outStats) {
+    mrt::Engine* eng = unwrap(e);
+    if (!eng) return MRT_ERROR_INVALID_HANDLE;
+    return guarded([&] {
+        mrtCommitStats s{};
+        s.structSize = sizeof(s);
+        const mrtResult r = eng->commit(&s);
+        if (outStats && outStats->structSize >= sizeof(mrtCommitStats)) {
+            outStats->blasRebuilt = s.blasRebuilt;
+            outStats->tlasRebuilt = s.tlasRebuilt;
+            outStats->commitMs = s.commitMs;
+        }
+        return r;
+    });
+}
+
+MRT_API mrtResult mrtSetRenderSettings(mrtEngine* e, const mrtRenderSettings* d) {
+    mrt::Engine* eng = unwrap(e);
+    if (!eng || !validStruct(d)) return MRT_ERROR_INVALID_ARGUMENT;
+    return guarded([&] {
+        mrt::Settings s;
+        s.width = d->width;
+        s.height = d->height;
+        s.maxBounces = d->maxBounces;
+        s.sppLimit = d->sppLimit;
+        s.exposureEV = d->exposureEV;
+        s.fireflyClamp = d->fireflyClamp;
+        s.tonemap = uint32_t(d->tonemap);
+        s.denoise = d->denoise != 0;
+        return eng->setSettings(s);
+    });
+}
+
+MRT_API mrtResult mrtRenderFrame(mrtEngine* e, mrtFrameInfo* outInfo) {
+    mrt::Engine* eng = unwrap(e);
+    if (!eng) return MRT_ERROR_INVALID_HANDLE;
+    return guarded([&] { return eng->renderFrames(1, outInfo); });
+}
+
+MRT_API mrtResult mrtReadFramebuffer(mrtEngine* e, mrtPixelFormat fmt, void* dst, size_t dstSize) {
+    mrt::Engine* eng = unwrap(e);
+    if (!eng || !dst) return MRT_ERROR_INVALID_ARGUMENT;
+    return guarded([&] { return eng->readFramebuffer(fmt, dst, dstSize); });
+}
+
+MRT_API void mrtResetAccumulation(mrtEngine* e) {
+    if (mrt::Engine* eng = unwrap(e)) eng->resetAccumulation();
+}
+
+MRT_API void mrtSetLogCallback(mrtLogFn fn, void* user) { mrt::setLogCallback(fn, user); }
+
+MRT_API const char* mrtResultToString(mrtResult r) { return mrt::resultName(r); }
+
+MRT_API const char* mrtGetLastErrorMessage(void) { return mrt::lastError().c_str(); }
+
+// ---- extensions (include/mrt_ext.h) --------------------------------------------
+
+MRT_API mrtResult mrtxRenderFrames(mrtEngine* e, uint32_t count, mrtFrameInfo* outInfo) {
+    mrt::Engine* eng = unwrap(e);
+    if (!eng) return MRT_ERROR_INVALID_HANDLE;
+    return guarded([&] { return eng->renderFrames(count, outInfo); });
+}
+
+MRT_API mrtResult mrtxTraceRays(mrtEngine* e, const mrtxRay* rays, uint32_t count, mrtxHit* hits) {
+    mrt::Engine* eng = unwrap(e);
+    if (!eng) return MRT_ERROR_INVALID_HANDLE;
+    if (count && (!rays || !hits)) return MRT_ERROR_INVALID_ARGUMENT;
+    return guarded([&] { return eng->traceRays(rays, count, hits); });
+}
+
+MRT_API mrtResult mrtxTraceShadowRays(mrtEngine* e, const mrtxRay* rays, uint32_t count, uint32_t* occluded) {
+    mrt::Engine* eng = unwrap(e);
+    if (!eng) return MRT_ERROR_INVALID_HANDLE;
+    if (count && (!rays || !occluded)) return MRT_ERROR_INVALID_ARGUMENT;
+    return guarded([&] { return eng->traceShadowRays(rays, count, occluded); });
+}
+
+MRT_API mrtResult mrtxReadAccumulation(mrtEngine* e, double* dst, size_t dstSize, uint32_t* outSpp) {
+    mrt::Engine* eng = unwrap(e);
+    if (!eng || !dst) return MRT_ERROR_INVALID_ARGUMENT;
+    return guarded([&] { return eng->readAccumulation(dst, dstSize, outSpp); });
+}
+
+MRT_API mrtResult mrtxGetStats(mrtEngine* e, mrtxStats* out) {
+    mrt::Engine* eng = unwrap(e);
+    if (!eng || !validStruct(out)) return MRT_ERROR_INVALID_ARGUMENT;
+    return guarded([&] { return eng->getStats(out); });
+}
+
+MRT_API mrtResult mrtxBuildEnvCdf(mrtEngine* e, const float* rgba, uint32_t w, uint32_t h, float* cdfOut,
+                                  float* integralOut) {
+    mrt::Engine* eng = unwrap(e);
+    if (!eng) return MRT_ERROR_INVALID_HANDLE;
+    return guarded([&] { return eng->buildEnvCdf(rgba, w, h, cdfOut, integralOut); });
+}
+
+MRT_API mrtResult mrtxSetSampleStream(mrtEngine* e, uint32_t offset, uint32_t stride) {
+    mrt::Engine* eng = unwrap(e);
+    if (!eng) return MRT_ERROR_INVALID_HANDLE;
+    return guarded([&] { return eng->setSampleStream(offset, stride); });
+}
+
+MRT_API mrtResult mrtxCopyAccumulationDevice(mrtEngine* e, void* devPtr, size_t bytes, int32_t accumulate) {
+    mrt::Engine* eng = unwrap(e);
+    if (!eng) return MRT_ERROR_INVALID_HANDLE;
+    return guarded([&] { return eng->copyAccumulationDevice(devPtr, bytes, accumulate != 0); });
+}
+
+}  // extern "C"

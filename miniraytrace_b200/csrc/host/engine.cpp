@@ -1,0 +1,914 @@
+// Engine implementation: commit (packing, BVH builds, environment CDF),
+// rendering, readback. Reference behaviour is cited per function.
+#include "engine.h"
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <future>
+#include <thread>
+
+#include "../cuda/device_api.h"
+
+namespace mrt {
+
+// ---------------------------------------------------------------- buffers --
+
+mrtResult DeviceBuffer::ensure(size_t n) {
+    n = std::max<size_t>(n, 16);
+    if (ptr && bytes >= n) return MRT_SUCCESS;
+    // grow by 1.5x like the reference's scene buffers (Renderer.cpp:323-330)
+    const size_t cap = std::max(n, bytes + bytes / 2);
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    bytes = 0;
+    MRT_CUDA(cudaMalloc(&ptr, cap));
+    bytes = cap;
+    return MRT_SUCCESS;
+}
+
+mrtResult DeviceBuffer::upload(const void* src, size_t n, cudaStream_t s) {
+    MRT_TRY(ensure(n));
+    if (n) MRT_CUDA(cudaMemcpyAsync(ptr, src, n, cudaMemcpyHostToDevice, s));
+    return MRT_SUCCESS;
+}
+
+void DeviceBuffer::release() {
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    bytes = 0;
+}
+
+namespace {
+
+// A node whose inverted box fails every slab test: traversal of an empty
+// scene ends at the root (reference Renderer.cpp:49-58).
+MrtNode sentinelNode() {
+    MrtNode n{};
+    for (int k = 0; k < 3; ++k) {
+        n.lo[k] = 3.402823466e38f;
+        n.hi[k] = -3.402823466e38f;
+    }
+    n.leftOrPrim = 0;
+    n.packed = 1u << 2;
+    return n;
+}
+
+inline float clamp01(float x) { return std::min(std::max(x, 0.0f), 1.0f); }
+
+void normalize3(float v[3]) {
+    const float inv = 1.0f / std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+    v[0] *= inv;
+    v[1] *= inv;
+    v[2] *= inv;
+}
+void cross3(const float a[3], const float b[3], float r[3]) {
+    r[0] = a[1] * b[2] - b[1] * a[2];
+    r[1] = a[2] * b[0] - b[2] * a[0];
+    r[2] = a[0] * b[1] - b[0] * a[1];
+}
+
+// Inverse of a row-major affine 3x4 [R | t], computed in double and rounded.
+void invertAffine(const float m[12], float out[12]) {
+    const double a = m[0], b = m[1], c = m[2], d = m[4], e = m[5], f = m[6], g = m[8], h = m[9], i = m[10];
+    const double A = e * i - f * h, B = -(d * i - f * g), C = d * h - e * g;
+    const double det = a * A + b * B + c * C;
+    const double inv = det != 0.0 ? 1.0 / det : 0.0;
+    const double r[9] = {A * inv,
+                         -(b * i - c * h) * inv,
+                         (b * f - c * e) * inv,
+                         B * inv,
+                         (a * i - c * g) * inv,
+                         -(a * f - c * d) * inv,
+                         C * inv,
+                         -(a * h - b * g) * inv,
+                         (a * e - b * d) * inv};
+    const double t[3] = {m[3], m[7], m[11]};
+    for (int row = 0; row < 3; ++row) {
+        for (int col = 0; col < 3; ++col) out[row * 4 + col] = float(r[row * 3 + col]);
+        out[row * 4 + 3] = float(-(r[row * 3] * t[0] + r[row * 3 + 1] * t[1] + r[row * 3 + 2] * t[2]));
+    }
+}
+
+// World bounds of a box under a row-major 3x4 transform (8 corners, as
+// reference MathTypes.hpp:35-45).
+Box3 transformBox(const Box3& b, const float m[12]) {
+    Box3 o;
+    for (int k = 0; k < 3; ++k) {
+        o.lo[k] = 3.402823466e38f;
+        o.hi[k] = -3.402823466e38f;
+    }
+    for (int i = 0; i < 8; ++i) {
+        const float c[3] = {(i & 1) ? b.hi[0] : b.lo[0], (i & 2) ? b.hi[1] : b.lo[1], (i & 4) ? b.hi[2] : b.lo[2]};
+        for (int r = 0; r < 3; ++r) {
+            const float v = m[r * 4] * c[0] + m[r * 4 + 1] * c[1] + m[r * 4 + 2] * c[2] + m[r * 4 + 3];
+            o.lo[r] = std::min(o.lo[r], v);
+            o.hi[r] = std::max(o.hi[r], v);
+        }
+    }
+    return o;
+}
+
+}  // namespace
+
+// Upload that counts the bytes a commit moves host-to-device.
+mrtResult Engine::up(DeviceBuffer& b, const void* src, size_t n) {
+    m_stats.commitH2DBytes += n;
+    return b.upload(src, n, m_stream);
+}
+
+// ------------------------------------------------------------- lifecycle --
+
+mrtResult Engine::create(const mrtEngineDesc& desc, Engine** out) {
+    Engine* e = new Engine();
+    const mrtResult r = e->init(desc);
+    if (r != MRT_SUCCESS) {
+        delete e;
+        return r;
+    }
+    *out = e;
+    return MRT_SUCCESS;
+}
+
+mrtResult Engine::init(const mrtEngineDesc& desc) {
+    if (desc.width > 0 && desc.height > 0) {
+        m_settings.width = desc.width;
+        m_settings.height = desc.height;
+    }
+    m_validation = desc.enableValidation != 0;
+    m_hostThreads = std::max(1u, std::thread::hardware_concurrency());
+    int count = 0;
+    const cudaError_t ce = cudaGetDeviceCount(&count);
+    if (ce != cudaSuccess || count == 0)
+        return fail(MRT_ERROR_VULKAN_INIT,
+                    std::string("No CUDA device available (") + (ce != cudaSuccess ? cudaGetErrorString(ce) : "0 devices") +
+                        "). This build needs an NVIDIA B200-class GPU (sm_100a) and driver.");
+    for (int i = 0; i < count; ++i) {
+        cudaDeviceProp p{};
+        if (cudaGetDeviceProperties(&p, i) == cudaSuccess)
+            log(LogLevel::Info, "CUDA device [" + std::to_string(i) + "]: " + p.name + " (sm_" +
+                                    std::to_string(p.major) + std::to_string(p.minor) + ", " +
+                                    std::to_string(p.multiProcessorCount) + " SMs)");
+    }
+    if (desc.gpuIndex1 > 0) {
+        const uint32_t idx = desc.gpuIndex1 - 1;
+        if (idx >= uint32_t(count))
+            return fail(MRT_ERROR_VULKAN_INIT, "Requested GPU index " + std::to_string(idx) + " is out of range (" +
+                                                   std::to_string(count) + " device(s) found).");
+        m_device = int(idx);
+    } else {
+        m_device = 0;
+    }
+    const cudaError_t se = cudaSetDevice(m_device);
+    if (se != cudaSuccess)
+        return fail(MRT_ERROR_VULKAN_INIT, std::string("cudaSetDevice failed: ") + cudaGetErrorString(se));
+    cudaDeviceProp prop{};
+    MRT_CUDA(cudaGetDeviceProperties(&prop, m_device));
+    if (prop.major != 10)
+        return fail(MRT_ERROR_SHADER_LOAD, std::string("GPU ") + prop.name + " (sm_" + std::to_string(prop.major) +
+                                               std::to_string(prop.minor) +
+                                               ") cannot run this build's kernels, which are compiled for sm_100a only.");
+    MRT_CUDA(cudaStreamCreateWithFlags(&m_stream, cudaStreamNonBlocking));
+    MRT_CUDA(cudaEventCreate(&m_ev0));
+    MRT_CUDA(cudaEventCreate(&m_ev1));
+    m_copyEvents.resize(16);
+    for (auto& ev : m_copyEvents) MRT_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    log(LogLevel::Info, std::string("GPU: ") + prop.name);
+
+    // pre-commit frames traverse an empty scene safely
+    const MrtNode s = sentinelNode();
+    MRT_TRY(m_nodes.upload(&s, sizeof(s), m_stream));
+    m_nodeCount = 1;
+    m_tlasRoot = 0;
+    const MrtMaterial defMat{{0.8f, 0.8f, 0.8f, 1.0f}, {0, 0, 0, 0.5f}, {0, 0, 1.45f, 0}, {-1, -1, -1, -1, -1, -1, -1, -1}};
+    MRT_TRY(m_materials.upload(&defMat, sizeof(defMat), m_stream));
+    std::vector<MrtTexture> table(MRT_MAX_TEXTURES);
+    std::memset(table.data(), 0, table.size() * sizeof(MrtTexture));
+    MRT_TRY(m_texTable.upload(table.data(), table.size() * sizeof(MrtTexture), m_stream));
+    m_texGeneration.assign(MRT_MAX_TEXTURES, 0);
+    const float black[4] = {0, 0, 0, 1};
+    MRT_TRY(m_envTexels.upload(black, sizeof(black), m_stream));
+    MRT_TRY(m_envCdf.ensure(16));
+    // 1-vertex placeholders so every pointer in the parameter block is valid
+    MRT_TRY(m_triVerts.ensure(48));
+    MRT_TRY(m_triIndex.ensure(16));
+    MRT_TRY(m_normals.ensure(16));
+    MRT_TRY(m_uvs.ensure(16));
+    MRT_TRY(m_tangents.ensure(16));
+    MRT_TRY(m_instances.ensure(sizeof(MrtInstance)));
+    MRT_TRY(m_lights.ensure(sizeof(MrtLight)));
+    MRT_TRY(m_flags.ensure(16));
+    MRT_CUDA(cudaMemsetAsync(m_flags.ptr, 0, 16, m_stream));
+    MRT_TRY(m_rayCounters.ensure(64));
+    MRT_CUDA(cudaMemsetAsync(m_rayCounters.ptr, 0, 64, m_stream));
+    MRT_TRY(allocateFrame());
+    MRT_CUDA(cudaStreamSynchronize(m_stream));
+    m_stats.structSize = sizeof(mrtxStats);
+    return MRT_SUCCESS;
+}
+
+Engine::~Engine() {
+    if (m_stream) {
+        cudaSetDevice(m_device);
+        cudaStreamSynchronize(m_stream);
+    }
+    DeviceBuffer* bufs[] = {&m_nodes,     &m_triVerts, &m_triIndex,   &m_normals,      &m_uvs,        &m_tangents,
+                            &m_instances, &m_materials, &m_lights,     &m_envTexels,    &m_envCdf,     &m_envSin,
+                            &m_envRowSums, &m_envIntegral, &m_texTable, &m_accum,       &m_out32,      &m_out8,
+                            &m_flags,     &m_rayCounters, &m_queryRays, &m_queryOut};
+    for (DeviceBuffer* b : bufs) b->release();
+    for (auto& t : m_texData) t.release();
+    if (m_pinned) cudaFreeHost(m_pinned);
+    for (auto& ev : m_copyEvents)
+        if (ev) cudaEventDestroy(ev);
+    if (m_ev0) cudaEventDestroy(m_ev0);
+    if (m_ev1) cudaEventDestroy(m_ev1);
+    if (m_stream) cudaStreamDestroy(m_stream);
+}
+
+mrtResult Engine::checkAlive() {
+    if (m_lost)
+        return fail(MRT_ERROR_DEVICE_LOST, "The CUDA context of this engine hit an unrecoverable error; destroy it.");
+    const cudaError_t e = cudaSetDevice(m_device);
+    if (e != cudaSuccess) return guard(fromCuda(e, "cudaSetDevice"));
+    return MRT_SUCCESS;
+}
+
+mrtResult Engine::guard(mrtResult r) {
+    if (r == MRT_ERROR_DEVICE_LOST) m_lost = true;
+    return r;
+}
+
+mrtResult Engine::allocateFrame() {
+    const size_t pixels = size_t(m_settings.width) * m_settings.height;
+    MRT_TRY(m_accum.ensure(pixels * 32));
+    MRT_CUDA(cudaMemsetAsync(m_accum.ptr, 0, pixels * 32, m_stream));
+    MRT_TRY(m_out32.ensure(pixels * 16));
+    MRT_TRY(m_out8.ensure(pixels * 4));
+    return MRT_SUCCESS;
+}
+
+// ---------------------------------------------------------------- settings --
+
+// reference Renderer.cpp:115-127: a resize reallocates; resize, maxBounces or
+// fireflyClamp changes restart accumulation.
+mrtResult Engine::setSettings(const Settings& s) {
+    MRT_TRY(checkAlive());
+    if (s.width == 0 || s.height == 0) return fail(MRT_ERROR_INVALID_ARGUMENT, "render size must be non-zero");
+    const bool resize = s.width != m_settings.width || s.height != m_settings.height;
+    const bool reset = resize || s.maxBounces != m_settings.maxBounces || s.fireflyClamp != m_settings.fireflyClamp;
+    m_settings = s;
+    if (resize) MRT_TRY(guard(allocateFrame()));
+    if (reset) resetAccumulation();
+    return MRT_SUCCESS;
+}
+
+void Engine::resetAccumulation() { m_frameIndex = 0; }
+
+mrtResult Engine::setSampleStream(uint32_t offset, uint32_t stride) {
+    if (stride == 0) return fail(MRT_ERROR_INVALID_ARGUMENT, "sample stream stride must be >= 1");
+    m_streamOffset = offset;
+    m_streamStride = stride;
+    resetAccumulation();
+    return MRT_SUCCESS;
+}
+
+// ------------------------------------------------------------------ commit --
+
+// reference Engine.cpp:44-55: camera/env-parameter-only changes restart
+// accumulation without touching device scene data.
+mrtResult Engine::commit(mrtCommitStats* stats) {
+    MRT_TRY(checkAlive());
+    const uint32_t light = DirtyCamera | DirtyEnvParams;
+    const uint32_t d = m_scene.dirty();
+    if (d != DirtyNone && (d & ~light) == 0) {
+        m_scene.clearDirty();
+        resetAccumulation();
+        if (stats) {
+            stats->blasRebuilt = 0;
+            stats->tlasRebuilt = 0;
+            stats->commitMs = 0.0f;
+        }
+        return MRT_SUCCESS;
+    }
+    return guard(sync(stats));
+}
+
+// reference Renderer.cpp:290-320
+mrtResult Engine::sync(mrtCommitStats* stats) {
+    const auto t0 = std::chrono::steady_clock::now();
+    const uint32_t dirty = m_scene.dirty();
+    if (dirty == DirtyNone) {
+        if (stats) {
+            stats->blasRebuilt = 0;
+            stats->tlasRebuilt = 0;
+            stats->commitMs = 0.0f;
+        }
+        return MRT_SUCCESS;
+    }
+    MRT_CUDA(cudaStreamSynchronize(m_stream));
+    uint32_t rebuilt = 0;
+    m_stats.commitBvhMs = 0.0f;
+    m_stats.commitEnvCdfMs = 0.0f;
+    m_stats.commitUploadMs = 0.0f;
+    m_stats.commitH2DBytes = 0;
+    if (dirty & DirtyTextures) MRT_TRY(uploadTextures());
+    if (dirty & DirtyMaterials) MRT_TRY(packMaterials());
+    if (dirty & DirtyGeometry) MRT_TRY(packGeometry(rebuilt));
+    const bool tlas = (dirty & (DirtyGeometry | DirtyInstances | DirtyMaterials)) != 0;
+    if (tlas) MRT_TRY(packInstances());
+    if (dirty & DirtyEnv) MRT_TRY(packEnvironment());
+    if (dirty & (DirtyLights | DirtyEnv)) MRT_TRY(packLights());
+    MRT_CUDA(cudaStreamSynchronize(m_stream));
+    m_scene.clearDirty();
+    resetAccumulation();
+    const float ms = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    m_stats.commitTotalMs = ms;
+    if (stats) {
+        stats->blasRebuilt = rebuilt;
+        stats->tlasRebuilt = tlas ? 1 : 0;
+        stats->commitMs = ms;
+    }
+    return MRT_SUCCESS;
+}
+
+// reference Renderer.cpp:510-550 (clamps, default material at index 0, texture
+// ids resolved to slots, -1 for none)
+mrtResult Engine::packMaterials() {
+    std::vector<MrtMaterial> mats;
+    mats.reserve(m_scene.materials().size() + 1);
+    MrtMaterial def{{0.8f, 0.8f, 0.8f, 1.0f}, {0, 0, 0, 0.5f}, {0, 0, 1.45f, 0}, {-1, -1, -1, -1, -1, -1, -1, -1}};
+    mats.push_back(def);
+    m_materialIndex.clear();
+    for (const auto& [id, m] : m_scene.materials()) {
+        MrtMaterial g{};
+        g.baseColorOpacity[0] = m.baseColor[0];
+        g.baseColorOpacity[1] = m.baseColor[1];
+        g.baseColorOpacity[2] = m.baseColor[2];
+        g.baseColorOpacity[3] = m.opacity;
+        g.emissionRoughness[0] = m.emission[0];
+        g.emissionRoughness[1] = m.emission[1];
+        g.emissionRoughness[2] = m.emission[2];
+        g.emissionRoughness[3] = clamp01(m.roughness);
+        g.params[0] = clamp01(m.metallic);
+        g.params[1] = clamp01(m.transmission);
+        g.params[2] = std::max(m.ior, 1.0f);
+        g.params[3] = 0.0f;
+        for (int k = 0; k < 8; ++k) g.tex[k] = -1;
+        for (int k = 0; k < 5; ++k) {
+            const uint32_t slot = m_scene.textureSlot(m.tex[k]);
+            g.tex[k] = (slot == ~0u || slot >= MRT_MAX_TEXTURES) ? -1 : int32_t(slot);
+        }
+        m_materialIndex[id] = uint32_t(mats.size());
+        mats.push_back(g);
+    }
+    return up(m_materials, mats.data(), mats.size() * sizeof(MrtMaterial));
+}
+
+// reference Renderer.cpp:333-446: rebuild dirty BLASes (concurrently), then
+// repack every mesh into the global arrays in id order with triangles in
+// BLAS leaf order and node indices rebased.
+mrtResult Engine::packGeometry(uint32_t& rebuilt) {
+    auto& meshes = m_scene.meshes();
+    for (auto it = m_blas.begin(); it != m_blas.end();)
+        it = meshes.count(it->first) ? std::next(it) : m_blas.erase(it);
+    const auto tb = std::chrono::steady_clock::now();
+    std::vector<std::pair<uint32_t, std::future<BvhResult>>> jobs;
+    const unsigned threads = m_hostThreads;
+    for (auto& [id, mesh] : meshes) {
+        if (!mesh.blasDirty && m_blas.count(id)) continue;
+        MeshData* m = &mesh;
+        jobs.emplace_back(id, std::async(std::launch::async, [m, threads] {
+                              const size_t nt = m->indices.size() / 3;
+                              std::vector<Box3> boxes(nt);
+                              for (size_t t = 0; t < nt; ++t) {
+                                  Box3& b = boxes[t];
+                                  for (int k = 0; k < 3; ++k) {
+                                      b.lo[k] = 3.402823466e38f;
+                                      b.hi[k] = -3.402823466e38f;
+                                  }
+                                  for (int c = 0; c < 3; ++c) {
+                                      const V4f& p = m->positions[m->indices[t * 3 + c]];
+                                      const float v[3] = {p.x, p.y, p.z};
+                                      for (int k = 0; k < 3; ++k) {
+                                          b.lo[k] = std::min(b.lo[k], v[k]);
+                                          b.hi[k] = std::max(b.hi[k], v[k]);
+                                      }
+                                  }
+                              }
+                              return buildBvh(boxes, 4, threads);
+                          }));
+    }
+    for (auto& [id, fut] : jobs) {
+        m_blas[id].bvh = fut.get();
+        meshes[id].blasDirty = false;
+    }
+    rebuilt = uint32_t(jobs.size());
+    m_stats.commitBvhMs += std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - tb).count();
+
+    size_t nv = 0, nt = 0, nn = 0;
+    for (auto& [id, mesh] : meshes) {
+        nv += mesh.positions.size();
+        nt += mesh.indices.size() / 3;
+        nn += m_blas[id].bvh.nodes.size();
+    }
+    std::vector<float4> triVerts(nt * 3);
+    std::vector<uint4> triIndex(nt);
+    std::vector<V4f> normals;
+    std::vector<V2f> uvs;
+    std::vector<V4f> tangents;
+    normals.reserve(nv);
+    uvs.reserve(nv);
+    tangents.reserve(nv);
+    std::vector<MrtNode> nodes;
+    nodes.reserve(nn + 1);
+    uint32_t vbase = 0, tbase = 0;
+    for (auto& [id, mesh] : meshes) {
+        Blas& b = m_blas[id];
+        b.nodeBase = uint32_t(nodes.size());
+        normals.insert(normals.end(), mesh.normals.begin(), mesh.normals.end());
+        if (mesh.uvs.empty()) uvs.insert(uvs.end(), mesh.positions.size(), V2f{0, 0});
+        else uvs.insert(uvs.end(), mesh.uvs.begin(), mesh.uvs.end());
+        if (mesh.tangents.empty()) tangents.insert(tangents.end(), mesh.positions.size(), V4f{1, 0, 0, 1});
+        else tangents.insert(tangents.end(), mesh.tangents.begin(), mesh.tangents.end());
+        const uint32_t* idx = mesh.indices.data();
+        const auto& order = b.bvh.primOrder;
+        for (size_t k = 0; k < order.size(); ++k) {
+            const uint32_t lt = order[k];
+            const uint32_t i0 = idx[lt * 3], i1 = idx[lt * 3 + 1], i2 = idx[lt * 3 + 2];
+            const V4f& p0 = mesh.positions[i0];
+            const V4f& p1 = mesh.positions[i1];
+            const V4f& p2 = mesh.positions[i2];
+            const size_t slot = tbase + k;
+            uint32_t origBits = lt, slotBits = uint32_t(slot);
+            float fo, fs;
+            std::memcpy(&fo, &origBits, 4);
+            std::memcpy(&fs, &slotBits, 4);
+            triVerts[slot * 3 + 0] = make_float4(p0.x, p0.y, p0.z, fo);
+            triVerts[slot * 3 + 1] = make_float4(p1.x, p1.y, p1.z, fs);
+            triVerts[slot * 3 + 2] = make_float4(p2.x, p2.y, p2.z, 0.0f);
+            triIndex[slot] = make_uint4(i0 + vbase, i1 + vbase, i2 + vbase, lt);
+        }
+        for (MrtNode n : b.bvh.nodes) {
+            n.leftOrPrim += ((n.packed >> 2) == 0) ? b.nodeBase : tbase;
+            nodes.push_back(n);
+        }
+        vbase += uint32_t(mesh.positions.size());
+        tbase += uint32_t(order.size());
+    }
+    m_blasNodeCount = uint32_t(nodes.size());
+    m_triCount = uint32_t(nt);
+    const auto tu = std::chrono::steady_clock::now();
+    // node buffer keeps room for the TLAS (2 * instances + 1) behind the BLAS region
+    const size_t tlasCap = std::max<size_t>(2 * m_scene.instances().size() + 1, 4);
+    MRT_TRY(m_nodes.ensure((nodes.size() + tlasCap) * sizeof(MrtNode)));
+    if (!nodes.empty())
+        MRT_CUDA(cudaMemcpyAsync(m_nodes.ptr, nodes.data(), nodes.size() * sizeof(MrtNode), cudaMemcpyHostToDevice,
+                                 m_stream));
+    m_stats.commitH2DBytes += nodes.size() * sizeof(MrtNode);
+    MRT_TRY(up(m_triVerts, triVerts.data(), triVerts.size() * sizeof(float4)));
+    MRT_TRY(up(m_triIndex, triIndex.data(), triIndex.size() * sizeof(uint4)));
+    MRT_TRY(up(m_normals, normals.data(), normals.size() * sizeof(V4f)));
+    MRT_TRY(up(m_uvs, uvs.data(), uvs.size() * sizeof(V2f)));
+    MRT_TRY(up(m_tangents, tangents.data(), tangents.size() * sizeof(V4f)));
+    MRT_CUDA(cudaStreamSynchronize(m_stream));
+    m_stats.commitUploadMs += std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - tu).count();
+    return MRT_SUCCESS;
+}
+
+// reference Renderer.cpp:448-508: TLAS over instance world bounds (leaf size
+// 1), instances stored in TLAS leaf order, TLAS nodes after the BLAS nodes.
+mrtResult Engine::packInstances() {
+    std::vector<const InstanceData*> flat;
+    std::vector<uint32_t> ids;
+    std::vector<Box3> boxes;
+    for (const auto& [id, in] : m_scene.instances()) {
+        auto it = m_blas.find(in.mesh);
+        if (it == m_blas.end() || it->second.bvh.nodes.empty()) continue;
+        flat.push_back(&in);
+        ids.push_back(id);
+        boxes.push_back(transformBox(it->second.bvh.bounds, in.o2w));
+    }
+    const auto tb = std::chrono::steady_clock::now();
+    BvhResult tlas = buildBvh(boxes, 1, 1);
+    m_stats.commitBvhMs += std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - tb).count();
+    if (tlas.nodes.empty()) tlas.nodes.push_back(sentinelNode());
+    std::vector<MrtInstance> gi;
+    gi.reserve(flat.size());
+    for (uint32_t oi : tlas.primOrder) {
+        const InstanceData* in = flat[oi];
+        MrtInstance g{};
+        std::memcpy(g.o2w, in->o2w, sizeof(g.o2w));
+        invertAffine(in->o2w, g.w2o);
+        g.blasRoot = m_blas[in->mesh].nodeBase;
+        auto mi = m_materialIndex.find(in->material);
+        g.materialIndex = mi != m_materialIndex.end() ? mi->second : 0;
+        g.userId = ids[oi];
+        g.meshId = in->mesh;
+        gi.push_back(g);
+    }
+    m_tlasRoot = m_blasNodeCount;
+    for (MrtNode& n : tlas.nodes)
+        if ((n.packed >> 2) == 0) n.leftOrPrim += m_tlasRoot;
+    m_instanceCount = uint32_t(gi.size());
+    const size_t need = (size_t(m_tlasRoot) + tlas.nodes.size()) * sizeof(MrtNode);
+    if (m_nodes.bytes < need) {
+        // instance count outgrew the reserved TLAS room: grow, keeping the BLAS part
+        DeviceBuffer bigger;
+        MRT_TRY(bigger.ensure(need + need / 2));
+        MRT_CUDA(cudaMemcpyAsync(bigger.ptr, m_nodes.ptr, size_t(m_tlasRoot) * sizeof(MrtNode),
+                                 cudaMemcpyDeviceToDevice, m_stream));
+        MRT_CUDA(cudaStreamSynchronize(m_stream));
+        m_nodes.release();
+        m_nodes = bigger;
+    }
+    MRT_CUDA(cudaMemcpyAsync(static_cast<MrtNode*>(m_nodes.ptr) + m_tlasRoot, tlas.nodes.data(),
+                             tlas.nodes.size() * sizeof(MrtNode), cudaMemcpyHostToDevice, m_stream));
+    m_stats.commitH2DBytes += tlas.nodes.size() * sizeof(MrtNode);
+    m_nodeCount = m_tlasRoot + uint32_t(tlas.nodes.size());
+    MRT_TRY(up(m_instances, gi.data(), gi.size() * sizeof(MrtInstance)));
+    MRT_CUDA(cudaStreamSynchronize(m_stream));
+    return MRT_SUCCESS;
+}
+
+// reference Renderer.cpp:552-603
+mrtResult Engine::packLights() {
+    std::vector<MrtLight> lights;
+    if (m_scene.hasEnvironment()) {
+        MrtLight g{};
+        g.type = MRT_DLIGHT_ENV;
+        lights.push_back(g);
+    }
+    for (const auto& [id, l] : m_scene.lights()) {
+        MrtLight g{};
+        if (l.type == MRT_LIGHT_SUN) {
+            g.type = MRT_DLIGHT_SUN;
+            float d[3] = {l.direction[0], l.direction[1], l.direction[2]};
+            normalize3(d);
+            g.p0[0] = d[0];
+            g.p0[1] = d[1];
+            g.p0[2] = d[2];
+            g.p0[3] = std::cos(std::max(l.angularRadius, 1e-4f));
+            std::memcpy(g.p1, l.radiance, 12);
+        } else if (l.type == MRT_LIGHT_POINT) {
+            g.type = MRT_DLIGHT_POINT;
+            std::memcpy(g.p0, l.position, 12);
+            std::memcpy(g.p1, l.radiance, 12);
+        } else {
+            g.type = MRT_DLIGHT_RECT;
+            float c[3];
+            cross3(l.edge0, l.edge1, c);
+            std::memcpy(g.p0, l.corner, 12);
+            g.p0[3] = std::sqrt(c[0] * c[0] + c[1] * c[1] + c[2] * c[2]);
+            std::memcpy(g.p1, l.edge0, 12);
+            std::memcpy(g.p2, l.edge1, 12);
+            std::memcpy(g.p3, l.radiance, 12);
+            g.p3[3] = l.twoSided ? 1.0f : 0.0f;
+        }
+        lights.push_back(g);
+    }
+    m_lightCount = uint32_t(lights.size());
+    if (lights.empty()) return MRT_SUCCESS;
+    return up(m_lights, lights.data(), lights.size() * sizeof(MrtLight));
+}
+
+// Environment map upload + CDF on the device (reference Renderer.cpp:605-662
+// builds it on the CPU).
+mrtResult Engine::packEnvironment() {
+    m_hasEnv = m_scene.hasEnvironment();
+    if (!m_hasEnv) {
+        m_envW = m_envH = 0;
+        return MRT_SUCCESS;
+    }
+    const TextureData& env = m_scene.environment();
+    const auto tu = std::chrono::steady_clock::now();
+    MRT_TRY(up(m_envTexels, env.data.data(), env.data.size()));
+    m_stats.commitUploadMs += std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - tu).count();
+    float integral = 1.0f;
+    MRT_TRY(runEnvCdf(nullptr, env.width, env.height, integral));
+    m_envW = env.width;
+    m_envH = env.height;
+    m_envIntegralHost = integral;
+    return MRT_SUCCESS;
+}
+
+// Runs the CDF kernel over the texels already in m_envTexels (rgba == NULL)
+// or over `rgba` uploaded first. Leaves the CDF in m_envCdf.
+mrtResult Engine::runEnvCdf(const float* rgba, uint32_t w, uint32_t h, float& integral) {
+    if (rgba) MRT_TRY(up(m_envTexels, rgba, size_t(w) * h * 16));
+    std::vector<float> sinTheta(h);
+    const float pi = 3.14159265358979323846f;
+    const float dTheta = pi / float(h);
+    for (uint32_t y = 0; y < h; ++y) sinTheta[y] = std::sin((float(y) + 0.5f) * dTheta);
+    MRT_TRY(up(m_envSin, sinTheta.data(), h * sizeof(float)));
+    MRT_TRY(m_envCdf.ensure((size_t(w) * h + h) * sizeof(float)));
+    MRT_TRY(m_envRowSums.ensure(size_t(h) * sizeof(double)));
+    MRT_TRY(m_envIntegral.ensure(16));
+    MRT_CUDA(cudaEventRecord(m_ev0, m_stream));
+    MRT_CUDA(mrtcu_env_cdf(m_envTexels.as<float4>(), m_envSin.as<float>(), w, h, m_envCdf.as<float>(),
+                           m_envRowSums.as<double>(), m_envIntegral.as<float>(), m_stream));
+    MRT_CUDA(cudaEventRecord(m_ev1, m_stream));
+    MRT_CUDA(cudaMemcpyAsync(&integral, m_envIntegral.ptr, sizeof(float), cudaMemcpyDeviceToHost, m_stream));
+    MRT_CUDA(cudaStreamSynchronize(m_stream));
+    float ms = 0.0f;
+    MRT_CUDA(cudaEventElapsedTime(&ms, m_ev0, m_ev1));
+    m_stats.commitEnvCdfMs = ms;
+    return MRT_SUCCESS;
+}
+
+// reference Renderer.cpp:664-708: per-slot upload when the slot's generation
+// changed; removed slots revert to the white placeholder.
+mrtResult Engine::uploadTextures() {
+    const auto& tex = m_scene.textures();
+    const size_t slots = std::min<size_t>(tex.size(), MRT_MAX_TEXTURES);
+    std::vector<MrtTexture> table(MRT_MAX_TEXTURES);
+    std::memset(table.data(), 0, table.size() * sizeof(MrtTexture));
+    for (size_t s = 0; s < slots; ++s) {
+        const TextureData& t = tex[s];
+        if (m_texGeneration[s] != t.generation) {
+            if (t.data.empty()) m_texData[s].release();
+            else MRT_TRY(m_texData[s].upload(t.data.data(), t.data.size(), m_stream));
+            m_texGeneration[s] = t.generation;
+        }
+        if (!t.data.empty() && m_texData[s].ptr) {
+            table[s].texels = m_texData[s].ptr;
+            table[s].width = t.width;
+            table[s].height = t.height;
+            table[s].format = t.format;
+        }
+    }
+    if (tex.size() > MRT_MAX_TEXTURES) log(LogLevel::Warn, "Texture count exceeds 64 slots; extra textures ignored");
+    return up(m_texTable, table.data(), table.size() * sizeof(MrtTexture));
+}
+
+// ----------------------------------------------------------------- render --
+
+// reference Renderer.cpp:711-764 fillGlobals (camera basis, frustum)
+void Engine::fillParams(MrtFrameParams& p) const {
+    std::memset(&p, 0, sizeof(p));
+    float pos[3], fwd[3], upHint[3], l, r, b, t;
+    bool ortho = false;
+    if (m_scene.usesCameraEx()) {
+        const CameraExData& c = m_scene.cameraEx();
+        std::memcpy(pos, c.position, 12);
+        std::memcpy(fwd, c.forward, 12);
+        normalize3(fwd);
+        std::memcpy(upHint, c.up, 12);
+        l = c.left;
+        r = c.right;
+        b = c.bottom;
+        t = c.top;
+        ortho = c.projection == MRT_CAMERA_ORTHOGRAPHIC;
+    } else {
+        const CameraData& c = m_scene.camera();
+        std::memcpy(pos, c.position, 12);
+        fwd[0] = c.target[0] - pos[0];
+        fwd[1] = c.target[1] - pos[1];
+        fwd[2] = c.target[2] - pos[2];
+        normalize3(fwd);
+        std::memcpy(upHint, c.up, 12);
+        const float aspect = float(m_settings.width) / float(m_settings.height);
+        const float tanHalf = std::tan(c.fovYDeg * 0.01745329251994329576923690768489f * 0.5f);
+        r = tanHalf * aspect;
+        l = -r;
+        t = tanHalf;
+        b = -t;
+    }
+    float right[3];
+    cross3(fwd, upHint, right);
+    if (std::sqrt(right[0] * right[0] + right[1] * right[1] + right[2] * right[2]) < 1e-6f) {
+        right[0] = 1.0f;
+        right[1] = right[2] = 0.0f;
+    } else {
+        normalize3(right);
+    }
+    float up[3];
+    cross3(right, fwd, up);
+    std::memcpy(p.camPos, pos, 12);
+    std::memcpy(p.camRight, right, 12);
+    std::memcpy(p.camUp, up, 12);
+    std::memcpy(p.camForward, fwd, 12);
+    p.frustum[0] = l;
+    p.frustum[1] = r;
+    p.frustum[2] = b;
+    p.frustum[3] = t;
+    p.width = m_settings.width;
+    p.height = m_settings.height;
+    p.maxBounces = std::min<uint32_t>(m_settings.maxBounces, MRT_MAX_BOUNCES_CAP);
+    p.lightCount = m_lightCount;
+    p.envW = m_hasEnv ? m_envW : 0;
+    p.envH = m_hasEnv ? m_envH : 0;
+    p.flags = (m_hasEnv ? uint32_t(MRT_FLAG_HAS_ENV) : 0u) | (ortho ? uint32_t(MRT_FLAG_ORTHO) : 0u);
+    p.tlasRoot = m_tlasRoot;
+    p.envRotation = m_scene.envRotation();
+    p.envIntensity = m_scene.envIntensity();
+    p.envIntegral = m_envIntegralHost;
+    p.fireflyClamp = m_settings.fireflyClamp;
+    p.streamOffset = m_streamOffset;
+    p.streamStride = m_streamStride;
+    p.nodeCount = m_nodeCount;
+    p.instanceCount = m_instanceCount;
+    p.nodes = m_nodes.as<MrtNode>();
+    p.triVerts = m_triVerts.as<float4>();
+    p.triIndex = m_triIndex.as<uint4>();
+    p.normals = m_normals.as<float4>();
+    p.uvs = m_uvs.as<float2>();
+    p.tangents = m_tangents.as<float4>();
+    p.instances = m_instances.as<MrtInstance>();
+    p.materials = m_materials.as<MrtMaterial>();
+    p.lights = m_lights.as<MrtLight>();
+    p.envTexels = m_envTexels.as<float4>();
+    p.envCdf = m_envCdf.as<float>();
+    p.textures = m_texTable.as<MrtTexture>();
+    p.accum = m_accum.as<double>();
+    p.errorFlags = m_flags.as<uint32_t>();
+    p.rayCounters = m_rayCounters.as<unsigned long long>();
+}
+
+mrtResult Engine::checkErrorFlags() {
+    uint32_t flags = 0;
+    MRT_CUDA(cudaMemcpyAsync(&flags, m_flags.ptr, sizeof(flags), cudaMemcpyDeviceToHost, m_stream));
+    MRT_CUDA(cudaStreamSynchronize(m_stream));
+    if (flags) {
+        MRT_CUDA(cudaMemsetAsync(m_flags.ptr, 0, sizeof(uint32_t), m_stream));
+        log(LogLevel::Warn, "traversal stack limit reached in at least one ray (flags " + std::to_string(flags) +
+                                "); affected rays may miss geometry");
+    }
+    return MRT_SUCCESS;
+}
+
+// reference Engine.cpp:57-60 + Renderer.cpp:773-843: implicit commit, one
+// sample per pixel per frame, no-op once sppLimit is reached.
+mrtResult Engine::renderFrames(uint32_t count, mrtFrameInfo* info) {
+    const auto t0 = std::chrono::steady_clock::now();
+    MRT_TRY(commit(nullptr));
+    uint32_t n = 0;
+    if (m_frameIndex < m_settings.sppLimit) n = std::min(count, m_settings.sppLimit - m_frameIndex);
+    m_stats.kernelLaunches = 0;
+    if (n > 0) {
+        MrtFrameParams p;
+        fillParams(p);
+        MRT_CUDA(cudaMemsetAsync(m_rayCounters.ptr, 0, 64, m_stream));
+        MRT_CUDA(cudaEventRecord(m_ev0, m_stream));
+        const cudaError_t le = mrtcu_pathtrace(&p, m_frameIndex, n, m_stream);
+        if (le != cudaSuccess) return guard(fromCuda(le, "path tracing launch"));
+        MRT_CUDA(cudaEventRecord(m_ev1, m_stream));
+        const cudaError_t se = cudaStreamSynchronize(m_stream);
+        if (se != cudaSuccess) return guard(fromCuda(se, "path tracing kernel"));
+        float ms = 0.0f;
+        MRT_CUDA(cudaEventElapsedTime(&ms, m_ev0, m_ev1));
+        m_stats.lastRenderMs = ms;
+        m_stats.lastRenderSpp = n;
+        m_stats.kernelLaunches = 1;
+        MRT_TRY(guard(checkErrorFlags()));
+        unsigned long long ctr[5];
+        MRT_CUDA(cudaMemcpy(ctr, m_rayCounters.ptr, sizeof(ctr), cudaMemcpyDeviceToHost));
+        m_stats.raysClosest = ctr[0];
+        m_stats.raysShadow = ctr[1];
+        m_stats.nodeFetches = ctr[2];
+        m_stats.triTests = ctr[3];
+        m_stats.surfaceHits = ctr[4];
+        m_frameIndex += n;
+        m_resolveExposure = std::exp2(m_settings.exposureEV);
+        m_resolveTonemap = m_settings.tonemap;
+    }
+    if (info && info->structSize >= sizeof(mrtFrameInfo)) {
+        info->spp = m_frameIndex;
+        info->converged = m_frameIndex >= m_settings.sppLimit ? 1 : 0;
+        info->denoised = 0;
+        info->frameMs = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    }
+    return MRT_SUCCESS;
+}
+
+// Device -> pinned staging -> caller memory, in chunks so the host copy of
+// one chunk overlaps the PCIe transfer of the next.
+mrtResult Engine::download(void* dst, const void* src, size_t bytes) {
+    if (m_pinnedBytes < bytes) {
+        if (m_pinned) cudaFreeHost(m_pinned);
+        m_pinned = nullptr;
+        m_pinnedBytes = 0;
+        MRT_CUDA(cudaMallocHost(&m_pinned, bytes));
+        m_pinnedBytes = bytes;
+    }
+    const size_t chunk = size_t(4) << 20;
+    const size_t nChunks = (bytes + chunk - 1) / chunk;
+    size_t issued = 0;
+    auto issue = [&](size_t c) -> mrtResult {
+        const size_t off = c * chunk, len = std::min(chunk, bytes - off);
+        MRT_CUDA(cudaMemcpyAsync(static_cast<char*>(m_pinned) + off, static_cast<const char*>(src) + off, len,
+                                 cudaMemcpyDeviceToHost, m_stream));
+        MRT_CUDA(cudaEventRecord(m_copyEvents[c % m_copyEvents.size()], m_stream));
+        return MRT_SUCCESS;
+    };
+    const size_t window = m_copyEvents.size();
+    for (; issued < std::min(nChunks, window); ++issued) MRT_TRY(issue(issued));
+    for (size_t c = 0; c < nChunks; ++c) {
+        MRT_CUDA(cudaEventSynchronize(m_copyEvents[c % window]));
+        const size_t off = c * chunk, len = std::min(chunk, bytes - off);
+        std::memcpy(static_cast<char*>(dst) + off, static_cast<const char*>(m_pinned) + off, len);
+        if (issued < nChunks) MRT_TRY(issue(issued++));
+    }
+    return MRT_SUCCESS;
+}
+
+// reference Renderer.cpp:892-909
+mrtResult Engine::readFramebuffer(mrtPixelFormat fmt, void* dst, size_t dstSize) {
+    MRT_TRY(checkAlive());
+    const size_t pixels = size_t(m_settings.width) * m_settings.height;
+    if (fmt == MRT_PIXEL_RGBA8_SRGB) {
+        if (dstSize < pixels * 4) return fail(MRT_ERROR_INVALID_ARGUMENT, "dst too small for RGBA8 readback");
+        MRT_CUDA(mrtcu_resolve_rgba8(m_accum.as<double>(), pixels, m_resolveExposure, m_resolveTonemap,
+                                     m_out8.as<uchar4>(), m_stream));
+        return guard(download(dst, m_out8.ptr, pixels * 4));
+    }
+    if (fmt != MRT_PIXEL_RGBA32F_LINEAR) return fail(MRT_ERROR_INVALID_ARGUMENT, "unknown pixel format");
+    if (dstSize < pixels * 16) return fail(MRT_ERROR_INVALID_ARGUMENT, "dst too small for RGBA32F readback");
+    MRT_CUDA(mrtcu_readback_rgba32f(m_accum.as<double>(), pixels, m_frameIndex, m_out32.as<float4>(), m_stream));
+    return guard(download(dst, m_out32.ptr, pixels * 16));
+}
+
+// ---------------------------------------------------------------- queries --
+
+mrtResult Engine::traceRays(const mrtxRay* rays, uint32_t n, mrtxHit* hits) {
+    MRT_TRY(commit(nullptr));
+    if (n == 0) return MRT_SUCCESS;
+    MrtFrameParams p;
+    fillParams(p);
+    MRT_TRY(m_queryRays.upload(rays, size_t(n) * sizeof(mrtxRay), m_stream));
+    MRT_TRY(m_queryOut.ensure(size_t(n) * sizeof(mrtxHit)));
+    MRT_CUDA(mrtcu_trace_closest(&p, m_queryRays.as<MrtQueryRay>(), n, m_queryOut.as<MrtQueryHit>(), m_stream));
+    MRT_CUDA(cudaMemcpyAsync(hits, m_queryOut.ptr, size_t(n) * sizeof(mrtxHit), cudaMemcpyDeviceToHost, m_stream));
+    const cudaError_t se = cudaStreamSynchronize(m_stream);
+    if (se != cudaSuccess) return guard(fromCuda(se, "trace query kernel"));
+    return guard(checkErrorFlags());
+}
+
+mrtResult Engine::traceShadowRays(const mrtxRay* rays, uint32_t n, uint32_t* occluded) {
+    MRT_TRY(commit(nullptr));
+    if (n == 0) return MRT_SUCCESS;
+    MrtFrameParams p;
+    fillParams(p);
+    MRT_TRY(m_queryRays.upload(rays, size_t(n) * sizeof(mrtxRay), m_stream));
+    MRT_TRY(m_queryOut.ensure(size_t(n) * sizeof(uint32_t)));
+    MRT_CUDA(mrtcu_trace_any(&p, m_queryRays.as<MrtQueryRay>(), n, m_queryOut.as<uint32_t>(), m_stream));
+    MRT_CUDA(cudaMemcpyAsync(occluded, m_queryOut.ptr, size_t(n) * 4, cudaMemcpyDeviceToHost, m_stream));
+    const cudaError_t se = cudaStreamSynchronize(m_stream);
+    if (se != cudaSuccess) return guard(fromCuda(se, "shadow query kernel"));
+    return guard(checkErrorFlags());
+}
+
+mrtResult Engine::readAccumulation(double* dst, size_t dstSize, uint32_t* spp) {
+    MRT_TRY(checkAlive());
+    const size_t bytes = size_t(m_settings.width) * m_settings.height * 32;
+    if (dstSize < bytes) return fail(MRT_ERROR_INVALID_ARGUMENT, "dst too small for the accumulation buffer");
+    MRT_TRY(guard(download(dst, m_accum.ptr, bytes)));
+    if (spp) *spp = m_frameIndex;
+    return MRT_SUCCESS;
+}
+
+mrtResult Engine::getStats(mrtxStats* out) const {
+    mrtxStats s = m_stats;
+    s.structSize = sizeof(mrtxStats);
+    s.bvhNodes = m_nodeCount;
+    s.triangles = m_triCount;
+    s.instances = m_instanceCount;
+    uint64_t bytes = 0;
+    const DeviceBuffer* bufs[] = {&m_nodes,     &m_triVerts,  &m_triIndex,   &m_normals,     &m_uvs,
+                                  &m_tangents,  &m_instances, &m_materials,  &m_lights,      &m_envTexels,
+                                  &m_envCdf,    &m_envSin,    &m_envRowSums, &m_envIntegral, &m_texTable,
+                                  &m_accum,     &m_out32,     &m_out8,       &m_flags,       &m_rayCounters,
+                                  &m_queryRays, &m_queryOut};
+    for (const DeviceBuffer* b : bufs) bytes += b->bytes;
+    for (const auto& t : m_texData) bytes += t.bytes;
+    s.deviceBytes = bytes;
+    *out = s;
+    return MRT_SUCCESS;
+}
+
+mrtResult Engine::buildEnvCdf(const float* rgba, uint32_t w, uint32_t h, float* cdf, float* integral) {
+    MRT_TRY(checkAlive());
+    if (!rgba || !cdf || !integral || w == 0 || h == 0)
+        return fail(MRT_ERROR_INVALID_ARGUMENT, "mrtxBuildEnvCdf: null pointer or empty image");
+    float integ = 1.0f;
+    MRT_TRY(guard(runEnvCdf(rgba, w, h, integ)));
+    MRT_CUDA(cudaMemcpy(cdf, m_envCdf.ptr, (size_t(w) * h + h) * sizeof(float), cudaMemcpyDeviceToHost));
+    *integral = integ;
+    // the scratch buffers now hold this image, not the scene's: rebuild on next commit
+    if (m_hasEnv) m_scene.markDirty(DirtyEnv | DirtyLights);
+    return MRT_SUCCESS;
+}
+
+mrtResult Engine::copyAccumulationDevice(void* dev, size_t bytes, bool accumulate) {
+    MRT_TRY(checkAlive());
+    const size_t need = size_t(m_settings.width) * m_settings.height * 32;
+    if (!dev || bytes < need) return fail(MRT_ERROR_INVALID_ARGUMENT, "device buffer missing or too small");
+    if (accumulate) MRT_CUDA(mrtcu_add_f64(m_accum.as<double>(), static_cast<const double*>(dev), need / 8, m_stream));
+    else MRT_CUDA(cudaMemcpyAsync(dev, m_accum.ptr, need, cudaMemcpyDeviceToDevice, m_stream));
+    const cudaError_t se = cudaStreamSynchronize(m_stream);
+    if (se != cudaSuccess) return guard(fromCuda(se, "accumulation copy"));
+    return MRT_SUCCESS;
+}
+
+}  // namespace mrt

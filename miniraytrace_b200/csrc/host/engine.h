@@ -1,0 +1,124 @@
+// The engine behind one mrtEngine handle: scene store, device-resident scene
+// arrays, accumulation buffers and the per-frame launch logic. It combines
+// the roles of the reference's Engine facade (core/src/Engine.cpp) and
+// Renderer (core/src/render/Renderer.cpp) on a CUDA device.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <map>
+#include <vector>
+
+#include "../../../include/mrt_ext.h"
+#include "../common/device_types.h"
+#include "bvh_build.h"
+#include "common.h"
+#include "scene.h"
+
+namespace mrt {
+
+// Grow-only device allocation.
+struct DeviceBuffer {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    mrtResult ensure(size_t n);
+    mrtResult upload(const void* src, size_t n, cudaStream_t s);
+    void release();
+    template <class T> T* as() const { return static_cast<T*>(ptr); }
+};
+
+struct Settings {  // reference SceneTypes.hpp:142-152 defaults
+    uint32_t width = 1280, height = 720, maxBounces = 8, sppLimit = 1024;
+    float exposureEV = 0.0f, fireflyClamp = 50.0f;
+    uint32_t tonemap = MRT_TONEMAP_ACES;
+    bool denoise = true;
+};
+
+class Engine {
+public:
+    static mrtResult create(const mrtEngineDesc& desc, Engine** out);
+    ~Engine();
+
+    Scene& scene() { return m_scene; }
+
+    mrtResult setSettings(const Settings& s);
+    void resetAccumulation();
+    mrtResult commit(mrtCommitStats* stats);
+    mrtResult renderFrames(uint32_t count, mrtFrameInfo* info);
+    mrtResult readFramebuffer(mrtPixelFormat fmt, void* dst, size_t dstSize);
+
+    mrtResult traceRays(const mrtxRay* rays, uint32_t n, mrtxHit* hits);
+    mrtResult traceShadowRays(const mrtxRay* rays, uint32_t n, uint32_t* occluded);
+    mrtResult readAccumulation(double* dst, size_t dstSize, uint32_t* spp);
+    mrtResult getStats(mrtxStats* out) const;
+    mrtResult buildEnvCdf(const float* rgba, uint32_t w, uint32_t h, float* cdf, float* integral);
+    mrtResult setSampleStream(uint32_t offset, uint32_t stride);
+    mrtResult copyAccumulationDevice(void* dev, size_t bytes, bool accumulate);
+
+private:
+    Engine() = default;
+    mrtResult init(const mrtEngineDesc& desc);
+    mrtResult checkAlive();
+    mrtResult guard(mrtResult r);  // records a device loss
+    mrtResult allocateFrame();
+    mrtResult up(DeviceBuffer& b, const void* src, size_t n);
+    mrtResult sync(mrtCommitStats* stats);  // reference Renderer::syncScene
+    mrtResult packMaterials();
+    mrtResult packGeometry(uint32_t& rebuilt);
+    mrtResult packInstances();
+    mrtResult packLights();
+    mrtResult packEnvironment();
+    mrtResult uploadTextures();
+    mrtResult runEnvCdf(const float* rgba, uint32_t w, uint32_t h, float& integral);
+    void fillParams(MrtFrameParams& p) const;
+    mrtResult checkErrorFlags();
+    mrtResult download(void* dst, const void* src, size_t bytes);
+
+    int m_device = 0;
+    cudaStream_t m_stream = nullptr;
+    cudaEvent_t m_ev0 = nullptr, m_ev1 = nullptr;
+    std::vector<cudaEvent_t> m_copyEvents;
+    bool m_lost = false;
+    bool m_validation = false;
+    unsigned m_hostThreads = 1;
+
+    Scene m_scene;
+    Settings m_settings;
+
+    // device scene
+    DeviceBuffer m_nodes, m_triVerts, m_triIndex, m_normals, m_uvs, m_tangents;
+    DeviceBuffer m_instances, m_materials, m_lights;
+    DeviceBuffer m_envTexels, m_envCdf, m_envSin, m_envRowSums, m_envIntegral;
+    DeviceBuffer m_texTable;
+    DeviceBuffer m_texData[MRT_MAX_TEXTURES];
+    std::vector<uint32_t> m_texGeneration;
+    // device frame state
+    DeviceBuffer m_accum, m_out32, m_out8, m_flags, m_rayCounters, m_queryRays, m_queryOut;
+    void* m_pinned = nullptr;
+    size_t m_pinnedBytes = 0;
+
+    // host-side packing state
+    struct Blas {
+        BvhResult bvh;
+        uint32_t nodeBase = 0;
+    };
+    std::map<uint32_t, Blas> m_blas;
+    std::map<uint32_t, uint32_t> m_materialIndex;
+    uint32_t m_nodeCount = 0, m_blasNodeCount = 0, m_triCount = 0;
+    uint32_t m_tlasRoot = 0, m_instanceCount = 0, m_lightCount = 0;
+    uint32_t m_envW = 0, m_envH = 0;
+    float m_envIntegralHost = 1.0f;
+    bool m_hasEnv = false;
+
+    // accumulation
+    uint32_t m_frameIndex = 0;  // samples per pixel accumulated since reset
+    uint32_t m_streamOffset = 0, m_streamStride = 1;
+    float m_resolveExposure = 1.0f;
+    uint32_t m_resolveTonemap = MRT_TONEMAP_ACES;
+
+    // statistics
+    mrtxStats m_stats{};
+};
+
+}  // namespace mrt

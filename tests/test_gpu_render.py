@@ -1,0 +1,352 @@
+"""Rendering parity and ABI semantics on the GPU, through the C ABI.
+
+Image parity gate: at config 1 (256x256, 16 spp, same pcg4d streams, firefly
+clamp equal on both sides) at least 99.9% of pixels match the FP32 oracle
+within 1e-3 relative (per channel, |gpu - ref| <= 1e-3 * |ref| + 1e-6).
+
+The known-answer tests restate the reference's GPU tests
+(tests/camera_tests.cpp, commit_tests.cpp, tiling_regression_tests.cpp,
+readback_bench_tests.cpp, material_texture_tests.cpp, gpu_selection_tests.cpp).
+"""
+import os
+import time
+
+import numpy as np
+import pytest
+
+from miniraytrace_b200 import abi, scenes
+
+pytestmark = pytest.mark.gpu
+THREADS = max(1, min(32, os.cpu_count() or 1))
+
+
+def parity_fraction(img, ref, rtol=1e-3, atol=1e-6):
+    d = np.abs(img[..., :3].astype(np.float64) - ref[..., :3].astype(np.float64))
+    ok = (d <= rtol * np.abs(ref[..., :3]) + atol).all(-1)
+    return ok.mean()
+
+
+def render_both(gpu, oracle_lib, s, spp):
+    e = gpu.Engine(s.settings["width"], s.settings["height"])
+    s.apply(e)
+    for _ in range(spp):
+        e.render_frame()
+    img = e.read_framebuffer(abi.MRT_PIXEL_RGBA32F_LINEAR)
+    o = oracle_lib.OracleScene(s.settings["width"], s.settings["height"])
+    s.apply(o)
+    o.commit()
+    acc = o.render_f32(0, spp, threads=THREADS)
+    ref = oracle_lib.readback_f32(acc, spp).reshape(img.shape)
+    return e, img, ref, acc
+
+
+def test_config1_image_parity(gpu, oracle_lib):
+    s = scenes.box_sphere()
+    e, img, ref, acc = render_both(gpu, oracle_lib, s, 16)
+    assert (img[..., 3] == 1.0).all()
+    assert np.isfinite(img).all()
+    frac = parity_fraction(img, ref)
+    print(f"config-1 parity: {frac * 100:.4f}% of pixels within 1e-3")
+    assert frac >= 0.999
+    # RGBA8: resolve of the same accumulation within 1 LSB
+    rgba8 = e.read_framebuffer(abi.MRT_PIXEL_RGBA8_SRGB)
+    ref8 = oracle_lib.resolve_rgba8(acc.reshape(img.shape), 0.0, abi.MRT_TONEMAP_LINEAR)
+    close = (np.abs(rgba8.astype(int) - ref8.astype(int)) <= 1).all(-1).mean()
+    assert close >= 0.999 and (rgba8[..., 3] == 255).all()
+    e.close()
+
+
+def test_environment_scene_parity(gpu, oracle_lib):
+    """Config-2 features at a small size: env importance sampling + MIS,
+    GGX conductors, dielectrics, instancing, diffuse terrain."""
+    s = scenes.terrain(width=96, height=64, spp=4, grid=48, spheres=24, sky=(256, 128))
+    e, img, ref, _ = render_both(gpu, oracle_lib, s, 4)
+    frac = parity_fraction(img, ref)
+    print(f"terrain parity: {frac * 100:.4f}% of pixels within 1e-3")
+    assert frac >= 0.999
+    e.close()
+
+
+def test_render_frames_equals_repeated_render_frame(gpu):
+    s = scenes.box_sphere(64, 64)
+    a = gpu.Engine(64, 64)
+    s.apply(a)
+    for _ in range(5):
+        a.render_frame()
+    b = gpu.Engine(64, 64)
+    s.apply(b)
+    info = b.render_frames(5)
+    assert info["spp"] == 5
+    ia, ib = a.read_framebuffer(), b.read_framebuffer()
+    np.testing.assert_allclose(ia, ib, rtol=1e-6, atol=1e-7)
+    acc, spp = b.read_accumulation()
+    assert spp == 5 and (acc[..., 3] == 5).all()
+    a.close()
+    b.close()
+
+
+def test_spp_limit_and_reset(gpu):
+    s = scenes.box_sphere(32, 32)
+    e = gpu.Engine(32, 32)
+    s.apply(e)
+    st = dict(s.settings)
+    st["spp_limit"] = 3
+    e.set_render_settings(**st)
+    infos = [e.render_frame() for _ in range(5)]
+    assert [i["spp"] for i in infos] == [1, 2, 3, 3, 3]
+    assert [i["converged"] for i in infos] == [False, False, True, True, True]
+    e.reset_accumulation()
+    z = e.read_framebuffer()
+    assert (z[..., :3] == 0).all() and (z[..., 3] == 1).all()
+    assert e.render_frame()["spp"] == 1
+    e.close()
+
+
+# ---- reference tests/camera_tests.cpp ----------------------------------------------
+
+def emissive_quad_engine(gpu, w, h, z):
+    e = gpu.Engine(w, h)
+    e.set_render_settings(width=w, height=h, max_bounces=0, spp_limit=1, denoise=False)
+    s = 1000.0
+    pos = np.array([[-s, -s, z], [s, -s, z], [s, s, z], [-s, -s, z], [s, s, z], [-s, s, z]], np.float32)
+    mesh = e.add_mesh(pos, np.arange(6, dtype=np.uint32))
+    mat = e.add_material(base_color=(0, 0, 0), emission=(1.0, 0.5, 0.25))
+    e.add_instance(mesh, None, mat)
+    return e
+
+
+def render32(e):
+    e.render_frame()
+    return e.read_framebuffer(abi.MRT_PIXEL_RGBA32F_LINEAR)
+
+
+def test_camera_ex_matches_legacy(gpu):
+    legacy = emissive_quad_engine(gpu, 48, 48, -20.0)
+    legacy.set_camera(position=(0, 0, 0), target=(0, 0, -1), up=(0, 1, 0), fov_y_deg=90.0)
+    a = render32(legacy)
+    ex = emissive_quad_engine(gpu, 48, 48, -20.0)
+    ex.set_camera_ex(position=(0, 0, 0), forward=(0, 0, -1), up=(0, 1, 0), left=-1, right=1, bottom=-1, top=1)
+    b = render32(ex)
+    assert np.array_equal(a, b)
+    assert np.array_equal(a[..., :3], np.broadcast_to(np.array([1.0, 0.5, 0.25], np.float32), a[..., :3].shape))
+
+
+def test_orthographic_distance_invariance(gpu):
+    imgs = []
+    for eye in (0.0, 30.0):
+        e = emissive_quad_engine(gpu, 32, 32, -50.0)
+        e.set_camera_ex(projection=abi.MRT_CAMERA_ORTHOGRAPHIC, position=(0, 0, eye), forward=(0, 0, -1),
+                        up=(0, 1, 0), left=-1, right=1, bottom=-1, top=1)
+        imgs.append(render32(e))
+    assert np.array_equal(imgs[0], imgs[1])
+
+
+def test_asymmetric_crop(gpu):
+    big = emissive_quad_engine(gpu, 64, 32, -20.0)
+    big.set_camera_ex(forward=(0, 0, -1), up=(0, 1, 0), left=-1, right=1, bottom=-1, top=1)
+    a = render32(big)
+    crop = emissive_quad_engine(gpu, 32, 32, -20.0)
+    crop.set_camera_ex(forward=(0, 0, -1), up=(0, 1, 0), left=0, right=1, bottom=-1, top=1)
+    b = render32(crop)
+    assert np.array_equal(a[:, 32:, :3], b[..., :3])
+
+
+# ---- reference tests/commit_tests.cpp -------------------------------------------------
+
+def small_engine(gpu, w=64, h=64, spp_limit=4):
+    e = gpu.Engine(w, h)
+    e.set_render_settings(width=w, height=h, spp_limit=spp_limit, denoise=False)
+    return e
+
+
+TRI = np.array([[-0.5, -0.5, 0.0], [0.5, -0.5, 0.0], [0.0, 0.5, 0.0]], np.float32)
+
+
+def add_triangle(e, mat=0):
+    mesh = e.add_mesh(TRI, np.arange(3, dtype=np.uint32))
+    e.add_instance(mesh, None, mat)
+
+
+def test_commit_noop(gpu):
+    e = small_engine(gpu)
+    st = e.commit()
+    assert st["blasRebuilt"] == 0 and st["tlasRebuilt"] is False
+
+
+def test_commit_rebuilds_once(gpu):
+    e = small_engine(gpu)
+    add_triangle(e)
+    st = e.commit()
+    assert st["blasRebuilt"] == 1 and st["tlasRebuilt"] is True
+    st2 = e.commit()
+    assert st2["blasRebuilt"] == 0 and st2["tlasRebuilt"] is False
+
+
+def test_camera_only_commit_is_lightweight(gpu):
+    e = small_engine(gpu)
+    add_triangle(e)
+    e.commit()
+    e.set_camera(position=(0, 0, 6))
+    st = e.commit()
+    assert st["blasRebuilt"] == 0 and st["tlasRebuilt"] is False
+
+
+def test_explicit_commit_matches_implicit(gpu):
+    a = small_engine(gpu)
+    add_triangle(a)
+    a.commit()
+    ia = a.render_frame()
+    b = small_engine(gpu)
+    add_triangle(b)
+    ib = b.render_frame()
+    assert ia["spp"] == ib["spp"]
+    assert np.array_equal(a.read_framebuffer(), b.read_framebuffer())
+
+
+# ---- reference tests/tiling_regression_tests.cpp ---------------------------------------
+
+def test_small_emissive_triangle_visible(gpu):
+    e = small_engine(gpu)
+    pos = np.array([[-0.6, -0.6, 0.0], [0.6, -0.6, 0.0], [0.0, 0.6, 0.0]], np.float32)
+    mesh = e.add_mesh(pos, np.arange(3, dtype=np.uint32))
+    mat = e.add_material(base_color=(1.0, 0.2, 0.1), emission=(2.0, 0.4, 0.2))
+    e.add_instance(mesh, None, mat)
+    e.set_camera(position=(0, 0, 3), target=(0, 0, 0), up=(0, 1, 0), fov_y_deg=45.0)
+    e.commit()
+    for _ in range(4):
+        e.render_frame()
+    rgba8 = e.read_framebuffer(abi.MRT_PIXEL_RGBA8_SRGB)
+    assert int(rgba8[..., 0].max()) > 10
+
+
+# ---- reference tests/readback_bench_tests.cpp ---------------------------------------
+
+def test_readback_1080p_fast_and_opaque(gpu):
+    e = gpu.Engine(1920, 1080)
+    e.set_render_settings(width=1920, height=1080, spp_limit=1, denoise=False)
+    e.render_frame()
+    buf = np.empty((1080, 1920, 4), np.float32)
+    e.read_framebuffer(out=buf)
+    t0 = time.perf_counter()
+    for _ in range(20):
+        e.read_framebuffer(out=buf)
+    ms = (time.perf_counter() - t0) / 20 * 1e3
+    print(f"1080p RGBA32F readback: {ms:.3f} ms/call")
+    assert ms < 20.0
+    assert (buf[..., 3] == 1.0).all()
+
+
+def test_readback_rejects_small_dst(gpu):
+    import ctypes as C
+    e = gpu.Engine(16, 16)
+    small = np.empty(16 * 16 * 4 - 1, np.float32)
+    lib = gpu.load_library()
+    r = lib.mrtReadFramebuffer(e.h, abi.MRT_PIXEL_RGBA32F_LINEAR, small.ctypes.data_as(C.c_void_p), small.nbytes)
+    assert r == abi.MRT_ERROR_INVALID_ARGUMENT
+    r = lib.mrtReadFramebuffer(e.h, abi.MRT_PIXEL_RGBA8_SRGB, small.ctypes.data_as(C.c_void_p), 16 * 16 * 4 - 1)
+    assert r == abi.MRT_ERROR_INVALID_ARGUMENT
+
+
+# ---- reference tests/material_texture_tests.cpp ---------------------------------------
+
+def one_pixel(r, g, b):
+    return np.array([[[r, g, b, 255]]], np.uint8)
+
+
+def test_removed_material_falls_back(gpu):
+    e = small_engine(gpu, 32, 32, 2)
+    mat = e.add_material(base_color=(1, 0, 0))
+    add_triangle(e, mat)
+    e.commit()
+    e.remove_material(mat)
+    e.render_frame()
+
+
+def test_texture_slot_recycling_and_fallback(gpu):
+    e = small_engine(gpu, 32, 32, 2)
+    t1 = e.add_texture(one_pixel(255, 0, 0), abi.MRT_TEX_RGBA8_UNORM)
+    assert t1 != 0
+    e.remove_texture(t1)
+    t2 = e.add_texture(one_pixel(0, 255, 0), abi.MRT_TEX_RGBA8_UNORM)
+    mat = e.add_material(base_color_tex=t2)
+    add_triangle(e, mat)
+    e.commit()
+    e.render_frame()
+    e.remove_texture(t2)
+    e.commit()
+    e.render_frame()
+
+
+def test_texture_thrash_stays_bounded(gpu):
+    e = small_engine(gpu, 32, 32, 2)
+    prev = e.add_texture(one_pixel(10, 20, 30), abi.MRT_TEX_RGBA8_UNORM)
+    e.commit()
+    base = e.stats()["deviceBytes"]
+    for i in range(300):
+        e.remove_texture(prev)
+        prev = e.add_texture(one_pixel(i % 256, 0, 0), abi.MRT_TEX_RGBA8_UNORM)
+        assert prev != 0
+        if i % 37 == 0:
+            e.commit()
+    e.commit()
+    assert e.stats()["deviceBytes"] <= base + 4096
+    e.render_frame()
+
+
+def test_textured_material_parity(gpu, oracle_lib):
+    """Base-color (sRGB), roughness (UNORM) and emission textures on the
+    config-1 box, compared with the oracle."""
+    s = scenes.box_sphere(64, 64)
+    rng = np.random.default_rng(3)
+    tex = rng.integers(0, 256, (8, 8, 4), dtype=np.uint8)
+    uv = np.array([[0, 0], [1, 0], [1, 1], [0, 1]], np.float32)
+    for m in s.meshes[:5]:
+        m.uvs = uv
+    e = gpu.Engine(64, 64)
+    o = oracle_lib.OracleScene(64, 64)
+    out = []
+    for t in (e, o):
+        s.apply(t)
+        tid = t.add_texture(tex, abi.MRT_TEX_RGBA8_SRGB)
+        tid2 = t.add_texture(tex, abi.MRT_TEX_RGBA8_UNORM)
+        mid = t.add_material(base_color=(1, 1, 1), base_color_tex=tid, roughness_tex=tid2, emission=(0.2, 0.2, 0.2),
+                             emission_tex=tid2)
+        mesh = t.add_mesh(np.array([[-1, 0.01, 1], [1, 0.01, 1], [1, 0.01, -1], [-1, 0.01, -1]], np.float32),
+                          np.array([0, 1, 2, 0, 2, 3], np.uint32), None, uv)
+        t.add_instance(mesh, np.array([[0.5, 0, 0, 0], [0, 1, 0, 0], [0, 0, 0.5, 0.4]], np.float32), mid)
+        t.commit()
+    for _ in range(4):
+        e.render_frame()
+    img = e.read_framebuffer()
+    ref = oracle_lib.readback_f32(o.render_f32(0, 4, threads=THREADS), 4).reshape(img.shape)
+    assert parity_fraction(img, ref) >= 0.999
+
+
+def test_point_and_rect_lights_parity(gpu, oracle_lib):
+    s = scenes.box_sphere(64, 64)
+    s.lights = [dict(type=abi.MRT_LIGHT_POINT, position=(0.3, 1.6, 0.2), radiance=(5.0, 4.0, 3.0)),
+                dict(type=abi.MRT_LIGHT_RECT, corner=(-0.4, 1.99, -0.4), edge0=(0.8, 0, 0), edge1=(0, 0, 0.8),
+                     radiance=(6.0, 6.0, 6.0), two_sided=True)]
+    e, img, ref, _ = render_both(gpu, oracle_lib, s, 4)
+    assert parity_fraction(img, ref) >= 0.999
+
+
+# ---- reference tests/gpu_selection_tests.cpp -------------------------------------------
+
+def test_out_of_range_gpu_index_fails_clearly(gpu):
+    with pytest.raises(gpu.MrtError) as e:
+        gpu.Engine(16, 16, gpu_index1=10000)
+    assert e.value.code == abi.MRT_ERROR_VULKAN_INIT
+    assert "out of range" in gpu.last_error()
+
+
+def test_env_cdf_kernel_matches_oracle(gpu, oracle_lib):
+    e = gpu.Engine(16, 16)
+    for w, h in ((64, 32), (2048, 1024), (4096, 2048)):
+        sky = scenes.procedural_sky(w, h)
+        cdf, integ = e.build_env_cdf(sky)
+        rcdf, rinteg = oracle_lib.env_cdf(sky)
+        ulp = np.abs(cdf.view(np.int32).astype(np.int64) - rcdf.view(np.int32).astype(np.int64))
+        assert ulp.max() <= 2, (w, h, ulp.max())
+        assert abs(integ - rinteg) <= 1e-6 * abs(rinteg)
+    e.close()

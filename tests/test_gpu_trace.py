@@ -1,0 +1,145 @@
+"""Traversal parity (GPU, through the C ABI extension mrtxTraceRays).
+
+Gate: closest-hit primitive ids bit-exact against the brute-force oracle
+(Moeller-Trumbore over every triangle in original order, reference
+tests/bvh_tests.cpp:145-151) on non-degenerate rays, t within 1e-6 relative.
+A ray is non-degenerate when the oracle's hit has smallest barycentric
+>= 1e-5 and the second-nearest accepted t differs by more than 1e-5 relative.
+The GPU uses a watertight test (Woop et al. 2013), which may legitimately
+differ from Moeller-Trumbore only on the excluded near-edge / near-tie rays.
+"""
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from miniraytrace_b200 import scenes
+
+GOLDEN = Path(__file__).resolve().parent / "golden"
+pytestmark = pytest.mark.gpu
+
+
+def nondegenerate(bf, t2, mb):
+    t = bf["t"]
+    return (bf["hit"] == 1) & (mb >= 1e-5) & (np.abs(t2 - t) > 1e-5 * np.abs(t))
+
+
+def check_parity(gh, bf, t2, mb, min_hits=50):
+    nd = nondegenerate(bf, t2, mb)
+    miss = bf["hit"] == 0
+    assert nd.sum() >= min_hits
+    assert (gh["hit"][nd] == 1).all()
+    assert np.array_equal(gh["prim"][nd], bf["prim"][nd])
+    assert np.array_equal(gh["instance"][nd], bf["instance"][nd])
+    rel = np.abs(gh["t"][nd] - bf["t"][nd]) / np.abs(bf["t"][nd])
+    assert rel.max() <= 1e-6, rel.max()
+    # clear misses stay misses (a watertight hit may only appear on a near-edge ray)
+    assert (gh["hit"][miss] == 0).mean() >= 0.999
+    return nd.sum()
+
+
+def soup(target, tris):
+    pos = np.asarray(tris, np.float32).reshape(-1, 3)
+    mesh = target.add_mesh(pos, np.arange(pos.shape[0], dtype=np.uint32))
+    target.add_instance(mesh, None, 0)
+    target.commit()
+
+
+def test_bvh_tests_rays_vs_bruteforce(gpu, oracle_lib):
+    g = np.load(GOLDEN / "bvh_cases.npz")
+    e = gpu.Engine(16, 16)
+    o = oracle_lib.OracleScene(16, 16)
+    soup(e, g["tris7"])
+    soup(o, g["tris7"])
+    rays = g["rays123"]
+    gh = e.trace_rays(rays[:, :3], rays[:, 3:])
+    bf, t2, mb = o.trace_bruteforce(rays[:, :3], rays[:, 3:])
+    check_parity(gh, bf, t2, mb)
+    occ = e.trace_shadow_rays(rays[:, :3], rays[:, 3:])
+    assert (occ[bf["hit"] == 0] == 0).mean() >= 0.999
+    assert (occ[nondegenerate(bf, t2, mb)] == 1).all()
+    e.close()
+
+
+def test_dense_soup_many_rays(gpu, oracle_lib):
+    rng = np.random.default_rng(11)
+    n = 4000
+    base = rng.uniform(-5, 5, (n, 3)).astype(np.float32)
+    tris = np.concatenate([base, base + rng.uniform(-0.6, 0.6, (n, 3)), base + rng.uniform(-0.6, 0.6, (n, 3))], 1)
+    e = gpu.Engine(16, 16)
+    o = oracle_lib.OracleScene(16, 16)
+    soup(e, tris)
+    soup(o, tris)
+    m = 20000
+    org = rng.uniform(-8, 8, (m, 3)).astype(np.float32)
+    d = rng.normal(size=(m, 3)).astype(np.float32)
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    gh = e.trace_rays(org, d)
+    bf, t2, mb = o.trace_bruteforce(org, d, threads=8)
+    assert check_parity(gh, bf, t2, mb, min_hits=2000) > 2000
+    e.close()
+
+
+def test_instanced_scene_primary_rays(gpu, oracle_lib):
+    """Box + sphere (config 1) and translated/scaled instances."""
+    s = scenes.box_sphere(64, 64)
+    pos, idx, nrm = scenes.icosphere(2)
+    s.meshes.append(scenes.MeshSpec(pos, idx, nrm))
+    for k, (x, y, z, r) in enumerate([(0.6, 1.4, -0.3, 0.2), (-0.5, 1.2, 0.4, 0.15), (0.2, 1.7, 0.5, 0.1)]):
+        s.instances.append((len(s.meshes) - 1, np.array([[r, 0, 0, x], [0, r, 0, y], [0, 0, r, z]], np.float32), 0))
+    e = gpu.Engine(64, 64)
+    o = oracle_lib.OracleScene(64, 64)
+    s.apply(e)
+    s.apply(o)
+    e.commit()
+    o.commit()
+    rng = np.random.default_rng(5)
+    m = 30000
+    org = np.tile(np.array([[0.0, 1.0, 3.6]], np.float32), (m, 1))
+    d = np.stack([rng.uniform(-0.45, 0.45, m), rng.uniform(-0.5, 0.4, m), -np.ones(m)], 1).astype(np.float32)
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    gh = e.trace_rays(org, d)
+    bf, t2, mb = o.trace_bruteforce(org, d, threads=8)
+    check_parity(gh, bf, t2, mb, min_hits=20000)
+    # secondary rays from inside the box in all directions
+    org2 = rng.uniform([-0.9, 0.1, -0.9], [0.9, 1.9, 0.9], (m, 3)).astype(np.float32)
+    d2 = rng.normal(size=(m, 3)).astype(np.float32)
+    d2 /= np.linalg.norm(d2, axis=1, keepdims=True)
+    gh2 = e.trace_rays(org2, d2)
+    bf2, t22, mb2 = o.trace_bruteforce(org2, d2, threads=8)
+    check_parity(gh2, bf2, t22, mb2, min_hits=20000)
+    e.close()
+
+
+def test_heightfield_rays(gpu, oracle_lib):
+    pos, idx, nrm, _ = scenes.heightfield(96)
+    e = gpu.Engine(16, 16)
+    o = oracle_lib.OracleScene(16, 16)
+    for t in (e, o):
+        mesh = t.add_mesh(pos, idx, nrm)
+        t.add_instance(mesh, None, 0)
+        t.commit()
+    rng = np.random.default_rng(9)
+    m = 20000
+    org = np.stack([rng.uniform(-1, 1, m), np.full(m, 0.8), rng.uniform(-1, 1, m)], 1).astype(np.float32)
+    d = np.stack([rng.uniform(-0.6, 0.6, m), -np.ones(m), rng.uniform(-0.6, 0.6, m)], 1).astype(np.float32)
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    gh = e.trace_rays(org, d)
+    bf, t2, mb = o.trace_bruteforce(org, d, threads=8)
+    check_parity(gh, bf, t2, mb, min_hits=10000)
+    e.close()
+
+
+def test_empty_scene_and_tmax(gpu):
+    e = gpu.Engine(8, 8)
+    gh = e.trace_rays(np.zeros((4, 3)), np.tile([[0, 0, -1.0]], (4, 1)))
+    assert (gh["hit"] == 0).all()
+    tri = np.array([[-1, -1, -2], [1, -1, -2], [0, 1, -2]], np.float32)
+    soup(e, tri)
+    gh = e.trace_rays(np.zeros((3, 3)), np.tile([[0, 0, -1.0]], (3, 1)), t_max=np.float32(5.0))
+    assert (gh["hit"] == 1).all() and np.allclose(gh["t"], 2.0)
+    gh = e.trace_rays(np.zeros((1, 3)), [[0, 0, -1.0]], t_max=1.5)
+    assert gh["hit"][0] == 0
+    occ = e.trace_shadow_rays(np.zeros((2, 3)), [[0, 0, -1.0], [0, 0, 1.0]])
+    assert list(occ) == [1, 0]
+    e.close()

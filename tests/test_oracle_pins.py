@@ -1,0 +1,149 @@
+"""Pins the CPU oracle before it is trusted as the checker.
+
+- BVH: the oracle's restated builder must produce exactly the nodes and
+  primitive order of the reference's own BvhBuilder (core/src/accel/Bvh.cpp,
+  compiled from its sources into oracle/_ref), on the input sets of the
+  reference's tests/bvh_tests.cpp (fixtures) and on fresh random sets.
+- The reference's BVH tests (topology, traversal == brute force, degenerate
+  inputs: bvh_tests.cpp:91-188) are restated against the oracle.
+- pcg4d golden vectors; environment-CDF fixture and properties.
+"""
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+GOLDEN = Path(__file__).resolve().parent / "golden"
+
+
+def tri_aabbs(t):
+    t = np.asarray(t, np.float32).reshape(-1, 3, 3)
+    return np.concatenate([t.min(1), t.max(1)], 1)
+
+
+@pytest.fixture(scope="module")
+def cases():
+    return np.load(GOLDEN / "bvh_cases.npz")
+
+
+@pytest.mark.parametrize("key", ["42", "7"])
+def test_oracle_bvh_equals_reference_fixture(oracle_lib, cases, key):
+    nodes, order = oracle_lib.bvh_build(tri_aabbs(cases["tris" + key]), 4)
+    assert np.array_equal(nodes.view(np.uint32).reshape(-1, 8), cases["nodes" + key])
+    assert np.array_equal(order, cases["order" + key])
+
+
+@pytest.mark.parametrize("seed,n,leaf", [(1, 1, 4), (2, 3, 4), (3, 1000, 4), (4, 3000, 1), (5, 20000, 4)])
+def test_oracle_bvh_equals_reference_build(oracle_lib, seed, n, leaf):
+    if oracle_lib.load_ref_bvh() is None:
+        pytest.skip("reference BVH library not built (reference checkout absent)")
+    rng = np.random.default_rng(seed)
+    lo = rng.uniform(-50, 50, (n, 3)).astype(np.float32)
+    hi = lo + rng.exponential(1.0, (n, 3)).astype(np.float32)
+    if n > 100:  # include exact duplicates and flat boxes
+        hi[:10] = lo[:10]
+        lo[10:20] = lo[0]
+        hi[10:20] = hi[0]
+    ab = np.concatenate([lo, hi], 1)
+    a_nodes, a_order = oracle_lib.bvh_build(ab, leaf)
+    b_nodes, b_order = oracle_lib.bvh_build(ab, leaf, use_reference=True)
+    assert a_nodes.tobytes() == b_nodes.tobytes()
+    assert np.array_equal(a_order, b_order)
+
+
+def test_bvh_topology(oracle_lib, cases):
+    """bvh_tests.cpp:91-119: every primitive exactly once, children in range."""
+    nodes, order = oracle_lib.bvh_build(tri_aabbs(cases["tris42"]), 4)
+    n = cases["tris42"].shape[0]
+    assert order.size == n and len(nodes) > 0
+    seen = np.zeros(n, np.int64)
+    leaf_prims = 0
+    for nd in nodes:
+        count = int(nd["packed"]) >> 2
+        if count == 0:
+            assert int(nd["leftOrPrim"]) + 1 < len(nodes)
+        else:
+            leaf_prims += count
+            for i in range(count):
+                seen[order[int(nd["leftOrPrim"]) + i]] += 1
+    assert leaf_prims == n
+    assert (seen == 1).all()
+
+
+def test_bvh_degenerate_inputs(oracle_lib):
+    """bvh_tests.cpp:165-188."""
+    nodes, order = oracle_lib.bvh_build(np.zeros((0, 6), np.float32), 4)
+    assert len(nodes) == 0
+    nodes, order = oracle_lib.bvh_build(np.array([[0, 0, 0, 1, 1, 1]], np.float32), 4)
+    assert len(nodes) == 1 and (int(nodes[0]["packed"]) >> 2) == 1
+    same = np.tile(np.array([[1, 2, 3, 1, 2, 3]], np.float32), (100, 1))
+    nodes, order = oracle_lib.bvh_build(same, 4)
+    assert sum(int(nd["packed"]) >> 2 for nd in nodes) == 100
+
+
+def _soup_scene(oracle_lib, tris):
+    o = oracle_lib.OracleScene(16, 16)
+    pos = np.asarray(tris, np.float32).reshape(-1, 3)
+    idx = np.arange(pos.shape[0], dtype=np.uint32)
+    mesh = o.add_mesh(pos, idx)
+    inst = o.add_instance(mesh, None, 0)
+    o.commit()
+    return o, inst
+
+
+def test_bvh_traversal_matches_bruteforce(oracle_lib, cases):
+    """bvh_tests.cpp:121-163 on the same triangles (seed 7) and rays (seed 123):
+    hit/miss agrees, t within 1e-4 relative, and more than 50 hits."""
+    o, _ = _soup_scene(oracle_lib, cases["tris7"])
+    rays = cases["rays123"]
+    bvh = o.trace_rays(rays[:, :3], rays[:, 3:])
+    bf, t2, mb = o.trace_bruteforce(rays[:, :3], rays[:, 3:])
+    assert np.array_equal(bvh["hit"], bf["hit"])
+    h = bf["hit"] == 1
+    assert h.sum() > 50
+    np.testing.assert_allclose(bvh["t"][h], bf["t"][h], rtol=1e-4)
+    # with the same Moeller-Trumbore test the closest triangle is identical
+    assert (bvh["prim"][h] == bf["prim"][h]).mean() > 0.999
+
+
+def test_shadow_rays_agree_with_closest_hit(oracle_lib, cases):
+    o, _ = _soup_scene(oracle_lib, cases["tris7"])
+    rays = cases["rays123"]
+    bvh = o.trace_rays(rays[:, :3], rays[:, 3:])
+    occ = o.trace_shadow_rays(rays[:, :3], rays[:, 3:])
+    assert np.array_equal(occ, bvh["hit"])
+
+
+def test_pcg4d_golden(oracle_lib):
+    g = np.load(GOLDEN / "pcg4d.npz")
+    assert np.array_equal(oracle_lib.pcg4d(g["states"]), g["out"])
+
+
+def test_env_cdf_golden_and_properties(oracle_lib):
+    g = np.load(GOLDEN / "env_cdf.npz")
+    cdf, integral = oracle_lib.env_cdf(g["sky"])
+    assert np.array_equal(cdf, g["cdf"])
+    assert np.float32(integral) == g["integral"]
+    h, w = g["sky"].shape[:2]
+    rows = cdf[: w * h].reshape(h, w)
+    assert (np.diff(rows, axis=1) >= 0).all()
+    assert np.allclose(rows[:, -1], 1.0, atol=1e-6)
+    marg = cdf[w * h:]
+    assert (np.diff(marg) >= 0).all() and abs(marg[-1] - 1.0) < 1e-6
+    # integral ~ sum of luminance * sin(theta) * dtheta * dphi
+    sky = g["sky"].astype(np.float64)
+    lum = 0.2126 * sky[..., 0] + 0.7152 * sky[..., 1] + 0.0722 * sky[..., 2]
+    th = (np.arange(h) + 0.5) * np.pi / h
+    ref = (lum * np.sin(th)[:, None]).sum() * (np.pi / h) * (2 * np.pi / w)
+    assert abs(integral - ref) / ref < 1e-5
+
+
+def test_readback_and_resolve_semantics(oracle_lib):
+    acc = np.array([[2.0, 4.0, 6.0, 2.0], [0.0, 0.0, 0.0, 0.0]], np.float32)
+    out = oracle_lib.readback_f32(acc, 2)
+    assert np.array_equal(out, np.array([[1, 2, 3, 1], [0, 0, 0, 1]], np.float32))
+    out0 = oracle_lib.readback_f32(acc, 0)
+    assert (out0[:, :3] == 0).all() and (out0[:, 3] == 1).all()
+    rgba8 = oracle_lib.resolve_rgba8(acc, 0.0, 0)
+    assert rgba8[0, 3] == 255 and rgba8[0, 0] == 255  # mean 1.0 -> white
+    assert (rgba8[1, :3] == 0).all()
