@@ -104,7 +104,7 @@ typedef struct MrtFrameParams {
     // frame index streamOffset + n * streamStride (reference stream:
     // offset 0, stride 1, pathtrace.comp:105).
     uint32_t streamOffset, streamStride;
-    uint32_t nodeCount, instanceCount;
+    uint32_t nodeCount, instanceCount, triCount, materialCount;
     // scene arrays (device pointers)
     const MrtNode* nodes;
     const float4* triVerts;

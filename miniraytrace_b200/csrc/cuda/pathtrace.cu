@@ -47,7 +47,7 @@ MRT_DEV Surface makeSurface(const MrtFrameParams& P, float3 rayDir, const HitRec
         nGeom = -nGeom;
         nShade = -nShade;
     }
-    s.mat = in->materialIndex;
+    s.mat = in->materialIndex < P.materialCount ? in->materialIndex : 0u;
     const MrtMaterial& m = P.materials[s.mat];
     if (m.tex[3] >= 0) {  // tangent-space normal map
         const float4 ta = ldg4(P.tangents + tri.x), tb = ldg4(P.tangents + tri.y), tc = ldg4(P.tangents + tri.z);
@@ -217,6 +217,7 @@ __global__ void __launch_bounds__(128) pathtraceKernel(MrtFrameParams P, uint32_
             a[1] = make_double2(a1.x + sz, a1.y + double(sampleCount));
         }
         if (!pc.ok) atomicOr(P.errorFlags, 1u);
+        if (pc.tc.bad) atomicOr(P.errorFlags, 2u);
     }
     warpAddCounters(P.rayCounters, pc);
 }
@@ -230,6 +231,7 @@ __global__ void traceClosestKernel(MrtFrameParams P, const MrtQueryRay* __restri
     TraversalCounters tc;
     const bool ok = traceClosest(P, f3p(r.origin), f3p(r.dir), r.tMax, h, tc);
     if (!ok) atomicOr(P.errorFlags, 1u);
+    if (tc.bad) atomicOr(P.errorFlags, 2u);
     MrtQueryHit out;
     out.pad[0] = out.pad[1] = 0;
     if (h.tri != 0xffffffffu) {
@@ -258,6 +260,7 @@ __global__ void traceAnyKernel(MrtFrameParams P, const MrtQueryRay* __restrict__
     TraversalCounters tc;
     occluded[i] = traceAny(P, f3p(r.origin), f3p(r.dir), r.tMax, ok, tc) ? 1u : 0u;
     if (!ok) atomicOr(P.errorFlags, 1u);
+    if (tc.bad) atomicOr(P.errorFlags, 2u);
 }
 
 }  // namespace

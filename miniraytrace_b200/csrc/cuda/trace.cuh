@@ -23,6 +23,10 @@
 #define MRT_EPS_RAY 1e-4f
 #define MRT_TLAS_STACK 32
 #define MRT_BLAS_STACK 48
+// Upper bound on node visits of one traversal. A well-formed BVH never gets
+// near it; it only turns a malformed tree into an error flag instead of an
+// endless loop.
+#define MRT_MAX_VISITS (1u << 22)
 
 struct TraceRay {
     float3 o, d;
@@ -122,12 +126,20 @@ MRT_DEV bool hitTriangle(const float4* __restrict__ tv, uint32_t tri, float3 o, 
 
 // Per-thread traffic counters for the roofline's algorithmic bytes: node
 // records fetched (32 B each) and triangle tests (48 B each).
+// `bad` records an out-of-range index met during traversal: the access is
+// redirected to a valid element and the ray is reported through the error
+// flag instead of reading outside the scene arrays.
 struct TraversalCounters {
     uint32_t nodes = 0, tris = 0;
+    bool bad = false;
 };
 
-MRT_DEV void loadNode(const MrtNode* __restrict__ nodes, uint32_t i, float4& a, float4& b, TraversalCounters& c) {
-    const float4* p = reinterpret_cast<const float4*>(nodes + i);
+MRT_DEV void loadNode(const MrtFrameParams& P, uint32_t i, float4& a, float4& b, TraversalCounters& c) {
+    if (i >= P.nodeCount) {
+        c.bad = true;
+        i = 0;
+    }
+    const float4* p = reinterpret_cast<const float4*>(P.nodes + i);
     a = ldg4(p);
     b = ldg4(p + 1);
     c.nodes++;
@@ -142,18 +154,20 @@ MRT_DEV bool closestBlas(const MrtFrameParams& P, uint32_t root, uint32_t inst, 
     uint32_t stack[MRT_BLAS_STACK];
     int sp = 0;
     float4 na, nb;
-    loadNode(P.nodes, root, na, nb, tc);
+    loadNode(P, root, na, nb, tc);
     if (!(slabNode(na, nb, o, inv, tMax) < __int_as_float(0x7f800000))) return true;
     uint32_t node = root;
     bool ok = true;
+    uint32_t visits = 0;
     for (;;) {
+        if (++visits > MRT_MAX_VISITS) { ok = false; return false; }
         const uint32_t packed = __float_as_uint(nb.w);
         const uint32_t first = __float_as_uint(na.w);
         const uint32_t count = packed >> 2;
         if (count == 0) {
             float4 a0, b0, a1, b1;
-            loadNode(P.nodes, first, a0, b0, tc);
-            loadNode(P.nodes, first + 1, a1, b1, tc);
+            loadNode(P, first, a0, b0, tc);
+            loadNode(P, first + 1, a1, b1, tc);
             const float t0 = slabNode(a0, b0, o, inv, tMax);
             const float t1 = slabNode(a1, b1, o, inv, tMax);
             const bool h0 = t0 < __int_as_float(0x7f800000), h1 = t1 < __int_as_float(0x7f800000);
@@ -177,6 +191,10 @@ MRT_DEV bool closestBlas(const MrtFrameParams& P, uint32_t root, uint32_t inst, 
             for (uint32_t i = 0; i < count; ++i) {
                 float t, u, v;
                 ++tc.tris;
+                if (first + i >= P.triCount) {
+                    tc.bad = true;
+                    break;
+                }
                 if (hitTriangle(P.triVerts, first + i, o, sh, tMax, t, u, v)) {
                     tMax = t;
                     hit.t = t;
@@ -191,7 +209,7 @@ MRT_DEV bool closestBlas(const MrtFrameParams& P, uint32_t root, uint32_t inst, 
         for (;;) {
             if (sp == 0) return ok;
             node = stack[--sp];
-            loadNode(P.nodes, node, na, nb, tc);
+            loadNode(P, node, na, nb, tc);
             if (slabNode(na, nb, o, inv, tMax) < __int_as_float(0x7f800000)) break;
         }
     }
@@ -203,21 +221,24 @@ MRT_DEV bool traceClosest(const MrtFrameParams& P, float3 o, float3 d, float tMa
     hit.tri = 0xffffffffu;
     hit.inst = 0;
     hit.u = hit.v = 0.0f;
+    if (P.instanceCount == 0) return true;  // empty scene (the TLAS root is a placeholder)
     const float3 inv = safeInv(d);
     uint32_t stack[MRT_TLAS_STACK];
     int sp = 0;
     float4 na, nb;
-    loadNode(P.nodes, P.tlasRoot, na, nb, tc);
+    loadNode(P, P.tlasRoot, na, nb, tc);
     if (!(slabNode(na, nb, o, inv, tMax) < __int_as_float(0x7f800000))) return true;
     bool ok = true;
+    uint32_t visits = 0;
     for (;;) {
+        if (++visits > MRT_MAX_VISITS) { ok = false; return false; }
         const uint32_t packed = __float_as_uint(nb.w);
         const uint32_t first = __float_as_uint(na.w);
         const uint32_t count = packed >> 2;
         if (count == 0) {
             float4 a0, b0, a1, b1;
-            loadNode(P.nodes, first, a0, b0, tc);
-            loadNode(P.nodes, first + 1, a1, b1, tc);
+            loadNode(P, first, a0, b0, tc);
+            loadNode(P, first + 1, a1, b1, tc);
             const float t0 = slabNode(a0, b0, o, inv, tMax);
             const float t1 = slabNode(a1, b1, o, inv, tMax);
             const bool h0 = t0 < __int_as_float(0x7f800000), h1 = t1 < __int_as_float(0x7f800000);
@@ -237,6 +258,10 @@ MRT_DEV bool traceClosest(const MrtFrameParams& P, float3 o, float3 d, float tMa
         } else {
             for (uint32_t i = 0; i < count; ++i) {
                 const uint32_t instIdx = first + i;
+                if (instIdx >= P.instanceCount) {
+                    tc.bad = true;
+                    break;
+                }
                 const MrtInstance* in = P.instances + instIdx;
                 const float3 oo = xformPoint(in->w2o, o), dd = xformDir(in->w2o, d);
                 ok &= closestBlas(P, in->blasRoot, instIdx, oo, dd, tMax, hit, tc);
@@ -244,7 +269,7 @@ MRT_DEV bool traceClosest(const MrtFrameParams& P, float3 o, float3 d, float tMa
         }
         for (;;) {
             if (sp == 0) return ok;
-            loadNode(P.nodes, stack[--sp], na, nb, tc);
+            loadNode(P, stack[--sp], na, nb, tc);
             if (slabNode(na, nb, o, inv, tMax) < __int_as_float(0x7f800000)) break;
         }
     }
@@ -258,16 +283,18 @@ MRT_DEV bool anyBlas(const MrtFrameParams& P, uint32_t root, float3 o, float3 d,
     uint32_t stack[MRT_BLAS_STACK];
     int sp = 0;
     float4 na, nb;
-    loadNode(P.nodes, root, na, nb, tc);
+    loadNode(P, root, na, nb, tc);
     if (!(slabNode(na, nb, o, inv, tMax) < __int_as_float(0x7f800000))) return false;
+    uint32_t visits = 0;
     for (;;) {
+        if (++visits > MRT_MAX_VISITS) { ok = false; return false; }
         const uint32_t packed = __float_as_uint(nb.w);
         const uint32_t first = __float_as_uint(na.w);
         const uint32_t count = packed >> 2;
         if (count == 0) {
             float4 a0, b0, a1, b1;
-            loadNode(P.nodes, first, a0, b0, tc);
-            loadNode(P.nodes, first + 1, a1, b1, tc);
+            loadNode(P, first, a0, b0, tc);
+            loadNode(P, first + 1, a1, b1, tc);
             const bool h0 = slabNode(a0, b0, o, inv, tMax) < __int_as_float(0x7f800000);
             const bool h1 = slabNode(a1, b1, o, inv, tMax) < __int_as_float(0x7f800000);
             if (h0 && h1) {
@@ -283,29 +310,36 @@ MRT_DEV bool anyBlas(const MrtFrameParams& P, uint32_t root, float3 o, float3 d,
             for (uint32_t i = 0; i < count; ++i) {
                 float t, u, v;
                 ++tc.tris;
+                if (first + i >= P.triCount) {
+                    tc.bad = true;
+                    break;
+                }
                 if (hitTriangle(P.triVerts, first + i, o, sh, tMax, t, u, v)) return true;
             }
         }
         if (sp == 0) return false;
-        loadNode(P.nodes, stack[--sp], na, nb, tc);
+        loadNode(P, stack[--sp], na, nb, tc);
     }
 }
 
 MRT_DEV bool traceAny(const MrtFrameParams& P, float3 o, float3 d, float tMax, bool& ok, TraversalCounters& tc) {
+    if (P.instanceCount == 0) return false;  // empty scene
     const float3 inv = safeInv(d);
     uint32_t stack[MRT_TLAS_STACK];
     int sp = 0;
     float4 na, nb;
-    loadNode(P.nodes, P.tlasRoot, na, nb, tc);
+    loadNode(P, P.tlasRoot, na, nb, tc);
     if (!(slabNode(na, nb, o, inv, tMax) < __int_as_float(0x7f800000))) return false;
+    uint32_t visits = 0;
     for (;;) {
+        if (++visits > MRT_MAX_VISITS) { ok = false; return false; }
         const uint32_t packed = __float_as_uint(nb.w);
         const uint32_t first = __float_as_uint(na.w);
         const uint32_t count = packed >> 2;
         if (count == 0) {
             float4 a0, b0, a1, b1;
-            loadNode(P.nodes, first, a0, b0, tc);
-            loadNode(P.nodes, first + 1, a1, b1, tc);
+            loadNode(P, first, a0, b0, tc);
+            loadNode(P, first + 1, a1, b1, tc);
             const bool h0 = slabNode(a0, b0, o, inv, tMax) < __int_as_float(0x7f800000);
             const bool h1 = slabNode(a1, b1, o, inv, tMax) < __int_as_float(0x7f800000);
             if (h0 && h1) {
@@ -319,12 +353,16 @@ MRT_DEV bool traceAny(const MrtFrameParams& P, float3 o, float3 d, float tMax, b
             }
         } else {
             for (uint32_t i = 0; i < count; ++i) {
+                if (first + i >= P.instanceCount) {
+                    tc.bad = true;
+                    break;
+                }
                 const MrtInstance* in = P.instances + first + i;
                 const float3 oo = xformPoint(in->w2o, o), dd = xformDir(in->w2o, d);
                 if (anyBlas(P, in->blasRoot, oo, dd, tMax, ok, tc)) return true;
             }
         }
         if (sp == 0) return false;
-        loadNode(P.nodes, stack[--sp], na, nb, tc);
+        loadNode(P, stack[--sp], na, nb, tc);
     }
 }

@@ -363,6 +363,7 @@ mrtResult Engine::packMaterials() {
         m_materialIndex[id] = uint32_t(mats.size());
         mats.push_back(g);
     }
+    m_materialCount = uint32_t(mats.size());
     return up(m_materials, mats.data(), mats.size() * sizeof(MrtMaterial));
 }
 
@@ -709,6 +710,8 @@ void Engine::fillParams(MrtFrameParams& p) const {
     p.streamStride = m_streamStride;
     p.nodeCount = m_nodeCount;
     p.instanceCount = m_instanceCount;
+    p.triCount = m_triCount;
+    p.materialCount = m_materialCount;
     p.nodes = m_nodes.as<MrtNode>();
     p.triVerts = m_triVerts.as<float4>();
     p.triIndex = m_triIndex.as<uint4>();
@@ -732,8 +735,9 @@ mrtResult Engine::checkErrorFlags() {
     MRT_CUDA(cudaStreamSynchronize(m_stream));
     if (flags) {
         MRT_CUDA(cudaMemsetAsync(m_flags.ptr, 0, sizeof(uint32_t), m_stream));
-        log(LogLevel::Warn, "traversal stack limit reached in at least one ray (flags " + std::to_string(flags) +
-                                "); affected rays may miss geometry");
+        log(LogLevel::Warn, std::string("traversal problem in at least one ray (flags ") + std::to_string(flags) +
+                                "): " + ((flags & 1u) ? "stack or visit budget exhausted " : "") +
+                                ((flags & 2u) ? "out-of-range scene index " : "") + "- affected rays may miss geometry");
     }
     return MRT_SUCCESS;
 }

@@ -105,7 +105,7 @@ private:
     };
     std::map<uint32_t, Blas> m_blas;
     std::map<uint32_t, uint32_t> m_materialIndex;
-    uint32_t m_nodeCount = 0, m_blasNodeCount = 0, m_triCount = 0;
+    uint32_t m_nodeCount = 0, m_blasNodeCount = 0, m_triCount = 0, m_materialCount = 1;
     uint32_t m_tlasRoot = 0, m_instanceCount = 0, m_lightCount = 0;
     uint32_t m_envW = 0, m_envH = 0;
     float m_envIntegralHost = 1.0f;

@@ -154,8 +154,21 @@ void Scene::copyMesh(const mrtMeshDesc& d, MeshData& out) {
     out.blasDirty = true;
 }
 
+namespace {
+// A descriptor the store can hold: positions and indices present, whole
+// triangles, every index inside the vertex array. The reference does not
+// check the last condition (an out-of-range index reads outside the vertex
+// buffer there); here such a mesh is rejected instead.
+bool meshDescUsable(const mrtMeshDesc& d) {
+    if (!d.positions || !d.indices || d.indexCount % 3 != 0) return false;
+    for (uint32_t i = 0; i < d.indexCount; ++i)
+        if (d.indices[i] >= d.vertexCount) return false;
+    return true;
+}
+}  // namespace
+
 uint32_t Scene::addMesh(const mrtMeshDesc& d) {
-    if (!d.positions || !d.indices || d.indexCount % 3 != 0) return MRT_INVALID_ID;
+    if (!meshDescUsable(d)) return MRT_INVALID_ID;
     const uint32_t id = m_nextId++;
     copyMesh(d, m_meshes[id]);
     markDirty(DirtyGeometry);
@@ -165,10 +178,9 @@ uint32_t Scene::addMesh(const mrtMeshDesc& d) {
 void Scene::updateMesh(uint32_t id, const mrtMeshDesc& d) {
     auto it = m_meshes.find(id);
     if (it == m_meshes.end()) return;
-    // The reference accepts any descriptor here; a descriptor that could not
-    // be added (no positions/indices or a ragged index count) is ignored so
-    // the store never holds a mesh the packer cannot read.
-    if (!d.positions || !d.indices || d.indexCount % 3 != 0) return;
+    // A descriptor that could not be added is ignored, so the store never
+    // holds a mesh the packer cannot read.
+    if (!meshDescUsable(d)) return;
     copyMesh(d, it->second);
     markDirty(DirtyGeometry);
 }
