@@ -225,7 +225,8 @@ def ours_arm(args):
     W, H, spp = scene.settings["width"], scene.settings["height"], scene.spp
     paths_per_step = W * H * spp
 
-    mrt.build.build()
+    from miniraytrace_b200 import build as mrt_build
+    mrt_build.build()
     eng = mrt.Engine(W, H, gpu_index1=local + 1)
     ids = scene.apply(eng)
     commit = eng.commit()

@@ -124,6 +124,57 @@ MRT_DEV bool hitTriangle(const float4* __restrict__ tv, uint32_t tri, float3 o, 
     return true;
 }
 
+// Round-to-nearest vector helpers with no fused multiply-add: they evaluate
+// exactly the IEEE single-precision operation sequence of the reference
+// shader expressions they restate.
+MRT_DEV float3 sub_rn(float3 a, float3 b) { return f3(__fsub_rn(a.x, b.x), __fsub_rn(a.y, b.y), __fsub_rn(a.z, b.z)); }
+MRT_DEV float dot_rn(float3 a, float3 b) {
+    return __fadd_rn(__fadd_rn(__fmul_rn(a.x, b.x), __fmul_rn(a.y, b.y)), __fmul_rn(a.z, b.z));
+}
+MRT_DEV float3 cross_rn(float3 a, float3 b) {
+    return f3(__fsub_rn(__fmul_rn(a.y, b.z), __fmul_rn(b.y, a.z)), __fsub_rn(__fmul_rn(a.z, b.x), __fmul_rn(b.z, a.x)),
+              __fsub_rn(__fmul_rn(a.x, b.y), __fmul_rn(b.x, a.y)));
+}
+// Row-major 3x4 transform with the column-by-column sum order of a GLSL
+// mat4 * vec4 product.
+MRT_DEV float3 xformPoint_rn(const float* m, float3 p) {
+    return f3(__fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(m[0], p.x), __fmul_rn(m[1], p.y)), __fmul_rn(m[2], p.z)), m[3]),
+              __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(m[4], p.x), __fmul_rn(m[5], p.y)), __fmul_rn(m[6], p.z)), m[7]),
+              __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(m[8], p.x), __fmul_rn(m[9], p.y)), __fmul_rn(m[10], p.z)), m[11]));
+}
+MRT_DEV float3 xformDir_rn(const float* m, float3 d) {
+    return f3(__fadd_rn(__fadd_rn(__fmul_rn(m[0], d.x), __fmul_rn(m[1], d.y)), __fmul_rn(m[2], d.z)),
+              __fadd_rn(__fadd_rn(__fmul_rn(m[4], d.x), __fmul_rn(m[5], d.y)), __fmul_rn(m[6], d.z)),
+              __fadd_rn(__fadd_rn(__fmul_rn(m[8], d.x), __fmul_rn(m[9], d.y)), __fmul_rn(m[10], d.z)));
+}
+
+// Re-evaluates the winning triangle with the reference's Moeller-Trumbore
+// arithmetic (intersect.glsl:21-45) to report its t and barycentrics: the
+// watertight test decides *which* triangle is hit, the reference formula
+// gives the hit parameters, so hit points match the reference's to the ulp.
+// Keeps the watertight values when the reference formula is degenerate for
+// this ray (|det| < 1e-12 or t outside (1e-4, tMax]).
+MRT_DEV void refineHit(const MrtFrameParams& P, float3 o, float3 d, HitRecord& hit) {
+    const MrtInstance* in = P.instances + hit.inst;
+    const float3 oo = xformPoint_rn(in->w2o, o), dd = xformDir_rn(in->w2o, d);
+    const float3 v0 = f3(ldg4(P.triVerts + 3 * hit.tri));
+    const float3 e1 = sub_rn(f3(ldg4(P.triVerts + 3 * hit.tri + 1)), v0);
+    const float3 e2 = sub_rn(f3(ldg4(P.triVerts + 3 * hit.tri + 2)), v0);
+    const float3 pv = cross_rn(dd, e2);
+    const float det = dot_rn(e1, pv);
+    if (!(fabsf(det) >= 1e-12f)) return;
+    const float invDet = __fdiv_rn(1.0f, det);
+    const float3 sv = sub_rn(oo, v0);
+    const float u = __fmul_rn(dot_rn(sv, pv), invDet);
+    const float3 q = cross_rn(sv, e1);
+    const float v = __fmul_rn(dot_rn(dd, q), invDet);
+    const float t = __fmul_rn(dot_rn(e2, q), invDet);
+    if (!(t > MRT_EPS_RAY) || !(t <= hit.t * 1.0001f)) return;
+    hit.t = t;
+    hit.u = u;
+    hit.v = v;
+}
+
 // Per-thread traffic counters for the roofline's algorithmic bytes: node
 // records fetched (32 B each) and triangle tests (48 B each).
 // `bad` records an out-of-range index met during traversal: the access is
@@ -268,7 +319,10 @@ MRT_DEV bool traceClosest(const MrtFrameParams& P, float3 o, float3 d, float tMa
             }
         }
         for (;;) {
-            if (sp == 0) return ok;
+            if (sp == 0) {
+                if (hit.tri != 0xffffffffu) refineHit(P, o, d, hit);
+                return ok;
+            }
             loadNode(P, stack[--sp], na, nb, tc);
             if (slabNode(na, nb, o, inv, tMax) < __int_as_float(0x7f800000)) break;
         }

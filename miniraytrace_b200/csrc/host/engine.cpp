@@ -69,25 +69,26 @@ void cross3(const float a[3], const float b[3], float r[3]) {
     r[2] = a[0] * b[1] - b[0] * a[1];
 }
 
-// Inverse of a row-major affine 3x4 [R | t], computed in double and rounded.
+// Inverse of a row-major affine 3x4 [R | t] in single precision: with the
+// columns c0, c1, c2 of R, the rows of R^-1 are (c1 x c2, c2 x c0, c0 x c1) /
+// det, det = c0 . (c1 x c2), and the translation becomes -R^-1 t. (The
+// reference inverts with glm::inverse, Renderer.cpp:475; both are exact for
+// identity and translate/scale-by-power-of-two transforms.)
 void invertAffine(const float m[12], float out[12]) {
-    const double a = m[0], b = m[1], c = m[2], d = m[4], e = m[5], f = m[6], g = m[8], h = m[9], i = m[10];
-    const double A = e * i - f * h, B = -(d * i - f * g), C = d * h - e * g;
-    const double det = a * A + b * B + c * C;
-    const double inv = det != 0.0 ? 1.0 / det : 0.0;
-    const double r[9] = {A * inv,
-                         -(b * i - c * h) * inv,
-                         (b * f - c * e) * inv,
-                         B * inv,
-                         (a * i - c * g) * inv,
-                         -(a * f - c * d) * inv,
-                         C * inv,
-                         -(a * h - b * g) * inv,
-                         (a * e - b * d) * inv};
-    const double t[3] = {m[3], m[7], m[11]};
+    const float c0[3] = {m[0], m[4], m[8]}, c1[3] = {m[1], m[5], m[9]}, c2[3] = {m[2], m[6], m[10]};
+    float r0[3], r1[3], r2[3];
+    cross3(c1, c2, r0);
+    cross3(c2, c0, r1);
+    cross3(c0, c1, r2);
+    const float invDet = 1.0f / (c0[0] * r0[0] + c0[1] * r0[1] + c0[2] * r0[2]);
+    const float* rows[3] = {r0, r1, r2};
+    const float t[3] = {m[3], m[7], m[11]};
     for (int row = 0; row < 3; ++row) {
-        for (int col = 0; col < 3; ++col) out[row * 4 + col] = float(r[row * 3 + col]);
-        out[row * 4 + 3] = float(-(r[row * 3] * t[0] + r[row * 3 + 1] * t[1] + r[row * 3 + 2] * t[2]));
+        const float i0 = rows[row][0] * invDet, i1 = rows[row][1] * invDet, i2 = rows[row][2] * invDet;
+        out[row * 4 + 0] = i0;
+        out[row * 4 + 1] = i1;
+        out[row * 4 + 2] = i2;
+        out[row * 4 + 3] = -(i0 * t[0] + i1 * t[1] + i2 * t[2]);
     }
 }
 

@@ -20,9 +20,15 @@ pytestmark = pytest.mark.gpu
 THREADS = max(1, min(32, os.cpu_count() or 1))
 
 
-def parity_fraction(img, ref, rtol=1e-3, atol=1e-6):
+def parity_fraction(img, ref, rtol=1e-3, atol=1e-6, report=8):
     d = np.abs(img[..., :3].astype(np.float64) - ref[..., :3].astype(np.float64))
     ok = (d <= rtol * np.abs(ref[..., :3]) + atol).all(-1)
+    bad = np.argwhere(~ok)
+    if len(bad) and report:
+        rel = (d / (np.abs(ref[..., :3]) + atol)).max(-1)
+        order = np.argsort(-rel[~ok])[:report]
+        for y, x in bad[order]:
+            print(f"  mismatch at ({x},{y}): gpu={img[y, x, :3]} ref={ref[y, x, :3]} rel={rel[y, x]:.3g}")
     return ok.mean()
 
 
