@@ -54,6 +54,7 @@ def parse_args():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--spp", type=int, default=0, help="samples per pixel per step (0 = the workload's 64)")
     return ap.parse_args()
 
 
@@ -222,6 +223,8 @@ def ours_arm(args):
         torch.cuda.set_device(0)
 
     scene = make_scene(args.config)
+    if args.spp > 0:
+        scene.spp = args.spp
     W, H, spp = scene.settings["width"], scene.settings["height"], scene.spp
     paths_per_step = W * H * spp
 

@@ -32,6 +32,12 @@ NVCC_FLAGS = ARCH + [
     "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
     "-I", str(CSRC), "-I", str(ROOT / "include"),
 ]
+# Per-file extra nvcc flags. The path-tracing translation unit is compiled
+# without multiply-add contraction so its shading arithmetic is the same
+# sequence of IEEE single-precision operations as the CPU evaluation (explicit
+# __fmaf_rn intrinsics still produce fused multiply-adds where wanted).
+NVCC_FILE_FLAGS = {"pathtrace.cu": ["-fmad=false"]}
+
 CXX_FLAGS = [
     "-O2", "-std=c++17", "-fPIC", "-fvisibility=hidden", "-ffp-contract=off",
     "-Wall", "-Wextra", "-Wno-unused-parameter",
@@ -77,7 +83,7 @@ def build(force: bool = False, verbose: bool = False) -> Path:
         obj = BUILD / (src.stem + ".cu.o")
         objs.append(obj)
         if force or _stale(obj, src, hdr):
-            jobs.append([NVCC, *NVCC_FLAGS, "-c", str(src), "-o", str(obj)])
+            jobs.append([NVCC, *NVCC_FLAGS, *NVCC_FILE_FLAGS.get(src.name, []), "-c", str(src), "-o", str(obj)])
     for src in cpp:
         obj = BUILD / (src.stem + ".o")
         objs.append(obj)

@@ -24,12 +24,13 @@ cudaError_t mrtcu_trace_closest(const MrtFrameParams* p, const MrtQueryRay* rays
 cudaError_t mrtcu_trace_any(const MrtFrameParams* p, const MrtQueryRay* rays, uint32_t n, uint32_t* occluded,
                             cudaStream_t stream);
 
-// Environment CDF (reference Renderer.cpp:620-655): texels = w*h float4,
-// sinTheta = h floats (sin((y + 0.5) * pi / h) as evaluated on the host),
-// cdf = w*h + h floats out, rowSums = h doubles of scratch, integral = one
+// Environment CDF (reference Renderer.cpp:620-655), bit-exact with the
+// reference's sequential sums: texels = w*h float4, sinTheta = h floats
+// (sin((y + 0.5) * pi / h) as evaluated on the host), cdf = w*h + h floats
+// out, rowSums = h doubles and rowInv = h floats of scratch, integral = one
 // float out (device memory).
 cudaError_t mrtcu_env_cdf(const float4* texels, const float* sinTheta, uint32_t w, uint32_t h, float* cdf,
-                          double* rowSums, float* integral, cudaStream_t stream);
+                          double* rowSums, float* rowInv, float* integral, cudaStream_t stream);
 
 // RGBA32F readback conversion: out[i] = (sum / count, 1) with the pixel's
 // own sample count; spp == 0 (nothing accumulated since the last reset)

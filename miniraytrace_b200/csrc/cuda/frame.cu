@@ -7,100 +7,82 @@
 
 namespace {
 
-constexpr int kCdfThreads = 512;
+// Environment CDF (reference Renderer.cpp:620-655), bit-exact with the
+// reference's sequential double-precision sums: every row is accumulated
+// left to right by one thread (rows in parallel), the marginal and the
+// integral top to bottom by one thread. The map is streamed through shared
+// memory in 32-row x 128-column tiles so global loads and stores stay
+// coalesced; the dependent double-add chain of one row is the critical path
+// (a few tens of microseconds for a 4096 x 2048 map).
+constexpr int kCdfRows = 32;
+constexpr int kCdfCols = 128;
 
-// Block-wide scan of one double per thread: `exclusive` receives the sum of
-// the values of all lower threads, `total` the sum over the block.
-__device__ void blockScan(double v, double* warpSums, double& exclusive, double& total) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int nw = blockDim.x >> 5;
-    double incl = v;
-    for (int off = 1; off < 32; off <<= 1) {
-        const double n = __shfl_up_sync(0xffffffffu, incl, off);
-        if (lane >= off) incl += n;
-    }
-    double excl = __shfl_up_sync(0xffffffffu, incl, 1);
-    if (lane == 0) excl = 0.0;
-    if (lane == 31) warpSums[warp] = incl;
-    __syncthreads();
-    if (warp == 0) {
-        const double s = lane < nw ? warpSums[lane] : 0.0;
-        double si = s;
-        for (int off = 1; off < 32; off <<= 1) {
-            const double n = __shfl_up_sync(0xffffffffu, si, off);
-            if (lane >= off) si += n;
+__global__ void __launch_bounds__(kCdfCols) envCdfRowsKernel(const float4* __restrict__ texels,
+                                                             const float* __restrict__ sinTheta, uint32_t w,
+                                                             uint32_t h, float* __restrict__ cdf,
+                                                             double* __restrict__ rowSums,
+                                                             float* __restrict__ rowInv) {
+    __shared__ float tile[kCdfRows][kCdfCols + 1];
+    const uint32_t y0 = blockIdx.x * kCdfRows;
+    const uint32_t rows = min(uint32_t(kCdfRows), h - y0);
+    const uint32_t tid = threadIdx.x;
+    double acc = 0.0;  // running row sum, owned by thread tid < rows
+    const double s = tid < rows ? double(sinTheta[y0 + tid]) : 0.0;
+    for (uint32_t c0 = 0; c0 < w; c0 += kCdfCols) {
+        const uint32_t cols = min(uint32_t(kCdfCols), w - c0);
+        for (uint32_t r = 0; r < rows; ++r) {
+            if (tid < cols) {
+                const float4 p = __ldg(texels + size_t(y0 + r) * w + c0 + tid);
+                // float luminance with the reference's operation order
+                tile[r][tid] =
+                    __fadd_rn(__fadd_rn(__fmul_rn(0.2126f, p.x), __fmul_rn(0.7152f, p.y)), __fmul_rn(0.0722f, p.z));
+            }
         }
-        if (lane < nw) warpSums[lane] = si;  // inclusive sums of warp totals
+        __syncthreads();
+        if (tid < rows) {
+            for (uint32_t c = 0; c < cols; ++c) {
+                acc += double(tile[tid][c]) * s;
+                tile[tid][c] = float(acc);
+            }
+        }
+        __syncthreads();
+        for (uint32_t r = 0; r < rows; ++r)
+            if (tid < cols) cdf[size_t(y0 + r) * w + c0 + tid] = tile[r][tid];
+        __syncthreads();
     }
-    __syncthreads();
-    const double before = warp > 0 ? warpSums[warp - 1] : 0.0;
-    exclusive = warp > 0 ? before + excl : excl;
-    total = warpSums[nw - 1];
-    __syncthreads();
+    if (tid < rows) {
+        rowSums[y0 + tid] = acc;
+        rowInv[y0 + tid] = acc > 0.0 ? float(1.0 / acc) : 0.0f;
+    }
 }
 
-// One block per row: lum * sin(theta) in double (the product of two floats is
-// exact in double), inclusive prefix along the row, stored as
-// float(prefix) * float(1 / rowSum) exactly as the reference's two-pass
-// normalisation (Renderer.cpp:632-646). Each thread owns a contiguous run of
-// the row; the row is staged through shared memory so global loads and
-// stores stay coalesced.
-__global__ void __launch_bounds__(kCdfThreads) envCdfRowsKernel(const float4* __restrict__ texels,
-                                                                const float* __restrict__ sinTheta, uint32_t w,
-                                                                float* __restrict__ cdf, double* __restrict__ rowSums) {
-    extern __shared__ float rowLum[];  // w floats
-    __shared__ double warpSums[32];
-    const uint32_t y = blockIdx.x;
-    const float4* row = texels + size_t(y) * w;
-    for (uint32_t x = threadIdx.x; x < w; x += blockDim.x) {
-        const float4 p = __ldg(row + x);
-        // float luminance with the reference's operation order, no contraction
-        rowLum[x] = __fadd_rn(__fadd_rn(__fmul_rn(0.2126f, p.x), __fmul_rn(0.7152f, p.y)), __fmul_rn(0.0722f, p.z));
-    }
-    __syncthreads();
-    const double s = double(sinTheta[y]);
-    const uint32_t per = (w + blockDim.x - 1) / blockDim.x;
-    const uint32_t b = threadIdx.x * per, e = min(w, b + per);
-    double local = 0.0;
-    for (uint32_t x = b; x < e; ++x) local += double(rowLum[x]) * s;
-    double run, rowSum;
-    blockScan(local, warpSums, run, rowSum);
-    // second pass: per-element prefix, written back into shared memory
-    for (uint32_t x = b; x < e; ++x) {
-        run += double(rowLum[x]) * s;
-        rowLum[x] = float(run);
-    }
-    __syncthreads();
-    const float inv = rowSum > 0.0 ? float(1.0 / rowSum) : 0.0f;
-    float* out = cdf + size_t(y) * w;
-    for (uint32_t x = threadIdx.x; x < w; x += blockDim.x) out[x] = __fmul_rn(rowLum[x], inv);
-    if (threadIdx.x == 0) rowSums[y] = rowSum;
+// conditional[x] *= float(1 / rowSum), as the reference's second row pass
+__global__ void envCdfNormalizeKernel(float* __restrict__ cdf, const float* __restrict__ rowInv, uint32_t w,
+                                      uint32_t h) {
+    const size_t n = size_t(w) * h;
+    for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
+        cdf[i] = __fmul_rn(cdf[i], rowInv[i / w]);
 }
 
-// One block: marginal CDF over rows and the integral (Renderer.cpp:642-655).
-__global__ void __launch_bounds__(1024) envCdfMarginalKernel(const double* __restrict__ rowSums, uint32_t w, uint32_t h,
-                                                             float* __restrict__ marginal, float* __restrict__ integral) {
-    __shared__ double warpSums[32];
-    const uint32_t per = (h + blockDim.x - 1) / blockDim.x;
-    const uint32_t b = threadIdx.x * per, e = min(h, b + per);
-    double local = 0.0;
-    for (uint32_t y = b; y < e; ++y) local += rowSums[y];
-    double run, tot;
-    blockScan(local, warpSums, run, tot);
-    for (uint32_t y = b; y < e; ++y) {
-        run += rowSums[y];
-        marginal[y] = tot > 0.0 ? float(run / tot) : 0.0f;
+// Marginal CDF and integral, sequential over rows (Renderer.cpp:642-655).
+__global__ void envCdfMarginalKernel(const double* __restrict__ rowSums, uint32_t w, uint32_t h,
+                                     float* __restrict__ marginal, float* __restrict__ integral) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const float pi = 3.14159265358979323846f;
+    const float dTheta = __fdiv_rn(pi, float(h));
+    const float dPhi = __fdiv_rn(__fmul_rn(2.0f, pi), float(w));
+    double integ = 0.0, total = 0.0;
+    for (uint32_t y = 0; y < h; ++y) {
+        integ = __dadd_rn(integ, __dmul_rn(__dmul_rn(rowSums[y], double(dTheta)), double(dPhi)));
+        total = __dadd_rn(total, rowSums[y]);
     }
-    if (threadIdx.x == 0) {
-        const float pi = 3.14159265358979323846f;
-        const float dTheta = pi / float(h);
-        const float dPhi = __fdiv_rn(__fmul_rn(2.0f, pi), float(w));
-        // integral = sum_y rowSum_y * dTheta * dPhi, evaluated as the total
-        // times the (exactly representable as double) float step product
-        const double integ = tot * double(dTheta) * double(dPhi);
-        const float f = float(integ);
-        *integral = f > 1e-8f ? f : 1e-8f;
+    double run = 0.0;
+    for (uint32_t y = 0; y < h; ++y) {
+        run = __dadd_rn(run, rowSums[y]);
+        marginal[y] = total > 0.0 ? float(__ddiv_rn(run, total)) : 0.0f;
     }
+    const float f = float(integ);
+    *integral = f > 1e-8f ? f : 1e-8f;
 }
 
 // Mean radiance per pixel. The reference divides by the host frame count
@@ -152,16 +134,12 @@ __global__ void addKernel(double* __restrict__ dst, const double* __restrict__ s
 }  // namespace
 
 extern "C" cudaError_t mrtcu_env_cdf(const float4* texels, const float* sinTheta, uint32_t w, uint32_t h, float* cdf,
-                                     double* rowSums, float* integral, cudaStream_t stream) {
+                                     double* rowSums, float* rowInv, float* integral, cudaStream_t stream) {
     if (w == 0 || h == 0) return cudaSuccess;
-    const size_t smem = size_t(w) * sizeof(float);
-    if (smem > 48 * 1024) {
-        const cudaError_t e =
-            cudaFuncSetAttribute(envCdfRowsKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-        if (e != cudaSuccess) return e;
-    }
-    envCdfRowsKernel<<<h, kCdfThreads, smem, stream>>>(texels, sinTheta, w, cdf, rowSums);
-    envCdfMarginalKernel<<<1, 1024, 0, stream>>>(rowSums, w, h, cdf + size_t(w) * h, integral);
+    envCdfRowsKernel<<<(h + kCdfRows - 1) / kCdfRows, kCdfCols, 0, stream>>>(texels, sinTheta, w, h, cdf, rowSums,
+                                                                              rowInv);
+    envCdfNormalizeKernel<<<148 * 4, 256, 0, stream>>>(cdf, rowInv, w, h);
+    envCdfMarginalKernel<<<1, 32, 0, stream>>>(rowSums, w, h, cdf + size_t(w) * h, integral);
     return cudaGetLastError();
 }
 

@@ -1,8 +1,12 @@
 // Shading for sm_100a: pcg4d RNG, texture lookups, the "Disney-lite" BSDF,
 // light sampling and surface reconstruction. Each function restates the
 // reference shader function named beside it with the same operation order.
+// This code is compiled without multiply-add contraction (-fmad=false) and
+// takes sin/cos/atan2/acos from detmath.h, so every sample evaluates the same
+// IEEE single-precision operations as the CPU evaluation of the shaders.
 #pragma once
 
+#include "../common/detmath.h"
 #include "../common/device_types.h"
 #include "vec.cuh"
 
@@ -46,7 +50,11 @@ MRT_DEV void buildOnb(float3 n, float3& t, float3& b) {
 }
 
 // ---- textures: bilinear, LOD 0, REPEAT in u and v -----------------------------------
-MRT_DEV float srgbToLinear(float c) { return c <= 0.04045f ? c / 12.92f : powf((c + 0.055f) / 1.055f, 2.4f); }
+// sRGB decode of an 8-bit channel: c <= 0.04045 ? c / 12.92 :
+// ((c + 0.055) / 1.055)^2.4 with the power taken in double and rounded.
+MRT_DEV float srgbToLinear(float c) {
+    return c <= 0.04045f ? c / 12.92f : float(pow(double((c + 0.055f) / 1.055f), 2.4));
+}
 MRT_DEV float4 texelFetch(const MrtTexture& t, uint32_t x, uint32_t y) {
     const size_t i = size_t(y) * t.width + x;
     if (t.format == MRT_DTEX_RGBA32F) return ldg4(reinterpret_cast<const float4*>(t.texels) + i);
@@ -106,11 +114,11 @@ MRT_DEV float ggxD(float3 h, float alpha) {  // bsdf.glsl:29-34
     const float a2 = alpha * alpha;
     const float c2 = h.z * h.z;
     const float d = c2 * (a2 - 1.0f) + 1.0f;
-    return a2 / fmaxf(MRT_PI * d * d, 1e-12f);
+    return a2 / mmax(MRT_PI * d * d, 1e-12f);
 }
 MRT_DEV float ggxLambda(float3 w, float alpha) {  // bsdf.glsl:36-40
     const float c2 = w.z * w.z;
-    const float t2 = fmaxf(1.0f - c2, 0.0f) / fmaxf(c2, 1e-12f);
+    const float t2 = mmax(1.0f - c2, 0.0f) / mmax(c2, 1e-12f);
     return 0.5f * (sqrtf(1.0f + alpha * alpha * t2) - 1.0f);
 }
 MRT_DEV float ggxG1(float3 w, float alpha) { return 1.0f / (1.0f + ggxLambda(w, alpha)); }
@@ -124,13 +132,13 @@ MRT_DEV float3 sampleGgxVndf(float3 wo, float alpha, float2 u) {  // bsdf.glsl:4
     const float3 T2 = cross(vh, T1);
     const float r = sqrtf(u.x);
     float sphi, cphi;
-    sincosf(MRT_TWO_PI * u.y, &sphi, &cphi);
+    detm::sincos(MRT_TWO_PI * u.y, &sphi, &cphi);
     const float t1 = r * cphi;
     float t2 = r * sphi;
     const float s = 0.5f * (1.0f + vh.z);
-    t2 = (1.0f - s) * sqrtf(fmaxf(1.0f - t1 * t1, 0.0f)) + s * t2;
-    const float3 nh = t1 * T1 + t2 * T2 + sqrtf(fmaxf(1.0f - t1 * t1 - t2 * t2, 0.0f)) * vh;
-    return normalize(f3(alpha * nh.x, alpha * nh.y, fmaxf(nh.z, 1e-6f)));
+    t2 = (1.0f - s) * sqrtf(mmax(1.0f - t1 * t1, 0.0f)) + s * t2;
+    const float3 nh = t1 * T1 + t2 * T2 + sqrtf(mmax(1.0f - t1 * t1 - t2 * t2, 0.0f)) * vh;
+    return normalize(f3(alpha * nh.x, alpha * nh.y, mmax(nh.z, 1e-6f)));
 }
 MRT_DEV float3 fresnelSchlick(float3 f0, float cosTheta) {  // bsdf.glsl:63-67
     const float m = clampf(1.0f - cosTheta, 0.0f, 1.0f);
@@ -165,7 +173,7 @@ MRT_DEV void lobeWeights(const Bsdf& m, float3 wo, float& wDiff, float& wSpec, f
 MRT_DEV void bsdfEval(const Bsdf& m, float3 wo, float3 wi, float3& f, float& pdf) {  // bsdf.glsl:100-144
     f = f3(0.0f);
     pdf = 0.0f;
-    const float alpha = fmaxf(m.roughness * m.roughness, 1e-3f);
+    const float alpha = mmax(m.roughness * m.roughness, 1e-3f);
     float wDiff, wSpec, wTrans;
     lobeWeights(m, wo, wDiff, wSpec, wTrans);
     const float eta = m.entering ? m.ior : 1.0f / m.ior;
@@ -180,8 +188,8 @@ MRT_DEV void bsdfEval(const Bsdf& m, float3 wo, float3 wi, float3& f, float& pdf
         const float g2 = ggxG2(wo, wi, alpha);
         const float3 f0 = mix3(f3(0.04f), m.baseColor, m.metallic);
         const float3 F = fresnelSchlick(f0, dot(wo, h));
-        f += d * g2 * F / fmaxf(4.0f * wo.z * wi.z, 1e-7f);
-        pdf += wSpec * ggxG1(wo, alpha) * d / fmaxf(4.0f * wo.z, 1e-7f);
+        f += d * g2 * F / mmax(4.0f * wo.z * wi.z, 1e-7f);
+        pdf += wSpec * ggxG1(wo, alpha) * d / mmax(4.0f * wo.z, 1e-7f);
     } else if (wTrans > 0.0f) {
         float3 h = normalize(wo + wi * eta);
         if (h.z < 0.0f) h = -h;
@@ -192,11 +200,11 @@ MRT_DEV void bsdfEval(const Bsdf& m, float3 wo, float3 wi, float3& f, float& pdf
             const float d = ggxD(h, alpha);
             const float g2 = ggxG2(wo, f3(wi.x, wi.y, -wi.z), alpha);
             float denom = woH + eta * wiH;
-            denom = fmaxf(denom * denom, 1e-7f);
+            denom = mmax(denom * denom, 1e-7f);
             const float jac = eta * eta * fabsf(wiH) / denom;
-            f += m.baseColor * (1.0f - F) * d * g2 * fabsf(woH) * jac / fmaxf(fabsf(wo.z * wi.z), 1e-7f) *
+            f += m.baseColor * (1.0f - F) * d * g2 * fabsf(woH) * jac / mmax(fabsf(wo.z * wi.z), 1e-7f) *
                  (1.0f - m.metallic) * m.transmission;
-            pdf += wTrans * (1.0f - F) * ggxG1(wo, alpha) * d * fabsf(woH) / fmaxf(wo.z, 1e-7f) * jac;
+            pdf += wTrans * (1.0f - F) * ggxG1(wo, alpha) * d * fabsf(woH) / mmax(wo.z, 1e-7f) * jac;
         }
     }
 }
@@ -208,7 +216,7 @@ struct BsdfSample {
 MRT_DEV BsdfSample bsdfSample(const Bsdf& m, float3 wo, Rng& rng) {  // bsdf.glsl:147-192
     BsdfSample s;
     s.valid = false;
-    const float alpha = fmaxf(m.roughness * m.roughness, 1e-3f);
+    const float alpha = mmax(m.roughness * m.roughness, 1e-3f);
     float wDiff, wSpec, wTrans;
     lobeWeights(m, wo, wDiff, wSpec, wTrans);
     const float eta = m.entering ? m.ior : 1.0f / m.ior;
@@ -218,8 +226,8 @@ MRT_DEV BsdfSample bsdfSample(const Bsdf& m, float3 wo, Rng& rng) {  // bsdf.gls
         const float2 u = rng2(rng);
         const float r = sqrtf(u.x);
         float sphi, cphi;
-        sincosf(MRT_TWO_PI * u.y, &sphi, &cphi);
-        wi = f3(r * cphi, r * sphi, sqrtf(fmaxf(1.0f - u.x, 0.0f)));
+        detm::sincos(MRT_TWO_PI * u.y, &sphi, &cphi);
+        wi = f3(r * cphi, r * sphi, sqrtf(mmax(1.0f - u.x, 0.0f)));
     } else if (pick < wDiff + wSpec) {
         const float3 h = sampleGgxVndf(wo, alpha, rng2(rng));
         wi = reflect(-wo, h);
@@ -250,16 +258,16 @@ MRT_DEV BsdfSample bsdfSample(const Bsdf& m, float3 wo, Rng& rng) {  // bsdf.gls
 
 // ---- lights.glsl --------------------------------------------------------------------
 MRT_DEV float2 dirToEquirect(const MrtFrameParams& P, float3 d) {  // lights.glsl:11-15
-    const float phi = atan2f(d.z, d.x) - P.envRotation;
-    const float theta = acosf(clampf(d.y, -1.0f, 1.0f));
+    const float phi = detm::atan2(d.z, d.x) - P.envRotation;
+    const float theta = detm::acos(clampf(d.y, -1.0f, 1.0f));
     return make_float2(fractf(phi / MRT_TWO_PI + 1.0f), theta / MRT_PI);
 }
 MRT_DEV float3 equirectToDir(const MrtFrameParams& P, float2 uv) {  // lights.glsl:17-22
     const float phi = uv.x * MRT_TWO_PI + P.envRotation;
     const float theta = uv.y * MRT_PI;
     float st, ct, sp, cp;
-    sincosf(theta, &st, &ct);
-    sincosf(phi, &sp, &cp);
+    detm::sincos(theta, &st, &ct);
+    detm::sincos(phi, &sp, &cp);
     return f3(st * cp, ct, st * sp);
 }
 MRT_DEV bool hasEnv(const MrtFrameParams& P) { return (P.flags & MRT_FLAG_HAS_ENV) != 0u; }
@@ -314,22 +322,22 @@ MRT_DEV LightSample sampleOneLight(const MrtFrameParams& P, float3 p, Rng& rng) 
         const float cosMax = l.p0[3];
         const float2 u = rng2(rng);
         const float cosT = mixf(1.0f, cosMax, u.x);
-        const float sinT = sqrtf(fmaxf(1.0f - cosT * cosT, 0.0f));
+        const float sinT = sqrtf(mmax(1.0f - cosT * cosT, 0.0f));
         float sphi, cphi;
-        sincosf(MRT_TWO_PI * u.y, &sphi, &cphi);
+        detm::sincos(MRT_TWO_PI * u.y, &sphi, &cphi);
         float3 t, b;
         const float3 n = f3p(l.p0);
         buildOnb(n, t, b);
         ls.wi = normalize(t * (sinT * cphi) + b * (sinT * sphi) + n * cosT);
         ls.radiance = f3p(l.p1);
-        const float conePdf = 1.0f / (MRT_TWO_PI * fmaxf(1.0f - cosMax, 1e-7f));
+        const float conePdf = 1.0f / (MRT_TWO_PI * mmax(1.0f - cosMax, 1e-7f));
         ls.pdf = conePdf * pickPdf;
         ls.dist = 1e30f;
         ls.delta = true;
         ls.valid = true;
     } else if (l.type == MRT_DLIGHT_POINT) {
         const float3 d = f3p(l.p0) - p;
-        const float d2 = fmaxf(dot(d, d), 1e-8f);
+        const float d2 = mmax(dot(d, d), 1e-8f);
         ls.dist = sqrtf(d2);
         ls.wi = d / ls.dist;
         ls.radiance = f3p(l.p1) / d2;
@@ -340,14 +348,14 @@ MRT_DEV LightSample sampleOneLight(const MrtFrameParams& P, float3 p, Rng& rng) 
         const float2 u = rng2(rng);
         const float3 q = f3p(l.p0) + f3p(l.p1) * u.x + f3p(l.p2) * u.y;
         const float3 d = q - p;
-        const float d2 = fmaxf(dot(d, d), 1e-8f);
+        const float d2 = mmax(dot(d, d), 1e-8f);
         ls.dist = sqrtf(d2);
         ls.wi = d / ls.dist;
         const float3 n = normalize(cross(f3p(l.p1), f3p(l.p2)));
         float cosL = dot(n, -ls.wi);
         if (l.p3[3] > 0.5f) cosL = fabsf(cosL);
         if (cosL < 1e-6f) return ls;
-        const float area = fmaxf(l.p0[3], 1e-8f);
+        const float area = mmax(l.p0[3], 1e-8f);
         ls.radiance = f3p(l.p3);
         ls.pdf = (d2 / (cosL * area)) * pickPdf;
         ls.delta = true;
@@ -358,4 +366,4 @@ MRT_DEV LightSample sampleOneLight(const MrtFrameParams& P, float3 p, Rng& rng) 
 MRT_DEV float envPickPdf(const MrtFrameParams& P) {  // lights.glsl:137-140
     return (hasEnv(P) && P.lightCount > 0) ? 1.0f / float(P.lightCount) : 0.0f;
 }
-MRT_DEV float balanceHeuristic(float a, float b) { return a / fmaxf(a + b, 1e-12f); }  // pathtrace.comp:96-98
+MRT_DEV float balanceHeuristic(float a, float b) { return a / mmax(a + b, 1e-12f); }  // pathtrace.comp:96-98

@@ -32,8 +32,13 @@ MRT_DEV float3 cross(float3 a, float3 b) {
 }
 MRT_DEV float length(float3 v) { return sqrtf(dot(v, v)); }
 MRT_DEV float3 normalize(float3 v) { return v * (1.0f / sqrtf(dot(v, v))); }
-MRT_DEV float maxComp(float3 v) { return fmaxf(v.x, fmaxf(v.y, v.z)); }
-MRT_DEV float clampf(float x, float lo, float hi) { return fminf(fmaxf(x, lo), hi); }
+// GLSL max/min as the shaders' CPU evaluation computes them: max(a, b) =
+// a < b ? b : a and min(a, b) = b < a ? b : a, so signed zeros and NaNs
+// resolve identically on both sides.
+MRT_DEV float mmax(float a, float b) { return a < b ? b : a; }
+MRT_DEV float mmin(float a, float b) { return b < a ? b : a; }
+MRT_DEV float maxComp(float3 v) { return mmax(v.x, mmax(v.y, v.z)); }
+MRT_DEV float clampf(float x, float lo, float hi) { return mmin(mmax(x, lo), hi); }
 MRT_DEV float mixf(float x, float y, float a) { return x * (1.0f - a) + y * a; }
 MRT_DEV float3 mix3(float3 x, float3 y, float a) { return x * (1.0f - a) + y * a; }
 MRT_DEV float fractf(float x) { return x - floorf(x); }

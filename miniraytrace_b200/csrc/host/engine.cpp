@@ -605,11 +605,12 @@ mrtResult Engine::runEnvCdf(const float* rgba, uint32_t w, uint32_t h, float& in
     for (uint32_t y = 0; y < h; ++y) sinTheta[y] = std::sin((float(y) + 0.5f) * dTheta);
     MRT_TRY(up(m_envSin, sinTheta.data(), h * sizeof(float)));
     MRT_TRY(m_envCdf.ensure((size_t(w) * h + h) * sizeof(float)));
-    MRT_TRY(m_envRowSums.ensure(size_t(h) * sizeof(double)));
+    MRT_TRY(m_envRowSums.ensure(size_t(h) * (sizeof(double) + sizeof(float))));
     MRT_TRY(m_envIntegral.ensure(16));
     MRT_CUDA(cudaEventRecord(m_ev0, m_stream));
     MRT_CUDA(mrtcu_env_cdf(m_envTexels.as<float4>(), m_envSin.as<float>(), w, h, m_envCdf.as<float>(),
-                           m_envRowSums.as<double>(), m_envIntegral.as<float>(), m_stream));
+                           m_envRowSums.as<double>(), reinterpret_cast<float*>(m_envRowSums.as<double>() + h),
+                           m_envIntegral.as<float>(), m_stream));
     MRT_CUDA(cudaEventRecord(m_ev1, m_stream));
     MRT_CUDA(cudaMemcpyAsync(&integral, m_envIntegral.ptr, sizeof(float), cudaMemcpyDeviceToHost, m_stream));
     MRT_CUDA(cudaStreamSynchronize(m_stream));

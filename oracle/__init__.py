@@ -51,6 +51,7 @@ def load():
             "orc_commit": (u32, [vp]),
             "orc_render_f32": (i32, [vp, vp, u32, u32, u32, vp, i32]),
             "orc_render_f64": (i32, [vp, vp, u32, u32, u32, vp, i32]),
+            "orc_render_f32_sum64": (i32, [vp, vp, u32, u32, u32, vp, i32]),
             "orc_trace": (i32, [vp, vp, u32, vp, i32]), "orc_trace_shadow": (i32, [vp, vp, u32, vp, i32]),
             "orc_trace_bruteforce": (i32, [vp, vp, u32, vp, vp, vp, i32]),
             "orc_bvh_build": (u32, [vp, u32, u32, vp, vp]), "orc_env_cdf": (f32, [vp, u32, u32, vp]),
@@ -209,6 +210,18 @@ class OracleScene:
         if rc:
             raise RuntimeError("oracle not committed")
         return a
+
+    def render_f32_sum64(self, frame0, nframes, pixels=None, threads=8, sums=None):
+        """FP32 paths summed in double in sample order (the GPU's accumulation);
+        returns (npix, 3) float64 sums."""
+        pix = None if pixels is None else np.ascontiguousarray(np.asarray(pixels, np.uint32))
+        n = self.width * self.height if pix is None else pix.size
+        s = sums if sums is not None else np.zeros((n, 3), np.float64)
+        rc = self.lib.orc_render_f32_sum64(self.h, _p(pix), 0 if pix is None else pix.size, frame0, nframes, _p(s),
+                                           threads)
+        if rc:
+            raise RuntimeError("oracle not committed")
+        return s
 
     def render_f64(self, frame0, nframes, pixels=None, threads=8, sums=None):
         """FP64 evaluation of the same streams; returns (npix, 3) float64 sums."""

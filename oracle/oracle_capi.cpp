@@ -137,6 +137,30 @@ int orc_render_f32(void* s, const uint32_t* pixels, uint32_t npix, uint32_t fram
     return 0;
 }
 
+// FP32 paths (as orc_render_f32) summed in double in sample order:
+// sums[3*i..] += double(L). This is the accumulation the GPU engine keeps, so
+// its FP64 buffer can be compared bit for bit.
+int orc_render_f32_sum64(void* s, const uint32_t* pixels, uint32_t npix, uint32_t frame0, uint32_t nframes,
+                         double* sums, int threads) {
+    auto* o = static_cast<OracleScene*>(s);
+    if (!o->packed) return -1;
+    const Globals& g = o->globals;
+    const uint32_t total = pixels ? npix : g.width * g.height;
+    Tracer<float> tr{*o->packed, g};
+    parallelFor(total, threads, [&](uint32_t i) {
+        const uint32_t p = pixels ? pixels[i] : i;
+        const uint32_t px = p % g.width, py = p / g.width;
+        double* a = sums + size_t(i) * 3;
+        for (uint32_t f = frame0; f < frame0 + nframes; ++f) {
+            const V3<float> L = tr.tracePath(px, py, f);
+            a[0] += double(L.x);
+            a[1] += double(L.y);
+            a[2] += double(L.z);
+        }
+    });
+    return 0;
+}
+
 // FP64 evaluation of the same sample streams; sums[3*i..] += L for each
 // frame in [frame0, frame0 + nframes). Sample f of the stream uses frame
 // index f * stride + offset when stride > 0.

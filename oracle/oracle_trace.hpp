@@ -19,9 +19,24 @@
 #include <cmath>
 #include <cstdint>
 
+#include "../miniraytrace_b200/csrc/common/detmath.h"
 #include "oracle_scene.hpp"
 
 namespace orc {
+
+// GLSL sin/cos/atan/acos. FP32 mode uses the deterministic implementations
+// of detmath.h (the GLSL builtins' precision is implementation-defined; these
+// are within 1-3 ulp and evaluate identically on CPU and GPU); FP64 mode uses
+// libm.
+inline void msincos(float x, float& s, float& c) { detm::sincos(x, &s, &c); }
+inline void msincos(double x, double& s, double& c) {
+    s = std::sin(x);
+    c = std::cos(x);
+}
+inline float matan2(float y, float x) { return detm::atan2(y, x); }
+inline double matan2(double y, double x) { return std::atan2(y, x); }
+inline float macos(float x) { return detm::acos(x); }
+inline double macos(double x) { return std::acos(x); }
 
 // ---- random.glsl:6-31 -------------------------------------------------------
 struct U4 {
@@ -75,8 +90,10 @@ template <class T> inline void buildOnb(V3<T> n, V3<T>& t, V3<T>& b) {
 }
 
 // ---- textures -----------------------------------------------------------------
+// sRGB decode of an 8-bit channel (the sampler's SRGB format conversion):
+// c <= 0.04045 ? c / 12.92 : ((c + 0.055) / 1.055)^2.4, power in double.
 inline float srgbToLinear(float c) {
-    return c <= 0.04045f ? c / 12.92f : std::pow((c + 0.055f) / 1.055f, 2.4f);
+    return c <= 0.04045f ? c / 12.92f : float(std::pow(double((c + 0.055f) / 1.055f), 2.4));
 }
 inline V4<float> texel(const TextureData& t, int64_t x, int64_t y) {
     const size_t i = size_t(y) * t.w + size_t(x);
@@ -294,8 +311,10 @@ template <class T> struct Tracer {
         const V3<T> T2 = cross(vh, T1);
         const T r = std::sqrt(u.x);
         const T phi = C<T>::TWO_PI * u.y;
-        const T t1 = r * std::cos(phi);
-        T t2 = r * std::sin(phi);
+        T sphi, cphi;
+        msincos(phi, sphi, cphi);
+        const T t1 = r * cphi;
+        T t2 = r * sphi;
         const T s = T(0.5) * (T(1) + vh.z);
         t2 = (T(1) - s) * std::sqrt(mmax(T(1) - t1 * t1, T(0))) + s * t2;
         const V3<T> nh = t1 * T1 + t2 * T2 + std::sqrt(mmax(T(1) - t1 * t1 - t2 * t2, T(0))) * vh;
@@ -318,7 +337,9 @@ template <class T> struct Tracer {
     static V2<T> sampleCosineHemispherePdf(V2<T> u, V3<T>& wi) {  // bsdf.glsl:79-84
         const T r = std::sqrt(u.x);
         const T phi = C<T>::TWO_PI * u.y;
-        wi = V3<T>(r * std::cos(phi), r * std::sin(phi), std::sqrt(mmax(T(1) - u.x, T(0))));
+        T sphi, cphi;
+        msincos(phi, sphi, cphi);
+        wi = V3<T>(r * cphi, r * sphi, std::sqrt(mmax(T(1) - u.x, T(0))));
         return V2<T>(wi.z, wi.z * C<T>::INV_PI);
     }
     static void lobeWeights(const Bsdf& m, V3<T> wo, T& wDiff, T& wSpec, T& wTrans) {  // bsdf.glsl:87-95
@@ -423,15 +444,17 @@ template <class T> struct Tracer {
 
     // ---- lights.glsl -------------------------------------------------------------
     V2<T> dirToEquirect(V3<T> d) const {  // lights.glsl:11-15
-        const T phi = std::atan2(d.z, d.x) - T(g.envRotation);
-        const T theta = std::acos(clampv(d.y, T(-1), T(1)));
+        const T phi = matan2(d.z, d.x) - T(g.envRotation);
+        const T theta = macos(clampv(d.y, T(-1), T(1)));
         return V2<T>(fract(phi / C<T>::TWO_PI + T(1)), theta / C<T>::PI);
     }
     V3<T> equirectToDir(V2<T> uv) const {  // lights.glsl:17-22
         const T phi = uv.x * C<T>::TWO_PI + T(g.envRotation);
         const T theta = uv.y * C<T>::PI;
-        const T st = std::sin(theta);
-        return V3<T>(st * std::cos(phi), std::cos(theta), st * std::sin(phi));
+        T st, ct, sp, cp;
+        msincos(theta, st, ct);
+        msincos(phi, sp, cp);
+        return V3<T>(st * cp, ct, st * sp);
     }
     V3<T> envLookup(V2<T> uv) const {
         const V4<T> c = sampleBilinear<T>(P.env, uv.x, uv.y);
@@ -496,7 +519,9 @@ template <class T> struct Tracer {
             V3<T> t, b;
             const V3<T> n = cv<T>(l.p0);
             buildOnb(n, t, b);
-            ls.wiWorld = normalize(t * (sinT * std::cos(phi)) + b * (sinT * std::sin(phi)) + n * cosT);
+            T sphi, cphi;
+            msincos(phi, sphi, cphi);
+            ls.wiWorld = normalize(t * (sinT * cphi) + b * (sinT * sphi) + n * cosT);
             ls.radiance = cv<T>(l.p1);
             const T conePdf = T(1) / (C<T>::TWO_PI * mmax(T(1) - cosMax, T(1e-7)));
             ls.pdf = conePdf * pickPdf;
