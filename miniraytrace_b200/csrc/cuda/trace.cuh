@@ -11,8 +11,10 @@
 //   - a visited internal node tests both children's boxes (one 64-byte
 //     fetch, the pair is adjacent), descends into the nearer and pushes the
 //     farther, so culling uses the current closest t;
-//   - box exits are widened by 2 ulps-worth (x 1.00000024, Ize 2013) so a
-//     rounding error in the slab test can never cull a real hit;
+//   - box exits are widened by 1 + 2*gamma(3) = 1 + 3 * 2^-23 (Ize 2013) so a
+//     rounding error in the slab test can never cull a real hit (the
+//     reference's exact-comparison slab test occasionally drops a hit or an
+//     occluder whose point lies on its leaf box's face);
 //   - stacks are bounded and an overflow sets an error flag instead of
 //     writing out of bounds.
 #pragma once
@@ -78,7 +80,7 @@ MRT_DEV float slab(const float* lo, const float* hi, float3 o, float3 inv, float
     const float ty0 = (lo[1] - o.y) * inv.y, ty1 = (hi[1] - o.y) * inv.y;
     const float tz0 = (lo[2] - o.z) * inv.z, tz1 = (hi[2] - o.z) * inv.z;
     const float tEnter = fmaxf(fmaxf(fminf(tx0, tx1), fminf(ty0, ty1)), fmaxf(fminf(tz0, tz1), 0.0f));
-    const float tExit = fminf(fminf(fmaxf(tx0, tx1), fmaxf(ty0, ty1)), fminf(fmaxf(tz0, tz1), tMax)) * 1.00000024f;
+    const float tExit = fminf(fminf(fmaxf(tx0, tx1), fmaxf(ty0, ty1)), fminf(fmaxf(tz0, tz1), tMax)) * 1.00000036f;
     return tEnter <= tExit ? tEnter : __int_as_float(0x7f800000);
 }
 

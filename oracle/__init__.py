@@ -57,6 +57,7 @@ def load():
             "orc_bvh_build": (u32, [vp, u32, u32, vp, vp]), "orc_env_cdf": (f32, [vp, u32, u32, vp]),
             "orc_readback_f32": (None, [vp, u32, u32, vp]), "orc_resolve_rgba8": (None, [vp, u32, f32, u32, vp]),
             "orc_pcg4d": (None, [vp, u32, vp]), "orc_stats": (None, [vp, vp]),
+            "orc_set_bruteforce": (None, [vp, i32]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(lib, name)
@@ -199,6 +200,12 @@ class OracleScene:
 
     def commit(self):
         return self.lib.orc_commit(self.h)
+
+    def set_bruteforce(self, mode: int):
+        """Diagnostic: closest hits of render_f32_sum64 by testing every
+        triangle (1 = reference Moeller-Trumbore test, 2 = watertight test
+        with the hit reported by the reference formula, 0 = BVH walk)."""
+        self.lib.orc_set_bruteforce(self.h, int(mode))
 
     def render_f32(self, frame0, nframes, pixels=None, threads=8, accum=None):
         """Reference-order FP32 accumulation; returns (npix, 4) float32."""

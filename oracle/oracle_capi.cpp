@@ -21,6 +21,7 @@ struct OracleScene {
     Scene scene;
     std::unique_ptr<Packed> packed;
     Globals globals{};
+    int bruteForce = 0;  // 1: brute force with the reference test, 2: with the watertight test
 };
 
 template <class Fn>
@@ -100,6 +101,10 @@ void orc_set_settings(void* s, const mrtRenderSettings* d) {
     st.tonemap = d->tonemap;
 }
 
+// Diagnostic switch: closest-hit rays of orc_render_f32_sum64 test every
+// triangle instead of walking the BVH.
+void orc_set_bruteforce(void* s, int mode) { static_cast<OracleScene*>(s)->bruteForce = mode; }
+
 // Pack the scene (BVH builds, CDF). Returns the number of BVH nodes.
 uint32_t orc_commit(void* s) {
     auto* o = static_cast<OracleScene*>(s);
@@ -147,6 +152,8 @@ int orc_render_f32_sum64(void* s, const uint32_t* pixels, uint32_t npix, uint32_
     const Globals& g = o->globals;
     const uint32_t total = pixels ? npix : g.width * g.height;
     Tracer<float> tr{*o->packed, g};
+    tr.bruteForce = o->bruteForce != 0;
+    tr.watertight = o->bruteForce == 2;
     parallelFor(total, threads, [&](uint32_t i) {
         const uint32_t p = pixels ? pixels[i] : i;
         const uint32_t px = p % g.width, py = p / g.width;

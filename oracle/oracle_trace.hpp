@@ -144,6 +144,8 @@ template <class T> struct Hit {
 template <class T> struct Tracer {
     const Packed& P;
     const Globals& g;
+    bool bruteForce = false;  // diagnostic: closest hit by testing every triangle
+    bool watertight = false;  // diagnostic: brute force decides with the watertight test
 
     // intersect.glsl:10-18
     T intersectAabb(const BvhNode& n, V3<T> o, V3<T> invDir, T tMax) const {
@@ -209,6 +211,7 @@ template <class T> struct Tracer {
     }
     // intersect.glsl:88-125
     Hit<T> traceRay(const Ray<T>& ray) const {
+        if (bruteForce) return traceBrute(ray);
         Hit<T> hit;
         hit.hit = false;
         hit.t = ray.tMax;
@@ -235,6 +238,85 @@ template <class T> struct Tracer {
         }
         return hit;
     }
+    // Every triangle of every instance, instances and triangles in packed
+    // order, keeping the first strictly closest hit.
+    Hit<T> traceBrute(const Ray<T>& ray) const {
+        Hit<T> hit;
+        hit.hit = false;
+        hit.t = ray.tMax;
+        T tMax = ray.tMax;
+        for (uint32_t ii = 0; ii < P.instances.size(); ++ii) {
+            const GpuInstance& in = P.instances[ii];
+            const V3<T> oObj = wToO(in, ray.origin, true), dObj = wToO(in, ray.dir, false);
+            // the BLAS covers a contiguous triangle range: walk its leaves
+            uint32_t stack[64];
+            int sp = 0;
+            stack[sp++] = in.blasRoot;
+            while (sp > 0) {
+                const BvhNode& n = P.nodes[stack[--sp]];
+                const uint32_t count = n.packed >> 2;
+                if (count == 0) {
+                    stack[sp++] = n.leftOrPrim;
+                    stack[sp++] = n.leftOrPrim + 1;
+                    continue;
+                }
+                for (uint32_t i = 0; i < count; ++i) {
+                    V2<T> b;
+                    const T t = watertight ? intersectWatertight(n.leftOrPrim + i, oObj, dObj, tMax, b)
+                                           : intersectTriangle(n.leftOrPrim + i, oObj, dObj, tMax, b);
+                    if (t > T(0)) {
+                        tMax = t;
+                        hit.t = t;
+                        hit.tri = n.leftOrPrim + i;
+                        hit.inst = ii;
+                        hit.bary = b;
+                        hit.hit = true;
+                    }
+                }
+            }
+        }
+        if (watertight && hit.hit) {  // report t/bary with the reference formula
+            const GpuInstance& in = P.instances[hit.inst];
+            V2<T> b;
+            const T t = intersectTriangle(hit.tri, wToO(in, ray.origin, true), wToO(in, ray.dir, false),
+                                          hit.t * T(1.0001), b);
+            if (t > T(0)) {
+                hit.t = t;
+                hit.bary = b;
+            }
+        }
+        return hit;
+    }
+    // Woop, Benthin and Wald 2013 watertight test (diagnostic twin of the
+    // GPU kernel's decision), t in (1e-4, tMax).
+    T intersectWatertight(uint32_t tri, V3<T> o, V3<T> d, T tMax, V2<T>& bary) const {
+        const uint32_t* tr = &P.tris[size_t(tri) * 4];
+        const V3<T> A = cv<T>(P.positions[tr[0]]) - o, B = cv<T>(P.positions[tr[1]]) - o,
+                    Cc = cv<T>(P.positions[tr[2]]) - o;
+        const T ax = std::fabs(d.x), ay = std::fabs(d.y), az = std::fabs(d.z);
+        int kz = (ax > ay) ? (ax > az ? 0 : 2) : (ay > az ? 1 : 2);
+        int kx = kz == 2 ? 0 : kz + 1, ky = kx == 2 ? 0 : kx + 1;
+        if (d[kz] < T(0)) std::swap(kx, ky);
+        const T sx = d[kx] / d[kz], sy = d[ky] / d[kz], sz = T(1) / d[kz];
+        const T Ax = A[kx] - sx * A[kz], Ay = A[ky] - sy * A[kz];
+        const T Bx = B[kx] - sx * B[kz], By = B[ky] - sy * B[kz];
+        const T Cx = Cc[kx] - sx * Cc[kz], Cy = Cc[ky] - sy * Cc[kz];
+        T U = Cx * By - Cy * Bx, V = Ax * Cy - Ay * Cx, W = Bx * Ay - By * Ax;
+        if (U == T(0) || V == T(0) || W == T(0)) {
+            U = T(double(Cx) * double(By) - double(Cy) * double(Bx));
+            V = T(double(Ax) * double(Cy) - double(Ay) * double(Cx));
+            W = T(double(Bx) * double(Ay) - double(By) * double(Ax));
+        }
+        if ((U < T(0) || V < T(0) || W < T(0)) && (U > T(0) || V > T(0) || W > T(0))) return T(-1);
+        const T det = U + V + W;
+        if (det == T(0)) return T(-1);
+        const T Tt = U * (sz * A[kz]) + V * (sz * B[kz]) + W * (sz * Cc[kz]);
+        const T rcp = T(1) / det;
+        const T t = Tt * rcp;
+        if (!(t > C<T>::EPS_RAY && t < tMax)) return T(-1);
+        bary = V2<T>(V * rcp, W * rcp);
+        return t;
+    }
     V3<T> wToO(const GpuInstance& in, V3<T> v, bool point) const {
         const auto& m = in.worldToObject.m;
         V3<T> r(T(m[0][0]) * v.x + T(m[1][0]) * v.y + T(m[2][0]) * v.z,
@@ -245,6 +327,7 @@ template <class T> struct Tracer {
     }
     // intersect.glsl:128-178
     bool traceShadowRay(const Ray<T>& ray) const {
+        if (bruteForce) return traceBrute(ray).hit;
         const T tMax = ray.tMax;
         const V3<T> invDir = V3<T>(T(1)) / ray.dir;
         uint32_t stack[64];
