@@ -124,6 +124,28 @@ typedef struct MrtFrameParams {
     unsigned long long* rayCounters;  // [closest, shadow], NULL = not counted
 } MrtFrameParams;
 
+// Wavefront path state (structure of arrays, one slot per path in flight).
+// A wave renders `spp` samples of every pixel: slot = s * pixels + pixel.
+// Each bounce runs extend (closest hit of the queued rays), shade (surface,
+// NEE sample, BSDF sample, Russian roulette; appends the continuing paths to
+// the other queue and the shadow rays to the shadow queue) and shadow
+// (any-hit; adds the NEE contribution of unoccluded rays).
+typedef struct MrtWaveState {
+    float4* rayO;       // origin.xyz, w = pdf of the BSDF sample that made the ray
+    float4* rayD;       // direction.xyz, w = bits(bounce)
+    float4* beta;       // throughput.xyz, w = bits(RNG counter)
+    float4* L;          // radiance.xyz
+    float4* hit;        // t, u, v, bits(triangle slot; 0xffffffff = miss)
+    uint32_t* hitInst;  // instance slot of the hit
+    uint32_t* queue[2]; // active slot lists, alternating per bounce
+    float4* shO;        // shadow ray origin.xyz, w = tMax
+    float4* shD;        // shadow ray direction.xyz, w = bits(slot)
+    float4* shC;        // contribution added when the shadow ray is unoccluded
+    uint32_t* counts;   // [0], [1] = queue lengths, [2] = shadow queue length
+    uint32_t capacity;  // slots
+    uint32_t pad;
+} MrtWaveState;
+
 // One query ray of mrtxTraceRays (same layout as mrtxRay) and its hit.
 typedef struct MrtQueryRay {
     float origin[3];

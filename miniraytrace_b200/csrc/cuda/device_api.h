@@ -13,10 +13,12 @@
 extern "C" {
 #endif
 
-// Path tracing: samples [sampleBase, sampleBase + sampleCount) of every pixel;
-// sampleBase == 0 overwrites the accumulation, otherwise it adds.
-cudaError_t mrtcu_pathtrace(const MrtFrameParams* p, uint32_t sampleBase, uint32_t sampleCount,
-                            cudaStream_t stream);
+// One wave of the wavefront path tracer: samples [sampleBase, sampleBase +
+// samples) of every pixel (width * height * samples <= s->capacity slots);
+// sampleBase == 0 overwrites the accumulation, otherwise it adds. Adds the
+// number of kernels launched to *launches.
+cudaError_t mrtcu_wave(const MrtFrameParams* p, const MrtWaveState* s, uint32_t sampleBase, uint32_t samples,
+                       uint32_t* launches, cudaStream_t stream);
 
 // Trace queries (closest hit / any hit) for n device-resident rays.
 cudaError_t mrtcu_trace_closest(const MrtFrameParams* p, const MrtQueryRay* rays, uint32_t n, MrtQueryHit* hits,

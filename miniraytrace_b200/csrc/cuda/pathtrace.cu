@@ -1,12 +1,16 @@
 // Progressive path tracing on sm_100a, plus the trace-query kernels.
 //
-// pathtraceKernel restates reference core/shaders/pathtrace.comp:100-233 (one
+// The path tracer restates reference core/shaders/pathtrace.comp:100-233 (one
 // path per pixel per sample, NEE + MIS against the environment, Russian
-// roulette from bounce 3, firefly clamp, NaN guard), with these B200 choices:
-//   - a launch renders `sampleCount` consecutive samples per pixel and keeps
-//     the running sum in registers, so the FP64 accumulation buffer is read
-//     and written once per launch, not once per sample;
-//   - accumulation is FP64 (double4 per pixel: r, g, b, count);
+// roulette from bounce 3, firefly clamp, NaN guard) as a wavefront: a wave
+// holds `samples` paths of every pixel in slot arrays in HBM, and each bounce
+// runs three kernels over compacted queues (extend: closest hit; shade:
+// surface, NEE, BSDF, roulette; shadow: any hit), so a warp always works on
+// 32 live paths of one stage instead of idling on finished ones. Per path the
+// arithmetic and the order of random draws are exactly the reference's.
+// Other B200 choices:
+//   - accumulation is FP64 (double4 per pixel: r, g, b, count), the wave's
+//     samples summed per pixel in sample order;
 //   - traversal is the watertight two-level walk of trace.cuh;
 //   - the first-hit AOV buffers of the reference are not produced (they only
 //     feed an optional OIDN denoiser and are not readable through the ABI).
@@ -86,15 +90,54 @@ MRT_DEV Bsdf makeBsdf(const MrtFrameParams& P, const Surface& s) {
     return b;
 }
 
-struct PathCounters {
-    uint32_t closest, shadow, hits;
-    TraversalCounters tc;
-    bool ok;
+// Adds v[0..4] (closest rays, shadow rays, node records fetched, triangle
+// tests, surface hits) to ctr, one atomic per warp and counter.
+MRT_DEV void warpAddCounters(unsigned long long* ctr, const uint32_t (&c)[5]) {
+    if (ctr == nullptr) return;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+        unsigned long long v = c[k];
+        for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+        if ((threadIdx.x & 31) == 0 && v) atomicAdd(ctr + k, v);
+    }
+}
+
+// Warp-aggregated queue append: every lane of the warp must call it; lanes
+// with pred get consecutive indices from one atomicAdd on *count.
+MRT_DEV uint32_t warpAppend(uint32_t* count, bool pred) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t mask = __ballot_sync(0xffffffffu, pred);
+    if (mask == 0) return 0xffffffffu;
+    const int leader = __ffs(mask) - 1;
+    uint32_t base = 0;
+    if (int(lane) == leader) base = atomicAdd(count, uint32_t(__popc(mask)));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    return pred ? base + uint32_t(__popc(mask & ((1u << lane) - 1u))) : 0xffffffffu;
+}
+
+struct WaveArgs {
+    uint32_t pixels;      // W * H
+    uint32_t slots;       // pixels * samples of this wave
+    uint32_t sampleBase;  // sample index (since reset) of the wave's first sample
+    uint32_t samples;     // samples per pixel in this wave
 };
 
-// One path (pathtrace.comp:100-225): returns the clamped, NaN-guarded radiance.
-MRT_DEV float3 tracePath(const MrtFrameParams& P, uint32_t px, uint32_t py, uint32_t frame, PathCounters& pc) {
-    Rng rng{px, py, frame, 0u};
+MRT_DEV uint32_t frameOf(const MrtFrameParams& P, const WaveArgs& A, uint32_t slot) {
+    return P.streamOffset + (A.sampleBase + slot / A.pixels) * P.streamStride;
+}
+
+// Camera rays of every slot of the wave (pathtrace.comp:101-130).
+__global__ void __launch_bounds__(256) waveInitKernel(MrtFrameParams P, MrtWaveState S, WaveArgs A) {
+    const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot == 0) {
+        S.counts[0] = A.slots;
+        S.counts[1] = 0;
+        S.counts[2] = 0;
+    }
+    if (slot >= A.slots) return;
+    const uint32_t pixel = slot % A.pixels;
+    const uint32_t px = pixel % P.width, py = pixel / P.width;
+    Rng rng{px, py, frameOf(P, A, slot), 0u};
     const float2 jitter = rng2(rng);
     const float u = (float(px) + jitter.x) / float(P.width);
     const float v = (float(py) + jitter.y) / float(P.height);
@@ -108,118 +151,209 @@ MRT_DEV float3 tracePath(const MrtFrameParams& P, uint32_t px, uint32_t py, uint
         ro = f3p(P.camPos);
         rd = normalize(f3p(P.camForward) + sx * f3p(P.camRight) + sy * f3p(P.camUp));
     }
-    float3 L = f3(0.0f), beta = f3(1.0f);
-    float prevBsdfPdf = 0.0f;
-    for (uint32_t bounce = 0; bounce <= P.maxBounces; ++bounce) {
-        HitRecord hit;
-        pc.closest++;
-        pc.ok &= traceClosest(P, ro, rd, 1e30f, hit, pc.tc);
-        if (hit.tri == 0xffffffffu) {
-            const float3 env = envRadiance(P, rd);
-            if (maxComp(env) > 0.0f) {
-                float w = 1.0f;
-                if (bounce > 0u) w = balanceHeuristic(prevBsdfPdf, envPdf(P, rd) * envPickPdf(P));
-                L += beta * env * w;
-            }
-            break;
-        }
-        pc.hits++;
-        const Surface s = makeSurface(P, rd, hit);
-        const MrtMaterial& mat = P.materials[s.mat];
-        const float opacity = mat.baseColorOpacity[3];
-        if (opacity < 1.0f && rng1(rng) >= opacity) {  // stochastic alpha pass-through
-            ro = s.pos + rd * MRT_EPS_RAY;
-            continue;
-        }
-        float3 emission = f3p(mat.emissionRoughness);
-        if (mat.tex[4] >= 0) emission = emission * texRgb(P, mat.tex[4], s.uv);
-        if (maxComp(emission) > 0.0f && s.frontFace) L += beta * emission;
-        const Bsdf bsdf = makeBsdf(P, s);
-        float3 Tn, Bn;
-        buildOnb(s.nShade, Tn, Bn);
-        const float3 nd = -rd;
-        float3 wo = f3(dot(nd, Tn), dot(nd, Bn), dot(nd, s.nShade));
-        if (wo.z < 1e-6f) wo.z = 1e-6f;
-        wo = normalize(wo);
-        // next-event estimation (pathtrace.comp:180-197)
-        const LightSample ls = sampleOneLight(P, s.pos, rng);
-        if (ls.valid && ls.pdf > 1e-9f) {
-            const float3 wi = f3(dot(ls.wi, Tn), dot(ls.wi, Bn), dot(ls.wi, s.nShade));
-            float3 f;
-            float bsdfPdf;
-            bsdfEval(bsdf, wo, wi, f, bsdfPdf);
-            if (maxComp(f) > 0.0f) {
-                const float3 so = s.pos + s.nGeom * (wi.z > 0.0f ? MRT_EPS_RAY : -MRT_EPS_RAY);
-                pc.shadow++;
-                if (!traceAny(P, so, ls.wi, ls.dist - 2.0f * MRT_EPS_RAY, pc.ok, pc.tc)) {
-                    const float w = ls.delta ? 1.0f : balanceHeuristic(ls.pdf, bsdfPdf);
-                    L += beta * f * fabsf(wi.z) * ls.radiance * w / ls.pdf;
+    S.rayO[slot] = make_float4(ro.x, ro.y, ro.z, 0.0f);
+    S.rayD[slot] = make_float4(rd.x, rd.y, rd.z, __uint_as_float(0u));
+    S.beta[slot] = make_float4(1.0f, 1.0f, 1.0f, __uint_as_float(rng.w));
+    S.L[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    S.queue[0][slot] = slot;
+}
+
+// Closest hit of every queued ray (intersect.glsl:88-125 traceRay).
+__global__ void __launch_bounds__(128) waveExtendKernel(MrtFrameParams P, MrtWaveState S, uint32_t cur) {
+    const uint32_t* __restrict__ q = S.queue[cur];
+    const uint32_t n = S.counts[cur];
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        S.counts[cur ^ 1u] = 0;  // next queue and shadow queue fill during shade
+        S.counts[2] = 0;
+    }
+    uint32_t c[5] = {0, 0, 0, 0, 0};
+    TraversalCounters tc;
+    bool ok = true;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t slot = q[i];
+        const float4 o = S.rayO[slot], d = S.rayD[slot];
+        HitRecord h;
+        ok &= traceClosest(P, f3(o), f3(d), 1e30f, h, tc);
+        S.hit[slot] = make_float4(h.t, h.u, h.v, __uint_as_float(h.tri));
+        S.hitInst[slot] = h.inst;
+        c[0]++;
+    }
+    if (!ok) atomicOr(P.errorFlags, 1u);
+    if (tc.bad) atomicOr(P.errorFlags, 2u);
+    c[2] = tc.nodes;
+    c[3] = tc.tris;
+    warpAddCounters(P.rayCounters, c);
+}
+
+// Shading of every queued path at its hit (pathtrace.comp:133-216): miss ->
+// environment with MIS; hit -> alpha pass-through, emission, one-light NEE
+// (a shadow ray with its contribution is queued), BSDF sample, Russian
+// roulette, next ray queued. The draws from the path's pcg4d stream happen in
+// the reference's order; the counter lives in beta.w between bounces.
+__global__ void __launch_bounds__(128) waveShadeKernel(MrtFrameParams P, MrtWaveState S, WaveArgs A, uint32_t cur) {
+    const uint32_t* __restrict__ q = S.queue[cur];
+    uint32_t* __restrict__ qn = S.queue[cur ^ 1u];
+    const uint32_t n = S.counts[cur];
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    uint32_t c[5] = {0, 0, 0, 0, 0};
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i - lane < n; i += stride) {
+        const bool valid = i < n;
+        bool cont = false, shadow = false;
+        uint32_t slot = 0;
+        float3 shOrig = f3(0.0f), shDir = f3(0.0f), shContrib = f3(0.0f);
+        float shTMax = 0.0f;
+        if (valid) {
+            slot = q[i];
+            const float4 o4 = S.rayO[slot], d4 = S.rayD[slot], b4 = S.beta[slot], L4 = S.L[slot];
+            const float4 h4 = S.hit[slot];
+            const uint32_t pixel = slot % A.pixels;
+            Rng rng{pixel % P.width, pixel / P.width, frameOf(P, A, slot), __float_as_uint(b4.w)};
+            const uint32_t bounce = __float_as_uint(d4.w);
+            float3 ro = f3(o4), rd = f3(d4), beta = f3(b4), L = f3(L4);
+            float prevBsdfPdf = o4.w;
+            const uint32_t tri = __float_as_uint(h4.w);
+            if (tri == 0xffffffffu) {
+                const float3 env = envRadiance(P, rd);
+                if (maxComp(env) > 0.0f) {
+                    float w = 1.0f;
+                    if (bounce > 0u) w = balanceHeuristic(prevBsdfPdf, envPdf(P, rd) * envPickPdf(P));
+                    L += beta * env * w;
+                }
+            } else {
+                c[4]++;
+                HitRecord hit;
+                hit.t = h4.x;
+                hit.u = h4.y;
+                hit.v = h4.z;
+                hit.tri = tri;
+                hit.inst = S.hitInst[slot];
+                const Surface s = makeSurface(P, rd, hit);
+                const MrtMaterial& mat = P.materials[s.mat];
+                const float opacity = mat.baseColorOpacity[3];
+                if (opacity < 1.0f && rng1(rng) >= opacity) {  // stochastic alpha pass-through
+                    ro = s.pos + rd * MRT_EPS_RAY;
+                    cont = bounce + 1u <= P.maxBounces;
+                } else {
+                    float3 emission = f3p(mat.emissionRoughness);
+                    if (mat.tex[4] >= 0) emission = emission * texRgb(P, mat.tex[4], s.uv);
+                    if (maxComp(emission) > 0.0f && s.frontFace) L += beta * emission;
+                    const Bsdf bsdf = makeBsdf(P, s);
+                    float3 Tn, Bn;
+                    buildOnb(s.nShade, Tn, Bn);
+                    const float3 nd = -rd;
+                    float3 wo = f3(dot(nd, Tn), dot(nd, Bn), dot(nd, s.nShade));
+                    if (wo.z < 1e-6f) wo.z = 1e-6f;
+                    wo = normalize(wo);
+                    const LightSample ls = sampleOneLight(P, s.pos, rng);
+                    if (ls.valid && ls.pdf > 1e-9f) {
+                        const float3 wi = f3(dot(ls.wi, Tn), dot(ls.wi, Bn), dot(ls.wi, s.nShade));
+                        float3 f;
+                        float bsdfPdf;
+                        bsdfEval(bsdf, wo, wi, f, bsdfPdf);
+                        if (maxComp(f) > 0.0f) {
+                            const float w = ls.delta ? 1.0f : balanceHeuristic(ls.pdf, bsdfPdf);
+                            shadow = true;
+                            shOrig = s.pos + s.nGeom * (wi.z > 0.0f ? MRT_EPS_RAY : -MRT_EPS_RAY);
+                            shDir = ls.wi;
+                            shTMax = ls.dist - 2.0f * MRT_EPS_RAY;
+                            shContrib = beta * f * fabsf(wi.z) * ls.radiance * w / ls.pdf;
+                        }
+                    }
+                    const BsdfSample bs = bsdfSample(bsdf, wo, rng);
+                    if (bs.valid) {
+                        const float3 wiWorld = normalize(Tn * bs.wi.x + Bn * bs.wi.y + s.nShade * bs.wi.z);
+                        beta *= bs.f * fabsf(bs.wi.z) / bs.pdf;
+                        prevBsdfPdf = bs.pdf;
+                        bool alive = true;
+                        if (bounce >= 3u) {
+                            const float p = clampf(maxComp(beta), 0.05f, 0.95f);
+                            if (rng1(rng) >= p) alive = false;
+                            else beta /= p;
+                        }
+                        if (alive) {
+                            ro = s.pos + s.nGeom * (bs.wi.z > 0.0f ? MRT_EPS_RAY : -MRT_EPS_RAY);
+                            rd = wiWorld;
+                            cont = bounce + 1u <= P.maxBounces;
+                        }
+                    }
                 }
             }
+            S.L[slot] = make_float4(L.x, L.y, L.z, 0.0f);
+            if (cont) {
+                S.rayO[slot] = make_float4(ro.x, ro.y, ro.z, prevBsdfPdf);
+                S.rayD[slot] = make_float4(rd.x, rd.y, rd.z, __uint_as_float(bounce + 1u));
+                S.beta[slot] = make_float4(beta.x, beta.y, beta.z, __uint_as_float(rng.w));
+            }
         }
-        // BSDF bounce (pathtrace.comp:200-216)
-        const BsdfSample bs = bsdfSample(bsdf, wo, rng);
-        if (!bs.valid) break;
-        const float3 wiWorld = normalize(Tn * bs.wi.x + Bn * bs.wi.y + s.nShade * bs.wi.z);
-        beta *= bs.f * fabsf(bs.wi.z) / bs.pdf;
-        prevBsdfPdf = bs.pdf;
-        if (bounce >= 3u) {
-            const float p = clampf(maxComp(beta), 0.05f, 0.95f);
-            if (rng1(rng) >= p) break;
-            beta /= p;
+        const uint32_t qi = warpAppend(&S.counts[cur ^ 1u], cont);
+        if (cont) qn[qi] = slot;
+        const uint32_t si = warpAppend(&S.counts[2], shadow);
+        if (shadow) {
+            S.shO[si] = make_float4(shOrig.x, shOrig.y, shOrig.z, shTMax);
+            S.shD[si] = make_float4(shDir.x, shDir.y, shDir.z, __uint_as_float(slot));
+            S.shC[si] = make_float4(shContrib.x, shContrib.y, shContrib.z, 0.0f);
         }
-        ro = s.pos + s.nGeom * (bs.wi.z > 0.0f ? MRT_EPS_RAY : -MRT_EPS_RAY);
-        rd = wiWorld;
     }
-    if (P.fireflyClamp > 0.0f) {
-        const float m = maxComp(L);
-        if (m > P.fireflyClamp) L *= P.fireflyClamp / m;
-    }
-    if (isnan(L.x) || isnan(L.y) || isnan(L.z) || isinf(L.x) || isinf(L.y) || isinf(L.z)) L = f3(0.0f);
-    return L;
+    warpAddCounters(P.rayCounters, c);
 }
 
-// Adds the warp's counters to ctr[0..4] = closest rays, shadow rays, node
-// records fetched, triangle tests, surface hits (one atomic per warp).
-MRT_DEV void warpAddCounters(unsigned long long* ctr, const PathCounters& pc) {
-    if (ctr == nullptr) return;
-    unsigned long long v[5] = {pc.closest, pc.shadow, pc.tc.nodes, pc.tc.tris, pc.hits};
-#pragma unroll
-    for (int k = 0; k < 5; ++k) {
-        for (int off = 16; off > 0; off >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], off);
-        if ((threadIdx.x & 31) == 0 && v[k]) atomicAdd(ctr + k, v[k]);
+// Any-hit test of every queued shadow ray; unoccluded rays add their NEE
+// contribution to their path (pathtrace.comp:192-195). A path has at most
+// one shadow ray per bounce, so the update needs no atomics.
+__global__ void __launch_bounds__(128) waveShadowKernel(MrtFrameParams P, MrtWaveState S) {
+    const uint32_t n = S.counts[2];
+    uint32_t c[5] = {0, 0, 0, 0, 0};
+    TraversalCounters tc;
+    bool ok = true;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float4 o = S.shO[i], d = S.shD[i];
+        c[1]++;
+        if (!traceAny(P, f3(o), f3(d), o.w, ok, tc)) {
+            const uint32_t slot = __float_as_uint(d.w);
+            const float4 cc = S.shC[i];
+            float4 L = S.L[slot];
+            L.x = L.x + cc.x;
+            L.y = L.y + cc.y;
+            L.z = L.z + cc.z;
+            S.L[slot] = L;
+        }
     }
+    if (!ok) atomicOr(P.errorFlags, 1u);
+    if (tc.bad) atomicOr(P.errorFlags, 2u);
+    c[2] = tc.nodes;
+    c[3] = tc.tris;
+    warpAddCounters(P.rayCounters, c);
 }
 
-// 128 threads = a 16 x 8 pixel tile; each warp covers 8 x 4 pixels.
-__global__ void __launch_bounds__(128) pathtraceKernel(MrtFrameParams P, uint32_t sampleBase, uint32_t sampleCount) {
-    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const uint32_t px = blockIdx.x * 16 + (warp & 1) * 8 + (lane & 7);
-    const uint32_t py = blockIdx.y * 8 + (warp >> 1) * 4 + (lane >> 3);
-    const bool active = px < P.width && py < P.height;
-    PathCounters pc{0, 0, 0, TraversalCounters{}, true};
-    if (active) {
-        double sx = 0.0, sy = 0.0, sz = 0.0;
-        for (uint32_t s = 0; s < sampleCount; ++s) {
-            const uint32_t frame = P.streamOffset + (sampleBase + s) * P.streamStride;
-            const float3 L = tracePath(P, px, py, frame, pc);
-            sx += double(L.x);
-            sy += double(L.y);
-            sz += double(L.z);
+// Firefly clamp and NaN guard of every finished path (pathtrace.comp:219-225),
+// then the FP64 accumulation: per pixel, the wave's samples are added in
+// sample order (pathtrace.comp:227-228).
+__global__ void __launch_bounds__(256) waveFinalizeKernel(MrtFrameParams P, MrtWaveState S, WaveArgs A) {
+    const uint32_t pixel = blockIdx.x * blockDim.x + threadIdx.x;
+    if (pixel >= A.pixels) return;
+    double sx = 0.0, sy = 0.0, sz = 0.0;
+    for (uint32_t s = 0; s < A.samples; ++s) {
+        const float4 l4 = S.L[s * A.pixels + pixel];
+        float3 L = f3(l4);
+        if (P.fireflyClamp > 0.0f) {
+            const float m = maxComp(L);
+            if (m > P.fireflyClamp) L *= P.fireflyClamp / m;
         }
-        double2* a = reinterpret_cast<double2*>(P.accum + 4 * (size_t(py) * P.width + px));
-        if (sampleBase == 0) {
-            a[0] = make_double2(sx, sy);
-            a[1] = make_double2(sz, double(sampleCount));
-        } else {
-            const double2 a0 = a[0], a1 = a[1];
-            a[0] = make_double2(a0.x + sx, a0.y + sy);
-            a[1] = make_double2(a1.x + sz, a1.y + double(sampleCount));
-        }
-        if (!pc.ok) atomicOr(P.errorFlags, 1u);
-        if (pc.tc.bad) atomicOr(P.errorFlags, 2u);
+        if (isnan(L.x) || isnan(L.y) || isnan(L.z) || isinf(L.x) || isinf(L.y) || isinf(L.z)) L = f3(0.0f);
+        sx += double(L.x);
+        sy += double(L.y);
+        sz += double(L.z);
     }
-    warpAddCounters(P.rayCounters, pc);
+    double2* acc = reinterpret_cast<double2*>(P.accum + 4 * size_t(pixel));
+    if (A.sampleBase == 0) {
+        acc[0] = make_double2(sx, sy);
+        acc[1] = make_double2(sz, double(A.samples));
+    } else {
+        const double2 a0 = acc[0], a1 = acc[1];
+        acc[0] = make_double2(a0.x + sx, a0.y + sy);
+        acc[1] = make_double2(a1.x + sz, a1.y + double(A.samples));
+    }
 }
 
 __global__ void traceClosestKernel(MrtFrameParams P, const MrtQueryRay* __restrict__ rays, uint32_t n,
@@ -265,11 +399,43 @@ __global__ void traceAnyKernel(MrtFrameParams P, const MrtQueryRay* __restrict__
 
 }  // namespace
 
-extern "C" cudaError_t mrtcu_pathtrace(const MrtFrameParams* p, uint32_t sampleBase, uint32_t sampleCount,
-                                       cudaStream_t stream) {
-    if (p->width == 0 || p->height == 0 || sampleCount == 0) return cudaSuccess;
-    const dim3 grid((p->width + 15) / 16, (p->height + 7) / 8);
-    pathtraceKernel<<<grid, 128, 0, stream>>>(*p, sampleBase, sampleCount);
+namespace {
+// Persistent grid for the queue kernels: enough resident blocks to fill every
+// SM, each block striding over the queue.
+int persistentBlocks(const void* kernel, int threads) {
+    int dev = 0, sms = 0, perSm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kernel, threads, 0);
+    return sms * (perSm > 0 ? perSm : 1);
+}
+}  // namespace
+
+extern "C" cudaError_t mrtcu_wave(const MrtFrameParams* p, const MrtWaveState* s, uint32_t sampleBase,
+                                  uint32_t samples, uint32_t* launches, cudaStream_t stream) {
+    const uint32_t pixels = p->width * p->height;
+    if (pixels == 0 || samples == 0) return cudaSuccess;
+    if (uint64_t(pixels) * samples > s->capacity) return cudaErrorInvalidValue;
+    static int gExtend = 0, gShade = 0, gShadow = 0;
+    if (gExtend == 0) {
+        gExtend = persistentBlocks(reinterpret_cast<const void*>(waveExtendKernel), 128);
+        gShade = persistentBlocks(reinterpret_cast<const void*>(waveShadeKernel), 128);
+        gShadow = persistentBlocks(reinterpret_cast<const void*>(waveShadowKernel), 128);
+    }
+    WaveArgs A{pixels, pixels * samples, sampleBase, samples};
+    uint32_t n = 0;
+    waveInitKernel<<<(A.slots + 255) / 256, 256, 0, stream>>>(*p, *s, A);
+    ++n;
+    for (uint32_t b = 0; b <= p->maxBounces; ++b) {
+        const uint32_t cur = b & 1u;
+        waveExtendKernel<<<gExtend, 128, 0, stream>>>(*p, *s, cur);
+        waveShadeKernel<<<gShade, 128, 0, stream>>>(*p, *s, A, cur);
+        waveShadowKernel<<<gShadow, 128, 0, stream>>>(*p, *s);
+        n += 3;
+    }
+    waveFinalizeKernel<<<(pixels + 255) / 256, 256, 0, stream>>>(*p, *s, A);
+    ++n;
+    if (launches) *launches += n;
     return cudaGetLastError();
 }
 

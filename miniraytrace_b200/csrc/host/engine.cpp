@@ -217,7 +217,7 @@ Engine::~Engine() {
     DeviceBuffer* bufs[] = {&m_nodes,     &m_triVerts, &m_triIndex,   &m_normals,      &m_uvs,        &m_tangents,
                             &m_instances, &m_materials, &m_lights,     &m_envTexels,    &m_envCdf,     &m_envSin,
                             &m_envRowSums, &m_envIntegral, &m_texTable, &m_accum,       &m_out32,      &m_out8,
-                            &m_flags,     &m_rayCounters, &m_queryRays, &m_queryOut};
+                            &m_flags,     &m_rayCounters, &m_queryRays, &m_queryOut, &m_wave};
     for (DeviceBuffer* b : bufs) b->release();
     for (auto& t : m_texData) t.release();
     if (m_pinned) cudaFreeHost(m_pinned);
@@ -247,6 +247,45 @@ mrtResult Engine::allocateFrame() {
     MRT_CUDA(cudaMemsetAsync(m_accum.ptr, 0, pixels * 32, m_stream));
     MRT_TRY(m_out32.ensure(pixels * 16));
     MRT_TRY(m_out8.ensure(pixels * 4));
+    m_waveSamples = 0;  // wave slots depend on the frame size
+    return MRT_SUCCESS;
+}
+
+// Wavefront state for waves of up to `samples` samples per pixel, capped so
+// a wave holds at most 2^23 paths (~1.2 GB of state at 140 bytes a path).
+mrtResult Engine::ensureWave(uint32_t samples) {
+    const uint64_t pixels = uint64_t(m_settings.width) * m_settings.height;
+    const uint64_t maxSlots = uint64_t(1) << 23;
+    uint32_t k = uint32_t(std::max<uint64_t>(1, std::min<uint64_t>(samples, maxSlots / std::max<uint64_t>(pixels, 1))));
+    k = std::min<uint32_t>(k, 64);
+    if (m_waveSamples >= k) return MRT_SUCCESS;
+    const uint64_t slots = pixels * k;
+    if (slots > 0xffffffffull) return fail(MRT_ERROR_INVALID_ARGUMENT, "frame too large for one wave");
+    // per slot: rayO, rayD, beta, L, hit (5 x 16 B), hitInst + 2 queues (3 x 4 B),
+    // shadow origin/dir/contribution (3 x 16 B)
+    const size_t bytes = size_t(slots) * (5 * 16 + 3 * 4 + 3 * 16) + 64;
+    MRT_TRY(m_wave.ensure(bytes));
+    char* base = static_cast<char*>(m_wave.ptr);
+    auto carve = [&](size_t n) {
+        char* p = base;
+        base += n;
+        return p;
+    };
+    MrtWaveState& w = m_waveState;
+    w.rayO = reinterpret_cast<float4*>(carve(slots * 16));
+    w.rayD = reinterpret_cast<float4*>(carve(slots * 16));
+    w.beta = reinterpret_cast<float4*>(carve(slots * 16));
+    w.L = reinterpret_cast<float4*>(carve(slots * 16));
+    w.hit = reinterpret_cast<float4*>(carve(slots * 16));
+    w.shO = reinterpret_cast<float4*>(carve(slots * 16));
+    w.shD = reinterpret_cast<float4*>(carve(slots * 16));
+    w.shC = reinterpret_cast<float4*>(carve(slots * 16));
+    w.hitInst = reinterpret_cast<uint32_t*>(carve(slots * 4));
+    w.queue[0] = reinterpret_cast<uint32_t*>(carve(slots * 4));
+    w.queue[1] = reinterpret_cast<uint32_t*>(carve(slots * 4));
+    w.counts = reinterpret_cast<uint32_t*>(carve(64));
+    w.capacity = uint32_t(slots);
+    m_waveSamples = k;
     return MRT_SUCCESS;
 }
 
@@ -753,12 +792,18 @@ mrtResult Engine::renderFrames(uint32_t count, mrtFrameInfo* info) {
     if (m_frameIndex < m_settings.sppLimit) n = std::min(count, m_settings.sppLimit - m_frameIndex);
     m_stats.kernelLaunches = 0;
     if (n > 0) {
+        MRT_TRY(guard(ensureWave(n)));
         MrtFrameParams p;
         fillParams(p);
         MRT_CUDA(cudaMemsetAsync(m_rayCounters.ptr, 0, 64, m_stream));
+        uint32_t launches = 0;
         MRT_CUDA(cudaEventRecord(m_ev0, m_stream));
-        const cudaError_t le = mrtcu_pathtrace(&p, m_frameIndex, n, m_stream);
-        if (le != cudaSuccess) return guard(fromCuda(le, "path tracing launch"));
+        for (uint32_t done = 0; done < n;) {
+            const uint32_t k = std::min(n - done, m_waveSamples);
+            const cudaError_t le = mrtcu_wave(&p, &m_waveState, m_frameIndex + done, k, &launches, m_stream);
+            if (le != cudaSuccess) return guard(fromCuda(le, "path tracing launch"));
+            done += k;
+        }
         MRT_CUDA(cudaEventRecord(m_ev1, m_stream));
         const cudaError_t se = cudaStreamSynchronize(m_stream);
         if (se != cudaSuccess) return guard(fromCuda(se, "path tracing kernel"));
@@ -766,7 +811,7 @@ mrtResult Engine::renderFrames(uint32_t count, mrtFrameInfo* info) {
         MRT_CUDA(cudaEventElapsedTime(&ms, m_ev0, m_ev1));
         m_stats.lastRenderMs = ms;
         m_stats.lastRenderSpp = n;
-        m_stats.kernelLaunches = 1;
+        m_stats.kernelLaunches = launches;
         MRT_TRY(guard(checkErrorFlags()));
         unsigned long long ctr[5];
         MRT_CUDA(cudaMemcpy(ctr, m_rayCounters.ptr, sizeof(ctr), cudaMemcpyDeviceToHost));
@@ -885,7 +930,7 @@ mrtResult Engine::getStats(mrtxStats* out) const {
                                   &m_tangents,  &m_instances, &m_materials,  &m_lights,      &m_envTexels,
                                   &m_envCdf,    &m_envSin,    &m_envRowSums, &m_envIntegral, &m_texTable,
                                   &m_accum,     &m_out32,     &m_out8,       &m_flags,       &m_rayCounters,
-                                  &m_queryRays, &m_queryOut};
+                                  &m_queryRays, &m_queryOut,    &m_wave};
     for (const DeviceBuffer* b : bufs) bytes += b->bytes;
     for (const auto& t : m_texData) bytes += t.bytes;
     s.deviceBytes = bytes;

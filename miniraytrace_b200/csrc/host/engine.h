@@ -62,6 +62,7 @@ private:
     mrtResult checkAlive();
     mrtResult guard(mrtResult r);  // records a device loss
     mrtResult allocateFrame();
+    mrtResult ensureWave(uint32_t samples);
     mrtResult up(DeviceBuffer& b, const void* src, size_t n);
     mrtResult sync(mrtCommitStats* stats);  // reference Renderer::syncScene
     mrtResult packMaterials();
@@ -95,6 +96,9 @@ private:
     std::vector<uint32_t> m_texGeneration;
     // device frame state
     DeviceBuffer m_accum, m_out32, m_out8, m_flags, m_rayCounters, m_queryRays, m_queryOut;
+    DeviceBuffer m_wave;  // wavefront path state (one allocation, carved into MrtWaveState arrays)
+    MrtWaveState m_waveState{};
+    uint32_t m_waveSamples = 0;  // samples per pixel one wave holds
     void* m_pinned = nullptr;
     size_t m_pinnedBytes = 0;
 
