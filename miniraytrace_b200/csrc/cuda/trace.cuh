@@ -199,17 +199,18 @@ MRT_DEV void loadNode(const MrtFrameParams& P, uint32_t i, float4& a, float4& b,
 }
 
 // Closest hit within one BLAS (object-space ray). Updates tMax and hit.
-// Returns false on a stack overflow.
+// Stack entries carry the far child's entry distance, so a popped subtree
+// that starts beyond the current closest hit is skipped without fetching it.
+// Returns false on a stack overflow or an exhausted visit budget.
 MRT_DEV bool closestBlas(const MrtFrameParams& P, uint32_t root, uint32_t inst, float3 o, float3 d, float& tMax,
                          HitRecord& hit, TraversalCounters& tc) {
     const float3 inv = safeInv(d);
     const Shear sh = makeShear(d);
-    uint32_t stack[MRT_BLAS_STACK];
+    uint2 stack[MRT_BLAS_STACK];
     int sp = 0;
     float4 na, nb;
     loadNode(P, root, na, nb, tc);
     if (!(slabNode(na, nb, o, inv, tMax) < __int_as_float(0x7f800000))) return true;
-    uint32_t node = root;
     bool ok = true;
     uint32_t visits = 0;
     for (;;) {
@@ -226,16 +227,13 @@ MRT_DEV bool closestBlas(const MrtFrameParams& P, uint32_t root, uint32_t inst, 
             const bool h0 = t0 < __int_as_float(0x7f800000), h1 = t1 < __int_as_float(0x7f800000);
             if (h0 && h1) {
                 const bool firstNear = t0 <= t1;
-                const uint32_t farNode = firstNear ? first + 1 : first;
-                if (sp < MRT_BLAS_STACK) stack[sp++] = farNode;
+                if (sp < MRT_BLAS_STACK) stack[sp++] = make_uint2(firstNear ? first + 1 : first, __float_as_uint(firstNear ? t1 : t0));
                 else ok = false;
-                node = firstNear ? first : first + 1;
                 na = firstNear ? a0 : a1;
                 nb = firstNear ? b0 : b1;
                 continue;
             }
             if (h0 || h1) {
-                node = h0 ? first : first + 1;
                 na = h0 ? a0 : a1;
                 nb = h0 ? b0 : b1;
                 continue;
@@ -258,12 +256,14 @@ MRT_DEV bool closestBlas(const MrtFrameParams& P, uint32_t root, uint32_t inst, 
                 }
             }
         }
-        // pop, skipping entries the current tMax already culls
+        // pop the nearest pending subtree that can still hold a closer hit
         for (;;) {
             if (sp == 0) return ok;
-            node = stack[--sp];
-            loadNode(P, node, na, nb, tc);
-            if (slabNode(na, nb, o, inv, tMax) < __int_as_float(0x7f800000)) break;
+            const uint2 e = stack[--sp];
+            if (__uint_as_float(e.y) <= tMax * 1.00000036f) {
+                loadNode(P, e.x, na, nb, tc);
+                break;
+            }
         }
     }
 }
@@ -276,7 +276,7 @@ MRT_DEV bool traceClosest(const MrtFrameParams& P, float3 o, float3 d, float tMa
     hit.u = hit.v = 0.0f;
     if (P.instanceCount == 0) return true;  // empty scene (the TLAS root is a placeholder)
     const float3 inv = safeInv(d);
-    uint32_t stack[MRT_TLAS_STACK];
+    uint2 stack[MRT_TLAS_STACK];
     int sp = 0;
     float4 na, nb;
     loadNode(P, P.tlasRoot, na, nb, tc);
@@ -297,7 +297,7 @@ MRT_DEV bool traceClosest(const MrtFrameParams& P, float3 o, float3 d, float tMa
             const bool h0 = t0 < __int_as_float(0x7f800000), h1 = t1 < __int_as_float(0x7f800000);
             if (h0 && h1) {
                 const bool firstNear = t0 <= t1;
-                if (sp < MRT_TLAS_STACK) stack[sp++] = firstNear ? first + 1 : first;
+                if (sp < MRT_TLAS_STACK) stack[sp++] = make_uint2(firstNear ? first + 1 : first, __float_as_uint(firstNear ? t1 : t0));
                 else ok = false;
                 na = firstNear ? a0 : a1;
                 nb = firstNear ? b0 : b1;
@@ -325,8 +325,11 @@ MRT_DEV bool traceClosest(const MrtFrameParams& P, float3 o, float3 d, float tMa
                 if (hit.tri != 0xffffffffu) refineHit(P, o, d, hit);
                 return ok;
             }
-            loadNode(P, stack[--sp], na, nb, tc);
-            if (slabNode(na, nb, o, inv, tMax) < __int_as_float(0x7f800000)) break;
+            const uint2 e = stack[--sp];
+            if (__uint_as_float(e.y) <= tMax * 1.00000036f) {
+                loadNode(P, e.x, na, nb, tc);
+                break;
+            }
         }
     }
 }

@@ -252,10 +252,12 @@ mrtResult Engine::allocateFrame() {
 }
 
 // Wavefront state for waves of up to `samples` samples per pixel, capped so
-// a wave holds at most 2^23 paths (~1.2 GB of state at 140 bytes a path).
+// a wave holds at most 2^25 paths (~4.7 GB of state at 140 bytes a path):
+// large waves amortise the last bounces, whose few long rays run at the
+// latency of one traversal.
 mrtResult Engine::ensureWave(uint32_t samples) {
     const uint64_t pixels = uint64_t(m_settings.width) * m_settings.height;
-    const uint64_t maxSlots = uint64_t(1) << 23;
+    const uint64_t maxSlots = uint64_t(1) << 25;
     uint32_t k = uint32_t(std::max<uint64_t>(1, std::min<uint64_t>(samples, maxSlots / std::max<uint64_t>(pixels, 1))));
     k = std::min<uint32_t>(k, 64);
     if (m_waveSamples >= k) return MRT_SUCCESS;
