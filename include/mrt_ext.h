@@ -75,10 +75,16 @@ typedef struct mrtxStats {
     /* counters of the last render call (all samples of all pixels) */
     uint64_t raysClosest;  /* closest-hit rays traced */
     uint64_t raysShadow;   /* shadow (any-hit) rays traced */
-    uint64_t nodeFetches;  /* 32-byte BVH node records read */
-    uint64_t triTests;     /* ray/triangle tests (48 bytes of vertices each) */
+    uint64_t nodeFetches;  /* BVH node records read by closest-hit rays */
+    uint64_t triTests;     /* ray/triangle tests of closest-hit rays */
     uint64_t surfaceHits;  /* hits shaded (one surface gather each) */
     uint64_t commitH2DBytes; /* bytes copied host-to-device by the last commit */
+    uint64_t shadowNodeFetches; /* BVH node records read by shadow rays */
+    uint64_t shadowTriTests;    /* ray/triangle tests of shadow rays */
+    uint32_t nodeBytes;    /* bytes of one BVH node record */
+    uint32_t triBytes;     /* bytes read by one ray/triangle test */
+    /* device time of the last render call per wavefront stage (CUDA events) */
+    float extendMs, shadeMs, shadowMs, otherMs;
 } mrtxStats;
 MRT_API mrtResult mrtxGetStats(mrtEngine*, mrtxStats* out);
 

@@ -120,7 +120,10 @@ class Stats(_Sized):
                 ("commitTotalMs", C.c_float), ("bvhNodes", C.c_uint32), ("triangles", C.c_uint32),
                 ("instances", C.c_uint32), ("kernelLaunches", C.c_uint32), ("deviceBytes", C.c_uint64),
                 ("raysClosest", C.c_uint64), ("raysShadow", C.c_uint64), ("nodeFetches", C.c_uint64),
-                ("triTests", C.c_uint64), ("surfaceHits", C.c_uint64), ("commitH2DBytes", C.c_uint64)]
+                ("triTests", C.c_uint64), ("surfaceHits", C.c_uint64), ("commitH2DBytes", C.c_uint64),
+                ("shadowNodeFetches", C.c_uint64), ("shadowTriTests", C.c_uint64), ("nodeBytes", C.c_uint32),
+                ("triBytes", C.c_uint32), ("extendMs", C.c_float), ("shadeMs", C.c_float), ("shadowMs", C.c_float),
+                ("otherMs", C.c_float)]
 
 
 LOG_FN = C.CFUNCTYPE(None, C.c_int, C.c_char_p, C.c_void_p)

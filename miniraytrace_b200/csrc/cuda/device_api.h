@@ -16,9 +16,11 @@ extern "C" {
 // One wave of the wavefront path tracer: samples [sampleBase, sampleBase +
 // samples) of every pixel (width * height * samples <= s->capacity slots);
 // sampleBase == 0 overwrites the accumulation, otherwise it adds. Adds the
-// number of kernels launched to *launches.
+// number of kernels launched to *launches. stageEvents (may be NULL) holds 6
+// events per bounce; events 6b..6b+3 are recorded before extend, between
+// extend and shade, between shade and shadow, and after shadow of bounce b.
 cudaError_t mrtcu_wave(const MrtFrameParams* p, const MrtWaveState* s, uint32_t sampleBase, uint32_t samples,
-                       uint32_t* launches, cudaStream_t stream);
+                       uint32_t* launches, const cudaEvent_t* stageEvents, cudaStream_t stream);
 
 // Trace queries (closest hit / any hit) for n device-resident rays.
 cudaError_t mrtcu_trace_closest(const MrtFrameParams* p, const MrtQueryRay* rays, uint32_t n, MrtQueryHit* hits,

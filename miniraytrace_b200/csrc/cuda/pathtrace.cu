@@ -90,12 +90,14 @@ MRT_DEV Bsdf makeBsdf(const MrtFrameParams& P, const Surface& s) {
     return b;
 }
 
-// Adds v[0..4] (closest rays, shadow rays, node records fetched, triangle
-// tests, surface hits) to ctr, one atomic per warp and counter.
-MRT_DEV void warpAddCounters(unsigned long long* ctr, const uint32_t (&c)[5]) {
+// Counter slots: closest rays, shadow rays, closest-hit node records fetched,
+// closest-hit triangle tests, surface hits, shadow node records, shadow
+// triangle tests. Added to ctr with one atomic per warp and counter.
+enum { kCtrClosest, kCtrShadow, kCtrExtNodes, kCtrExtTris, kCtrHits, kCtrShNodes, kCtrShTris, kCtrCount };
+MRT_DEV void warpAddCounters(unsigned long long* ctr, const uint32_t (&c)[kCtrCount]) {
     if (ctr == nullptr) return;
 #pragma unroll
-    for (int k = 0; k < 5; ++k) {
+    for (int k = 0; k < kCtrCount; ++k) {
         unsigned long long v = c[k];
         for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
         if ((threadIdx.x & 31) == 0 && v) atomicAdd(ctr + k, v);
@@ -166,7 +168,7 @@ __global__ void __launch_bounds__(128) waveExtendKernel(MrtFrameParams P, MrtWav
         S.counts[cur ^ 1u] = 0;  // next queue and shadow queue fill during shade
         S.counts[2] = 0;
     }
-    uint32_t c[5] = {0, 0, 0, 0, 0};
+    uint32_t c[kCtrCount] = {};
     TraversalCounters tc;
     bool ok = true;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -176,12 +178,12 @@ __global__ void __launch_bounds__(128) waveExtendKernel(MrtFrameParams P, MrtWav
         ok &= traceClosest(P, f3(o), f3(d), 1e30f, h, tc);
         S.hit[slot] = make_float4(h.t, h.u, h.v, __uint_as_float(h.tri));
         S.hitInst[slot] = h.inst;
-        c[0]++;
+        c[kCtrClosest]++;
     }
     if (!ok) atomicOr(P.errorFlags, 1u);
     if (tc.bad) atomicOr(P.errorFlags, 2u);
-    c[2] = tc.nodes;
-    c[3] = tc.tris;
+    c[kCtrExtNodes] = tc.nodes;
+    c[kCtrExtTris] = tc.tris;
     warpAddCounters(P.rayCounters, c);
 }
 
@@ -196,7 +198,7 @@ __global__ void __launch_bounds__(128) waveShadeKernel(MrtFrameParams P, MrtWave
     const uint32_t n = S.counts[cur];
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t stride = gridDim.x * blockDim.x;
-    uint32_t c[5] = {0, 0, 0, 0, 0};
+    uint32_t c[kCtrCount] = {};
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i - lane < n; i += stride) {
         const bool valid = i < n;
         bool cont = false, shadow = false;
@@ -221,7 +223,7 @@ __global__ void __launch_bounds__(128) waveShadeKernel(MrtFrameParams P, MrtWave
                     L += beta * env * w;
                 }
             } else {
-                c[4]++;
+                c[kCtrHits]++;
                 HitRecord hit;
                 hit.t = h4.x;
                 hit.u = h4.y;
@@ -303,12 +305,12 @@ __global__ void __launch_bounds__(128) waveShadeKernel(MrtFrameParams P, MrtWave
 // one shadow ray per bounce, so the update needs no atomics.
 __global__ void __launch_bounds__(128) waveShadowKernel(MrtFrameParams P, MrtWaveState S) {
     const uint32_t n = S.counts[2];
-    uint32_t c[5] = {0, 0, 0, 0, 0};
+    uint32_t c[kCtrCount] = {};
     TraversalCounters tc;
     bool ok = true;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const float4 o = S.shO[i], d = S.shD[i];
-        c[1]++;
+        c[kCtrShadow]++;
         if (!traceAny(P, f3(o), f3(d), o.w, ok, tc)) {
             const uint32_t slot = __float_as_uint(d.w);
             const float4 cc = S.shC[i];
@@ -321,8 +323,8 @@ __global__ void __launch_bounds__(128) waveShadowKernel(MrtFrameParams P, MrtWav
     }
     if (!ok) atomicOr(P.errorFlags, 1u);
     if (tc.bad) atomicOr(P.errorFlags, 2u);
-    c[2] = tc.nodes;
-    c[3] = tc.tris;
+    c[kCtrShNodes] = tc.nodes;
+    c[kCtrShTris] = tc.tris;
     warpAddCounters(P.rayCounters, c);
 }
 
@@ -412,7 +414,8 @@ int persistentBlocks(const void* kernel, int threads) {
 }  // namespace
 
 extern "C" cudaError_t mrtcu_wave(const MrtFrameParams* p, const MrtWaveState* s, uint32_t sampleBase,
-                                  uint32_t samples, uint32_t* launches, cudaStream_t stream) {
+                                  uint32_t samples, uint32_t* launches, const cudaEvent_t* stageEvents,
+                                  cudaStream_t stream) {
     const uint32_t pixels = p->width * p->height;
     if (pixels == 0 || samples == 0) return cudaSuccess;
     if (uint64_t(pixels) * samples > s->capacity) return cudaErrorInvalidValue;
@@ -428,9 +431,14 @@ extern "C" cudaError_t mrtcu_wave(const MrtFrameParams* p, const MrtWaveState* s
     ++n;
     for (uint32_t b = 0; b <= p->maxBounces; ++b) {
         const uint32_t cur = b & 1u;
+        const cudaEvent_t* ev = stageEvents ? stageEvents + 6 * b : nullptr;
+        if (ev) cudaEventRecord(ev[0], stream);
         waveExtendKernel<<<gExtend, 128, 0, stream>>>(*p, *s, cur);
+        if (ev) cudaEventRecord(ev[1], stream);
         waveShadeKernel<<<gShade, 128, 0, stream>>>(*p, *s, A, cur);
+        if (ev) cudaEventRecord(ev[2], stream);
         waveShadowKernel<<<gShadow, 128, 0, stream>>>(*p, *s);
+        if (ev) cudaEventRecord(ev[3], stream);
         n += 3;
     }
     waveFinalizeKernel<<<(pixels + 255) / 256, 256, 0, stream>>>(*p, *s, A);

@@ -223,6 +223,8 @@ Engine::~Engine() {
     if (m_pinned) cudaFreeHost(m_pinned);
     for (auto& ev : m_copyEvents)
         if (ev) cudaEventDestroy(ev);
+    for (auto& ev : m_stageEvents)
+        if (ev) cudaEventDestroy(ev);
     if (m_ev0) cudaEventDestroy(m_ev0);
     if (m_ev1) cudaEventDestroy(m_ev1);
     if (m_stream) cudaStreamDestroy(m_stream);
@@ -799,10 +801,19 @@ mrtResult Engine::renderFrames(uint32_t count, mrtFrameInfo* info) {
         fillParams(p);
         MRT_CUDA(cudaMemsetAsync(m_rayCounters.ptr, 0, 64, m_stream));
         uint32_t launches = 0;
+        const uint32_t waves = (n + m_waveSamples - 1) / m_waveSamples;
+        const size_t perWave = size_t(6) * (p.maxBounces + 1);
+        while (m_stageEvents.size() < waves * perWave) {
+            cudaEvent_t ev;
+            MRT_CUDA(cudaEventCreate(&ev));
+            m_stageEvents.push_back(ev);
+        }
         MRT_CUDA(cudaEventRecord(m_ev0, m_stream));
-        for (uint32_t done = 0; done < n;) {
+        uint32_t wave = 0;
+        for (uint32_t done = 0; done < n; ++wave) {
             const uint32_t k = std::min(n - done, m_waveSamples);
-            const cudaError_t le = mrtcu_wave(&p, &m_waveState, m_frameIndex + done, k, &launches, m_stream);
+            const cudaError_t le = mrtcu_wave(&p, &m_waveState, m_frameIndex + done, k, &launches,
+                                              m_stageEvents.data() + wave * perWave, m_stream);
             if (le != cudaSuccess) return guard(fromCuda(le, "path tracing launch"));
             done += k;
         }
@@ -812,16 +823,36 @@ mrtResult Engine::renderFrames(uint32_t count, mrtFrameInfo* info) {
         float ms = 0.0f;
         MRT_CUDA(cudaEventElapsedTime(&ms, m_ev0, m_ev1));
         m_stats.lastRenderMs = ms;
+        float ext = 0.0f, sha = 0.0f, shw = 0.0f;
+        for (uint32_t w = 0; w < waves; ++w)
+            for (uint32_t b = 0; b <= p.maxBounces; ++b) {
+                const cudaEvent_t* ev = m_stageEvents.data() + w * perWave + 6 * b;
+                float a = 0.0f, c = 0.0f, d = 0.0f;
+                MRT_CUDA(cudaEventElapsedTime(&a, ev[0], ev[1]));
+                MRT_CUDA(cudaEventElapsedTime(&c, ev[1], ev[2]));
+                MRT_CUDA(cudaEventElapsedTime(&d, ev[2], ev[3]));
+                ext += a;
+                sha += c;
+                shw += d;
+            }
+        m_stats.extendMs = ext;
+        m_stats.shadeMs = sha;
+        m_stats.shadowMs = shw;
+        m_stats.otherMs = ms - ext - sha - shw;
         m_stats.lastRenderSpp = n;
         m_stats.kernelLaunches = launches;
         MRT_TRY(guard(checkErrorFlags()));
-        unsigned long long ctr[5];
+        unsigned long long ctr[7];
         MRT_CUDA(cudaMemcpy(ctr, m_rayCounters.ptr, sizeof(ctr), cudaMemcpyDeviceToHost));
         m_stats.raysClosest = ctr[0];
         m_stats.raysShadow = ctr[1];
         m_stats.nodeFetches = ctr[2];
         m_stats.triTests = ctr[3];
         m_stats.surfaceHits = ctr[4];
+        m_stats.shadowNodeFetches = ctr[5];
+        m_stats.shadowTriTests = ctr[6];
+        m_stats.nodeBytes = sizeof(MrtNode);
+        m_stats.triBytes = 48;
         m_frameIndex += n;
         m_resolveExposure = std::exp2(m_settings.exposureEV);
         m_resolveTonemap = m_settings.tonemap;

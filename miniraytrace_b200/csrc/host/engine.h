@@ -80,6 +80,7 @@ private:
     cudaStream_t m_stream = nullptr;
     cudaEvent_t m_ev0 = nullptr, m_ev1 = nullptr;
     std::vector<cudaEvent_t> m_copyEvents;
+    std::vector<cudaEvent_t> m_stageEvents;  // 6 per bounce per wave of one render call
     bool m_lost = false;
     bool m_validation = false;
     unsigned m_hostThreads = 1;
