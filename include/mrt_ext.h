@@ -106,6 +106,17 @@ MRT_API mrtResult mrtxSetSampleStream(mrtEngine*, uint32_t offset, uint32_t stri
 MRT_API mrtResult mrtxCopyAccumulationDevice(mrtEngine*, void* devPtr, size_t bytes,
                                              int32_t accumulate);
 
+/* Host-side build of the acceleration structure the engine uses for a mesh,
+ * for inspection and tests (no device needed): an 8-wide compressed BVH over
+ * `count` boxes (6 floats each: lo xyz, hi xyz) with leaves of at most
+ * maxLeafPrims (1..3) primitives. nodesOut receives up to nodeCapacity
+ * 80-byte node records (layout: miniraytrace_b200/csrc/common/device_types.h
+ * MrtWideNode), primOrderOut `count` primitive indices in leaf order.
+ * Builds on the binned-SAH binary builder (the reference builds a binary
+ * tree on the CPU, core/src/accel/Bvh.cpp:137-156). */
+MRT_API mrtResult mrtxBuildWideBvh(const float* aabbs, uint32_t count, uint32_t maxLeafPrims, void* nodesOut,
+                                   uint32_t nodeCapacity, uint32_t* primOrderOut, uint32_t* nodeCountOut);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif

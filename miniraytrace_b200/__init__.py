@@ -307,6 +307,21 @@ class Engine:
                "mrtxCopyAccumulationDevice")
 
 
+def build_wide_bvh(aabbs, max_leaf_prims=3):
+    """Host build of the engine's 8-wide BVH over (N, 6) boxes:
+    (nodes as a WIDE_NODE_DTYPE array, primitive order)."""
+    lib = load_library()
+    a = np.ascontiguousarray(np.asarray(aabbs, np.float32).reshape(-1, 6))
+    n = a.shape[0]
+    cap = max(1, n)
+    nodes = np.zeros(cap, dtype=abi.WIDE_NODE_DTYPE)
+    order = np.zeros(max(1, n), np.uint32)
+    count = C.c_uint32()
+    _check(lib.mrtxBuildWideBvh(_ptr(a), n, max_leaf_prims, _ptr(nodes), cap, _ptr(order), C.byref(count)),
+           "mrtxBuildWideBvh")
+    return nodes[:count.value].copy(), order[:n].copy()
+
+
 def make_rays(origins, dirs, t_max=1e30):
     o = np.asarray(origins, np.float32).reshape(-1, 3)
     d = np.asarray(dirs, np.float32).reshape(-1, 3)

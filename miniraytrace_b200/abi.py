@@ -171,4 +171,10 @@ FUNCTIONS = [
                                   C.POINTER(C.c_float)]),
     ("mrtxSetSampleStream", C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32]),
     ("mrtxCopyAccumulationDevice", C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, C.c_int32]),
+    ("mrtxBuildWideBvh", C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p,
+                                   C.POINTER(C.c_uint32)]),
 ]
+
+# numpy dtype of one 80-byte MrtWideNode
+WIDE_NODE_DTYPE = [("p", "<f4", 3), ("e", "u1", 3), ("imask", "u1"), ("childBase", "<u4"), ("primBase", "<u4"),
+                   ("meta", "u1", 8), ("qlo", "u1", (3, 8)), ("qhi", "u1", (3, 8))]

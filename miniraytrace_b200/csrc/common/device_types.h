@@ -50,6 +50,21 @@ typedef struct MrtNode {
     uint32_t packed;  // (count << 2) | split axis
 } MrtNode;
 
+// 8-wide compressed BVH node, 80 bytes (five 16-byte loads); see
+// csrc/host/wide_bvh.h for the encoding. Bytes 0-15: origin + exponents +
+// internal mask; 16-31: child/primitive bases + meta bytes; 32-79: the eight
+// quantised child boxes, axis-major (lo x, lo y, lo z, hi x, hi y, hi z).
+typedef struct MrtWideNode {
+    float p[3];
+    uint8_t e[3];
+    uint8_t imask;
+    uint32_t childBase;
+    uint32_t primBase;
+    uint8_t meta[8];
+    uint8_t qlo[3][8];
+    uint8_t qhi[3][8];
+} MrtWideNode;
+
 // Instance: row-major 3x4 transforms (rows of [R | t]).
 typedef struct MrtInstance {
     float w2o[12];
@@ -106,7 +121,7 @@ typedef struct MrtFrameParams {
     uint32_t streamOffset, streamStride;
     uint32_t nodeCount, instanceCount, triCount, materialCount;
     // scene arrays (device pointers)
-    const MrtNode* nodes;
+    const MrtWideNode* nodes;  // 8-wide BVH: every BLAS, then the TLAS
     const float4* triVerts;
     const uint4* triIndex;
     const float4* normals;

@@ -8,23 +8,22 @@
 // Differences from the reference, by design:
 //   - watertight ray/triangle test (Woop, Benthin, Wald, JCGT 2013) instead of
 //     Moeller-Trumbore: no ray slips through a shared edge or vertex;
-//   - a visited internal node tests both children's boxes (one 64-byte
-//     fetch, the pair is adjacent), descends into the nearer and pushes the
-//     farther, so culling uses the current closest t;
+//   - 8-wide compressed BVH nodes (five 128-bit loads test eight child
+//     boxes), traversed by groups: a stack entry is a node's remaining
+//     child-hit mask, children are taken in ray-octant order, leaf
+//     triangles of a node are tested before descending;
 //   - box exits are widened by 1 + 2*gamma(3) = 1 + 3 * 2^-23 (Ize 2013) so a
 //     rounding error in the slab test can never cull a real hit (the
 //     reference's exact-comparison slab test occasionally drops a hit or an
 //     occluder whose point lies on its leaf box's face);
 //   - stacks are bounded and an overflow sets an error flag instead of
-//     writing out of bounds.
+//     writing out of bounds; node, triangle and instance indices are checked.
 #pragma once
 
 #include "../common/device_types.h"
 #include "vec.cuh"
 
 #define MRT_EPS_RAY 1e-4f
-#define MRT_TLAS_STACK 32
-#define MRT_BLAS_STACK 48
 // Upper bound on node visits of one traversal. A well-formed BVH never gets
 // near it; it only turns a malformed tree into an error flag instead of an
 // endless loop.
@@ -71,23 +70,6 @@ MRT_DEV float3 safeInv(float3 d) {
     const float big = 1e30f;
     return f3(d.x != 0.0f ? 1.0f / d.x : copysignf(big, d.x), d.y != 0.0f ? 1.0f / d.y : copysignf(big, d.y),
               d.z != 0.0f ? 1.0f / d.z : copysignf(big, d.z));
-}
-
-// Slab test; returns the entry distance, or +inf when the box is missed or
-// starts beyond tMax.
-MRT_DEV float slab(const float* lo, const float* hi, float3 o, float3 inv, float tMax) {
-    const float tx0 = (lo[0] - o.x) * inv.x, tx1 = (hi[0] - o.x) * inv.x;
-    const float ty0 = (lo[1] - o.y) * inv.y, ty1 = (hi[1] - o.y) * inv.y;
-    const float tz0 = (lo[2] - o.z) * inv.z, tz1 = (hi[2] - o.z) * inv.z;
-    const float tEnter = fmaxf(fmaxf(fminf(tx0, tx1), fminf(ty0, ty1)), fmaxf(fminf(tz0, tz1), 0.0f));
-    const float tExit = fminf(fminf(fmaxf(tx0, tx1), fmaxf(ty0, ty1)), fminf(fmaxf(tz0, tz1), tMax)) * 1.00000036f;
-    return tEnter <= tExit ? tEnter : __int_as_float(0x7f800000);
-}
-
-MRT_DEV float slabNode(const float4& a, const float4& b, float3 o, float3 inv, float tMax) {
-    const float lo[3] = {a.x, a.y, a.z};
-    const float hi[3] = {b.x, b.y, b.z};
-    return slab(lo, hi, o, inv, tMax);
 }
 
 // Watertight test (Woop et al. 2013). Accepts t in (1e-4, tMax); both faces.
@@ -177,98 +159,153 @@ MRT_DEV void refineHit(const MrtFrameParams& P, float3 o, float3 d, HitRecord& h
     hit.v = v;
 }
 
-// Per-thread traffic counters for the roofline's algorithmic bytes: node
-// records fetched (32 B each) and triangle tests (48 B each).
-// `bad` records an out-of-range index met during traversal: the access is
-// redirected to a valid element and the ray is reported through the error
-// flag instead of reading outside the scene arrays.
+// Per-thread traffic counters for the roofline's algorithmic bytes: wide node
+// records fetched (80 B each) and triangle tests (48 B each). `bad` records an
+// out-of-range index met during traversal: the access is redirected to a
+// valid element and the ray is reported through the error flag instead of
+// reading outside the scene arrays.
 struct TraversalCounters {
     uint32_t nodes = 0, tris = 0;
     bool bad = false;
 };
 
-MRT_DEV void loadNode(const MrtFrameParams& P, uint32_t i, float4& a, float4& b, TraversalCounters& c) {
-    if (i >= P.nodeCount) {
-        c.bad = true;
-        i = 0;
+// Decoded hits of one wide node.
+struct WideHits {
+    uint32_t childBase;  // first internal child node
+    uint32_t primBase;   // first leaf primitive
+    uint32_t nodeBits;   // bits 24-31: internal children hit (ray-ordered), bits 0-7: internal slot mask
+    uint32_t primBits;   // bits 0-23: leaf primitives hit, relative to primBase
+};
+
+// Exact float of a byte: 2^23 + b - 2^23.
+MRT_DEV float byteToFloat(uint32_t b) { return __uint_as_float(0x4B000000u | b) - 8388608.0f; }
+
+// Tests the ray against the eight quantised child boxes of node `idx`.
+// Child boxes decode as p + q * 2^(e-127) (the host quantised them
+// conservatively for exactly this arithmetic); internal-child hits land on
+// bit 24 + (slot XOR oct), so taking bits from the top visits the slots the
+// ray reaches first first.
+MRT_DEV WideHits intersectWide(const MrtFrameParams& P, uint32_t idx, float3 o, float3 inv, uint32_t oct, float tMax,
+                               TraversalCounters& tc) {
+    if (idx >= P.nodeCount) {
+        tc.bad = true;
+        idx = 0;
     }
-    const float4* p = reinterpret_cast<const float4*>(P.nodes + i);
-    a = ldg4(p);
-    b = ldg4(p + 1);
-    c.nodes++;
+    const float4* q = reinterpret_cast<const float4*>(P.nodes + idx);
+    const float4 q0 = ldg4(q), q1 = ldg4(q + 1), q2 = ldg4(q + 2), q3 = ldg4(q + 3), q4 = ldg4(q + 4);
+    tc.nodes++;
+    const uint32_t eb = __float_as_uint(q0.w);
+    const float sx = __uint_as_float((eb & 0xffu) << 23), sy = __uint_as_float(((eb >> 8) & 0xffu) << 23),
+                sz = __uint_as_float(((eb >> 16) & 0xffu) << 23);
+    const uint32_t imask = eb >> 24;
+    WideHits h;
+    h.childBase = __float_as_uint(q1.x);
+    h.primBase = __float_as_uint(q1.y);
+    h.nodeBits = imask;
+    h.primBits = 0;
+    const uint32_t meta[2] = {__float_as_uint(q1.z), __float_as_uint(q1.w)};
+    const uint32_t lx[2] = {__float_as_uint(q2.x), __float_as_uint(q2.y)};
+    const uint32_t ly[2] = {__float_as_uint(q2.z), __float_as_uint(q2.w)};
+    const uint32_t lz[2] = {__float_as_uint(q3.x), __float_as_uint(q3.y)};
+    const uint32_t hx[2] = {__float_as_uint(q3.z), __float_as_uint(q3.w)};
+    const uint32_t hy[2] = {__float_as_uint(q4.x), __float_as_uint(q4.y)};
+    const uint32_t hz[2] = {__float_as_uint(q4.z), __float_as_uint(q4.w)};
+#pragma unroll
+    for (int half = 0; half < 2; ++half) {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const uint32_t sh = 8u * uint32_t(j);
+            const uint32_t m = (meta[half] >> sh) & 0xffu;
+            if (m == 0u) continue;
+            const float bx0 = q0.x + byteToFloat((lx[half] >> sh) & 0xffu) * sx;
+            const float by0 = q0.y + byteToFloat((ly[half] >> sh) & 0xffu) * sy;
+            const float bz0 = q0.z + byteToFloat((lz[half] >> sh) & 0xffu) * sz;
+            const float bx1 = q0.x + byteToFloat((hx[half] >> sh) & 0xffu) * sx;
+            const float by1 = q0.y + byteToFloat((hy[half] >> sh) & 0xffu) * sy;
+            const float bz1 = q0.z + byteToFloat((hz[half] >> sh) & 0xffu) * sz;
+            const float tx0 = (bx0 - o.x) * inv.x, tx1 = (bx1 - o.x) * inv.x;
+            const float ty0 = (by0 - o.y) * inv.y, ty1 = (by1 - o.y) * inv.y;
+            const float tz0 = (bz0 - o.z) * inv.z, tz1 = (bz1 - o.z) * inv.z;
+            const float tEnter = fmaxf(fmaxf(fminf(tx0, tx1), fminf(ty0, ty1)), fmaxf(fminf(tz0, tz1), 0.0f));
+            const float tExit =
+                fminf(fminf(fmaxf(tx0, tx1), fmaxf(ty0, ty1)), fminf(fmaxf(tz0, tz1), tMax)) * 1.00000036f;
+            if (tEnter <= tExit) {
+                const uint32_t slot = uint32_t(half * 4 + j);
+                if ((imask >> slot) & 1u) h.nodeBits |= 1u << ((m & 31u) ^ oct);
+                else h.primBits |= (m >> 5) << (m & 31u);
+            }
+        }
+    }
+    return h;
 }
 
+// Ray octant for child ordering: bit k set when direction component k > 0.
+MRT_DEV uint32_t rayOctant(float3 d) { return (d.x > 0.0f ? 1u : 0u) | (d.y > 0.0f ? 2u : 0u) | (d.z > 0.0f ? 4u : 0u); }
+
+// Node index of the internal child on hit bit b (24..31) of a group.
+MRT_DEV uint32_t childIndex(uint32_t childBase, uint32_t imask, uint32_t b, uint32_t oct) {
+    const uint32_t slot = (b - 24u) ^ oct;
+    return childBase + uint32_t(__popc(imask & ((1u << slot) - 1u)));
+}
+
+#define MRT_WIDE_STACK 32
+#define MRT_WIDE_TLAS_STACK 16
+
 // Closest hit within one BLAS (object-space ray). Updates tMax and hit.
-// Stack entries carry the far child's entry distance, so a popped subtree
-// that starts beyond the current closest hit is skipped without fetching it.
 // Returns false on a stack overflow or an exhausted visit budget.
 MRT_DEV bool closestBlas(const MrtFrameParams& P, uint32_t root, uint32_t inst, float3 o, float3 d, float& tMax,
                          HitRecord& hit, TraversalCounters& tc) {
     const float3 inv = safeInv(d);
     const Shear sh = makeShear(d);
-    uint2 stack[MRT_BLAS_STACK];
+    const uint32_t oct = rayOctant(d);
+    uint2 stack[MRT_WIDE_STACK];
     int sp = 0;
-    float4 na, nb;
-    loadNode(P, root, na, nb, tc);
-    if (!(slabNode(na, nb, o, inv, tMax) < __int_as_float(0x7f800000))) return true;
     bool ok = true;
+    WideHits g = intersectWide(P, root, o, inv, oct, tMax, tc);
     uint32_t visits = 0;
     for (;;) {
-        if (++visits > MRT_MAX_VISITS) { ok = false; return false; }
-        const uint32_t packed = __float_as_uint(nb.w);
-        const uint32_t first = __float_as_uint(na.w);
-        const uint32_t count = packed >> 2;
-        if (count == 0) {
-            float4 a0, b0, a1, b1;
-            loadNode(P, first, a0, b0, tc);
-            loadNode(P, first + 1, a1, b1, tc);
-            const float t0 = slabNode(a0, b0, o, inv, tMax);
-            const float t1 = slabNode(a1, b1, o, inv, tMax);
-            const bool h0 = t0 < __int_as_float(0x7f800000), h1 = t1 < __int_as_float(0x7f800000);
-            if (h0 && h1) {
-                const bool firstNear = t0 <= t1;
-                if (sp < MRT_BLAS_STACK) stack[sp++] = make_uint2(firstNear ? first + 1 : first, __float_as_uint(firstNear ? t1 : t0));
+        if (++visits > MRT_MAX_VISITS) return false;
+        while (g.primBits) {
+            const uint32_t b = uint32_t(__ffs(g.primBits) - 1);
+            g.primBits &= g.primBits - 1u;
+            const uint32_t tri = g.primBase + b;
+            ++tc.tris;
+            if (tri >= P.triCount) {
+                tc.bad = true;
+                continue;
+            }
+            float t, u, v;
+            if (hitTriangle(P.triVerts, tri, o, sh, tMax, t, u, v)) {
+                tMax = t;
+                hit.t = t;
+                hit.u = u;
+                hit.v = v;
+                hit.tri = tri;
+                hit.inst = inst;
+            }
+        }
+        if (g.nodeBits & 0xff000000u) {
+            const uint32_t b = 31u - uint32_t(__clz(g.nodeBits & 0xff000000u));
+            const uint32_t rest = g.nodeBits & ~(1u << b);
+            const uint32_t child = childIndex(g.childBase, g.nodeBits & 0xffu, b, oct);
+            if (rest & 0xff000000u) {
+                if (sp < MRT_WIDE_STACK) stack[sp++] = make_uint2(g.childBase, rest);
                 else ok = false;
-                na = firstNear ? a0 : a1;
-                nb = firstNear ? b0 : b1;
-                continue;
             }
-            if (h0 || h1) {
-                na = h0 ? a0 : a1;
-                nb = h0 ? b0 : b1;
-                continue;
-            }
-        } else {
-            for (uint32_t i = 0; i < count; ++i) {
-                float t, u, v;
-                ++tc.tris;
-                if (first + i >= P.triCount) {
-                    tc.bad = true;
-                    break;
-                }
-                if (hitTriangle(P.triVerts, first + i, o, sh, tMax, t, u, v)) {
-                    tMax = t;
-                    hit.t = t;
-                    hit.u = u;
-                    hit.v = v;
-                    hit.tri = first + i;
-                    hit.inst = inst;
-                }
-            }
+            g = intersectWide(P, child, o, inv, oct, tMax, tc);
+            continue;
         }
-        // pop the nearest pending subtree that can still hold a closer hit
-        for (;;) {
-            if (sp == 0) return ok;
-            const uint2 e = stack[--sp];
-            if (__uint_as_float(e.y) <= tMax * 1.00000036f) {
-                loadNode(P, e.x, na, nb, tc);
-                break;
-            }
-        }
+        if (sp == 0) return ok;
+        const uint2 e = stack[--sp];
+        g.childBase = e.x;
+        g.nodeBits = e.y;
+        g.primBits = 0;
     }
 }
 
-// Closest hit over the scene (reference intersect.glsl:88-125).
+// Closest hit over the scene (reference intersect.glsl:88-125): the TLAS's
+// leaf primitives are instances; each hit instance's BLAS is walked with the
+// ray in its object space.
 MRT_DEV bool traceClosest(const MrtFrameParams& P, float3 o, float3 d, float tMax, HitRecord& hit, TraversalCounters& tc) {
     hit.t = tMax;
     hit.tri = 0xffffffffu;
@@ -276,152 +313,133 @@ MRT_DEV bool traceClosest(const MrtFrameParams& P, float3 o, float3 d, float tMa
     hit.u = hit.v = 0.0f;
     if (P.instanceCount == 0) return true;  // empty scene (the TLAS root is a placeholder)
     const float3 inv = safeInv(d);
-    uint2 stack[MRT_TLAS_STACK];
+    const uint32_t oct = rayOctant(d);
+    uint2 stack[MRT_WIDE_TLAS_STACK];
     int sp = 0;
-    float4 na, nb;
-    loadNode(P, P.tlasRoot, na, nb, tc);
-    if (!(slabNode(na, nb, o, inv, tMax) < __int_as_float(0x7f800000))) return true;
     bool ok = true;
+    WideHits g = intersectWide(P, P.tlasRoot, o, inv, oct, tMax, tc);
     uint32_t visits = 0;
     for (;;) {
-        if (++visits > MRT_MAX_VISITS) { ok = false; return false; }
-        const uint32_t packed = __float_as_uint(nb.w);
-        const uint32_t first = __float_as_uint(na.w);
-        const uint32_t count = packed >> 2;
-        if (count == 0) {
-            float4 a0, b0, a1, b1;
-            loadNode(P, first, a0, b0, tc);
-            loadNode(P, first + 1, a1, b1, tc);
-            const float t0 = slabNode(a0, b0, o, inv, tMax);
-            const float t1 = slabNode(a1, b1, o, inv, tMax);
-            const bool h0 = t0 < __int_as_float(0x7f800000), h1 = t1 < __int_as_float(0x7f800000);
-            if (h0 && h1) {
-                const bool firstNear = t0 <= t1;
-                if (sp < MRT_TLAS_STACK) stack[sp++] = make_uint2(firstNear ? first + 1 : first, __float_as_uint(firstNear ? t1 : t0));
+        if (++visits > MRT_MAX_VISITS) return false;
+        while (g.primBits) {
+            const uint32_t b = uint32_t(__ffs(g.primBits) - 1);
+            g.primBits &= g.primBits - 1u;
+            const uint32_t instIdx = g.primBase + b;
+            if (instIdx >= P.instanceCount) {
+                tc.bad = true;
+                continue;
+            }
+            const MrtInstance* in = P.instances + instIdx;
+            const float3 oo = xformPoint(in->w2o, o), dd = xformDir(in->w2o, d);
+            ok &= closestBlas(P, in->blasRoot, instIdx, oo, dd, tMax, hit, tc);
+        }
+        if (g.nodeBits & 0xff000000u) {
+            const uint32_t b = 31u - uint32_t(__clz(g.nodeBits & 0xff000000u));
+            const uint32_t rest = g.nodeBits & ~(1u << b);
+            const uint32_t child = childIndex(g.childBase, g.nodeBits & 0xffu, b, oct);
+            if (rest & 0xff000000u) {
+                if (sp < MRT_WIDE_TLAS_STACK) stack[sp++] = make_uint2(g.childBase, rest);
                 else ok = false;
-                na = firstNear ? a0 : a1;
-                nb = firstNear ? b0 : b1;
-                continue;
             }
-            if (h0 || h1) {
-                na = h0 ? a0 : a1;
-                nb = h0 ? b0 : b1;
-                continue;
-            }
-        } else {
-            for (uint32_t i = 0; i < count; ++i) {
-                const uint32_t instIdx = first + i;
-                if (instIdx >= P.instanceCount) {
-                    tc.bad = true;
-                    break;
-                }
-                const MrtInstance* in = P.instances + instIdx;
-                const float3 oo = xformPoint(in->w2o, o), dd = xformDir(in->w2o, d);
-                ok &= closestBlas(P, in->blasRoot, instIdx, oo, dd, tMax, hit, tc);
-            }
+            g = intersectWide(P, child, o, inv, oct, tMax, tc);
+            continue;
         }
-        for (;;) {
-            if (sp == 0) {
-                if (hit.tri != 0xffffffffu) refineHit(P, o, d, hit);
-                return ok;
-            }
-            const uint2 e = stack[--sp];
-            if (__uint_as_float(e.y) <= tMax * 1.00000036f) {
-                loadNode(P, e.x, na, nb, tc);
-                break;
-            }
-        }
+        if (sp == 0) break;
+        const uint2 e = stack[--sp];
+        g.childBase = e.x;
+        g.nodeBits = e.y;
+        g.primBits = 0;
     }
+    if (hit.tri != 0xffffffffu) refineHit(P, o, d, hit);
+    return ok;
 }
 
-// Any hit in (1e-4, tMax) (reference intersect.glsl:128-178).
+// Any hit in (1e-4, tMax) within one BLAS (reference intersect.glsl:128-178).
 MRT_DEV bool anyBlas(const MrtFrameParams& P, uint32_t root, float3 o, float3 d, float tMax, bool& ok,
                      TraversalCounters& tc) {
     const float3 inv = safeInv(d);
     const Shear sh = makeShear(d);
-    uint32_t stack[MRT_BLAS_STACK];
+    const uint32_t oct = rayOctant(d);
+    uint2 stack[MRT_WIDE_STACK];
     int sp = 0;
-    float4 na, nb;
-    loadNode(P, root, na, nb, tc);
-    if (!(slabNode(na, nb, o, inv, tMax) < __int_as_float(0x7f800000))) return false;
+    WideHits g = intersectWide(P, root, o, inv, oct, tMax, tc);
     uint32_t visits = 0;
     for (;;) {
-        if (++visits > MRT_MAX_VISITS) { ok = false; return false; }
-        const uint32_t packed = __float_as_uint(nb.w);
-        const uint32_t first = __float_as_uint(na.w);
-        const uint32_t count = packed >> 2;
-        if (count == 0) {
-            float4 a0, b0, a1, b1;
-            loadNode(P, first, a0, b0, tc);
-            loadNode(P, first + 1, a1, b1, tc);
-            const bool h0 = slabNode(a0, b0, o, inv, tMax) < __int_as_float(0x7f800000);
-            const bool h1 = slabNode(a1, b1, o, inv, tMax) < __int_as_float(0x7f800000);
-            if (h0 && h1) {
-                if (sp < MRT_BLAS_STACK) stack[sp++] = first + 1;
-                else ok = false;
-            }
-            if (h0 || h1) {
-                na = h0 ? a0 : a1;
-                nb = h0 ? b0 : b1;
+        if (++visits > MRT_MAX_VISITS) {
+            ok = false;
+            return false;
+        }
+        while (g.primBits) {
+            const uint32_t b = uint32_t(__ffs(g.primBits) - 1);
+            g.primBits &= g.primBits - 1u;
+            const uint32_t tri = g.primBase + b;
+            ++tc.tris;
+            if (tri >= P.triCount) {
+                tc.bad = true;
                 continue;
             }
-        } else {
-            for (uint32_t i = 0; i < count; ++i) {
-                float t, u, v;
-                ++tc.tris;
-                if (first + i >= P.triCount) {
-                    tc.bad = true;
-                    break;
-                }
-                if (hitTriangle(P.triVerts, first + i, o, sh, tMax, t, u, v)) return true;
+            float t, u, v;
+            if (hitTriangle(P.triVerts, tri, o, sh, tMax, t, u, v)) return true;
+        }
+        if (g.nodeBits & 0xff000000u) {
+            const uint32_t b = 31u - uint32_t(__clz(g.nodeBits & 0xff000000u));
+            const uint32_t rest = g.nodeBits & ~(1u << b);
+            const uint32_t child = childIndex(g.childBase, g.nodeBits & 0xffu, b, oct);
+            if (rest & 0xff000000u) {
+                if (sp < MRT_WIDE_STACK) stack[sp++] = make_uint2(g.childBase, rest);
+                else ok = false;
             }
+            g = intersectWide(P, child, o, inv, oct, tMax, tc);
+            continue;
         }
         if (sp == 0) return false;
-        loadNode(P, stack[--sp], na, nb, tc);
+        const uint2 e = stack[--sp];
+        g.childBase = e.x;
+        g.nodeBits = e.y;
+        g.primBits = 0;
     }
 }
 
 MRT_DEV bool traceAny(const MrtFrameParams& P, float3 o, float3 d, float tMax, bool& ok, TraversalCounters& tc) {
     if (P.instanceCount == 0) return false;  // empty scene
     const float3 inv = safeInv(d);
-    uint32_t stack[MRT_TLAS_STACK];
+    const uint32_t oct = rayOctant(d);
+    uint2 stack[MRT_WIDE_TLAS_STACK];
     int sp = 0;
-    float4 na, nb;
-    loadNode(P, P.tlasRoot, na, nb, tc);
-    if (!(slabNode(na, nb, o, inv, tMax) < __int_as_float(0x7f800000))) return false;
+    WideHits g = intersectWide(P, P.tlasRoot, o, inv, oct, tMax, tc);
     uint32_t visits = 0;
     for (;;) {
-        if (++visits > MRT_MAX_VISITS) { ok = false; return false; }
-        const uint32_t packed = __float_as_uint(nb.w);
-        const uint32_t first = __float_as_uint(na.w);
-        const uint32_t count = packed >> 2;
-        if (count == 0) {
-            float4 a0, b0, a1, b1;
-            loadNode(P, first, a0, b0, tc);
-            loadNode(P, first + 1, a1, b1, tc);
-            const bool h0 = slabNode(a0, b0, o, inv, tMax) < __int_as_float(0x7f800000);
-            const bool h1 = slabNode(a1, b1, o, inv, tMax) < __int_as_float(0x7f800000);
-            if (h0 && h1) {
-                if (sp < MRT_TLAS_STACK) stack[sp++] = first + 1;
-                else ok = false;
-            }
-            if (h0 || h1) {
-                na = h0 ? a0 : a1;
-                nb = h0 ? b0 : b1;
+        if (++visits > MRT_MAX_VISITS) {
+            ok = false;
+            return false;
+        }
+        while (g.primBits) {
+            const uint32_t b = uint32_t(__ffs(g.primBits) - 1);
+            g.primBits &= g.primBits - 1u;
+            const uint32_t instIdx = g.primBase + b;
+            if (instIdx >= P.instanceCount) {
+                tc.bad = true;
                 continue;
             }
-        } else {
-            for (uint32_t i = 0; i < count; ++i) {
-                if (first + i >= P.instanceCount) {
-                    tc.bad = true;
-                    break;
-                }
-                const MrtInstance* in = P.instances + first + i;
-                const float3 oo = xformPoint(in->w2o, o), dd = xformDir(in->w2o, d);
-                if (anyBlas(P, in->blasRoot, oo, dd, tMax, ok, tc)) return true;
+            const MrtInstance* in = P.instances + instIdx;
+            const float3 oo = xformPoint(in->w2o, o), dd = xformDir(in->w2o, d);
+            if (anyBlas(P, in->blasRoot, oo, dd, tMax, ok, tc)) return true;
+        }
+        if (g.nodeBits & 0xff000000u) {
+            const uint32_t b = 31u - uint32_t(__clz(g.nodeBits & 0xff000000u));
+            const uint32_t rest = g.nodeBits & ~(1u << b);
+            const uint32_t child = childIndex(g.childBase, g.nodeBits & 0xffu, b, oct);
+            if (rest & 0xff000000u) {
+                if (sp < MRT_WIDE_TLAS_STACK) stack[sp++] = make_uint2(g.childBase, rest);
+                else ok = false;
             }
+            g = intersectWide(P, child, o, inv, oct, tMax, tc);
+            continue;
         }
         if (sp == 0) return false;
-        loadNode(P, stack[--sp], na, nb, tc);
+        const uint2 e = stack[--sp];
+        g.childBase = e.x;
+        g.nodeBits = e.y;
+        g.primBits = 0;
     }
 }

@@ -9,9 +9,11 @@
 // anything else -> MRT_ERROR_UNKNOWN).
 #include <cstring>
 #include <new>
+#include <vector>
 
 #include "../../../include/mrt_ext.h"
 #include "engine.h"
+#include "wide_bvh.h"
 
 namespace {
 
@@ -259,6 +261,27 @@ MRT_API mrtResult mrtxCopyAccumulationDevice(mrtEngine* e, void* devPtr, size_t 
     mrt::Engine* eng = unwrap(e);
     if (!eng) return MRT_ERROR_INVALID_HANDLE;
     return guarded([&] { return eng->copyAccumulationDevice(devPtr, bytes, accumulate != 0); });
+}
+
+MRT_API mrtResult mrtxBuildWideBvh(const float* aabbs, uint32_t count, uint32_t maxLeafPrims, void* nodesOut,
+                                   uint32_t nodeCapacity, uint32_t* primOrderOut, uint32_t* nodeCountOut) {
+    if ((count && (!aabbs || !primOrderOut)) || !nodeCountOut || (nodeCapacity && !nodesOut))
+        return MRT_ERROR_INVALID_ARGUMENT;
+    return guarded([&] {
+        std::vector<mrt::Box3> boxes(count);
+        for (uint32_t i = 0; i < count; ++i)
+            for (int k = 0; k < 3; ++k) {
+                boxes[i].lo[k] = aabbs[i * 6 + k];
+                boxes[i].hi[k] = aabbs[i * 6 + 3 + k];
+            }
+        const mrt::WideBvh w = mrt::collapseToWide(mrt::buildBvh(boxes, 1, 4), maxLeafPrims);
+        *nodeCountOut = uint32_t(w.nodes.size());
+        if (w.nodes.size() > nodeCapacity)
+            return mrt::fail(MRT_ERROR_INVALID_ARGUMENT, "mrtxBuildWideBvh: node capacity too small");
+        if (!w.nodes.empty()) std::memcpy(nodesOut, w.nodes.data(), w.nodes.size() * sizeof(MrtWideNode));
+        if (count) std::memcpy(primOrderOut, w.primOrder.data(), size_t(count) * 4);
+        return MRT_SUCCESS;
+    });
 }
 
 }  // extern "C"

@@ -42,16 +42,11 @@ void DeviceBuffer::release() {
 
 namespace {
 
-// A node whose inverted box fails every slab test: traversal of an empty
-// scene ends at the root (reference Renderer.cpp:49-58).
-MrtNode sentinelNode() {
-    MrtNode n{};
-    for (int k = 0; k < 3; ++k) {
-        n.lo[k] = 3.402823466e38f;
-        n.hi[k] = -3.402823466e38f;
-    }
-    n.leftOrPrim = 0;
-    n.packed = 1u << 2;
+// A wide node with no children: the TLAS root of an empty scene (the
+// reference parks an inverted-box sentinel there, Renderer.cpp:49-58).
+MrtWideNode emptyNode() {
+    MrtWideNode n;
+    std::memset(&n, 0, sizeof(n));
     return n;
 }
 
@@ -178,7 +173,7 @@ mrtResult Engine::init(const mrtEngineDesc& desc) {
     log(LogLevel::Info, std::string("GPU: ") + prop.name);
 
     // pre-commit frames traverse an empty scene safely
-    const MrtNode s = sentinelNode();
+    const MrtWideNode s = emptyNode();
     MRT_TRY(m_nodes.upload(&s, sizeof(s), m_stream));
     m_nodeCount = 1;
     m_tlasRoot = 0;
@@ -419,7 +414,7 @@ mrtResult Engine::packGeometry(uint32_t& rebuilt) {
     for (auto it = m_blas.begin(); it != m_blas.end();)
         it = meshes.count(it->first) ? std::next(it) : m_blas.erase(it);
     const auto tb = std::chrono::steady_clock::now();
-    std::vector<std::pair<uint32_t, std::future<BvhResult>>> jobs;
+    std::vector<std::pair<uint32_t, std::future<WideBvh>>> jobs;
     const unsigned threads = m_hostThreads;
     for (auto& [id, mesh] : meshes) {
         if (!mesh.blasDirty && m_blas.count(id)) continue;
@@ -442,7 +437,9 @@ mrtResult Engine::packGeometry(uint32_t& rebuilt) {
                                       }
                                   }
                               }
-                              return buildBvh(boxes, 4, threads);
+                              // binary SAH tree down to single triangles, collapsed to
+                              // 8-wide nodes with leaves of up to 3 triangles
+                              return collapseToWide(buildBvh(boxes, 1, threads), 3);
                           }));
     }
     for (auto& [id, fut] : jobs) {
@@ -466,7 +463,7 @@ mrtResult Engine::packGeometry(uint32_t& rebuilt) {
     normals.reserve(nv);
     uvs.reserve(nv);
     tangents.reserve(nv);
-    std::vector<MrtNode> nodes;
+    std::vector<MrtWideNode> nodes;
     nodes.reserve(nn + 1);
     uint32_t vbase = 0, tbase = 0;
     for (auto& [id, mesh] : meshes) {
@@ -495,8 +492,9 @@ mrtResult Engine::packGeometry(uint32_t& rebuilt) {
             triVerts[slot * 3 + 2] = make_float4(p2.x, p2.y, p2.z, 0.0f);
             triIndex[slot] = make_uint4(i0 + vbase, i1 + vbase, i2 + vbase, lt);
         }
-        for (MrtNode n : b.bvh.nodes) {
-            n.leftOrPrim += ((n.packed >> 2) == 0) ? b.nodeBase : tbase;
+        for (MrtWideNode n : b.bvh.nodes) {
+            n.childBase += b.nodeBase;
+            n.primBase += tbase;
             nodes.push_back(n);
         }
         vbase += uint32_t(mesh.positions.size());
@@ -505,13 +503,13 @@ mrtResult Engine::packGeometry(uint32_t& rebuilt) {
     m_blasNodeCount = uint32_t(nodes.size());
     m_triCount = uint32_t(nt);
     const auto tu = std::chrono::steady_clock::now();
-    // node buffer keeps room for the TLAS (2 * instances + 1) behind the BLAS region
-    const size_t tlasCap = std::max<size_t>(2 * m_scene.instances().size() + 1, 4);
-    MRT_TRY(m_nodes.ensure((nodes.size() + tlasCap) * sizeof(MrtNode)));
+    // node buffer keeps room for the TLAS (at most one wide node per instance) behind the BLAS region
+    const size_t tlasCap = std::max<size_t>(m_scene.instances().size() + 1, 4);
+    MRT_TRY(m_nodes.ensure((nodes.size() + tlasCap) * sizeof(MrtWideNode)));
     if (!nodes.empty())
-        MRT_CUDA(cudaMemcpyAsync(m_nodes.ptr, nodes.data(), nodes.size() * sizeof(MrtNode), cudaMemcpyHostToDevice,
-                                 m_stream));
-    m_stats.commitH2DBytes += nodes.size() * sizeof(MrtNode);
+        MRT_CUDA(cudaMemcpyAsync(m_nodes.ptr, nodes.data(), nodes.size() * sizeof(MrtWideNode),
+                                 cudaMemcpyHostToDevice, m_stream));
+    m_stats.commitH2DBytes += nodes.size() * sizeof(MrtWideNode);
     MRT_TRY(up(m_triVerts, triVerts.data(), triVerts.size() * sizeof(float4)));
     MRT_TRY(up(m_triIndex, triIndex.data(), triIndex.size() * sizeof(uint4)));
     MRT_TRY(up(m_normals, normals.data(), normals.size() * sizeof(V4f)));
@@ -536,9 +534,9 @@ mrtResult Engine::packInstances() {
         boxes.push_back(transformBox(it->second.bvh.bounds, in.o2w));
     }
     const auto tb = std::chrono::steady_clock::now();
-    BvhResult tlas = buildBvh(boxes, 1, 1);
+    WideBvh tlas = collapseToWide(buildBvh(boxes, 1, 1), 1);
     m_stats.commitBvhMs += std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - tb).count();
-    if (tlas.nodes.empty()) tlas.nodes.push_back(sentinelNode());
+    if (tlas.nodes.empty()) tlas.nodes.push_back(emptyNode());
     std::vector<MrtInstance> gi;
     gi.reserve(flat.size());
     for (uint32_t oi : tlas.primOrder) {
@@ -554,23 +552,22 @@ mrtResult Engine::packInstances() {
         gi.push_back(g);
     }
     m_tlasRoot = m_blasNodeCount;
-    for (MrtNode& n : tlas.nodes)
-        if ((n.packed >> 2) == 0) n.leftOrPrim += m_tlasRoot;
+    for (MrtWideNode& n : tlas.nodes) n.childBase += m_tlasRoot;
     m_instanceCount = uint32_t(gi.size());
-    const size_t need = (size_t(m_tlasRoot) + tlas.nodes.size()) * sizeof(MrtNode);
+    const size_t need = (size_t(m_tlasRoot) + tlas.nodes.size()) * sizeof(MrtWideNode);
     if (m_nodes.bytes < need) {
         // instance count outgrew the reserved TLAS room: grow, keeping the BLAS part
         DeviceBuffer bigger;
         MRT_TRY(bigger.ensure(need + need / 2));
-        MRT_CUDA(cudaMemcpyAsync(bigger.ptr, m_nodes.ptr, size_t(m_tlasRoot) * sizeof(MrtNode),
+        MRT_CUDA(cudaMemcpyAsync(bigger.ptr, m_nodes.ptr, size_t(m_tlasRoot) * sizeof(MrtWideNode),
                                  cudaMemcpyDeviceToDevice, m_stream));
         MRT_CUDA(cudaStreamSynchronize(m_stream));
         m_nodes.release();
         m_nodes = bigger;
     }
-    MRT_CUDA(cudaMemcpyAsync(static_cast<MrtNode*>(m_nodes.ptr) + m_tlasRoot, tlas.nodes.data(),
-                             tlas.nodes.size() * sizeof(MrtNode), cudaMemcpyHostToDevice, m_stream));
-    m_stats.commitH2DBytes += tlas.nodes.size() * sizeof(MrtNode);
+    MRT_CUDA(cudaMemcpyAsync(static_cast<MrtWideNode*>(m_nodes.ptr) + m_tlasRoot, tlas.nodes.data(),
+                             tlas.nodes.size() * sizeof(MrtWideNode), cudaMemcpyHostToDevice, m_stream));
+    m_stats.commitH2DBytes += tlas.nodes.size() * sizeof(MrtWideNode);
     m_nodeCount = m_tlasRoot + uint32_t(tlas.nodes.size());
     MRT_TRY(up(m_instances, gi.data(), gi.size() * sizeof(MrtInstance)));
     MRT_CUDA(cudaStreamSynchronize(m_stream));
@@ -757,7 +754,7 @@ void Engine::fillParams(MrtFrameParams& p) const {
     p.instanceCount = m_instanceCount;
     p.triCount = m_triCount;
     p.materialCount = m_materialCount;
-    p.nodes = m_nodes.as<MrtNode>();
+    p.nodes = m_nodes.as<MrtWideNode>();
     p.triVerts = m_triVerts.as<float4>();
     p.triIndex = m_triIndex.as<uint4>();
     p.normals = m_normals.as<float4>();
@@ -851,7 +848,7 @@ mrtResult Engine::renderFrames(uint32_t count, mrtFrameInfo* info) {
         m_stats.surfaceHits = ctr[4];
         m_stats.shadowNodeFetches = ctr[5];
         m_stats.shadowTriTests = ctr[6];
-        m_stats.nodeBytes = sizeof(MrtNode);
+        m_stats.nodeBytes = sizeof(MrtWideNode);
         m_stats.triBytes = 48;
         m_frameIndex += n;
         m_resolveExposure = std::exp2(m_settings.exposureEV);

@@ -13,6 +13,7 @@
 #include "../../../include/mrt_ext.h"
 #include "../common/device_types.h"
 #include "bvh_build.h"
+#include "wide_bvh.h"
 #include "common.h"
 #include "scene.h"
 
@@ -105,7 +106,7 @@ private:
 
     // host-side packing state
     struct Blas {
-        BvhResult bvh;
+        WideBvh bvh;  // 8-wide BVH over the mesh's triangles (object space)
         uint32_t nodeBase = 0;
     };
     std::map<uint32_t, Blas> m_blas;

@@ -1,0 +1,156 @@
+"""The 8-wide compressed BVH (host build through mrtxBuildWideBvh): every
+primitive sits in exactly one leaf, every quantised child box contains its
+subtree under the kernel's decode arithmetic (p + q * 2^(e-127) in float32),
+and a traversal with those boxes reaches the brute-force closest triangle of
+every ray."""
+import numpy as np
+import pytest
+
+import miniraytrace_b200 as mrt
+
+
+def scale_of(e):
+    return (np.uint32(e) << np.uint32(23)).view(np.float32)
+
+
+def decode(node, slot):
+    p = node["p"].astype(np.float32)
+    s = np.array([scale_of(node["e"][a]) for a in range(3)], np.float32)
+    lo = p + node["qlo"][:, slot].astype(np.float32) * s
+    hi = p + node["qhi"][:, slot].astype(np.float32) * s
+    return lo.astype(np.float32), hi.astype(np.float32)
+
+
+def children(node):
+    out = []
+    internal_rank = 0
+    for slot in range(8):
+        m = int(node["meta"][slot])
+        if m == 0:
+            continue
+        if (int(node["imask"]) >> slot) & 1:
+            out.append((slot, "node", int(node["childBase"]) + internal_rank))
+            internal_rank += 1
+        else:
+            n = bin(m >> 5).count("1")
+            off = m & 31
+            out.append((slot, "leaf", (int(node["primBase"]) + off, n)))
+    return out
+
+
+def subtree_prims(nodes, order, idx):
+    prims = []
+    stack = [idx]
+    while stack:
+        nd = nodes[stack.pop()]
+        for slot, kind, ref in children(nd):
+            if kind == "node":
+                stack.append(ref)
+            else:
+                prims.extend(order[ref[0]:ref[0] + ref[1]].tolist())
+    return prims
+
+
+def tri_soup(n, seed):
+    rng = np.random.default_rng(seed)
+    base = rng.uniform(-10, 10, (n, 3))
+    tris = np.stack([base, base + rng.uniform(-0.8, 0.8, (n, 3)), base + rng.uniform(-0.8, 0.8, (n, 3))], 1)
+    return tris.astype(np.float32)
+
+
+@pytest.mark.parametrize("leaf", [1, 3])
+def test_structure_and_conservative_boxes(mrt_lib, leaf):
+    tris = tri_soup(3000, 4)
+    boxes = np.concatenate([tris.min(1), tris.max(1)], 1)
+    nodes, order = mrt.build_wide_bvh(boxes, leaf)
+    assert sorted(order.tolist()) == list(range(len(tris)))
+    seen = np.zeros(len(tris), int)
+    for ni, nd in enumerate(nodes):
+        kids = children(nd)
+        assert 1 <= len(kids) <= 8
+        for slot, kind, ref in kids:
+            lo, hi = decode(nd, slot)
+            if kind == "node":
+                assert ref < len(nodes)
+                prims = subtree_prims(nodes, order, ref)
+            else:
+                start, n = ref
+                assert 1 <= n <= leaf and (int(nd["meta"][slot]) & 31) < 24
+                prims = order[start:start + n].tolist()
+                seen[prims] += 1
+            pb = boxes[prims]
+            assert (lo <= pb[:, :3]).all() and (hi >= pb[:, 3:]).all(), (ni, slot)
+    assert (seen == 1).all()
+
+
+def moller_trumbore(o, d, tri):
+    e1, e2 = tri[1] - tri[0], tri[2] - tri[0]
+    p = np.cross(d, e2)
+    det = e1 @ p
+    if abs(det) < 1e-12:
+        return None
+    inv = 1.0 / det
+    s = o - tri[0]
+    u = (s @ p) * inv
+    if u < 0 or u > 1:
+        return None
+    q = np.cross(s, e1)
+    v = (d @ q) * inv
+    if v < 0 or u + v > 1:
+        return None
+    t = (e2 @ q) * inv
+    return t if t > 1e-4 else None
+
+
+def test_traversal_reaches_closest_hit(mrt_lib):
+    tris = tri_soup(600, 9).astype(np.float64)
+    boxes = np.concatenate([tris.min(1), tris.max(1)], 1).astype(np.float32)
+    nodes, order = mrt.build_wide_bvh(boxes, 3)
+    rng = np.random.default_rng(3)
+    checked = 0
+    for _ in range(150):
+        o = rng.uniform(-12, 12, 3)
+        target = tris[rng.integers(len(tris))].mean(0) + rng.normal(scale=0.2, size=3)
+        d = target - o
+        d /= np.linalg.norm(d)
+        best, best_t = None, np.inf
+        for i, tri in enumerate(tris):
+            t = moller_trumbore(o, d, tri)
+            if t is not None and t < best_t:
+                best, best_t = i, t
+        if best is None:
+            continue
+        # walk every node whose decoded box the ray enters before best_t
+        inv = 1.0 / np.where(d == 0, 1e-30, d)
+        reached = set()
+        stack = [0]
+        while stack:
+            nd = nodes[stack.pop()]
+            for slot, kind, ref in children(nd):
+                lo, hi = decode(nd, slot)
+                t0, t1 = (lo - o) * inv, (hi - o) * inv
+                te = max(np.minimum(t0, t1).max(), 0.0)
+                tx = min(np.maximum(t0, t1).min(), best_t * (1 + 1e-6))
+                if te > tx:
+                    continue
+                if kind == "node":
+                    stack.append(ref)
+                else:
+                    reached.update(order[ref[0]:ref[0] + ref[1]].tolist())
+        assert best in reached
+        checked += 1
+    assert checked > 40
+
+
+def test_degenerate_inputs(mrt_lib):
+    nodes, order = mrt.build_wide_bvh(np.zeros((0, 6), np.float32))
+    assert len(nodes) == 0
+    nodes, order = mrt.build_wide_bvh(np.array([[0, 0, 0, 1, 1, 1]], np.float32))
+    assert len(nodes) == 1 and list(order) == [0]
+    same = np.tile(np.array([[1, 2, 3, 1, 2, 3]], np.float32), (100, 1))
+    nodes, order = mrt.build_wide_bvh(same)
+    assert sorted(order.tolist()) == list(range(100))
+    # flat boxes (a heightfield seen from above has no thickness in leaves)
+    flat = np.array([[i, 0, j, i + 1, 0, j + 1] for i in range(10) for j in range(10)], np.float32)
+    nodes, order = mrt.build_wide_bvh(flat)
+    assert sorted(order.tolist()) == list(range(100))
