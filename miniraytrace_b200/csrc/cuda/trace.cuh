@@ -11,11 +11,14 @@
 //   - 8-wide compressed BVH nodes (five 128-bit loads test eight child
 //     boxes), traversed by groups: a stack entry is a node's remaining
 //     child-hit mask, children are taken in ray-octant order, leaf
-//     triangles of a node are tested before descending;
-//   - box exits are widened by 1 + 2*gamma(3) = 1 + 3 * 2^-23 (Ize 2013) so a
-//     rounding error in the slab test can never cull a real hit (the
-//     reference's exact-comparison slab test occasionally drops a hit or an
-//     occluder whose point lies on its leaf box's face);
+//     triangles of a node are tested before descending; TLAS and BLAS share
+//     one loop and one stack;
+//   - a conservative slab test: box planes are exact reals on a power-of-two
+//     grid and every rounding of the slab arithmetic is covered by a margin
+//     derived per node (see slabAxis), so no child box the ray really
+//     enters is culled (the reference's exact-comparison slab test
+//     occasionally drops a hit or an occluder whose point lies on its leaf
+//     box's face);
 //   - stacks are bounded and an overflow sets an error flag instead of
 //     writing out of bounds; node, triangle and instance indices are checked.
 #pragma once
@@ -169,24 +172,52 @@ struct TraversalCounters {
     bool bad = false;
 };
 
-// Decoded hits of one wide node.
-struct WideHits {
+// Child-hit masks of one wide node.
+struct WideGroup {
     uint32_t childBase;  // first internal child node
     uint32_t primBase;   // first leaf primitive
     uint32_t nodeBits;   // bits 24-31: internal children hit (ray-ordered), bits 0-7: internal slot mask
     uint32_t primBits;   // bits 0-23: leaf primitives hit, relative to primBase
 };
 
-// Exact float of a byte: 2^23 + b - 2^23.
-MRT_DEV float byteToFloat(uint32_t b) { return __uint_as_float(0x4B000000u | b) - 8388608.0f; }
+// Slab offsets of one node axis for one ray. The planes of the axis are the
+// exact reals P_q = p + q*s (s = 2^(e-127), q = 0..255); the ray meets P_q at
+//   t_q = (P_q - o) * inv = F_q * a + c,  F_q = 2^23 + 256 q,
+//   a = s * inv / 256 (exact),  c = (p - o) * inv - 2^23 * a,
+// one byte permute and one FMA per plane in the child loop. The float
+// evaluation of t_q differs from the real value by less than
+//   2 eps |(p-o) inv| + eps |c| (offsets)  +  2 eps (2^24 |a| + |c|)
+// (final rounding and the rounding of inv itself), eps = 2^-24; `err` is 5 eps
+// times the sum of the three magnitudes, plus 1e-37 for subnormal a. Near
+// planes take c - err and far planes c + err, so the computed entry never
+// exceeds the real entry and the computed exit never falls below the real
+// exit: no child the ray really enters is culled. Overflow (|inv| = 1e30 on
+// a huge node) yields inf or NaN, and the NaN-ignoring min/max treat those
+// planes as unbounded, which is again conservative.
+MRT_DEV void slabAxis(float p, uint32_t e, float o, float inv, float& a, float& cNear, float& cFar) {
+    a = __fmul_rn(__uint_as_float(e << 23), __fmul_rn(inv, 0.00390625f));
+    const float b = __fmul_rn(__fsub_rn(p, o), inv);
+    const float c = __fmaf_rn(-8388608.0f, a, b);
+    const float mag = __fmaf_rn(16777216.0f, fabsf(a), __fadd_rn(fabsf(b), fabsf(c)));
+    const float err = __fmaf_rn(mag, 2.9802322e-7f, 1e-37f);
+    cNear = __fsub_rn(c, err);
+    cFar = __fadd_rn(c, err);
+}
 
-// Tests the ray against the eight quantised child boxes of node `idx`.
-// Child boxes decode as p + q * 2^(e-127) (the host quantised them
-// conservatively for exactly this arithmetic); internal-child hits land on
-// bit 24 + (slot XOR oct), so taking bits from the top visits the slots the
-// ray reaches first first.
-MRT_DEV WideHits intersectWide(const MrtFrameParams& P, uint32_t idx, float3 o, float3 inv, uint32_t oct, float tMax,
-                               TraversalCounters& tc) {
+// F_q of byte j of a quantised-plane word: 0x4B0000 | q << 8 = 2^23 + 256 q.
+template <int j>
+MRT_DEV float planeF(uint32_t w) {
+    return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7404u | (uint32_t(j) << 4)));
+}
+
+// Tests the ray against the eight quantised child boxes of node `idx`
+// (record layout in MrtWideNode). Per child: six planes, three max, three
+// min, one compare. A hit adds the child's meta bits at its bit index:
+// internal children at 24 + (slot XOR oct), so taking bits from the top
+// visits the slots the ray reaches first first; leaves at their primitive
+// offset. Empty slots have meta 0 and add nothing.
+MRT_DEV WideGroup intersectWide(const MrtFrameParams& P, uint32_t idx, float3 o, float3 inv, uint32_t oct, float tMax,
+                                TraversalCounters& tc) {
     if (idx >= P.nodeCount) {
         tc.bad = true;
         idx = 0;
@@ -195,48 +226,52 @@ MRT_DEV WideHits intersectWide(const MrtFrameParams& P, uint32_t idx, float3 o, 
     const float4 q0 = ldg4(q), q1 = ldg4(q + 1), q2 = ldg4(q + 2), q3 = ldg4(q + 3), q4 = ldg4(q + 4);
     tc.nodes++;
     const uint32_t eb = __float_as_uint(q0.w);
-    const float sx = __uint_as_float((eb & 0xffu) << 23), sy = __uint_as_float(((eb >> 8) & 0xffu) << 23),
-                sz = __uint_as_float(((eb >> 16) & 0xffu) << 23);
-    const uint32_t imask = eb >> 24;
-    WideHits h;
-    h.childBase = __float_as_uint(q1.x);
-    h.primBase = __float_as_uint(q1.y);
-    h.nodeBits = imask;
-    h.primBits = 0;
-    const uint32_t meta[2] = {__float_as_uint(q1.z), __float_as_uint(q1.w)};
-    const uint32_t lx[2] = {__float_as_uint(q2.x), __float_as_uint(q2.y)};
-    const uint32_t ly[2] = {__float_as_uint(q2.z), __float_as_uint(q2.w)};
-    const uint32_t lz[2] = {__float_as_uint(q3.x), __float_as_uint(q3.y)};
-    const uint32_t hx[2] = {__float_as_uint(q3.z), __float_as_uint(q3.w)};
-    const uint32_t hy[2] = {__float_as_uint(q4.x), __float_as_uint(q4.y)};
-    const uint32_t hz[2] = {__float_as_uint(q4.z), __float_as_uint(q4.w)};
+    float ax, nx, fx, ay, ny, fy, az, nz, fz;
+    slabAxis(q0.x, eb & 0xffu, o.x, inv.x, ax, nx, fx);
+    slabAxis(q0.y, (eb >> 8) & 0xffu, o.y, inv.y, ay, ny, fy);
+    slabAxis(q0.z, (eb >> 16) & 0xffu, o.z, inv.z, az, nz, fz);
+    // a negative reciprocal makes the hi plane the near one
+    const bool swx = inv.x < 0.0f, swy = inv.y < 0.0f, swz = inv.z < 0.0f;
+    // tolerance of the triangle test's t against the box exit (the reference
+    // accepts hits by its own t, so a box must not be culled at the margin)
+    const float tMaxF = __fmul_rn(tMax, 1.000001f);
+    const uint32_t oct4 = oct * 0x01010101u;
+    uint32_t hits = 0;
 #pragma unroll
     for (int half = 0; half < 2; ++half) {
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const uint32_t sh = 8u * uint32_t(j);
-            const uint32_t m = (meta[half] >> sh) & 0xffu;
-            if (m == 0u) continue;
-            const float bx0 = q0.x + byteToFloat((lx[half] >> sh) & 0xffu) * sx;
-            const float by0 = q0.y + byteToFloat((ly[half] >> sh) & 0xffu) * sy;
-            const float bz0 = q0.z + byteToFloat((lz[half] >> sh) & 0xffu) * sz;
-            const float bx1 = q0.x + byteToFloat((hx[half] >> sh) & 0xffu) * sx;
-            const float by1 = q0.y + byteToFloat((hy[half] >> sh) & 0xffu) * sy;
-            const float bz1 = q0.z + byteToFloat((hz[half] >> sh) & 0xffu) * sz;
-            const float tx0 = (bx0 - o.x) * inv.x, tx1 = (bx1 - o.x) * inv.x;
-            const float ty0 = (by0 - o.y) * inv.y, ty1 = (by1 - o.y) * inv.y;
-            const float tz0 = (bz0 - o.z) * inv.z, tz1 = (bz1 - o.z) * inv.z;
-            const float tEnter = fmaxf(fmaxf(fminf(tx0, tx1), fminf(ty0, ty1)), fmaxf(fminf(tz0, tz1), 0.0f));
-            const float tExit =
-                fminf(fminf(fmaxf(tx0, tx1), fmaxf(ty0, ty1)), fminf(fmaxf(tz0, tz1), tMax)) * 1.00000036f;
-            if (tEnter <= tExit) {
-                const uint32_t slot = uint32_t(half * 4 + j);
-                if ((imask >> slot) & 1u) h.nodeBits |= 1u << ((m & 31u) ^ oct);
-                else h.primBits |= (m >> 5) << (m & 31u);
-            }
+        const uint32_t lx = __float_as_uint(half ? q2.y : q2.x), ly = __float_as_uint(half ? q2.w : q2.z);
+        const uint32_t lz = __float_as_uint(half ? q3.y : q3.x), hx = __float_as_uint(half ? q3.w : q3.z);
+        const uint32_t hy = __float_as_uint(half ? q4.y : q4.x), hz = __float_as_uint(half ? q4.w : q4.z);
+        const uint32_t wnx = swx ? hx : lx, wfx = swx ? lx : hx;
+        const uint32_t wny = swy ? hy : ly, wfy = swy ? ly : hy;
+        const uint32_t wnz = swz ? hz : lz, wfz = swz ? lz : hz;
+        // meta of four slots: internal children (low five bits 24..31) get
+        // their bit index XORed with the octant; leaves keep their offset
+        const uint32_t m4 = __float_as_uint(half ? q1.w : q1.z);
+        const uint32_t inner4 = (m4 & (m4 << 1)) & 0x10101010u;
+        const uint32_t bitIndex4 = (m4 ^ (oct4 & ((inner4 >> 4) * 0xffu))) & 0x1f1f1f1fu;
+        const uint32_t childBits4 = (m4 >> 5) & 0x07070707u;
+#define MRT_WIDE_CHILD(j)                                                                                   \
+        {                                                                                                   \
+            const float tnx = __fmaf_rn(planeF<j>(wnx), ax, nx), tfx = __fmaf_rn(planeF<j>(wfx), ax, fx);  \
+            const float tny = __fmaf_rn(planeF<j>(wny), ay, ny), tfy = __fmaf_rn(planeF<j>(wfy), ay, fy);  \
+            const float tnz = __fmaf_rn(planeF<j>(wnz), az, nz), tfz = __fmaf_rn(planeF<j>(wfz), az, fz);  \
+            const float tEnter = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, 0.0f));                                 \
+            const float tExit = fminf(fminf(tfx, tfy), fminf(tfz, tMaxF));                                 \
+            if (tEnter <= tExit) hits |= ((childBits4 >> (8 * j)) & 7u) << ((bitIndex4 >> (8 * j)) & 31u); \
         }
+        MRT_WIDE_CHILD(0)
+        MRT_WIDE_CHILD(1)
+        MRT_WIDE_CHILD(2)
+        MRT_WIDE_CHILD(3)
+#undef MRT_WIDE_CHILD
     }
-    return h;
+    WideGroup g;
+    g.childBase = __float_as_uint(q1.x);
+    g.primBase = __float_as_uint(q1.y);
+    g.nodeBits = (hits & 0xff000000u) | (eb >> 24);
+    g.primBits = hits & 0x00ffffffu;
+    return g;
 }
 
 // Ray octant for child ordering: bit k set when direction component k > 0.
@@ -248,43 +283,82 @@ MRT_DEV uint32_t childIndex(uint32_t childBase, uint32_t imask, uint32_t b, uint
     return childBase + uint32_t(__popc(imask & ((1u << slot) - 1u)));
 }
 
-#define MRT_WIDE_STACK 32
-#define MRT_WIDE_TLAS_STACK 16
+// Traversal stack entries (node groups), shared by the TLAS and the BLAS
+// being walked.
+#define MRT_WIDE_STACK 48
 
-// Closest hit within one BLAS (object-space ray). Updates tMax and hit.
-// Returns false on a stack overflow or an exhausted visit budget.
-MRT_DEV bool closestBlas(const MrtFrameParams& P, uint32_t root, uint32_t inst, float3 o, float3 d, float& tMax,
-                         HitRecord& hit, TraversalCounters& tc) {
-    const float3 inv = safeInv(d);
-    const Shear sh = makeShear(d);
-    const uint32_t oct = rayOctant(d);
-    uint2 stack[MRT_WIDE_STACK];
+// Two-level traversal in one loop (reference intersect.glsl:88-178): the
+// TLAS's leaf primitives are instances; on an instance the TLAS group is
+// parked, the ray is taken into object space and the instance's BLAS is
+// walked on top of the same stack, and the TLAS group resumes when the stack
+// is back at the depth it had on entry. One node test serves both levels.
+// kAny: stops at the first triangle with t in (1e-4, tMax) and returns true.
+// Otherwise: closest hit, tMax and `hit` updated. `ok` is cleared on a stack
+// overflow or an exhausted visit budget.
+template <bool kAny>
+MRT_DEV bool traceWide(const MrtFrameParams& P, float3 wo, float3 wd, float& tMax, HitRecord& hit, bool& ok,
+                       TraversalCounters& tc) {
+    if (P.instanceCount == 0) return false;  // empty scene (the TLAS root is a placeholder)
+    float3 o = wo;
+    float3 inv = safeInv(wd);
+    uint32_t oct = rayOctant(wd);
+    Shear sh = {0, 1, 2, 0.0f, 0.0f, 0.0f};  // set on BLAS entry
+    WideGroup g = {P.tlasRoot, 0u, 0x80000000u, 0u};  // a group whose only hit is the root
+    WideGroup parked = {0u, 0u, 0u, 0u};
+    uint32_t inst = 0;
+    int blasBase = -1;  // stack depth at BLAS entry; -1 while in the TLAS
     int sp = 0;
-    bool ok = true;
-    WideHits g = intersectWide(P, root, o, inv, oct, tMax, tc);
+    uint2 stack[MRT_WIDE_STACK];
     uint32_t visits = 0;
     for (;;) {
-        if (++visits > MRT_MAX_VISITS) return false;
-        while (g.primBits) {
-            const uint32_t b = uint32_t(__ffs(g.primBits) - 1);
-            g.primBits &= g.primBits - 1u;
-            const uint32_t tri = g.primBase + b;
-            ++tc.tris;
-            if (tri >= P.triCount) {
-                tc.bad = true;
+        if (g.primBits) {
+            if (blasBase >= 0) {
+                do {
+                    const uint32_t b = uint32_t(__ffs(g.primBits) - 1);
+                    g.primBits &= g.primBits - 1u;
+                    const uint32_t tri = g.primBase + b;
+                    ++tc.tris;
+                    if (tri >= P.triCount) {
+                        tc.bad = true;
+                        continue;
+                    }
+                    float t, u, v;
+                    if (hitTriangle(P.triVerts, tri, o, sh, tMax, t, u, v)) {
+                        if (kAny) return true;
+                        tMax = t;
+                        hit.t = t;
+                        hit.u = u;
+                        hit.v = v;
+                        hit.tri = tri;
+                        hit.inst = inst;
+                    }
+                } while (g.primBits);
+            } else {
+                const uint32_t b = uint32_t(__ffs(g.primBits) - 1);
+                g.primBits &= g.primBits - 1u;
+                const uint32_t instIdx = g.primBase + b;
+                if (instIdx >= P.instanceCount) {
+                    tc.bad = true;
+                    continue;
+                }
+                const MrtInstance* in = P.instances + instIdx;
+                parked = g;
+                blasBase = sp;
+                inst = instIdx;
+                o = xformPoint(in->w2o, wo);
+                const float3 d = xformDir(in->w2o, wd);
+                inv = safeInv(d);
+                oct = rayOctant(d);
+                sh = makeShear(d);
+                g = {in->blasRoot, 0u, 0x80000000u, 0u};
                 continue;
-            }
-            float t, u, v;
-            if (hitTriangle(P.triVerts, tri, o, sh, tMax, t, u, v)) {
-                tMax = t;
-                hit.t = t;
-                hit.u = u;
-                hit.v = v;
-                hit.tri = tri;
-                hit.inst = inst;
             }
         }
         if (g.nodeBits & 0xff000000u) {
+            if (++visits > MRT_MAX_VISITS) {
+                ok = false;
+                return false;
+            }
             const uint32_t b = 31u - uint32_t(__clz(g.nodeBits & 0xff000000u));
             const uint32_t rest = g.nodeBits & ~(1u << b);
             const uint32_t child = childIndex(g.childBase, g.nodeBits & 0xffu, b, oct);
@@ -295,7 +369,15 @@ MRT_DEV bool closestBlas(const MrtFrameParams& P, uint32_t root, uint32_t inst, 
             g = intersectWide(P, child, o, inv, oct, tMax, tc);
             continue;
         }
-        if (sp == 0) return ok;
+        if (sp == blasBase) {  // BLAS finished: resume the parked TLAS group
+            g = parked;
+            blasBase = -1;
+            o = wo;
+            inv = safeInv(wd);
+            oct = rayOctant(wd);
+            continue;
+        }
+        if (sp == 0) return false;
         const uint2 e = stack[--sp];
         g.childBase = e.x;
         g.nodeBits = e.y;
@@ -303,143 +385,21 @@ MRT_DEV bool closestBlas(const MrtFrameParams& P, uint32_t root, uint32_t inst, 
     }
 }
 
-// Closest hit over the scene (reference intersect.glsl:88-125): the TLAS's
-// leaf primitives are instances; each hit instance's BLAS is walked with the
-// ray in its object space.
+// Closest hit over the scene; t and barycentrics of the winner re-evaluated
+// with the reference's arithmetic. Returns false on a traversal error.
 MRT_DEV bool traceClosest(const MrtFrameParams& P, float3 o, float3 d, float tMax, HitRecord& hit, TraversalCounters& tc) {
     hit.t = tMax;
     hit.tri = 0xffffffffu;
     hit.inst = 0;
     hit.u = hit.v = 0.0f;
-    if (P.instanceCount == 0) return true;  // empty scene (the TLAS root is a placeholder)
-    const float3 inv = safeInv(d);
-    const uint32_t oct = rayOctant(d);
-    uint2 stack[MRT_WIDE_TLAS_STACK];
-    int sp = 0;
     bool ok = true;
-    WideHits g = intersectWide(P, P.tlasRoot, o, inv, oct, tMax, tc);
-    uint32_t visits = 0;
-    for (;;) {
-        if (++visits > MRT_MAX_VISITS) return false;
-        while (g.primBits) {
-            const uint32_t b = uint32_t(__ffs(g.primBits) - 1);
-            g.primBits &= g.primBits - 1u;
-            const uint32_t instIdx = g.primBase + b;
-            if (instIdx >= P.instanceCount) {
-                tc.bad = true;
-                continue;
-            }
-            const MrtInstance* in = P.instances + instIdx;
-            const float3 oo = xformPoint(in->w2o, o), dd = xformDir(in->w2o, d);
-            ok &= closestBlas(P, in->blasRoot, instIdx, oo, dd, tMax, hit, tc);
-        }
-        if (g.nodeBits & 0xff000000u) {
-            const uint32_t b = 31u - uint32_t(__clz(g.nodeBits & 0xff000000u));
-            const uint32_t rest = g.nodeBits & ~(1u << b);
-            const uint32_t child = childIndex(g.childBase, g.nodeBits & 0xffu, b, oct);
-            if (rest & 0xff000000u) {
-                if (sp < MRT_WIDE_TLAS_STACK) stack[sp++] = make_uint2(g.childBase, rest);
-                else ok = false;
-            }
-            g = intersectWide(P, child, o, inv, oct, tMax, tc);
-            continue;
-        }
-        if (sp == 0) break;
-        const uint2 e = stack[--sp];
-        g.childBase = e.x;
-        g.nodeBits = e.y;
-        g.primBits = 0;
-    }
+    traceWide<false>(P, o, d, tMax, hit, ok, tc);
     if (hit.tri != 0xffffffffu) refineHit(P, o, d, hit);
     return ok;
 }
 
-// Any hit in (1e-4, tMax) within one BLAS (reference intersect.glsl:128-178).
-MRT_DEV bool anyBlas(const MrtFrameParams& P, uint32_t root, float3 o, float3 d, float tMax, bool& ok,
-                     TraversalCounters& tc) {
-    const float3 inv = safeInv(d);
-    const Shear sh = makeShear(d);
-    const uint32_t oct = rayOctant(d);
-    uint2 stack[MRT_WIDE_STACK];
-    int sp = 0;
-    WideHits g = intersectWide(P, root, o, inv, oct, tMax, tc);
-    uint32_t visits = 0;
-    for (;;) {
-        if (++visits > MRT_MAX_VISITS) {
-            ok = false;
-            return false;
-        }
-        while (g.primBits) {
-            const uint32_t b = uint32_t(__ffs(g.primBits) - 1);
-            g.primBits &= g.primBits - 1u;
-            const uint32_t tri = g.primBase + b;
-            ++tc.tris;
-            if (tri >= P.triCount) {
-                tc.bad = true;
-                continue;
-            }
-            float t, u, v;
-            if (hitTriangle(P.triVerts, tri, o, sh, tMax, t, u, v)) return true;
-        }
-        if (g.nodeBits & 0xff000000u) {
-            const uint32_t b = 31u - uint32_t(__clz(g.nodeBits & 0xff000000u));
-            const uint32_t rest = g.nodeBits & ~(1u << b);
-            const uint32_t child = childIndex(g.childBase, g.nodeBits & 0xffu, b, oct);
-            if (rest & 0xff000000u) {
-                if (sp < MRT_WIDE_STACK) stack[sp++] = make_uint2(g.childBase, rest);
-                else ok = false;
-            }
-            g = intersectWide(P, child, o, inv, oct, tMax, tc);
-            continue;
-        }
-        if (sp == 0) return false;
-        const uint2 e = stack[--sp];
-        g.childBase = e.x;
-        g.nodeBits = e.y;
-        g.primBits = 0;
-    }
-}
-
+// Any hit in (1e-4, tMax) (reference intersect.glsl:128-178).
 MRT_DEV bool traceAny(const MrtFrameParams& P, float3 o, float3 d, float tMax, bool& ok, TraversalCounters& tc) {
-    if (P.instanceCount == 0) return false;  // empty scene
-    const float3 inv = safeInv(d);
-    const uint32_t oct = rayOctant(d);
-    uint2 stack[MRT_WIDE_TLAS_STACK];
-    int sp = 0;
-    WideHits g = intersectWide(P, P.tlasRoot, o, inv, oct, tMax, tc);
-    uint32_t visits = 0;
-    for (;;) {
-        if (++visits > MRT_MAX_VISITS) {
-            ok = false;
-            return false;
-        }
-        while (g.primBits) {
-            const uint32_t b = uint32_t(__ffs(g.primBits) - 1);
-            g.primBits &= g.primBits - 1u;
-            const uint32_t instIdx = g.primBase + b;
-            if (instIdx >= P.instanceCount) {
-                tc.bad = true;
-                continue;
-            }
-            const MrtInstance* in = P.instances + instIdx;
-            const float3 oo = xformPoint(in->w2o, o), dd = xformDir(in->w2o, d);
-            if (anyBlas(P, in->blasRoot, oo, dd, tMax, ok, tc)) return true;
-        }
-        if (g.nodeBits & 0xff000000u) {
-            const uint32_t b = 31u - uint32_t(__clz(g.nodeBits & 0xff000000u));
-            const uint32_t rest = g.nodeBits & ~(1u << b);
-            const uint32_t child = childIndex(g.childBase, g.nodeBits & 0xffu, b, oct);
-            if (rest & 0xff000000u) {
-                if (sp < MRT_WIDE_TLAS_STACK) stack[sp++] = make_uint2(g.childBase, rest);
-                else ok = false;
-            }
-            g = intersectWide(P, child, o, inv, oct, tMax, tc);
-            continue;
-        }
-        if (sp == 0) return false;
-        const uint2 e = stack[--sp];
-        g.childBase = e.x;
-        g.nodeBits = e.y;
-        g.primBits = 0;
-    }
+    HitRecord unused;
+    return traceWide<true>(P, o, d, tMax, unused, ok, tc);
 }

@@ -1,8 +1,8 @@
 """The 8-wide compressed BVH (host build through mrtxBuildWideBvh): every
 primitive sits in exactly one leaf, every quantised child box contains its
-subtree under the kernel's decode arithmetic (p + q * 2^(e-127) in float32),
-and a traversal with those boxes reaches the brute-force closest triangle of
-every ray."""
+subtree (planes are the exact reals p + q * 2^(e-127), p a multiple of the
+scale), nodes are well filled, and a traversal with those boxes reaches the
+brute-force closest triangle of every ray."""
 import numpy as np
 import pytest
 
@@ -10,15 +10,23 @@ import miniraytrace_b200 as mrt
 
 
 def scale_of(e):
-    return (np.uint32(e) << np.uint32(23)).view(np.float32)
+    return np.ldexp(1.0, int(e) - 127)
+
+
+def grid(node):
+    """Per axis: scale and the grid index k of the origin (p = k * s)."""
+    s = np.array([scale_of(node["e"][a]) for a in range(3)])
+    k = node["p"].astype(np.float64) / s
+    assert (k == np.floor(k)).all()
+    return s, k
 
 
 def decode(node, slot):
-    p = node["p"].astype(np.float32)
-    s = np.array([scale_of(node["e"][a]) for a in range(3)], np.float32)
-    lo = p + node["qlo"][:, slot].astype(np.float32) * s
-    hi = p + node["qhi"][:, slot].astype(np.float32) * s
-    return lo.astype(np.float32), hi.astype(np.float32)
+    # exact in float64 for the grid sizes these tests build
+    s, k = grid(node)
+    lo = (k + node["qlo"][:, slot]) * s
+    hi = (k + node["qhi"][:, slot]) * s
+    return lo, hi
 
 
 def children(node):
@@ -78,9 +86,16 @@ def test_structure_and_conservative_boxes(mrt_lib, leaf):
                 assert 1 <= n <= leaf and (int(nd["meta"][slot]) & 31) < 24
                 prims = order[start:start + n].tolist()
                 seen[prims] += 1
-            pb = boxes[prims]
-            assert (lo <= pb[:, :3]).all() and (hi >= pb[:, 3:]).all(), (ni, slot)
+            pb = boxes[prims].astype(np.float64)
+            s, k = grid(nd)
+            # grid-index comparison: exact for any float coordinates
+            assert (k + nd["qlo"][:, slot] <= pb[:, :3] / s).all(), (ni, slot)
+            assert (k + nd["qhi"][:, slot] >= pb[:, 3:] / s).all(), (ni, slot)
     assert (seen == 1).all()
+    # the SAH collapse fills nodes: well above the two or three children a
+    # collapse that only opens oversized subtrees leaves
+    fill = np.mean([len(children(nd)) for nd in nodes])
+    assert fill > 5.0, fill
 
 
 def moller_trumbore(o, d, tri):
