@@ -117,6 +117,44 @@ MRT_API mrtResult mrtxCopyAccumulationDevice(mrtEngine*, void* devPtr, size_t by
 MRT_API mrtResult mrtxBuildWideBvh(const float* aabbs, uint32_t count, uint32_t maxLeafPrims, void* nodesOut,
                                    uint32_t nodeCapacity, uint32_t* primOrderOut, uint32_t* nodeCountOut);
 
+/* Largest map height mrtxBuildEnvCdfNoAlloc accepts. */
+#define MRTX_ENV_CDF_NOALLOC_MAX_HEIGHT 8192u
+
+/* The environment importance-sampling CDF of mrtxBuildEnvCdf, computed from
+ * and into memory the caller already owns on the GPU, without allocating
+ * any device memory. No counterpart in the reference (its CDF is built on
+ * the host inside scene upload, Renderer.cpp:620-655).
+ *
+ * Who needs it: a caller whose device memory is all handed out by its own
+ * pool or budget (a host application that has reserved the GPU's memory,
+ * or a framework whose allocator owns it) cannot let a library call
+ * cudaMalloc behind its back, and a caller with latency-critical work on
+ * other streams cannot afford cudaFree, which synchronises the whole
+ * device. mrtxBuildEnvCdf grows engine-owned buffers as needed; this entry
+ * point takes no engine and keeps its scratch (row sums, the sin(theta)
+ * table, row reciprocals) in a fixed 128 KiB array compiled into the
+ * library, so maps are limited to MRTX_ENV_CDF_NOALLOC_MAX_HEIGHT rows
+ * (any width); a taller map fails with MRT_ERROR_INVALID_ARGUMENT.
+ *
+ *   devTexels       w*h RGBA32F texels (16 bytes each), device memory
+ *   devCdfOut       w*h + h floats, device memory: the same layout and
+ *                   values mrtxBuildEnvCdf returns in cdfOut
+ *   devIntegralOut  one float, device memory
+ *   stream          a cudaStream_t on the GPU that owns devTexels, or NULL
+ *                   for that GPU's legacy default stream
+ *
+ * All three pointers must be device (or managed) memory of one GPU; the
+ * work runs on that GPU and is asynchronous: results are complete when
+ * `stream` reaches the point of this call. The first call on each GPU does
+ * a one-time set-up (it looks up the scratch array's device address with
+ * cudaGetSymbolAddress and loads the kernels); make that first call before
+ * any stream capture. The scratch is shared by every call on a GPU: calls
+ * that overlap in time (other threads, other streams) race and corrupt
+ * each other's results, so serialise them. Nothing in the scratch has to
+ * be cleared between calls. */
+MRT_API mrtResult mrtxBuildEnvCdfNoAlloc(const float* devTexels, uint32_t w, uint32_t h, float* devCdfOut,
+                                         float* devIntegralOut, void* stream);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif

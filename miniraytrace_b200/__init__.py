@@ -307,6 +307,17 @@ class Engine:
                "mrtxCopyAccumulationDevice")
 
 
+def build_env_cdf_no_alloc(dev_texels: int, width: int, height: int, dev_cdf: int, dev_integral: int,
+                           stream: int = 0):
+    """mrtxBuildEnvCdfNoAlloc over device pointers (integers): texels
+    width*height RGBA32F, cdf width*height + height floats, integral one
+    float, all on one GPU; stream a cudaStream_t handle (0 = legacy default
+    stream). Asynchronous on that stream; allocates no device memory."""
+    lib = load_library()
+    _check(lib.mrtxBuildEnvCdfNoAlloc(C.c_void_p(dev_texels), width, height, C.c_void_p(dev_cdf),
+                                      C.c_void_p(dev_integral), C.c_void_p(stream)), "mrtxBuildEnvCdfNoAlloc")
+
+
 def build_wide_bvh(aabbs, max_leaf_prims=3):
     """Host build of the engine's 8-wide BVH over (N, 6) boxes:
     (nodes as a WIDE_NODE_DTYPE array, primitive order)."""

@@ -173,7 +173,11 @@ FUNCTIONS = [
     ("mrtxCopyAccumulationDevice", C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, C.c_int32]),
     ("mrtxBuildWideBvh", C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p,
                                    C.POINTER(C.c_uint32)]),
+    ("mrtxBuildEnvCdfNoAlloc", C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p]),
 ]
+
+# mrtxBuildEnvCdfNoAlloc's height limit (MRTX_ENV_CDF_NOALLOC_MAX_HEIGHT)
+ENV_CDF_NOALLOC_MAX_HEIGHT = 8192
 
 # numpy dtype of one 80-byte MrtWideNode
 WIDE_NODE_DTYPE = [("p", "<f4", 3), ("e", "u1", 3), ("imask", "u1"), ("childBase", "<u4"), ("primBase", "<u4"),

@@ -36,6 +36,14 @@ cudaError_t mrtcu_trace_any(const MrtFrameParams* p, const MrtQueryRay* rays, ui
 cudaError_t mrtcu_env_cdf(const float4* texels, const float* sinTheta, uint32_t w, uint32_t h, float* cdf,
                           double* rowSums, float* rowInv, float* integral, cudaStream_t stream);
 
+// Allocation-free variant over a static device scratch array (max
+// MRTX_ENV_CDF_NOALLOC_MAX_HEIGHT rows). _setup runs once per device with
+// that device current: it takes the scratch address (cudaGetSymbolAddress)
+// and loads the kernels. hostSinTheta (h floats) is copied into the scratch.
+cudaError_t mrtcu_env_cdf_noalloc_setup(int device, unsigned char** scratch);
+cudaError_t mrtcu_env_cdf_noalloc(unsigned char* scratch, const float4* texels, const float* hostSinTheta, uint32_t w,
+                                  uint32_t h, float* cdf, float* integral, cudaStream_t stream);
+
 // RGBA32F readback conversion: out[i] = (sum / count, 1) with the pixel's
 // own sample count; spp == 0 (nothing accumulated since the last reset)
 // gives (0, 0, 0, 1) as the reference does (Renderer.cpp:904).

@@ -3,6 +3,9 @@
 // the FP64 add used to combine replicas.
 #include <cuda_runtime.h>
 
+#include <mutex>
+
+#include "../../../include/mrt_ext.h"
 #include "device_api.h"
 
 namespace {
@@ -141,6 +144,51 @@ extern "C" cudaError_t mrtcu_env_cdf(const float4* texels, const float* sinTheta
     envCdfNormalizeKernel<<<148 * 4, 256, 0, stream>>>(cdf, rowInv, w, h);
     envCdfMarginalKernel<<<1, 32, 0, stream>>>(rowSums, w, h, cdf + size_t(w) * h, integral);
     return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free environment CDF (mrtxBuildEnvCdfNoAlloc). The scratch of
+// one call lives in this fixed device array instead of allocated buffers:
+// row sums (double) at byte 0, the sin(theta) table (float) at 8 * kMax, the
+// row reciprocals (float) at 12 * kMax, for maps of up to kMax rows
+// (128 KiB). Nothing in it has to start at zero: every element a kernel
+// reads was written earlier in the same call, in stream order. All calls on
+// one device share it, so calls that overlap in time race.
+namespace {
+constexpr uint32_t kNoAllocMaxRows = MRTX_ENV_CDF_NOALLOC_MAX_HEIGHT;
+constexpr int kNoAllocMaxDevices = 64;
+__device__ __align__(256) unsigned char g_envCdfScratch[size_t(kNoAllocMaxRows) * 16];
+std::mutex g_scratchMutex;
+unsigned char* g_scratchAddr[kNoAllocMaxDevices] = {};
+}  // namespace
+
+extern "C" cudaError_t mrtcu_env_cdf_noalloc_setup(int device, unsigned char** scratch) {
+    if (device < 0 || device >= kNoAllocMaxDevices) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(g_scratchMutex);
+    if (!g_scratchAddr[device]) {
+        void* addr = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&addr, g_envCdfScratch);
+        if (e != cudaSuccess) return e;
+        // load the three kernels now, so later calls load no code either
+        cudaFuncAttributes fa;
+        if ((e = cudaFuncGetAttributes(&fa, envCdfRowsKernel)) != cudaSuccess) return e;
+        if ((e = cudaFuncGetAttributes(&fa, envCdfNormalizeKernel)) != cudaSuccess) return e;
+        if ((e = cudaFuncGetAttributes(&fa, envCdfMarginalKernel)) != cudaSuccess) return e;
+        g_scratchAddr[device] = static_cast<unsigned char*>(addr);
+    }
+    *scratch = g_scratchAddr[device];
+    return cudaSuccess;
+}
+
+extern "C" cudaError_t mrtcu_env_cdf_noalloc(unsigned char* scratch, const float4* texels, const float* hostSinTheta,
+                                             uint32_t w, uint32_t h, float* cdf, float* integral, cudaStream_t stream) {
+    if (w == 0 || h == 0 || h > kNoAllocMaxRows) return cudaErrorInvalidValue;
+    double* rowSums = reinterpret_cast<double*>(scratch);
+    float* sinTheta = reinterpret_cast<float*>(scratch + size_t(kNoAllocMaxRows) * 8);
+    float* rowInv = reinterpret_cast<float*>(scratch + size_t(kNoAllocMaxRows) * 12);
+    const cudaError_t e = cudaMemcpyAsync(sinTheta, hostSinTheta, size_t(h) * sizeof(float), cudaMemcpyHostToDevice, stream);
+    if (e != cudaSuccess) return e;
+    return mrtcu_env_cdf(texels, sinTheta, w, h, cdf, rowSums, rowInv, integral, stream);
 }
 
 extern "C" cudaError_t mrtcu_readback_rgba32f(const double* accum, size_t npix, uint32_t spp, float4* out,

@@ -7,11 +7,14 @@
 // scene calls ignore bad handles, add-calls return MRT_INVALID_ID, and no C++
 // exception crosses the boundary (std::bad_alloc -> MRT_ERROR_OUT_OF_MEMORY,
 // anything else -> MRT_ERROR_UNKNOWN).
+#include <cmath>
 #include <cstring>
 #include <new>
+#include <string>
 #include <vector>
 
 #include "../../../include/mrt_ext.h"
+#include "../cuda/device_api.h"
 #include "engine.h"
 #include "wide_bvh.h"
 
@@ -282,6 +285,48 @@ MRT_API mrtResult mrtxBuildWideBvh(const float* aabbs, uint32_t count, uint32_t 
         if (count) std::memcpy(primOrderOut, w.primOrder.data(), size_t(count) * 4);
         return MRT_SUCCESS;
     });
+}
+
+// Allocation-free CDF: device pointers in and out, scratch in the static
+// device array of csrc/cuda/frame.cu. The sin(theta) table is the one
+// Engine::runEnvCdf builds (same float expression), held on this thread's
+// stack and copied into the scratch.
+MRT_API mrtResult mrtxBuildEnvCdfNoAlloc(const float* devTexels, uint32_t w, uint32_t h, float* devCdfOut,
+                                         float* devIntegralOut, void* stream) {
+    if (!devTexels || !devCdfOut || !devIntegralOut || w == 0 || h == 0)
+        return mrt::fail(MRT_ERROR_INVALID_ARGUMENT, "mrtxBuildEnvCdfNoAlloc: null pointer or empty image");
+    if (h > MRTX_ENV_CDF_NOALLOC_MAX_HEIGHT)
+        return mrt::fail(MRT_ERROR_INVALID_ARGUMENT, "mrtxBuildEnvCdfNoAlloc: height " + std::to_string(h) +
+                                                         " exceeds the maximum of " +
+                                                         std::to_string(MRTX_ENV_CDF_NOALLOC_MAX_HEIGHT) + " rows");
+    int device = -1;
+    for (const void* ptr : {static_cast<const void*>(devTexels), static_cast<const void*>(devCdfOut),
+                            static_cast<const void*>(devIntegralOut)}) {
+        cudaPointerAttributes at;
+        if (cudaPointerGetAttributes(&at, ptr) != cudaSuccess ||
+            (at.type != cudaMemoryTypeDevice && at.type != cudaMemoryTypeManaged)) {
+            cudaGetLastError();
+            return mrt::fail(MRT_ERROR_INVALID_ARGUMENT, "mrtxBuildEnvCdfNoAlloc: a pointer is not device memory");
+        }
+        if (device >= 0 && at.device != device)
+            return mrt::fail(MRT_ERROR_INVALID_ARGUMENT, "mrtxBuildEnvCdfNoAlloc: pointers on different GPUs");
+        device = at.device;
+    }
+    int previous = -1;
+    MRT_CUDA(cudaGetDevice(&previous));
+    if (previous != device) MRT_CUDA(cudaSetDevice(device));
+    float sinTheta[MRTX_ENV_CDF_NOALLOC_MAX_HEIGHT];
+    const float pi = 3.14159265358979323846f;
+    const float dTheta = pi / float(h);
+    for (uint32_t y = 0; y < h; ++y) sinTheta[y] = std::sin((float(y) + 0.5f) * dTheta);
+    unsigned char* scratch = nullptr;
+    cudaError_t e = mrtcu_env_cdf_noalloc_setup(device, &scratch);
+    if (e == cudaSuccess)
+        e = mrtcu_env_cdf_noalloc(scratch, reinterpret_cast<const float4*>(devTexels), sinTheta, w, h, devCdfOut,
+                                  devIntegralOut, static_cast<cudaStream_t>(stream));
+    if (previous != device) cudaSetDevice(previous);
+    if (e != cudaSuccess) return mrt::fromCuda(e, "mrtxBuildEnvCdfNoAlloc");
+    return MRT_SUCCESS;
 }
 
 }  // extern "C"
