@@ -143,13 +143,14 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def ncu_traffic_per_launch(config):
-    """DRAM bytes (read + write) per path-tracing launch of this workload from
-    the committed ncu summary (profiles/pathtrace_<config>.md), or None."""
+def ncu_dram_bytes_per_ray(config):
+    """DRAM bytes (read + write) of the extend kernel per closest-hit ray,
+    from the committed ncu summary (profiles/pathtrace_<config>.md; all extend
+    launches of a 1-spp frame of the same scene), or None."""
     p = ROOT / "profiles" / f"pathtrace_{config}.md"
     if not p.exists():
         return None
-    m = re.search(r"dram bytes per full launch:\s*([0-9.eE+]+)", p.read_text())
+    m = re.search(r"dram bytes per closest-hit ray:\s*([0-9.eE+]+)", p.read_text())
     return float(m.group(1)) if m else None
 
 
@@ -297,7 +298,9 @@ def ours_arm(args):
     ext_s = float(np.mean(ext_ms)) / 1e3
     achieved = algo_bytes / ext_s / 1e9
     peak, peak_kind = measured_peaks()
-    traffic = ncu_traffic_per_launch(args.config)
+    n_ext = max(1, c["extendLaunches"])
+    per_ray = ncu_dram_bytes_per_ray(args.config)
+    traffic = per_ray * c["raysClosest"] / n_ext if per_ray is not None else None
     rays = c["raysClosest"] + c["raysShadow"]
 
     # end to end through the C ABI with host buffers (rank-local)
@@ -360,11 +363,16 @@ def ours_arm(args):
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "peak_source": peak_kind, "kernel": "waveExtendKernel (closest hit), all launches of a step",
+                         "algorithmic_bytes_per_launch": algo_bytes / n_ext, "launches_per_step": n_ext,
+                         "ms_per_launch": ext_s * 1e3 / n_ext,
                          "algorithmic_bytes_per_step": algo_bytes, "kernel_s_per_step": ext_s,
                          "note": "algorithmic bytes = node records x %d B + triangle tests x %d B + rays x %d B of "
                                  "queue/ray/hit I/O, counted in the timed launches; most node and triangle reads "
-                                 "are served by L1/L2, so frac is against HBM but the data path is on-chip"
+                                 "are served by L1/L2, so frac is against HBM but the data path is on-chip; "
+                                 "traffic = ncu DRAM bytes per closest-hit ray (1-spp capture of the same scene) "
+                                 "x rays per step / launches per step"
                                  % (c["nodeBytes"], c["triBytes"], RAY_IO_BYTES)},
+            "rays_closest_per_step": c["raysClosest"],
             "clocks": clocks,
             "e2e": e2e,
             "cpu_baseline": cpu,

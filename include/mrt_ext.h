@@ -85,6 +85,7 @@ typedef struct mrtxStats {
     uint32_t triBytes;     /* bytes read by one ray/triangle test */
     /* device time of the last render call per wavefront stage (CUDA events) */
     float extendMs, shadeMs, shadowMs, otherMs;
+    uint32_t extendLaunches; /* closest-hit (extend) kernel launches of the last render call */
 } mrtxStats;
 MRT_API mrtResult mrtxGetStats(mrtEngine*, mrtxStats* out);
 
@@ -116,6 +117,24 @@ MRT_API mrtResult mrtxCopyAccumulationDevice(mrtEngine*, void* devPtr, size_t by
  * tree on the CPU, core/src/accel/Bvh.cpp:137-156). */
 MRT_API mrtResult mrtxBuildWideBvh(const float* aabbs, uint32_t count, uint32_t maxLeafPrims, void* nodesOut,
                                    uint32_t nodeCapacity, uint32_t* primOrderOut, uint32_t* nodeCountOut);
+
+/* Builders of mrtxBuildMeshBvh. */
+#define MRTX_BVH_HOST_SAH 0u     /* binned-SAH binary tree on the host (meshes below 65536 triangles) */
+#define MRTX_BVH_HOST_LBVH 1u    /* Morton-code LBVH on the host: the device builder's reference */
+#define MRTX_BVH_DEVICE_LBVH 2u  /* the same LBVH built on the engine's GPU (meshes of 65536+ triangles) */
+
+/* The 8-wide BVH the engine builds for a triangle mesh (positions: 3 floats
+ * per vertex; indices: 3 per triangle, each < vertexCount), from the chosen
+ * builder; every builder ends in the same SAH-optimal collapse to 8-wide
+ * nodes with leaves of at most maxLeafPrims (1..3) triangles. Output as
+ * mrtxBuildWideBvh. MRTX_BVH_DEVICE_LBVH needs an engine (its GPU); the
+ * host builders accept engine == NULL. The device and host LBVH builders
+ * return identical nodes and orders. Builds on the reference's per-mesh
+ * BLAS build (Renderer.cpp:333-446). */
+MRT_API mrtResult mrtxBuildMeshBvh(mrtEngine* engine, const float* positions, uint32_t vertexCount,
+                                   const uint32_t* indices, uint32_t triangleCount, uint32_t builder,
+                                   uint32_t maxLeafPrims, void* nodesOut, uint32_t nodeCapacity,
+                                   uint32_t* primOrderOut, uint32_t* nodeCountOut);
 
 /* Largest map height mrtxBuildEnvCdfNoAlloc accepts. */
 #define MRTX_ENV_CDF_NOALLOC_MAX_HEIGHT 8192u

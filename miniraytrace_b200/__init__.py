@@ -318,6 +318,24 @@ def build_env_cdf_no_alloc(dev_texels: int, width: int, height: int, dev_cdf: in
                                       C.c_void_p(dev_integral), C.c_void_p(stream)), "mrtxBuildEnvCdfNoAlloc")
 
 
+def build_mesh_bvh(positions, indices, builder=abi.MRTX_BVH_HOST_SAH, max_leaf_prims=3, engine=None):
+    """The engine's 8-wide BVH of a triangle mesh from one builder
+    (abi.MRTX_BVH_*): (nodes as a WIDE_NODE_DTYPE array, triangle order).
+    The device builder needs an Engine."""
+    lib = load_library()
+    p = np.ascontiguousarray(np.asarray(positions, np.float32).reshape(-1, 3))
+    i = np.ascontiguousarray(np.asarray(indices, np.uint32).reshape(-1, 3))
+    nt = i.shape[0]
+    cap = max(1, nt)
+    nodes = np.zeros(cap, dtype=abi.WIDE_NODE_DTYPE)
+    order = np.zeros(max(1, nt), np.uint32)
+    count = C.c_uint32()
+    handle = engine.h if engine is not None else None
+    _check(lib.mrtxBuildMeshBvh(handle, _ptr(p), p.shape[0], _ptr(i), nt, builder, max_leaf_prims, _ptr(nodes), cap,
+                                _ptr(order), C.byref(count)), "mrtxBuildMeshBvh")
+    return nodes[:count.value].copy(), order[:nt].copy()
+
+
 def build_wide_bvh(aabbs, max_leaf_prims=3):
     """Host build of the engine's 8-wide BVH over (N, 6) boxes:
     (nodes as a WIDE_NODE_DTYPE array, primitive order)."""

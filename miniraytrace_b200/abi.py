@@ -123,7 +123,7 @@ class Stats(_Sized):
                 ("triTests", C.c_uint64), ("surfaceHits", C.c_uint64), ("commitH2DBytes", C.c_uint64),
                 ("shadowNodeFetches", C.c_uint64), ("shadowTriTests", C.c_uint64), ("nodeBytes", C.c_uint32),
                 ("triBytes", C.c_uint32), ("extendMs", C.c_float), ("shadeMs", C.c_float), ("shadowMs", C.c_float),
-                ("otherMs", C.c_float)]
+                ("otherMs", C.c_float), ("extendLaunches", C.c_uint32)]
 
 
 LOG_FN = C.CFUNCTYPE(None, C.c_int, C.c_char_p, C.c_void_p)
@@ -173,8 +173,13 @@ FUNCTIONS = [
     ("mrtxCopyAccumulationDevice", C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, C.c_int32]),
     ("mrtxBuildWideBvh", C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p,
                                    C.POINTER(C.c_uint32)]),
+    ("mrtxBuildMeshBvh", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.c_uint32,
+                                   C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p, C.POINTER(C.c_uint32)]),
     ("mrtxBuildEnvCdfNoAlloc", C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p]),
 ]
+
+# mrtxBuildMeshBvh builders
+MRTX_BVH_HOST_SAH, MRTX_BVH_HOST_LBVH, MRTX_BVH_DEVICE_LBVH = 0, 1, 2
 
 # mrtxBuildEnvCdfNoAlloc's height limit (MRTX_ENV_CDF_NOALLOC_MAX_HEIGHT)
 ENV_CDF_NOALLOC_MAX_HEIGHT = 8192

@@ -36,7 +36,7 @@ NVCC_FLAGS = ARCH + [
 # without multiply-add contraction so its shading arithmetic is the same
 # sequence of IEEE single-precision operations as the CPU evaluation (explicit
 # __fmaf_rn intrinsics still produce fused multiply-adds where wanted).
-NVCC_FILE_FLAGS = {"pathtrace.cu": ["-fmad=false"]}
+NVCC_FILE_FLAGS = {"pathtrace.cu": ["-fmad=false"], "bvh_build.cu": ["-fmad=false"]}
 
 CXX_FLAGS = [
     "-O2", "-std=c++17", "-fPIC", "-fvisibility=hidden", "-ffp-contract=off",

@@ -58,6 +58,18 @@ cudaError_t mrtcu_resolve_rgba8(const double* accum, size_t npix, float exposure
 // dst[i] += src[i] for n doubles (combining replicas' accumulations).
 cudaError_t mrtcu_add_f64(double* dst, const double* src, size_t n, cudaStream_t stream);
 
+// Device build of one mesh's 8-wide BVH (bvh_build.cu): positions as
+// float4 (xyz used), indices 3 per triangle. Writes up to nodeCapacity
+// (>= triCount) nodes with mesh-relative childBase/primBase, primOrderOut
+// (triCount original triangle indices in leaf order), *nodeCountOut and the
+// root box (lo xyz, hi xyz). Synchronises `stream` (it reads the per-level
+// task counts). scratch: mrtcu_wide_bvh_scratch_bytes(triCount) bytes.
+size_t mrtcu_wide_bvh_scratch_bytes(uint32_t triCount);
+cudaError_t mrtcu_build_wide_bvh(const float4* positions, const uint32_t* indices, uint32_t triCount,
+                                 uint32_t maxLeaf, void* scratch, size_t scratchBytes, MrtWideNode* nodesOut,
+                                 uint32_t nodeCapacity, uint32_t* primOrderOut, uint32_t* nodeCountOut,
+                                 float boundsOut[6], uint32_t* launchesOut, cudaStream_t stream);
+
 #ifdef __cplusplus
 }
 #endif

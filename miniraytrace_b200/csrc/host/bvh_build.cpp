@@ -218,4 +218,23 @@ BvhResult buildBvh(const std::vector<Box3>& boxes, uint32_t maxLeaf, unsigned th
     return r;
 }
 
+std::vector<Box3> triangleBoxes(const float* positions, size_t stride, const uint32_t* indices, size_t nt) {
+    std::vector<Box3> boxes(nt);
+    for (size_t t = 0; t < nt; ++t) {
+        Box3& b = boxes[t];
+        for (int k = 0; k < 3; ++k) {
+            b.lo[k] = 3.402823466e38f;
+            b.hi[k] = -3.402823466e38f;
+        }
+        for (int c = 0; c < 3; ++c) {
+            const float* v = positions + size_t(indices[t * 3 + c]) * stride;
+            for (int k = 0; k < 3; ++k) {
+                b.lo[k] = std::min(b.lo[k], v[k]);
+                b.hi[k] = std::max(b.hi[k], v[k]);
+            }
+        }
+    }
+    return boxes;
+}
+
 }  // namespace mrt

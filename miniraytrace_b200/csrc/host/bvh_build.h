@@ -26,4 +26,9 @@ struct BvhResult {
 
 BvhResult buildBvh(const std::vector<Box3>& boxes, uint32_t maxLeaf, unsigned threads);
 
+// Boxes of nt triangles (indices 3 per triangle into positions with
+// `stride` floats per vertex, xyz first): min/max over the three vertices
+// in order, the arithmetic the device builder repeats.
+std::vector<Box3> triangleBoxes(const float* positions, size_t stride, const uint32_t* indices, size_t nt);
+
 }  // namespace mrt

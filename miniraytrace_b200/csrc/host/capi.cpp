@@ -16,6 +16,7 @@
 #include "../../../include/mrt_ext.h"
 #include "../cuda/device_api.h"
 #include "engine.h"
+#include "lbvh.h"
 #include "wide_bvh.h"
 
 namespace {
@@ -283,6 +284,41 @@ MRT_API mrtResult mrtxBuildWideBvh(const float* aabbs, uint32_t count, uint32_t 
             return mrt::fail(MRT_ERROR_INVALID_ARGUMENT, "mrtxBuildWideBvh: node capacity too small");
         if (!w.nodes.empty()) std::memcpy(nodesOut, w.nodes.data(), w.nodes.size() * sizeof(MrtWideNode));
         if (count) std::memcpy(primOrderOut, w.primOrder.data(), size_t(count) * 4);
+        return MRT_SUCCESS;
+    });
+}
+
+MRT_API mrtResult mrtxBuildMeshBvh(mrtEngine* engine, const float* positions, uint32_t vertexCount,
+                                   const uint32_t* indices, uint32_t triangleCount, uint32_t builder,
+                                   uint32_t maxLeafPrims, void* nodesOut, uint32_t nodeCapacity,
+                                   uint32_t* primOrderOut, uint32_t* nodeCountOut) {
+    if ((triangleCount && (!positions || !indices || !primOrderOut)) || !nodeCountOut || (nodeCapacity && !nodesOut))
+        return mrt::fail(MRT_ERROR_INVALID_ARGUMENT, "mrtxBuildMeshBvh: null pointer");
+    if (builder > MRTX_BVH_DEVICE_LBVH || maxLeafPrims < 1 || maxLeafPrims > 3)
+        return mrt::fail(MRT_ERROR_INVALID_ARGUMENT, "mrtxBuildMeshBvh: unknown builder or leaf size");
+    if (builder == MRTX_BVH_DEVICE_LBVH && !engine)
+        return mrt::fail(MRT_ERROR_INVALID_ARGUMENT, "mrtxBuildMeshBvh: the device builder needs an engine");
+    for (size_t i = 0; i < size_t(triangleCount) * 3; ++i)
+        if (indices[i] >= vertexCount) return mrt::fail(MRT_ERROR_INVALID_ARGUMENT, "mrtxBuildMeshBvh: index out of range");
+    return guarded([&] {
+        mrt::WideBvh w;
+        if (builder == MRTX_BVH_DEVICE_LBVH) {
+            std::vector<mrt::V4f> pos(vertexCount);
+            for (uint32_t v = 0; v < vertexCount; ++v)
+                pos[v] = mrt::V4f{positions[3 * v], positions[3 * v + 1], positions[3 * v + 2], 1.0f};
+            const mrtResult r = unwrap(engine)->buildMeshBvhDevice(pos.data(), pos.size(), indices, triangleCount,
+                                                                maxLeafPrims, w);
+            if (r != MRT_SUCCESS) return r;
+        } else {
+            const std::vector<mrt::Box3> boxes = mrt::triangleBoxes(positions, 3, indices, triangleCount);
+            w = mrt::collapseToWide(builder == MRTX_BVH_HOST_SAH ? mrt::buildBvh(boxes, 1, 4) : mrt::buildLbvh(boxes),
+                                    maxLeafPrims);
+        }
+        *nodeCountOut = uint32_t(w.nodes.size());
+        if (w.nodes.size() > nodeCapacity)
+            return mrt::fail(MRT_ERROR_INVALID_ARGUMENT, "mrtxBuildMeshBvh: node capacity too small");
+        if (!w.nodes.empty()) std::memcpy(nodesOut, w.nodes.data(), w.nodes.size() * sizeof(MrtWideNode));
+        if (triangleCount) std::memcpy(primOrderOut, w.primOrder.data(), size_t(triangleCount) * 4);
         return MRT_SUCCESS;
     });
 }

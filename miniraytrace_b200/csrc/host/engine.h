@@ -13,6 +13,7 @@
 #include "../../../include/mrt_ext.h"
 #include "../common/device_types.h"
 #include "bvh_build.h"
+#include "lbvh.h"
 #include "wide_bvh.h"
 #include "common.h"
 #include "scene.h"
@@ -56,6 +57,10 @@ public:
     mrtResult buildEnvCdf(const float* rgba, uint32_t w, uint32_t h, float* cdf, float* integral);
     mrtResult setSampleStream(uint32_t offset, uint32_t stride);
     mrtResult copyAccumulationDevice(void* dev, size_t bytes, bool accumulate);
+    // 8-wide BVH of one triangle mesh built on this engine's GPU (LBVH
+    // topology, SAH-optimal collapse), read back into `out`.
+    mrtResult buildMeshBvhDevice(const V4f* pos, size_t nv, const uint32_t* idx, size_t nt, uint32_t maxLeaf,
+                                 WideBvh& out);
 
 private:
     Engine() = default;
@@ -99,6 +104,7 @@ private:
     // device frame state
     DeviceBuffer m_accum, m_out32, m_out8, m_flags, m_rayCounters, m_queryRays, m_queryOut;
     DeviceBuffer m_wave;  // wavefront path state (one allocation, carved into MrtWaveState arrays)
+    DeviceBuffer m_bvhPos, m_bvhIdx, m_bvhScratch, m_bvhNodes, m_bvhPrims;  // device BVH builder
     MrtWaveState m_waveState{};
     uint32_t m_waveSamples = 0;  // samples per pixel one wave holds
     void* m_pinned = nullptr;

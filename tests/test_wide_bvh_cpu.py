@@ -169,3 +169,90 @@ def test_degenerate_inputs(mrt_lib):
     flat = np.array([[i, 0, j, i + 1, 0, j + 1] for i in range(10) for j in range(10)], np.float32)
     nodes, order = mrt.build_wide_bvh(flat)
     assert sorted(order.tolist()) == list(range(100))
+
+
+def soup_mesh(n, seed):
+    tris = tri_soup(n, seed)
+    return tris.reshape(-1, 3), np.arange(3 * n, dtype=np.uint32).reshape(-1, 3)
+
+
+def heightfield_mesh(k, seed):
+    rng = np.random.default_rng(seed)
+    x, z = np.meshgrid(np.linspace(-1, 1, k), np.linspace(-1, 1, k))
+    y = 0.05 * rng.standard_normal((k, k))
+    pos = np.stack([x, y, z], -1).reshape(-1, 3).astype(np.float32)
+    a = (np.arange(k - 1)[:, None] * k + np.arange(k - 1)[None, :]).ravel()
+    idx = np.concatenate([np.stack([a, a + 1, a + k], 1), np.stack([a + 1, a + k + 1, a + k], 1)])
+    return pos, idx.astype(np.uint32)
+
+
+@pytest.mark.parametrize("builder", [0, 1])
+def test_mesh_builders_structure(mrt_lib, builder):
+    pos, idx = soup_mesh(2000, 11)
+    tris = pos[idx]
+    boxes = np.concatenate([tris.min(1), tris.max(1)], 1)
+    nodes, order = mrt.build_mesh_bvh(pos, idx, builder)
+    assert sorted(order.tolist()) == list(range(len(idx)))
+    for ni, nd in enumerate(nodes):
+        s, k = grid(nd)
+        for slot, kind, ref in children(nd):
+            prims = subtree_prims(nodes, order, ref) if kind == "node" else order[ref[0]:ref[0] + ref[1]].tolist()
+            pb = boxes[prims].astype(np.float64)
+            assert (k + nd["qlo"][:, slot] <= pb[:, :3] / s).all(), (ni, slot)
+            assert (k + nd["qhi"][:, slot] >= pb[:, 3:] / s).all(), (ni, slot)
+
+
+def test_layout_follows_subtree_sizes(mrt_lib):
+    """The depth-first layout the device emission reproduces level by level:
+    a node's internal children are consecutive from childBase; child r's own
+    children start after all children of its parent plus the subtrees of
+    children 0..r-1; its primitives start after the parent's leaf primitives
+    plus the primitives of children 0..r-1."""
+    for builder, (pos, idx) in [(0, soup_mesh(1500, 2)), (1, soup_mesh(1500, 2)), (1, heightfield_mesh(40, 3))]:
+        nodes, order = mrt.build_mesh_bvh(pos, idx, builder)
+        below, prims = {}, {}
+
+        def sizes(w):
+            nb, npr = 0, 0
+            for slot, kind, ref in children(nodes[w]):
+                if kind == "node":
+                    b, p = sizes(ref)
+                    nb += 1 + b
+                    npr += p
+                else:
+                    npr += ref[1]
+            below[w], prims[w] = nb, npr
+            return nb, npr
+
+        sizes(0)
+        assert 1 + below[0] == len(nodes) and prims[0] == len(idx)
+        for w, nd in enumerate(nodes):
+            kids = children(nd)
+            internal = [ref for _, kind, ref in kids if kind == "node"]
+            leaf_prims = sum(ref[1] for _, kind, ref in kids if kind == "leaf")
+            assert internal == list(range(int(nd["childBase"]), int(nd["childBase"]) + len(internal)))
+            next_child = int(nd["childBase"]) + len(internal)
+            next_prim = int(nd["primBase"]) + leaf_prims
+            for c in internal:
+                assert int(nodes[c]["childBase"]) == next_child and int(nodes[c]["primBase"]) == next_prim, (w, c)
+                next_child += below[c]
+                next_prim += prims[c]
+
+
+def test_lbvh_degenerate_and_tiny_meshes(mrt_lib):
+    one = (np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0]], np.float32), np.array([[0, 1, 2]], np.uint32))
+    same = (np.tile(one[0], (1, 1)), np.tile(one[1], (50, 1)))  # 50 identical triangles
+    flat = heightfield_mesh(12, 1)
+    flat[0][:, 1] = 0.0
+    for pos, idx in (one, same, flat, soup_mesh(2, 1), soup_mesh(3, 1)):
+        nodes, order = mrt.build_mesh_bvh(pos, idx, 1)
+        assert sorted(order.tolist()) == list(range(len(idx)))
+        assert 1 <= len(nodes) <= max(1, len(idx))
+
+
+def test_mesh_builder_rejects_bad_input(mrt_lib):
+    pos, idx = soup_mesh(10, 1)
+    with pytest.raises(mrt.MrtError):
+        mrt.build_mesh_bvh(pos, idx + 100, 1)
+    with pytest.raises(mrt.MrtError):
+        mrt.build_mesh_bvh(pos, idx, 2)  # device builder without an engine
