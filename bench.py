@@ -58,6 +58,8 @@ def parse_args():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--spp", type=int, default=0, help="samples per pixel per step (0 = the workload's 64)")
+    ap.add_argument("--resolution", type=str, default="",
+                    help="WxH override for profiling captures of a smaller frame (default: the workload's)")
     return ap.parse_args()
 
 
@@ -229,6 +231,9 @@ def ours_arm(args):
     scene = make_scene(args.config)
     if args.spp > 0:
         scene.spp = args.spp
+    if args.resolution:
+        w, h = (int(v) for v in args.resolution.lower().split("x"))
+        scene.settings["width"], scene.settings["height"] = w, h
     W, H, spp = scene.settings["width"], scene.settings["height"], scene.spp
     paths_per_step = W * H * spp
 

@@ -195,7 +195,7 @@ MRT_API mrtResult mrtSetRenderSettings(mrtEngine* e, const mrtRenderSettings* d)
 MRT_API mrtResult mrtRenderFrame(mrtEngine* e, mrtFrameInfo* outInfo) {
     mrt::Engine* eng = unwrap(e);
     if (!eng) return MRT_ERROR_INVALID_HANDLE;
-    return guarded([&] { return eng->renderFrames(1, outInfo); });
+    return guarded([&] { return eng->renderFrames(1, outInfo, true); });
 }
 
 MRT_API mrtResult mrtReadFramebuffer(mrtEngine* e, mrtPixelFormat fmt, void* dst, size_t dstSize) {
@@ -245,7 +245,10 @@ MRT_API mrtResult mrtxReadAccumulation(mrtEngine* e, double* dst, size_t dstSize
 MRT_API mrtResult mrtxGetStats(mrtEngine* e, mrtxStats* out) {
     mrt::Engine* eng = unwrap(e);
     if (!eng || !validStruct(out)) return MRT_ERROR_INVALID_ARGUMENT;
-    return guarded([&] { return eng->getStats(out); });
+    return guarded([&] {
+        const mrtResult r = eng->flushPending();
+        return r != MRT_SUCCESS ? r : eng->getStats(out);
+    });
 }
 
 MRT_API mrtResult mrtxBuildEnvCdf(mrtEngine* e, const float* rgba, uint32_t w, uint32_t h, float* cdfOut,

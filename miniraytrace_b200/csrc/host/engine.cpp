@@ -304,13 +304,17 @@ mrtResult Engine::setSettings(const Settings& s) {
     if (s.width == 0 || s.height == 0) return fail(MRT_ERROR_INVALID_ARGUMENT, "render size must be non-zero");
     const bool resize = s.width != m_settings.width || s.height != m_settings.height;
     const bool reset = resize || s.maxBounces != m_settings.maxBounces || s.fireflyClamp != m_settings.fireflyClamp;
+    if (reset) m_pending = 0;  // dropped before any frame buffer is replaced
     m_settings = s;
     if (resize) MRT_TRY(guard(allocateFrame()));
     if (reset) resetAccumulation();
     return MRT_SUCCESS;
 }
 
-void Engine::resetAccumulation() { m_frameIndex = 0; }
+void Engine::resetAccumulation() {
+    m_frameIndex = 0;
+    m_pending = 0;  // queued samples would be discarded by the reset anyway
+}
 
 mrtResult Engine::setSampleStream(uint32_t offset, uint32_t stride) {
     if (stride == 0) return fail(MRT_ERROR_INVALID_ARGUMENT, "sample stream stride must be >= 1");
@@ -328,6 +332,9 @@ mrtResult Engine::commit(mrtCommitStats* stats) {
     MRT_TRY(checkAlive());
     const uint32_t light = DirtyCamera | DirtyEnvParams;
     const uint32_t d = m_scene.dirty();
+    // every commit that changes something resets the accumulation: queued
+    // samples are dropped before any device array is replaced
+    if (d != DirtyNone) m_pending = 0;
     if (d != DirtyNone && (d & ~light) == 0) {
         m_scene.clearDirty();
         resetAccumulation();
@@ -791,18 +798,52 @@ mrtResult Engine::checkErrorFlags() {
 }
 
 // reference Engine.cpp:57-60 + Renderer.cpp:773-843: implicit commit, one
-// sample per pixel per frame, no-op once sppLimit is reached.
-mrtResult Engine::renderFrames(uint32_t count, mrtFrameInfo* info) {
+// sample per pixel per frame, no-op once sppLimit is reached. With `defer`
+// (mrtRenderFrame) the samples are queued and rendered as one wave when a
+// full wave has accumulated or when anything reads or replaces the results
+// (flushPending); the reported spp counts queued samples, as the reference
+// counts rendered ones.
+mrtResult Engine::renderFrames(uint32_t count, mrtFrameInfo* info, bool defer) {
     const auto t0 = std::chrono::steady_clock::now();
     MRT_TRY(commit(nullptr));
+    const uint32_t queued = m_frameIndex + m_pending;
     uint32_t n = 0;
-    if (m_frameIndex < m_settings.sppLimit) n = std::min(count, m_settings.sppLimit - m_frameIndex);
+    if (queued < m_settings.sppLimit) n = std::min(count, m_settings.sppLimit - queued);
+    if (n > 0) {
+        if (m_pending == 0) fillParams(m_pendingParams);
+        m_pending += n;
+        m_resolveExposure = std::exp2(m_settings.exposureEV);
+        m_resolveTonemap = m_settings.tonemap;
+    }
+    if (m_pending > 0 && (!defer || m_pending >= waveCapacitySamples())) MRT_TRY(flushPending());
+    if (info && info->structSize >= sizeof(mrtFrameInfo)) {
+        info->spp = m_frameIndex + m_pending;
+        info->converged = m_frameIndex + m_pending >= m_settings.sppLimit ? 1 : 0;
+        info->denoised = 0;
+        info->frameMs = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    }
+    return MRT_SUCCESS;
+}
+
+// Samples per pixel of one full wave at the current resolution (the wave
+// state holds at most 2^25 paths and 64 samples).
+uint32_t Engine::waveCapacitySamples() const {
+    const uint64_t pixels = std::max<uint64_t>(uint64_t(m_settings.width) * m_settings.height, 1);
+    return uint32_t(std::max<uint64_t>(1, std::min<uint64_t>(64, (uint64_t(1) << 25) / pixels)));
+}
+
+// Renders the queued samples with the frame parameters captured when the
+// first of them was queued (the device scene cannot change meanwhile: every
+// commit that changes it resets the accumulation and drops the queue).
+mrtResult Engine::flushPending() {
+    if (m_pending == 0) return MRT_SUCCESS;
+    const uint32_t n = m_pending;
+    m_pending = 0;
     m_stats.kernelLaunches = 0;
     m_stats.extendLaunches = 0;
-    if (n > 0) {
+    {
         MRT_TRY(guard(ensureWave(n)));
-        MrtFrameParams p;
-        fillParams(p);
+        const MrtFrameParams p = m_pendingParams;
         MRT_CUDA(cudaMemsetAsync(m_rayCounters.ptr, 0, 64, m_stream));
         uint32_t launches = 0;
         const uint32_t waves = (n + m_waveSamples - 1) / m_waveSamples;
@@ -859,14 +900,6 @@ mrtResult Engine::renderFrames(uint32_t count, mrtFrameInfo* info) {
         m_stats.nodeBytes = sizeof(MrtWideNode);
         m_stats.triBytes = 48;
         m_frameIndex += n;
-        m_resolveExposure = std::exp2(m_settings.exposureEV);
-        m_resolveTonemap = m_settings.tonemap;
-    }
-    if (info && info->structSize >= sizeof(mrtFrameInfo)) {
-        info->spp = m_frameIndex;
-        info->converged = m_frameIndex >= m_settings.sppLimit ? 1 : 0;
-        info->denoised = 0;
-        info->frameMs = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
     }
     return MRT_SUCCESS;
 }
@@ -905,6 +938,7 @@ mrtResult Engine::download(void* dst, const void* src, size_t bytes) {
 // reference Renderer.cpp:892-909
 mrtResult Engine::readFramebuffer(mrtPixelFormat fmt, void* dst, size_t dstSize) {
     MRT_TRY(checkAlive());
+    MRT_TRY(flushPending());
     const size_t pixels = size_t(m_settings.width) * m_settings.height;
     if (fmt == MRT_PIXEL_RGBA8_SRGB) {
         if (dstSize < pixels * 4) return fail(MRT_ERROR_INVALID_ARGUMENT, "dst too small for RGBA8 readback");
@@ -921,6 +955,7 @@ mrtResult Engine::readFramebuffer(mrtPixelFormat fmt, void* dst, size_t dstSize)
 // ---------------------------------------------------------------- queries --
 
 mrtResult Engine::traceRays(const mrtxRay* rays, uint32_t n, mrtxHit* hits) {
+    MRT_TRY(flushPending());
     MRT_TRY(commit(nullptr));
     if (n == 0) return MRT_SUCCESS;
     MrtFrameParams p;
@@ -935,6 +970,7 @@ mrtResult Engine::traceRays(const mrtxRay* rays, uint32_t n, mrtxHit* hits) {
 }
 
 mrtResult Engine::traceShadowRays(const mrtxRay* rays, uint32_t n, uint32_t* occluded) {
+    MRT_TRY(flushPending());
     MRT_TRY(commit(nullptr));
     if (n == 0) return MRT_SUCCESS;
     MrtFrameParams p;
@@ -950,6 +986,7 @@ mrtResult Engine::traceShadowRays(const mrtxRay* rays, uint32_t n, uint32_t* occ
 
 mrtResult Engine::readAccumulation(double* dst, size_t dstSize, uint32_t* spp) {
     MRT_TRY(checkAlive());
+    MRT_TRY(flushPending());
     const size_t bytes = size_t(m_settings.width) * m_settings.height * 32;
     if (dstSize < bytes) return fail(MRT_ERROR_INVALID_ARGUMENT, "dst too small for the accumulation buffer");
     MRT_TRY(guard(download(dst, m_accum.ptr, bytes)));
@@ -978,6 +1015,7 @@ mrtResult Engine::getStats(mrtxStats* out) const {
 
 mrtResult Engine::buildEnvCdf(const float* rgba, uint32_t w, uint32_t h, float* cdf, float* integral) {
     MRT_TRY(checkAlive());
+    MRT_TRY(flushPending());
     if (!rgba || !cdf || !integral || w == 0 || h == 0)
         return fail(MRT_ERROR_INVALID_ARGUMENT, "mrtxBuildEnvCdf: null pointer or empty image");
     float integ = 1.0f;
@@ -991,6 +1029,7 @@ mrtResult Engine::buildEnvCdf(const float* rgba, uint32_t w, uint32_t h, float* 
 
 mrtResult Engine::copyAccumulationDevice(void* dev, size_t bytes, bool accumulate) {
     MRT_TRY(checkAlive());
+    MRT_TRY(flushPending());
     const size_t need = size_t(m_settings.width) * m_settings.height * 32;
     if (!dev || bytes < need) return fail(MRT_ERROR_INVALID_ARGUMENT, "device buffer missing or too small");
     if (accumulate) MRT_CUDA(mrtcu_add_f64(m_accum.as<double>(), static_cast<const double*>(dev), need / 8, m_stream));

@@ -47,7 +47,8 @@ public:
     mrtResult setSettings(const Settings& s);
     void resetAccumulation();
     mrtResult commit(mrtCommitStats* stats);
-    mrtResult renderFrames(uint32_t count, mrtFrameInfo* info);
+    mrtResult renderFrames(uint32_t count, mrtFrameInfo* info, bool defer = false);
+    mrtResult flushPending();  // renders queued samples
     mrtResult readFramebuffer(mrtPixelFormat fmt, void* dst, size_t dstSize);
 
     mrtResult traceRays(const mrtxRay* rays, uint32_t n, mrtxHit* hits);
@@ -69,6 +70,7 @@ private:
     mrtResult guard(mrtResult r);  // records a device loss
     mrtResult allocateFrame();
     mrtResult ensureWave(uint32_t samples);
+    uint32_t waveCapacitySamples() const;
     mrtResult up(DeviceBuffer& b, const void* src, size_t n);
     mrtResult sync(mrtCommitStats* stats);  // reference Renderer::syncScene
     mrtResult packMaterials();
@@ -125,6 +127,8 @@ private:
 
     // accumulation
     uint32_t m_frameIndex = 0;  // samples per pixel accumulated since reset
+    uint32_t m_pending = 0;     // samples queued by mrtRenderFrame, not yet rendered
+    MrtFrameParams m_pendingParams{};
     uint32_t m_streamOffset = 0, m_streamStride = 1;
     float m_resolveExposure = 1.0f;
     uint32_t m_resolveTonemap = MRT_TONEMAP_ACES;

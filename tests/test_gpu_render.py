@@ -396,3 +396,41 @@ def test_env_cdf_kernel_matches_oracle(gpu, oracle_lib):
         assert np.array_equal(cdf, rcdf), (w, h, int(np.sum(cdf != rcdf)))
         assert np.float32(integ) == np.float32(rinteg)
     e.close()
+
+
+def test_queued_frames_match_immediate_rendering(gpu):
+    """mrtRenderFrame queues samples and renders them as one wave (when a
+    full wave is queued or something reads the results); every observable
+    result equals rendering each frame at once: accumulation, frame info,
+    reads between frames, and a camera change dropping queued samples."""
+    s = scenes.box_sphere(64, 64)
+    a = gpu.Engine(64, 64)
+    s.apply(a)
+    b = gpu.Engine(64, 64)
+    s.apply(b)
+    # 70 frames: one full 64-sample wave flushes by itself, 6 stay queued
+    infos = [a.render_frame() for _ in range(70)]
+    assert [i["spp"] for i in infos] == list(range(1, 71))
+    b.render_frames(70)
+    acc_a, spp_a = a.read_accumulation()
+    acc_b, spp_b = b.read_accumulation()
+    assert spp_a == spp_b == 70
+    assert np.array_equal(acc_a, acc_b)
+    # reads in between flush what is queued
+    for _ in range(3):
+        a.render_frame()
+    b.render_frames(3)
+    assert np.array_equal(a.read_framebuffer(), b.read_framebuffer())
+    assert a.stats()["lastRenderSpp"] == 3
+    # a camera change drops queued samples: the reset would erase them
+    for _ in range(4):
+        a.render_frame()
+    cam = dict(s.camera)
+    cam["position"] = tuple(np.asarray(cam["position"]) * 1.1)
+    a.set_camera(**cam)
+    b.set_camera(**cam)
+    assert a.render_frame()["spp"] == 1
+    b.render_frames(1)
+    assert np.array_equal(a.read_accumulation()[0], b.read_accumulation()[0])
+    a.close()
+    b.close()
