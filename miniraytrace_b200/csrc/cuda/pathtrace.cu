@@ -135,6 +135,7 @@ __global__ void __launch_bounds__(256) waveInitKernel(MrtFrameParams P, MrtWaveS
         S.counts[0] = A.slots;
         S.counts[1] = 0;
         S.counts[2] = 0;
+        S.counts[4] = 0;  // extend fetch counter (kExtendHead) of bounce 0
     }
     if (slot >= A.slots) return;
     const uint32_t pixel = slot % A.pixels;
@@ -160,25 +161,69 @@ __global__ void __launch_bounds__(256) waveInitKernel(MrtFrameParams P, MrtWaveS
     S.queue[0][slot] = slot;
 }
 
+// Queue fetch counters of the persistent traversal kernels, in the wave's
+// counts[] block (counts[0..1]: path queues, counts[2]: shadow queue).
+enum { kExtendHead = 4, kShadowHead = 5 };
+
+// Lanes of a persistent traversal warp whose ray has finished take new rays
+// from the queue (one warp-aggregated atomic) once at least this many lanes
+// are idle, so warps do not idle on their longest ray (Aila and Laine 2009).
+#define MRT_REFILL_IDLE 8
+
+// Refill step shared by the traversal kernels: idle lanes get consecutive
+// queue positions; `drained` becomes true (warp-uniformly) once the whole
+// queue is handed out. Returns the lane's position, or 0xffffffff.
+MRT_DEV uint32_t refillLane(uint32_t* head, uint32_t n, bool active, bool& drained) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t idle = __ballot_sync(0xffffffffu, !active);
+    if (__popc(idle) < MRT_REFILL_IDLE) return 0xffffffffu;
+    const int leader = __ffs(idle) - 1;
+    uint32_t base = 0;
+    if (int(lane) == leader) base = atomicAdd(head, uint32_t(__popc(idle)));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (base + uint32_t(__popc(idle)) >= n) drained = true;
+    if (active) return 0xffffffffu;
+    const uint32_t i = base + uint32_t(__popc(idle & ((1u << lane) - 1u)));
+    return i < n ? i : 0xffffffffu;
+}
+
 // Closest hit of every queued ray (intersect.glsl:88-125 traceRay).
+// Persistent warps with lane refill; every lane of a warp stays in the loop
+// until the warp has no ray left.
 __global__ void __launch_bounds__(128) waveExtendKernel(MrtFrameParams P, MrtWaveState S, uint32_t cur) {
     const uint32_t* __restrict__ q = S.queue[cur];
     const uint32_t n = S.counts[cur];
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         S.counts[cur ^ 1u] = 0;  // next queue and shadow queue fill during shade
         S.counts[2] = 0;
+        S.counts[kShadowHead] = 0;
     }
     uint32_t c[kCtrCount] = {};
     TraversalCounters tc;
-    bool ok = true;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const uint32_t slot = q[i];
-        const float4 o = S.rayO[slot], d = S.rayD[slot];
-        HitRecord h;
-        ok &= traceClosest(P, f3(o), f3(d), 1e30f, h, tc);
-        S.hit[slot] = make_float4(h.t, h.u, h.v, __uint_as_float(h.tri));
-        S.hitInst[slot] = h.inst;
-        c[kCtrClosest]++;
+    bool ok = true, active = false, drained = false;
+    uint32_t slot = 0;
+    WideTrav T;
+    WideStack stack;
+    for (;;) {
+        if (!drained) {
+            const uint32_t i = refillLane(S.counts + kExtendHead, n, active, drained);
+            if (i != 0xffffffffu) {
+                slot = q[i];
+                const float4 o = S.rayO[slot], d = S.rayD[slot];
+                travBegin(P, T, f3(o), f3(d), 1e30f);
+                active = true;
+            }
+        }
+        if (!__any_sync(0xffffffffu, active)) break;
+        if (active && travStep<false>(P, T, stack, tc) != kTravRunning) {
+            HitRecord h = T.hit;
+            if (h.tri != 0xffffffffu) refineHit(P, T.wo, T.wd, h);
+            S.hit[slot] = make_float4(h.t, h.u, h.v, __uint_as_float(h.tri));
+            S.hitInst[slot] = h.inst;
+            ok &= T.ok;
+            c[kCtrClosest]++;
+            active = false;
+        }
     }
     if (!ok) atomicOr(P.errorFlags, 1u);
     if (tc.bad) atomicOr(P.errorFlags, 2u);
@@ -302,23 +347,44 @@ __global__ void __launch_bounds__(128) waveShadeKernel(MrtFrameParams P, MrtWave
 
 // Any-hit test of every queued shadow ray; unoccluded rays add their NEE
 // contribution to their path (pathtrace.comp:192-195). A path has at most
-// one shadow ray per bounce, so the update needs no atomics.
+// one shadow ray per bounce, so the update needs no atomics. Persistent
+// warps with lane refill, as the extend kernel.
 __global__ void __launch_bounds__(128) waveShadowKernel(MrtFrameParams P, MrtWaveState S) {
     const uint32_t n = S.counts[2];
+    if (blockIdx.x == 0 && threadIdx.x == 0) S.counts[kExtendHead] = 0;  // for the next bounce
     uint32_t c[kCtrCount] = {};
     TraversalCounters tc;
-    bool ok = true;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const float4 o = S.shO[i], d = S.shD[i];
-        c[kCtrShadow]++;
-        if (!traceAny(P, f3(o), f3(d), o.w, ok, tc)) {
-            const uint32_t slot = __float_as_uint(d.w);
-            const float4 cc = S.shC[i];
-            float4 L = S.L[slot];
-            L.x = L.x + cc.x;
-            L.y = L.y + cc.y;
-            L.z = L.z + cc.z;
-            S.L[slot] = L;
+    bool ok = true, active = false, drained = false;
+    uint32_t idx = 0;
+    WideTrav T;
+    WideStack stack;
+    for (;;) {
+        if (!drained) {
+            const uint32_t i = refillLane(S.counts + kShadowHead, n, active, drained);
+            if (i != 0xffffffffu) {
+                idx = i;
+                const float4 o = S.shO[i], d = S.shD[i];
+                travBegin(P, T, f3(o), f3(d), o.w);
+                active = true;
+                c[kCtrShadow]++;
+            }
+        }
+        if (!__any_sync(0xffffffffu, active)) break;
+        if (active) {
+            const int r = travStep<true>(P, T, stack, tc);
+            if (r != kTravRunning) {
+                ok &= T.ok;
+                if (r != kTravOccluded) {
+                    const uint32_t slot = __float_as_uint(S.shD[idx].w);
+                    const float4 cc = S.shC[idx];
+                    float4 L = S.L[slot];
+                    L.x = L.x + cc.x;
+                    L.y = L.y + cc.y;
+                    L.z = L.z + cc.z;
+                    S.L[slot] = L;
+                }
+                active = false;
+            }
         }
     }
     if (!ok) atomicOr(P.errorFlags, 1u);

@@ -287,119 +287,158 @@ MRT_DEV uint32_t childIndex(uint32_t childBase, uint32_t imask, uint32_t b, uint
 // being walked.
 #define MRT_WIDE_STACK 48
 
-// Two-level traversal in one loop (reference intersect.glsl:88-178): the
-// TLAS's leaf primitives are instances; on an instance the TLAS group is
-// parked, the ray is taken into object space and the instance's BLAS is
-// walked on top of the same stack, and the TLAS group resumes when the stack
-// is back at the depth it had on entry. One node test serves both levels.
-// kAny: stops at the first triangle with t in (1e-4, tMax) and returns true.
-// Otherwise: closest hit, tMax and `hit` updated. `ok` is cleared on a stack
-// overflow or an exhausted visit budget.
+// Traversal state of one ray, advanced one step at a time (travStep), so a
+// persistent warp can start a new ray in a lane whose ray has finished while
+// the other lanes keep walking. Two-level walk in one loop (reference
+// intersect.glsl:88-178): the TLAS's leaf primitives are instances; on an
+// instance the TLAS group is parked, the ray is taken into object space and
+// the instance's BLAS is walked on top of the same stack; the TLAS group
+// resumes when the stack is back at the depth it had on entry.
+struct WideTrav {
+    float3 wo, wd;      // world-space ray
+    float3 o, inv;      // ray of the level being walked
+    Shear sh;           // watertight-test constants (BLAS level)
+    uint32_t oct;
+    WideGroup g, parked;
+    uint32_t inst;
+    int blasBase;       // stack depth at BLAS entry; -1 while in the TLAS
+    int sp;
+    uint32_t visits;
+    float tMax;
+    HitRecord hit;
+    bool ok;            // cleared on a stack overflow or an exhausted visit budget
+};
+// The stack of node groups lives apart from WideTrav (an array the walk
+// indexes dynamically sits in local memory; kept separate, the scalar state
+// stays in registers).
+typedef uint2 WideStack[MRT_WIDE_STACK];
+
+MRT_DEV void travBegin(const MrtFrameParams& P, WideTrav& T, float3 o, float3 d, float tMax) {
+    T.wo = o;
+    T.wd = d;
+    T.o = o;
+    T.inv = safeInv(d);
+    T.oct = rayOctant(d);
+    T.sh = Shear{0, 1, 2, 0.0f, 0.0f, 0.0f};
+    // a group whose only hit is the root; none in an empty scene (the TLAS
+    // root is then a placeholder)
+    T.g = WideGroup{P.tlasRoot, 0u, P.instanceCount ? 0x80000000u : 0u, 0u};
+    T.parked = WideGroup{0u, 0u, 0u, 0u};
+    T.inst = 0;
+    T.blasBase = -1;
+    T.sp = 0;
+    T.visits = 0;
+    T.tMax = tMax;
+    T.hit.t = tMax;
+    T.hit.u = T.hit.v = 0.0f;
+    T.hit.tri = 0xffffffffu;
+    T.hit.inst = 0;
+    T.ok = true;
+}
+
+enum { kTravRunning = 0, kTravDone = 1, kTravOccluded = 2 };
+
+// One step: the triangles of the current group, then one node visit, one
+// instance entry or exit, or one stack pop. kAny: returns kTravOccluded at
+// the first triangle with t in (1e-4, tMax). Otherwise closest hit: T.tMax
+// and T.hit updated. Returns kTravDone when the walk is over.
 template <bool kAny>
-MRT_DEV bool traceWide(const MrtFrameParams& P, float3 wo, float3 wd, float& tMax, HitRecord& hit, bool& ok,
-                       TraversalCounters& tc) {
-    if (P.instanceCount == 0) return false;  // empty scene (the TLAS root is a placeholder)
-    float3 o = wo;
-    float3 inv = safeInv(wd);
-    uint32_t oct = rayOctant(wd);
-    Shear sh = {0, 1, 2, 0.0f, 0.0f, 0.0f};  // set on BLAS entry
-    WideGroup g = {P.tlasRoot, 0u, 0x80000000u, 0u};  // a group whose only hit is the root
-    WideGroup parked = {0u, 0u, 0u, 0u};
-    uint32_t inst = 0;
-    int blasBase = -1;  // stack depth at BLAS entry; -1 while in the TLAS
-    int sp = 0;
-    uint2 stack[MRT_WIDE_STACK];
-    uint32_t visits = 0;
-    for (;;) {
-        if (g.primBits) {
-            if (blasBase >= 0) {
-                do {
-                    const uint32_t b = uint32_t(__ffs(g.primBits) - 1);
-                    g.primBits &= g.primBits - 1u;
-                    const uint32_t tri = g.primBase + b;
-                    ++tc.tris;
-                    if (tri >= P.triCount) {
-                        tc.bad = true;
-                        continue;
-                    }
-                    float t, u, v;
-                    if (hitTriangle(P.triVerts, tri, o, sh, tMax, t, u, v)) {
-                        if (kAny) return true;
-                        tMax = t;
-                        hit.t = t;
-                        hit.u = u;
-                        hit.v = v;
-                        hit.tri = tri;
-                        hit.inst = inst;
-                    }
-                } while (g.primBits);
-            } else {
-                const uint32_t b = uint32_t(__ffs(g.primBits) - 1);
-                g.primBits &= g.primBits - 1u;
-                const uint32_t instIdx = g.primBase + b;
-                if (instIdx >= P.instanceCount) {
+MRT_DEV int travStep(const MrtFrameParams& P, WideTrav& T, WideStack& stack, TraversalCounters& tc) {
+    if (T.g.primBits) {
+        if (T.blasBase >= 0) {
+            do {
+                const uint32_t b = uint32_t(__ffs(T.g.primBits) - 1);
+                T.g.primBits &= T.g.primBits - 1u;
+                const uint32_t tri = T.g.primBase + b;
+                ++tc.tris;
+                if (tri >= P.triCount) {
                     tc.bad = true;
                     continue;
                 }
-                const MrtInstance* in = P.instances + instIdx;
-                parked = g;
-                blasBase = sp;
-                inst = instIdx;
-                o = xformPoint(in->w2o, wo);
-                const float3 d = xformDir(in->w2o, wd);
-                inv = safeInv(d);
-                oct = rayOctant(d);
-                sh = makeShear(d);
-                g = {in->blasRoot, 0u, 0x80000000u, 0u};
-                continue;
+                float t, u, v;
+                if (hitTriangle(P.triVerts, tri, T.o, T.sh, T.tMax, t, u, v)) {
+                    if (kAny) return kTravOccluded;
+                    T.tMax = t;
+                    T.hit.t = t;
+                    T.hit.u = u;
+                    T.hit.v = v;
+                    T.hit.tri = tri;
+                    T.hit.inst = T.inst;
+                }
+            } while (T.g.primBits);
+        } else {
+            const uint32_t b = uint32_t(__ffs(T.g.primBits) - 1);
+            T.g.primBits &= T.g.primBits - 1u;
+            const uint32_t instIdx = T.g.primBase + b;
+            if (instIdx >= P.instanceCount) {
+                tc.bad = true;
+                return kTravRunning;
             }
+            const MrtInstance* in = P.instances + instIdx;
+            T.parked = T.g;
+            T.blasBase = T.sp;
+            T.inst = instIdx;
+            T.o = xformPoint(in->w2o, T.wo);
+            const float3 d = xformDir(in->w2o, T.wd);
+            T.inv = safeInv(d);
+            T.oct = rayOctant(d);
+            T.sh = makeShear(d);
+            T.g = WideGroup{in->blasRoot, 0u, 0x80000000u, 0u};
+            return kTravRunning;
         }
-        if (g.nodeBits & 0xff000000u) {
-            if (++visits > MRT_MAX_VISITS) {
-                ok = false;
-                return false;
-            }
-            const uint32_t b = 31u - uint32_t(__clz(g.nodeBits & 0xff000000u));
-            const uint32_t rest = g.nodeBits & ~(1u << b);
-            const uint32_t child = childIndex(g.childBase, g.nodeBits & 0xffu, b, oct);
-            if (rest & 0xff000000u) {
-                if (sp < MRT_WIDE_STACK) stack[sp++] = make_uint2(g.childBase, rest);
-                else ok = false;
-            }
-            g = intersectWide(P, child, o, inv, oct, tMax, tc);
-            continue;
-        }
-        if (sp == blasBase) {  // BLAS finished: resume the parked TLAS group
-            g = parked;
-            blasBase = -1;
-            o = wo;
-            inv = safeInv(wd);
-            oct = rayOctant(wd);
-            continue;
-        }
-        if (sp == 0) return false;
-        const uint2 e = stack[--sp];
-        g.childBase = e.x;
-        g.nodeBits = e.y;
-        g.primBits = 0;
     }
+    if (T.g.nodeBits & 0xff000000u) {
+        if (++T.visits > MRT_MAX_VISITS) {
+            T.ok = false;
+            return kTravDone;
+        }
+        const uint32_t b = 31u - uint32_t(__clz(T.g.nodeBits & 0xff000000u));
+        const uint32_t rest = T.g.nodeBits & ~(1u << b);
+        const uint32_t child = childIndex(T.g.childBase, T.g.nodeBits & 0xffu, b, T.oct);
+        if (rest & 0xff000000u) {
+            if (T.sp < MRT_WIDE_STACK) stack[T.sp++] = make_uint2(T.g.childBase, rest);
+            else T.ok = false;
+        }
+        T.g = intersectWide(P, child, T.o, T.inv, T.oct, T.tMax, tc);
+        return kTravRunning;
+    }
+    if (T.sp == T.blasBase) {  // BLAS finished: resume the parked TLAS group
+        T.g = T.parked;
+        T.blasBase = -1;
+        T.o = T.wo;
+        T.inv = safeInv(T.wd);
+        T.oct = rayOctant(T.wd);
+        return kTravRunning;
+    }
+    if (T.sp == 0) return kTravDone;
+    const uint2 e = stack[--T.sp];
+    T.g.childBase = e.x;
+    T.g.nodeBits = e.y;
+    T.g.primBits = 0;
+    return kTravRunning;
 }
 
 // Closest hit over the scene; t and barycentrics of the winner re-evaluated
 // with the reference's arithmetic. Returns false on a traversal error.
 MRT_DEV bool traceClosest(const MrtFrameParams& P, float3 o, float3 d, float tMax, HitRecord& hit, TraversalCounters& tc) {
-    hit.t = tMax;
-    hit.tri = 0xffffffffu;
-    hit.inst = 0;
-    hit.u = hit.v = 0.0f;
-    bool ok = true;
-    traceWide<false>(P, o, d, tMax, hit, ok, tc);
+    WideTrav T;
+    WideStack stack;
+    travBegin(P, T, o, d, tMax);
+    while (travStep<false>(P, T, stack, tc) == kTravRunning) {
+    }
+    hit = T.hit;
     if (hit.tri != 0xffffffffu) refineHit(P, o, d, hit);
-    return ok;
+    return T.ok;
 }
 
 // Any hit in (1e-4, tMax) (reference intersect.glsl:128-178).
 MRT_DEV bool traceAny(const MrtFrameParams& P, float3 o, float3 d, float tMax, bool& ok, TraversalCounters& tc) {
-    HitRecord unused;
-    return traceWide<true>(P, o, d, tMax, unused, ok, tc);
+    WideTrav T;
+    WideStack stack;
+    travBegin(P, T, o, d, tMax);
+    int r;
+    while ((r = travStep<true>(P, T, stack, tc)) == kTravRunning) {
+    }
+    ok &= T.ok;
+    return r == kTravOccluded;
 }
