@@ -378,6 +378,10 @@ def ours_arm(args):
                                  "x rays per step / launches per step"
                                  % (c["nodeBytes"], c["triBytes"], RAY_IO_BYTES)},
             "rays_closest_per_step": c["raysClosest"],
+            "per_ray": {"closest_nodes": c["nodeFetches"] / max(1, c["raysClosest"]),
+                        "closest_tris": c["triTests"] / max(1, c["raysClosest"]),
+                        "shadow_nodes": c["shadowNodeFetches"] / max(1, c["raysShadow"]),
+                        "shadow_tris": c["shadowTriTests"] / max(1, c["raysShadow"])},
             "clocks": clocks,
             "e2e": e2e,
             "cpu_baseline": cpu,

@@ -168,7 +168,23 @@ enum { kExtendHead = 4, kShadowHead = 5 };
 // Lanes of a persistent traversal warp whose ray has finished take new rays
 // from the queue (one warp-aggregated atomic) once at least this many lanes
 // are idle, so warps do not idle on their longest ray (Aila and Laine 2009).
+#ifndef MRT_REFILL_IDLE
 #define MRT_REFILL_IDLE 8
+#endif
+// Threads per block of the traversal kernels and, when non-zero, the
+// minimum resident blocks per SM they are compiled for (which bounds their
+// registers; 0 leaves the register count to the compiler).
+#ifndef MRT_TRAV_THREADS
+#define MRT_TRAV_THREADS 128
+#endif
+#ifndef MRT_TRAV_MIN_BLOCKS
+#define MRT_TRAV_MIN_BLOCKS 7
+#endif
+#if MRT_TRAV_MIN_BLOCKS > 0
+#define MRT_TRAV_BOUNDS __launch_bounds__(MRT_TRAV_THREADS, MRT_TRAV_MIN_BLOCKS)
+#else
+#define MRT_TRAV_BOUNDS __launch_bounds__(MRT_TRAV_THREADS)
+#endif
 
 // Refill step shared by the traversal kernels: idle lanes get consecutive
 // queue positions; `drained` becomes true (warp-uniformly) once the whole
@@ -190,7 +206,7 @@ MRT_DEV uint32_t refillLane(uint32_t* head, uint32_t n, bool active, bool& drain
 // Closest hit of every queued ray (intersect.glsl:88-125 traceRay).
 // Persistent warps with lane refill; every lane of a warp stays in the loop
 // until the warp has no ray left.
-__global__ void __launch_bounds__(128) waveExtendKernel(MrtFrameParams P, MrtWaveState S, uint32_t cur) {
+__global__ void MRT_TRAV_BOUNDS waveExtendKernel(MrtFrameParams P, MrtWaveState S, uint32_t cur) {
     const uint32_t* __restrict__ q = S.queue[cur];
     const uint32_t n = S.counts[cur];
     if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -349,7 +365,7 @@ __global__ void __launch_bounds__(128) waveShadeKernel(MrtFrameParams P, MrtWave
 // contribution to their path (pathtrace.comp:192-195). A path has at most
 // one shadow ray per bounce, so the update needs no atomics. Persistent
 // warps with lane refill, as the extend kernel.
-__global__ void __launch_bounds__(128) waveShadowKernel(MrtFrameParams P, MrtWaveState S) {
+__global__ void MRT_TRAV_BOUNDS waveShadowKernel(MrtFrameParams P, MrtWaveState S) {
     const uint32_t n = S.counts[2];
     if (blockIdx.x == 0 && threadIdx.x == 0) S.counts[kExtendHead] = 0;  // for the next bounce
     uint32_t c[kCtrCount] = {};
@@ -487,9 +503,9 @@ extern "C" cudaError_t mrtcu_wave(const MrtFrameParams* p, const MrtWaveState* s
     if (uint64_t(pixels) * samples > s->capacity) return cudaErrorInvalidValue;
     static int gExtend = 0, gShade = 0, gShadow = 0;
     if (gExtend == 0) {
-        gExtend = persistentBlocks(reinterpret_cast<const void*>(waveExtendKernel), 128);
+        gExtend = persistentBlocks(reinterpret_cast<const void*>(waveExtendKernel), MRT_TRAV_THREADS);
         gShade = persistentBlocks(reinterpret_cast<const void*>(waveShadeKernel), 128);
-        gShadow = persistentBlocks(reinterpret_cast<const void*>(waveShadowKernel), 128);
+        gShadow = persistentBlocks(reinterpret_cast<const void*>(waveShadowKernel), MRT_TRAV_THREADS);
     }
     WaveArgs A{pixels, pixels * samples, sampleBase, samples};
     uint32_t n = 0;
@@ -499,11 +515,11 @@ extern "C" cudaError_t mrtcu_wave(const MrtFrameParams* p, const MrtWaveState* s
         const uint32_t cur = b & 1u;
         const cudaEvent_t* ev = stageEvents ? stageEvents + 6 * b : nullptr;
         if (ev) cudaEventRecord(ev[0], stream);
-        waveExtendKernel<<<gExtend, 128, 0, stream>>>(*p, *s, cur);
+        waveExtendKernel<<<gExtend, MRT_TRAV_THREADS, 0, stream>>>(*p, *s, cur);
         if (ev) cudaEventRecord(ev[1], stream);
         waveShadeKernel<<<gShade, 128, 0, stream>>>(*p, *s, A, cur);
         if (ev) cudaEventRecord(ev[2], stream);
-        waveShadowKernel<<<gShadow, 128, 0, stream>>>(*p, *s);
+        waveShadowKernel<<<gShadow, MRT_TRAV_THREADS, 0, stream>>>(*p, *s);
         if (ev) cudaEventRecord(ev[3], stream);
         n += 3;
     }

@@ -204,6 +204,19 @@ MRT_DEV void slabAxis(float p, uint32_t e, float o, float inv, float& a, float& 
     cFar = __fadd_rn(c, err);
 }
 
+// Three-input min / max (PTX ISA 8.8, sm_100+): one instruction each; like
+// fminf/fmaxf they return the non-NaN operands' extreme.
+MRT_DEV float max3f(float a, float b, float c) {
+    float r;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+MRT_DEV float min3f(float a, float b, float c) {
+    float r;
+    asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+
 // F_q of byte j of a quantised-plane word: 0x4B0000 | q << 8 = 2^23 + 256 q.
 template <int j>
 MRT_DEV float planeF(uint32_t w) {
@@ -211,8 +224,8 @@ MRT_DEV float planeF(uint32_t w) {
 }
 
 // Tests the ray against the eight quantised child boxes of node `idx`
-// (record layout in MrtWideNode). Per child: six planes, three max, three
-// min, one compare. A hit adds the child's meta bits at its bit index:
+// (record layout in MrtWideNode). Per child: six planes (a byte permute and
+// an FMA each), two max, two min, one compare. A hit adds the child's meta bits at its bit index:
 // internal children at 24 + (slot XOR oct), so taking bits from the top
 // visits the slots the ray reaches first first; leaves at their primitive
 // offset. Empty slots have meta 0 and add nothing.
@@ -256,9 +269,10 @@ MRT_DEV WideGroup intersectWide(const MrtFrameParams& P, uint32_t idx, float3 o,
             const float tnx = __fmaf_rn(planeF<j>(wnx), ax, nx), tfx = __fmaf_rn(planeF<j>(wfx), ax, fx);  \
             const float tny = __fmaf_rn(planeF<j>(wny), ay, ny), tfy = __fmaf_rn(planeF<j>(wfy), ay, fy);  \
             const float tnz = __fmaf_rn(planeF<j>(wnz), az, nz), tfz = __fmaf_rn(planeF<j>(wfz), az, fz);  \
-            const float tEnter = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, 0.0f));                                 \
-            const float tExit = fminf(fminf(tfx, tfy), fminf(tfz, tMaxF));                                 \
-            if (tEnter <= tExit) hits |= ((childBits4 >> (8 * j)) & 7u) << ((bitIndex4 >> (8 * j)) & 31u); \
+            const float tEnter = fmaxf(max3f(tnx, tny, tnz), 0.0f);                                        \
+            const float tExit = fminf(min3f(tfx, tfy, tfz), tMaxF);                                        \
+            if (tEnter <= tExit)                                                                           \
+                hits |= __byte_perm(childBits4, 0u, 0x4440u | (j)) << __byte_perm(bitIndex4, 0u, 0x4440u | (j)); \
         }
         MRT_WIDE_CHILD(0)
         MRT_WIDE_CHILD(1)
