@@ -231,7 +231,8 @@ __global__ void MRT_TRAV_BOUNDS waveExtendKernel(MrtFrameParams P, MrtWaveState 
             }
         }
         if (!__any_sync(0xffffffffu, active)) break;
-        if (active && travStep<false>(P, T, stack, tc) != kTravRunning) {
+        const int r = travWarpStep<false>(P, T, stack, tc, active);
+        if (active && r != kTravRunning) {
             HitRecord h = T.hit;
             if (h.tri != 0xffffffffu) refineHit(P, T.wo, T.wd, h);
             S.hit[slot] = make_float4(h.t, h.u, h.v, __uint_as_float(h.tri));
@@ -386,8 +387,8 @@ __global__ void MRT_TRAV_BOUNDS waveShadowKernel(MrtFrameParams P, MrtWaveState 
             }
         }
         if (!__any_sync(0xffffffffu, active)) break;
+        const int r = travWarpStep<true>(P, T, stack, tc, active);
         if (active) {
-            const int r = travStep<true>(P, T, stack, tc);
             if (r != kTravRunning) {
                 ok &= T.ok;
                 if (r != kTravOccluded) {

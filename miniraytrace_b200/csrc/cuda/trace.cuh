@@ -301,7 +301,7 @@ MRT_DEV uint32_t childIndex(uint32_t childBase, uint32_t imask, uint32_t b, uint
 // being walked.
 #define MRT_WIDE_STACK 48
 
-// Traversal state of one ray, advanced one step at a time (travStep), so a
+// Traversal state of one ray, advanced one step at a time (travWarpStep), so a
 // persistent warp can start a new ray in a lane whose ray has finished while
 // the other lanes keep walking. Two-level walk in one loop (reference
 // intersect.glsl:88-178): the TLAS's leaf primitives are instances; on an
@@ -320,6 +320,7 @@ struct WideTrav {
     uint32_t visits;
     float tMax;
     HitRecord hit;
+    uint32_t pendBase, pendBits;  // BLAS leaf hits of the last node, awaiting their triangle tests
     bool ok;            // cleared on a stack overflow or an exhausted visit budget
 };
 // The stack of node groups lives apart from WideTrav (an array the walk
@@ -347,46 +348,26 @@ MRT_DEV void travBegin(const MrtFrameParams& P, WideTrav& T, float3 o, float3 d,
     T.hit.u = T.hit.v = 0.0f;
     T.hit.tri = 0xffffffffu;
     T.hit.inst = 0;
+    T.pendBase = T.pendBits = 0;
     T.ok = true;
 }
 
 enum { kTravRunning = 0, kTravDone = 1, kTravOccluded = 2 };
 
-// One step: the triangles of the current group, then one node visit, one
-// instance entry or exit, or one stack pop. kAny: returns kTravOccluded at
-// the first triangle with t in (1e-4, tMax). Otherwise closest hit: T.tMax
-// and T.hit updated. Returns kTravDone when the walk is over.
-template <bool kAny>
-MRT_DEV int travStep(const MrtFrameParams& P, WideTrav& T, WideStack& stack, TraversalCounters& tc) {
-    if (T.g.primBits) {
-        if (T.blasBase >= 0) {
-            do {
-                const uint32_t b = uint32_t(__ffs(T.g.primBits) - 1);
-                T.g.primBits &= T.g.primBits - 1u;
-                const uint32_t tri = T.g.primBase + b;
-                ++tc.tris;
-                if (tri >= P.triCount) {
-                    tc.bad = true;
-                    continue;
-                }
-                float t, u, v;
-                if (hitTriangle(P.triVerts, tri, T.o, T.sh, T.tMax, t, u, v)) {
-                    if (kAny) return kTravOccluded;
-                    T.tMax = t;
-                    T.hit.t = t;
-                    T.hit.u = u;
-                    T.hit.v = v;
-                    T.hit.tri = tri;
-                    T.hit.inst = T.inst;
-                }
-            } while (T.g.primBits);
-        } else {
+// Node step of one lane with no triangles pending: bookkeeping (instance
+// entry, return to the TLAS, stack pops) until one node has been tested.
+// The BLAS leaf hits of that node become the lane's pending triangles; TLAS
+// leaf hits (instances) stay in the group and are entered on the next step.
+// Returns kTravDone when the walk is over.
+MRT_DEV int travNodeStep(const MrtFrameParams& P, WideTrav& T, WideStack& stack, TraversalCounters& tc) {
+    for (;;) {
+        if (T.g.primBits) {  // instances (BLAS leaf hits never stay in the group)
             const uint32_t b = uint32_t(__ffs(T.g.primBits) - 1);
             T.g.primBits &= T.g.primBits - 1u;
             const uint32_t instIdx = T.g.primBase + b;
             if (instIdx >= P.instanceCount) {
                 tc.bad = true;
-                return kTravRunning;
+                continue;
             }
             const MrtInstance* in = P.instances + instIdx;
             T.parked = T.g;
@@ -398,38 +379,103 @@ MRT_DEV int travStep(const MrtFrameParams& P, WideTrav& T, WideStack& stack, Tra
             T.oct = rayOctant(d);
             T.sh = makeShear(d);
             T.g = WideGroup{in->blasRoot, 0u, 0x80000000u, 0u};
+            continue;
+        }
+        if (T.g.nodeBits & 0xff000000u) {
+            if (++T.visits > MRT_MAX_VISITS) {
+                T.ok = false;
+                return kTravDone;
+            }
+            const uint32_t b = 31u - uint32_t(__clz(T.g.nodeBits & 0xff000000u));
+            const uint32_t rest = T.g.nodeBits & ~(1u << b);
+            const uint32_t child = childIndex(T.g.childBase, T.g.nodeBits & 0xffu, b, T.oct);
+            if (rest & 0xff000000u) {
+                if (T.sp < MRT_WIDE_STACK) stack[T.sp++] = make_uint2(T.g.childBase, rest);
+                else T.ok = false;
+            }
+            T.g = intersectWide(P, child, T.o, T.inv, T.oct, T.tMax, tc);
+            if (T.blasBase >= 0 && T.g.primBits) {
+                T.pendBase = T.g.primBase;
+                T.pendBits = T.g.primBits;
+                T.g.primBits = 0;
+            }
             return kTravRunning;
         }
-    }
-    if (T.g.nodeBits & 0xff000000u) {
-        if (++T.visits > MRT_MAX_VISITS) {
-            T.ok = false;
-            return kTravDone;
+        if (T.sp == T.blasBase) {  // BLAS finished: resume the parked TLAS group
+            T.g = T.parked;
+            T.blasBase = -1;
+            T.o = T.wo;
+            T.inv = safeInv(T.wd);
+            T.oct = rayOctant(T.wd);
+            continue;
         }
-        const uint32_t b = 31u - uint32_t(__clz(T.g.nodeBits & 0xff000000u));
-        const uint32_t rest = T.g.nodeBits & ~(1u << b);
-        const uint32_t child = childIndex(T.g.childBase, T.g.nodeBits & 0xffu, b, T.oct);
-        if (rest & 0xff000000u) {
-            if (T.sp < MRT_WIDE_STACK) stack[T.sp++] = make_uint2(T.g.childBase, rest);
-            else T.ok = false;
+        if (T.sp == 0) return kTravDone;
+        const uint2 e = stack[--T.sp];
+        T.g.childBase = e.x;
+        T.g.nodeBits = e.y;
+        T.g.primBits = 0;
+    }
+}
+
+// Triangle step: the lane's pending triangles. kAny: kTravOccluded at the
+// first triangle with t in (1e-4, tMax). Otherwise closest hit: T.tMax and
+// T.hit updated.
+template <bool kAny>
+MRT_DEV int travTriStep(const MrtFrameParams& P, WideTrav& T, TraversalCounters& tc) {
+    while (T.pendBits) {
+        const uint32_t b = uint32_t(__ffs(T.pendBits) - 1);
+        T.pendBits &= T.pendBits - 1u;
+        const uint32_t tri = T.pendBase + b;
+        ++tc.tris;
+        if (tri >= P.triCount) {
+            tc.bad = true;
+            continue;
         }
-        T.g = intersectWide(P, child, T.o, T.inv, T.oct, T.tMax, tc);
-        return kTravRunning;
+        float t, u, v;
+        if (hitTriangle(P.triVerts, tri, T.o, T.sh, T.tMax, t, u, v)) {
+            if (kAny) {
+                T.pendBits = 0;
+                return kTravOccluded;
+            }
+            T.tMax = t;
+            T.hit.t = t;
+            T.hit.u = u;
+            T.hit.v = v;
+            T.hit.tri = tri;
+            T.hit.inst = T.inst;
+        }
     }
-    if (T.sp == T.blasBase) {  // BLAS finished: resume the parked TLAS group
-        T.g = T.parked;
-        T.blasBase = -1;
-        T.o = T.wo;
-        T.inv = safeInv(T.wd);
-        T.oct = rayOctant(T.wd);
-        return kTravRunning;
-    }
-    if (T.sp == 0) return kTravDone;
-    const uint2 e = stack[--T.sp];
-    T.g.childBase = e.x;
-    T.g.nodeBits = e.y;
-    T.g.primBits = 0;
     return kTravRunning;
+}
+
+// One warp-wide traversal step; every lane of the warp calls it, `active`
+// lanes advance their ray. Triangle tests are batched across the warp
+// (after Ylitie et al. 2017, section 4): a lane whose node test found leaf
+// triangles waits with them pending, and the warp runs a triangle phase once
+// at least MRT_TRI_PHASE_PCT percent of its active lanes have triangles
+// pending, or no lane has node work left; otherwise lanes without pending
+// triangles test one node each. Returns the lane's kTrav* state.
+#ifndef MRT_TRI_PHASE_PCT
+#define MRT_TRI_PHASE_PCT 25
+#endif
+template <bool kAny>
+MRT_DEV int travWarpStep(const MrtFrameParams& P, WideTrav& T, WideStack& stack, TraversalCounters& tc,
+                         bool active) {
+    const bool pending = active && T.pendBits != 0;
+    const uint32_t pendLanes = __popc(__ballot_sync(0xffffffffu, pending));
+    const uint32_t activeLanes = __popc(__ballot_sync(0xffffffffu, active));
+    const bool triPhase = pendLanes * 100u >= activeLanes * MRT_TRI_PHASE_PCT || pendLanes == activeLanes;
+    if (triPhase) return pending ? travTriStep<kAny>(P, T, tc) : kTravRunning;
+    return active && !pending ? travNodeStep(P, T, stack, tc) : kTravRunning;
+}
+
+// The same walk for one ray on its own (trace queries).
+template <bool kAny>
+MRT_DEV int travRun(const MrtFrameParams& P, WideTrav& T, WideStack& stack, TraversalCounters& tc) {
+    for (;;) {
+        const int r = T.pendBits ? travTriStep<kAny>(P, T, tc) : travNodeStep(P, T, stack, tc);
+        if (r != kTravRunning) return r;
+    }
 }
 
 // Closest hit over the scene; t and barycentrics of the winner re-evaluated
@@ -438,8 +484,7 @@ MRT_DEV bool traceClosest(const MrtFrameParams& P, float3 o, float3 d, float tMa
     WideTrav T;
     WideStack stack;
     travBegin(P, T, o, d, tMax);
-    while (travStep<false>(P, T, stack, tc) == kTravRunning) {
-    }
+    travRun<false>(P, T, stack, tc);
     hit = T.hit;
     if (hit.tri != 0xffffffffu) refineHit(P, o, d, hit);
     return T.ok;
@@ -450,9 +495,7 @@ MRT_DEV bool traceAny(const MrtFrameParams& P, float3 o, float3 d, float tMax, b
     WideTrav T;
     WideStack stack;
     travBegin(P, T, o, d, tMax);
-    int r;
-    while ((r = travStep<true>(P, T, stack, tc)) == kTravRunning) {
-    }
+    const int r = travRun<true>(P, T, stack, tc);
     ok &= T.ok;
     return r == kTravOccluded;
 }
