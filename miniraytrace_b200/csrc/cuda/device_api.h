@@ -70,6 +70,18 @@ cudaError_t mrtcu_build_wide_bvh(const float4* positions, const uint32_t* indice
                                  uint32_t nodeCapacity, uint32_t* primOrderOut, uint32_t* nodeCountOut,
                                  float boundsOut[6], uint32_t* launchesOut, cudaStream_t stream);
 
+// Commit-time assembly (pack.cu). pack_triangles writes triangles k = 0..nt-1
+// of one mesh (leaf order prims[k]) to slot tbase + k of triVerts/triIndex
+// with vertex ids offset by vbase; error |= 1 on an out-of-range index.
+// rebase_nodes copies n mesh-relative wide nodes to dst + nodeBase with
+// childBase += nodeBase and primBase += triBase.
+cudaError_t mrtcu_pack_triangles(const float4* pos, uint32_t nv, const uint32_t* idx, const uint32_t* prims,
+                                 uint32_t nt, uint32_t vbase, uint32_t tbase, float4* triVerts, uint4* triIndex,
+                                 uint32_t* error, cudaStream_t stream);
+cudaError_t mrtcu_rebase_nodes(const MrtWideNode* src, uint32_t n, uint32_t nodeBase, uint32_t triBase,
+                               MrtWideNode* dst, cudaStream_t stream);
+cudaError_t mrtcu_fill_f4(float4* dst, size_t n, float4 value, cudaStream_t stream);
+
 #ifdef __cplusplus
 }
 #endif

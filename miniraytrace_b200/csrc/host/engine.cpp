@@ -219,8 +219,10 @@ Engine::~Engine() {
                             &m_instances, &m_materials, &m_lights,     &m_envTexels,    &m_envCdf,     &m_envSin,
                             &m_envRowSums, &m_envIntegral, &m_texTable, &m_accum,       &m_out32,      &m_out8,
                             &m_flags,     &m_rayCounters, &m_queryRays, &m_queryOut, &m_wave,
-                            &m_bvhPos,    &m_bvhIdx,    &m_bvhScratch, &m_bvhNodes,    &m_bvhPrims};
+                            &m_bvhPos,    &m_bvhIdx,    &m_bvhScratch, &m_bvhNodes,    &m_bvhPrims,
+                            &m_packError};
     for (DeviceBuffer* b : bufs) b->release();
+    for (auto& [id, b] : m_blas) b.release();
     for (auto& t : m_texData) t.release();
     if (m_pinned) cudaFreeHost(m_pinned);
     for (auto& ev : m_copyEvents)
@@ -420,24 +422,86 @@ mrtResult Engine::packMaterials() {
     return up(m_materials, mats.data(), mats.size() * sizeof(MrtMaterial));
 }
 
-// reference Renderer.cpp:333-446: rebuild dirty BLASes (concurrently), then
-// repack every mesh into the global arrays in id order with triangles in
-// BLAS leaf order and node indices rebased.
+void Engine::Blas::release() {
+    for (DeviceBuffer* d : {&pos, &idx, &normals, &uvs, &tangents, &nodes, &prims}) d->release();
+}
+
+size_t Engine::Blas::deviceBytes() const {
+    size_t n = 0;
+    for (const DeviceBuffer* d : {&pos, &idx, &normals, &uvs, &tangents, &nodes, &prims}) n += d->bytes;
+    return n;
+}
+
+// A changed mesh's vertex data and indices into its own device buffers
+// (missing uvs become zeros, missing tangents (1, 0, 0, 1), as the reference
+// packs them).
+mrtResult Engine::uploadMesh(const MeshData& m, Blas& b) {
+    const size_t nv = m.positions.size(), nt = m.indices.size() / 3;
+    b.vertexCount = uint32_t(nv);
+    b.triCount = uint32_t(nt);
+    MRT_TRY(up(b.pos, m.positions.data(), nv * sizeof(V4f)));
+    MRT_TRY(up(b.idx, m.indices.data(), nt * 3 * sizeof(uint32_t)));
+    MRT_TRY(up(b.normals, m.normals.data(), nv * sizeof(V4f)));
+    if (m.uvs.empty()) {
+        MRT_TRY(b.uvs.ensure(nv * sizeof(V2f)));
+        MRT_CUDA(cudaMemsetAsync(b.uvs.ptr, 0, nv * sizeof(V2f), m_stream));
+    } else {
+        MRT_TRY(up(b.uvs, m.uvs.data(), nv * sizeof(V2f)));
+    }
+    if (m.tangents.empty()) {
+        MRT_TRY(b.tangents.ensure(nv * sizeof(V4f)));
+        MRT_CUDA(mrtcu_fill_f4(b.tangents.as<float4>(), nv, make_float4(1.0f, 0.0f, 0.0f, 1.0f), m_stream));
+    } else {
+        MRT_TRY(up(b.tangents, m.tangents.data(), nv * sizeof(V4f)));
+    }
+    return MRT_SUCCESS;
+}
+
+// BVH of a mesh whose arrays are on the device, built there and copied into
+// the mesh's own node / order buffers (exactly sized).
+mrtResult Engine::buildBlasOnDevice(Blas& b) {
+    uint32_t count = 0;
+    MRT_TRY(buildBvhOnDevice(b.pos.as<float4>(), b.idx.as<uint32_t>(), b.triCount, 3, count, b.bounds));
+    b.nodeCount = count;
+    MRT_TRY(b.nodes.ensure(size_t(count) * sizeof(MrtWideNode)));
+    MRT_TRY(b.prims.ensure(size_t(b.triCount) * sizeof(uint32_t)));
+    MRT_CUDA(cudaMemcpyAsync(b.nodes.ptr, m_bvhNodes.ptr, size_t(count) * sizeof(MrtWideNode),
+                             cudaMemcpyDeviceToDevice, m_stream));
+    MRT_CUDA(cudaMemcpyAsync(b.prims.ptr, m_bvhPrims.ptr, size_t(b.triCount) * sizeof(uint32_t),
+                             cudaMemcpyDeviceToDevice, m_stream));
+    return MRT_SUCCESS;
+}
+
+// reference Renderer.cpp:333-446: rebuild dirty BLASes, then repack every
+// mesh into the global arrays in id order with triangles in BLAS leaf order
+// and node indices rebased. Here a changed mesh is uploaded once to its own
+// device buffers; large meshes get their BVH built on the GPU from those,
+// small ones on host threads (concurrently); the global arrays are then
+// assembled on the device (node rebase, triangle gather, attribute copies).
 mrtResult Engine::packGeometry(uint32_t& rebuilt) {
     auto& meshes = m_scene.meshes();
-    for (auto it = m_blas.begin(); it != m_blas.end();)
-        it = meshes.count(it->first) ? std::next(it) : m_blas.erase(it);
-    const auto tb = std::chrono::steady_clock::now();
-    std::vector<std::pair<uint32_t, std::future<WideBvh>>> jobs;
-    std::vector<uint32_t> deviceJobs;
-    const unsigned threads = m_hostThreads;
-    for (auto& [id, mesh] : meshes) {
-        if (!mesh.blasDirty && m_blas.count(id)) continue;
-        if (mesh.indices.size() / 3 >= kDeviceBuildMinTriangles) {
-            deviceJobs.push_back(id);
+    for (auto it = m_blas.begin(); it != m_blas.end();) {
+        if (meshes.count(it->first)) {
+            ++it;
             continue;
         }
-        MeshData* m = &mesh;
+        it->second.release();
+        it = m_blas.erase(it);
+    }
+    std::vector<uint32_t> changed;
+    for (auto& [id, mesh] : meshes)
+        if (mesh.blasDirty || !m_blas.count(id)) changed.push_back(id);
+
+    const auto tu = std::chrono::steady_clock::now();
+    for (uint32_t id : changed) MRT_TRY(uploadMesh(meshes[id], m_blas[id]));
+    m_stats.commitUploadMs += std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - tu).count();
+
+    const auto tb = std::chrono::steady_clock::now();
+    std::vector<std::pair<uint32_t, std::future<WideBvh>>> jobs;
+    const unsigned threads = m_hostThreads;
+    for (uint32_t id : changed) {
+        MeshData* m = &meshes[id];
+        if (m->indices.size() / 3 >= kDeviceBuildMinTriangles) continue;
         jobs.emplace_back(id, std::async(std::launch::async, [m, threads] {
                               const std::vector<Box3> boxes = triangleBoxes(
                                   &m->positions[0].x, 4, m->indices.data(), m->indices.size() / 3);
@@ -447,89 +511,66 @@ mrtResult Engine::packGeometry(uint32_t& rebuilt) {
                           }));
     }
     // large meshes on the GPU, while the host builds the small ones
-    for (uint32_t id : deviceJobs) {
-        MeshData& m = meshes[id];
-        WideBvh w;
-        MRT_TRY(buildMeshBvhDevice(m.positions.data(), m.positions.size(), m.indices.data(), m.indices.size() / 3, 3,
-                                   w));
-        m_blas[id].bvh = std::move(w);
-        m.blasDirty = false;
-    }
+    for (uint32_t id : changed)
+        if (meshes[id].indices.size() / 3 >= kDeviceBuildMinTriangles) MRT_TRY(buildBlasOnDevice(m_blas[id]));
     for (auto& [id, fut] : jobs) {
-        m_blas[id].bvh = fut.get();
-        meshes[id].blasDirty = false;
+        const WideBvh w = fut.get();
+        Blas& b = m_blas[id];
+        b.nodeCount = uint32_t(w.nodes.size());
+        b.bounds = w.bounds;
+        if (!w.nodes.empty()) MRT_TRY(up(b.nodes, w.nodes.data(), w.nodes.size() * sizeof(MrtWideNode)));
+        if (!w.primOrder.empty()) MRT_TRY(up(b.prims, w.primOrder.data(), w.primOrder.size() * sizeof(uint32_t)));
     }
-    rebuilt = uint32_t(jobs.size() + deviceJobs.size());
+    for (uint32_t id : changed) meshes[id].blasDirty = false;
+    rebuilt = uint32_t(changed.size());
     m_stats.commitBvhMs += std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - tb).count();
 
+    // global layout in mesh id order
+    const auto ta = std::chrono::steady_clock::now();
     size_t nv = 0, nt = 0, nn = 0;
-    for (auto& [id, mesh] : meshes) {
-        nv += mesh.positions.size();
-        nt += mesh.indices.size() / 3;
-        nn += m_blas[id].bvh.nodes.size();
+    for (auto& [id, b] : m_blas) {
+        b.nodeBase = uint32_t(nn);
+        nv += b.vertexCount;
+        nt += b.triCount;
+        nn += b.nodeCount;
     }
-    std::vector<float4> triVerts(nt * 3);
-    std::vector<uint4> triIndex(nt);
-    std::vector<V4f> normals;
-    std::vector<V2f> uvs;
-    std::vector<V4f> tangents;
-    normals.reserve(nv);
-    uvs.reserve(nv);
-    tangents.reserve(nv);
-    std::vector<MrtWideNode> nodes;
-    nodes.reserve(nn + 1);
-    uint32_t vbase = 0, tbase = 0;
-    for (auto& [id, mesh] : meshes) {
-        Blas& b = m_blas[id];
-        b.nodeBase = uint32_t(nodes.size());
-        normals.insert(normals.end(), mesh.normals.begin(), mesh.normals.end());
-        if (mesh.uvs.empty()) uvs.insert(uvs.end(), mesh.positions.size(), V2f{0, 0});
-        else uvs.insert(uvs.end(), mesh.uvs.begin(), mesh.uvs.end());
-        if (mesh.tangents.empty()) tangents.insert(tangents.end(), mesh.positions.size(), V4f{1, 0, 0, 1});
-        else tangents.insert(tangents.end(), mesh.tangents.begin(), mesh.tangents.end());
-        const uint32_t* idx = mesh.indices.data();
-        const auto& order = b.bvh.primOrder;
-        for (size_t k = 0; k < order.size(); ++k) {
-            const uint32_t lt = order[k];
-            const uint32_t i0 = idx[lt * 3], i1 = idx[lt * 3 + 1], i2 = idx[lt * 3 + 2];
-            const V4f& p0 = mesh.positions[i0];
-            const V4f& p1 = mesh.positions[i1];
-            const V4f& p2 = mesh.positions[i2];
-            const size_t slot = tbase + k;
-            uint32_t origBits = lt, slotBits = uint32_t(slot);
-            float fo, fs;
-            std::memcpy(&fo, &origBits, 4);
-            std::memcpy(&fs, &slotBits, 4);
-            triVerts[slot * 3 + 0] = make_float4(p0.x, p0.y, p0.z, fo);
-            triVerts[slot * 3 + 1] = make_float4(p1.x, p1.y, p1.z, fs);
-            triVerts[slot * 3 + 2] = make_float4(p2.x, p2.y, p2.z, 0.0f);
-            triIndex[slot] = make_uint4(i0 + vbase, i1 + vbase, i2 + vbase, lt);
-        }
-        for (MrtWideNode n : b.bvh.nodes) {
-            n.childBase += b.nodeBase;
-            n.primBase += tbase;
-            nodes.push_back(n);
-        }
-        vbase += uint32_t(mesh.positions.size());
-        tbase += uint32_t(order.size());
-    }
-    m_blasNodeCount = uint32_t(nodes.size());
-    m_triCount = uint32_t(nt);
-    const auto tu = std::chrono::steady_clock::now();
+    if (nt > 0x7fffffffu / 3 || nv > 0xffffffffu || nn > 0xffffffffu)
+        return fail(MRT_ERROR_INVALID_ARGUMENT, "scene too large");
     // node buffer keeps room for the TLAS (at most one wide node per instance) behind the BLAS region
     const size_t tlasCap = std::max<size_t>(m_scene.instances().size() + 1, 4);
-    MRT_TRY(m_nodes.ensure((nodes.size() + tlasCap) * sizeof(MrtWideNode)));
-    if (!nodes.empty())
-        MRT_CUDA(cudaMemcpyAsync(m_nodes.ptr, nodes.data(), nodes.size() * sizeof(MrtWideNode),
-                                 cudaMemcpyHostToDevice, m_stream));
-    m_stats.commitH2DBytes += nodes.size() * sizeof(MrtWideNode);
-    MRT_TRY(up(m_triVerts, triVerts.data(), triVerts.size() * sizeof(float4)));
-    MRT_TRY(up(m_triIndex, triIndex.data(), triIndex.size() * sizeof(uint4)));
-    MRT_TRY(up(m_normals, normals.data(), normals.size() * sizeof(V4f)));
-    MRT_TRY(up(m_uvs, uvs.data(), uvs.size() * sizeof(V2f)));
-    MRT_TRY(up(m_tangents, tangents.data(), tangents.size() * sizeof(V4f)));
+    MRT_TRY(m_nodes.ensure((nn + tlasCap) * sizeof(MrtWideNode)));
+    MRT_TRY(m_triVerts.ensure(nt * 3 * sizeof(float4)));
+    MRT_TRY(m_triIndex.ensure(nt * sizeof(uint4)));
+    MRT_TRY(m_normals.ensure(nv * sizeof(V4f)));
+    MRT_TRY(m_uvs.ensure(nv * sizeof(V2f)));
+    MRT_TRY(m_tangents.ensure(nv * sizeof(V4f)));
+    MRT_TRY(m_packError.ensure(16));
+    MRT_CUDA(cudaMemsetAsync(m_packError.ptr, 0, 4, m_stream));
+    uint32_t vbase = 0, tbase = 0;
+    for (auto& [id, b] : m_blas) {
+        MRT_CUDA(mrtcu_rebase_nodes(b.nodes.as<MrtWideNode>(), b.nodeCount, b.nodeBase, tbase,
+                                    m_nodes.as<MrtWideNode>(), m_stream));
+        MRT_CUDA(mrtcu_pack_triangles(b.pos.as<float4>(), b.vertexCount, b.idx.as<uint32_t>(), b.prims.as<uint32_t>(),
+                                      b.triCount, vbase, tbase, m_triVerts.as<float4>(), m_triIndex.as<uint4>(),
+                                      m_packError.as<uint32_t>(), m_stream));
+        if (b.vertexCount) {
+            MRT_CUDA(cudaMemcpyAsync(m_normals.as<V4f>() + vbase, b.normals.ptr, b.vertexCount * sizeof(V4f),
+                                     cudaMemcpyDeviceToDevice, m_stream));
+            MRT_CUDA(cudaMemcpyAsync(m_uvs.as<V2f>() + vbase, b.uvs.ptr, b.vertexCount * sizeof(V2f),
+                                     cudaMemcpyDeviceToDevice, m_stream));
+            MRT_CUDA(cudaMemcpyAsync(m_tangents.as<V4f>() + vbase, b.tangents.ptr, b.vertexCount * sizeof(V4f),
+                                     cudaMemcpyDeviceToDevice, m_stream));
+        }
+        vbase += b.vertexCount;
+        tbase += b.triCount;
+    }
+    uint32_t packError = 0;
+    MRT_CUDA(cudaMemcpyAsync(&packError, m_packError.ptr, 4, cudaMemcpyDeviceToHost, m_stream));
     MRT_CUDA(cudaStreamSynchronize(m_stream));
-    m_stats.commitUploadMs += std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - tu).count();
+    if (packError) return fail(MRT_ERROR_UNKNOWN, "scene packing met an out-of-range index");
+    m_blasNodeCount = uint32_t(nn);
+    m_triCount = uint32_t(nt);
+    m_stats.commitUploadMs += std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - ta).count();
     return MRT_SUCCESS;
 }
 
@@ -541,10 +582,10 @@ mrtResult Engine::packInstances() {
     std::vector<Box3> boxes;
     for (const auto& [id, in] : m_scene.instances()) {
         auto it = m_blas.find(in.mesh);
-        if (it == m_blas.end() || it->second.bvh.nodes.empty()) continue;
+        if (it == m_blas.end() || it->second.nodeCount == 0) continue;
         flat.push_back(&in);
         ids.push_back(id);
-        boxes.push_back(transformBox(it->second.bvh.bounds, in.o2w));
+        boxes.push_back(transformBox(it->second.bounds, in.o2w));
     }
     const auto tb = std::chrono::steady_clock::now();
     WideBvh tlas = collapseToWide(buildBvh(boxes, 1, 1), 1);
@@ -1005,8 +1046,10 @@ mrtResult Engine::getStats(mrtxStats* out) const {
                                   &m_tangents,  &m_instances, &m_materials,  &m_lights,      &m_envTexels,
                                   &m_envCdf,    &m_envSin,    &m_envRowSums, &m_envIntegral, &m_texTable,
                                   &m_accum,     &m_out32,     &m_out8,       &m_flags,       &m_rayCounters,
-                                  &m_queryRays, &m_queryOut,    &m_wave};
+                                  &m_queryRays, &m_queryOut,    &m_wave,       &m_bvhPos,      &m_bvhIdx,
+                                  &m_bvhScratch, &m_bvhNodes,  &m_bvhPrims,  &m_packError};
     for (const DeviceBuffer* b : bufs) bytes += b->bytes;
+    for (const auto& [id, b] : m_blas) bytes += b.deviceBytes();
     for (const auto& t : m_texData) bytes += t.bytes;
     s.deviceBytes = bytes;
     *out = s;
@@ -1039,6 +1082,26 @@ mrtResult Engine::copyAccumulationDevice(void* dev, size_t bytes, bool accumulat
     return MRT_SUCCESS;
 }
 
+mrtResult Engine::buildBvhOnDevice(const float4* pos, const uint32_t* idx, size_t nt, uint32_t maxLeaf,
+                                   uint32_t& count, Box3& bounds) {
+    count = 0;
+    if (nt == 0) return MRT_SUCCESS;
+    if (nt > 0x7fffffffu / 3) return fail(MRT_ERROR_INVALID_ARGUMENT, "mesh too large for the device BVH builder");
+    MRT_TRY(m_bvhScratch.ensure(mrtcu_wide_bvh_scratch_bytes(uint32_t(nt))));
+    MRT_TRY(m_bvhNodes.ensure(nt * sizeof(MrtWideNode)));
+    MRT_TRY(m_bvhPrims.ensure(nt * sizeof(uint32_t)));
+    float box[6];
+    const cudaError_t e = mrtcu_build_wide_bvh(pos, idx, uint32_t(nt), maxLeaf, m_bvhScratch.ptr, m_bvhScratch.bytes,
+                                               m_bvhNodes.as<MrtWideNode>(), uint32_t(nt), m_bvhPrims.as<uint32_t>(),
+                                               &count, box, nullptr, m_stream);
+    if (e != cudaSuccess) return guard(fromCuda(e, "device BVH build"));
+    for (int k = 0; k < 3; ++k) {
+        bounds.lo[k] = box[k];
+        bounds.hi[k] = box[3 + k];
+    }
+    return MRT_SUCCESS;
+}
+
 mrtResult Engine::buildMeshBvhDevice(const V4f* pos, size_t nv, const uint32_t* idx, size_t nt, uint32_t maxLeaf,
                                      WideBvh& out) {
     MRT_TRY(checkAlive());
@@ -1052,16 +1115,8 @@ mrtResult Engine::buildMeshBvhDevice(const V4f* pos, size_t nv, const uint32_t* 
         return fail(MRT_ERROR_INVALID_ARGUMENT, "mesh too large for the device BVH builder");
     MRT_TRY(up(m_bvhPos, pos, nv * sizeof(V4f)));
     MRT_TRY(up(m_bvhIdx, idx, nt * 3 * sizeof(uint32_t)));
-    MRT_TRY(m_bvhScratch.ensure(mrtcu_wide_bvh_scratch_bytes(uint32_t(nt))));
-    MRT_TRY(m_bvhNodes.ensure(nt * sizeof(MrtWideNode)));
-    MRT_TRY(m_bvhPrims.ensure(nt * sizeof(uint32_t)));
     uint32_t count = 0;
-    float bounds[6];
-    const cudaError_t e = mrtcu_build_wide_bvh(m_bvhPos.as<float4>(), m_bvhIdx.as<uint32_t>(), uint32_t(nt), maxLeaf,
-                                               m_bvhScratch.ptr, m_bvhScratch.bytes, m_bvhNodes.as<MrtWideNode>(),
-                                               uint32_t(nt), m_bvhPrims.as<uint32_t>(), &count, bounds, nullptr,
-                                               m_stream);
-    if (e != cudaSuccess) return guard(fromCuda(e, "device BVH build"));
+    MRT_TRY(buildBvhOnDevice(m_bvhPos.as<float4>(), m_bvhIdx.as<uint32_t>(), nt, maxLeaf, count, out.bounds));
     out.nodes.resize(count);
     out.primOrder.resize(nt);
     MRT_CUDA(cudaMemcpyAsync(out.nodes.data(), m_bvhNodes.ptr, count * sizeof(MrtWideNode), cudaMemcpyDeviceToHost,
@@ -1069,10 +1124,6 @@ mrtResult Engine::buildMeshBvhDevice(const V4f* pos, size_t nv, const uint32_t* 
     MRT_CUDA(cudaMemcpyAsync(out.primOrder.data(), m_bvhPrims.ptr, nt * sizeof(uint32_t), cudaMemcpyDeviceToHost,
                              m_stream));
     MRT_CUDA(cudaStreamSynchronize(m_stream));
-    for (int k = 0; k < 3; ++k) {
-        out.bounds.lo[k] = bounds[k];
-        out.bounds.hi[k] = bounds[3 + k];
-    }
     return MRT_SUCCESS;
 }
 

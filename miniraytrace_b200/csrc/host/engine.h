@@ -62,6 +62,10 @@ public:
     // topology, SAH-optimal collapse), read back into `out`.
     mrtResult buildMeshBvhDevice(const V4f* pos, size_t nv, const uint32_t* idx, size_t nt, uint32_t maxLeaf,
                                  WideBvh& out);
+    // Device build from device positions/indices into the builder's own
+    // output buffers (m_bvhNodes, m_bvhPrims).
+    mrtResult buildBvhOnDevice(const float4* pos, const uint32_t* idx, size_t nt, uint32_t maxLeaf, uint32_t& count,
+                               Box3& bounds);
 
 private:
     Engine() = default;
@@ -107,16 +111,27 @@ private:
     DeviceBuffer m_accum, m_out32, m_out8, m_flags, m_rayCounters, m_queryRays, m_queryOut;
     DeviceBuffer m_wave;  // wavefront path state (one allocation, carved into MrtWaveState arrays)
     DeviceBuffer m_bvhPos, m_bvhIdx, m_bvhScratch, m_bvhNodes, m_bvhPrims;  // device BVH builder
+    DeviceBuffer m_packError;  // error word of the commit-time assembly kernels
     MrtWaveState m_waveState{};
     uint32_t m_waveSamples = 0;  // samples per pixel one wave holds
     void* m_pinned = nullptr;
     size_t m_pinnedBytes = 0;
 
     // host-side packing state
+    // One mesh on the device: its own copies of the vertex data, indices and
+    // 8-wide BVH (object space, mesh-relative indices), uploaded or built when
+    // the mesh changes; commits assemble the global arrays from these.
     struct Blas {
-        WideBvh bvh;  // 8-wide BVH over the mesh's triangles (object space)
+        DeviceBuffer pos, idx, normals, uvs, tangents, nodes, prims;
+        uint32_t vertexCount = 0, triCount = 0, nodeCount = 0;
+        Box3 bounds{{3.402823466e38f, 3.402823466e38f, 3.402823466e38f},
+                    {-3.402823466e38f, -3.402823466e38f, -3.402823466e38f}};
         uint32_t nodeBase = 0;
+        void release();
+        size_t deviceBytes() const;
     };
+    mrtResult uploadMesh(const MeshData& m, Blas& b);
+    mrtResult buildBlasOnDevice(Blas& b);
     std::map<uint32_t, Blas> m_blas;
     std::map<uint32_t, uint32_t> m_materialIndex;
     uint32_t m_nodeCount = 0, m_blasNodeCount = 0, m_triCount = 0, m_materialCount = 1;
