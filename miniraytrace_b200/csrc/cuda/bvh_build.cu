@@ -135,17 +135,16 @@ __global__ void __launch_bounds__(kSortThreads) sortHistKernel(const uint32_t* _
     hist[threadIdx.x * tiles + blockIdx.x] = h[threadIdx.x];
 }
 
-// Exclusive scan of `len` words in place, one block.
-__global__ void __launch_bounds__(kScanThreads) scanKernel(uint32_t* __restrict__ data, uint32_t len) {
+// Exclusive scan of `len` words in place: each block scans a segment of
+// kScanSegment words (four per thread) and writes its total; the totals are
+// scanned by one block (a single segment) and added back to every segment.
+constexpr uint32_t kScanSegment = 4 * kScanThreads;
+
+// Block-wide exclusive scan of one value per thread; *total gets the sum.
+__device__ uint32_t blockExclusiveScan(uint32_t v, uint32_t* total) {
     __shared__ uint32_t warpSums[kScanThreads / 32];
-    const uint32_t chunk = (len + kScanThreads - 1) / kScanThreads;
-    const uint32_t b = threadIdx.x * chunk;
-    const uint32_t e = min(len, b + chunk);
-    uint32_t sum = 0;
-    for (uint32_t i = b; i < e; ++i) sum += data[i];
-    // block exclusive scan of the per-thread sums
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    uint32_t x = sum;
+    uint32_t x = v;
     for (int o = 1; o < 32; o <<= 1) {
         const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
         if (lane >= o) x += y;
@@ -161,12 +160,34 @@ __global__ void __launch_bounds__(kScanThreads) scanKernel(uint32_t* __restrict_
         if (lane < kScanThreads / 32) warpSums[lane] = w;
     }
     __syncthreads();
-    uint32_t run = x - sum + (warp > 0 ? warpSums[warp - 1] : 0u);
-    for (uint32_t i = b; i < e; ++i) {
-        const uint32_t v = data[i];
-        data[i] = run;
-        run += v;
+    const uint32_t excl = x - v + (warp > 0 ? warpSums[warp - 1] : 0u);
+    if (total) *total = warpSums[kScanThreads / 32 - 1];
+    __syncthreads();
+    return excl;
+}
+
+// Scans segment blockIdx.x of data in place; its total goes to sums[blockIdx.x].
+__global__ void __launch_bounds__(kScanThreads) scanSegmentsKernel(uint32_t* __restrict__ data, uint32_t len,
+                                                                   uint32_t* __restrict__ sums) {
+    const uint32_t b = blockIdx.x * kScanSegment + threadIdx.x * 4;
+    uint32_t v[4];
+    for (int k = 0; k < 4; ++k) v[k] = b + k < len ? data[b + k] : 0u;
+    const uint32_t t = v[0] + v[1] + v[2] + v[3];
+    uint32_t total = 0;
+    uint32_t run = blockExclusiveScan(t, &total);
+    for (int k = 0; k < 4; ++k) {
+        if (b + k < len) data[b + k] = run;
+        run += v[k];
     }
+    if (threadIdx.x == 0 && sums) sums[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(kScanThreads) addSegmentOffsetsKernel(uint32_t* __restrict__ data, uint32_t len,
+                                                                        const uint32_t* __restrict__ offsets) {
+    const uint32_t add = offsets[blockIdx.x];
+    const uint32_t b = blockIdx.x * kScanSegment + threadIdx.x * 4;
+    for (int k = 0; k < 4; ++k)
+        if (b + k < len) data[b + k] += add;
 }
 
 __global__ void __launch_bounds__(kSortThreads)
@@ -487,6 +508,7 @@ extern "C" size_t mrtcu_wide_bvh_scratch_bytes(uint32_t triCount) {
     b += 2 * alignUp(n * 16);              // triangle boxes
     b += 4 * alignUp(n * 4);               // keys / values, two buffers each
     b += alignUp(256 * tiles * 4);         // histogram
+    b += alignUp(kScanSegment * 4);        // scan segment totals
     b += 4 * alignUp(n * 4);               // left, right, first, count
     b += alignUp(2 * n * 4);               // parent
     b += 2 * alignUp(n * 16);              // internal boxes
@@ -510,6 +532,9 @@ extern "C" cudaError_t mrtcu_build_wide_bvh(const float4* positions, const uint3
         return cudaErrorInvalidValue;
     const uint32_t n = triCount;
     const uint32_t tiles = (n + kSortTile - 1) / kSortTile;
+    // the scan of the sort histogram takes at most kScanSegment segments
+    // (meshes of up to 134 M triangles)
+    if ((256u * uint64_t(tiles) + kScanSegment - 1) / kScanSegment > kScanSegment) return cudaErrorInvalidValue;
     Carve c{static_cast<char*>(scratch)};
     uint32_t* ctr = c.take<uint32_t>(kCtrWords);
     float4* triLo = c.take<float4>(n);
@@ -519,6 +544,7 @@ extern "C" cudaError_t mrtcu_build_wide_bvh(const float4* positions, const uint3
     uint32_t* valsA = c.take<uint32_t>(n);
     uint32_t* valsB = c.take<uint32_t>(n);
     uint32_t* hist = c.take<uint32_t>(size_t(256) * tiles);
+    uint32_t* segSums = c.take<uint32_t>(kScanSegment);
     Tree T;
     T.n = n;
     T.left = c.take<uint32_t>(n);
@@ -552,7 +578,15 @@ extern "C" cudaError_t mrtcu_build_wide_bvh(const float4* positions, const uint3
         uint32_t* kOut = pass & 1 ? keysA : keysB;
         uint32_t* vOut = pass & 1 ? valsA : valsB;
         sortHistKernel<<<tiles, kSortThreads, 0, stream>>>(kIn, n, shift, hist, tiles);
-        scanKernel<<<1, kScanThreads, 0, stream>>>(hist, 256u * tiles);
+        const uint32_t len = 256u * tiles, segments = (len + kScanSegment - 1) / kScanSegment;
+        if (segments == 1) {
+            scanSegmentsKernel<<<1, kScanThreads, 0, stream>>>(hist, len, nullptr);
+        } else {
+            scanSegmentsKernel<<<segments, kScanThreads, 0, stream>>>(hist, len, segSums);
+            scanSegmentsKernel<<<1, kScanThreads, 0, stream>>>(segSums, segments, nullptr);
+            addSegmentOffsetsKernel<<<segments, kScanThreads, 0, stream>>>(hist, len, segSums);
+            launches += 2;
+        }
         sortScatterKernel<<<tiles, kSortThreads, 0, stream>>>(kIn, vIn, kOut, vOut, n, shift, hist, tiles);
         launches += 3;
     }

@@ -42,6 +42,10 @@ void DeviceBuffer::release() {
 
 namespace {
 
+// Path state per wave slot: rayO, rayD, beta, L, hit (5 x 16 B), hitInst +
+// two queues (3 x 4 B), shadow origin/dir/contribution (3 x 16 B).
+constexpr size_t kWaveBytesPerSlot = 5 * 16 + 3 * 4 + 3 * 16;
+
 // Meshes with at least this many triangles get their BLAS built on the GPU
 // (LBVH topology, about 4% above the binned-SAH tree's cost on a terrain
 // heightfield, in milliseconds instead of a second on the host); smaller
@@ -167,6 +171,12 @@ mrtResult Engine::init(const mrtEngineDesc& desc) {
         return fail(MRT_ERROR_VULKAN_INIT, std::string("cudaSetDevice failed: ") + cudaGetErrorString(se));
     cudaDeviceProp prop{};
     MRT_CUDA(cudaGetDeviceProperties(&prop, m_device));
+    // paths in flight per wave: 2^27 (64 spp of a 1080p frame, 18.8 GB of
+    // path state; one wave per 64-spp step leaves one set of short
+    // late-bounce launches instead of one per wave), at most a quarter of
+    // the GPU's memory
+    m_maxWaveSlots = std::max<uint64_t>(1u << 20, std::min<uint64_t>(uint64_t(1) << 27,
+                                                                      prop.totalGlobalMem / 4 / kWaveBytesPerSlot));
     if (prop.major != 10)
         return fail(MRT_ERROR_SHADER_LOAD, std::string("GPU ") + prop.name + " (sm_" + std::to_string(prop.major) +
                                                std::to_string(prop.minor) +
@@ -263,15 +273,13 @@ mrtResult Engine::allocateFrame() {
 // latency of one traversal.
 mrtResult Engine::ensureWave(uint32_t samples) {
     const uint64_t pixels = uint64_t(m_settings.width) * m_settings.height;
-    const uint64_t maxSlots = uint64_t(1) << 25;
+    const uint64_t maxSlots = m_maxWaveSlots;
     uint32_t k = uint32_t(std::max<uint64_t>(1, std::min<uint64_t>(samples, maxSlots / std::max<uint64_t>(pixels, 1))));
     k = std::min<uint32_t>(k, 64);
     if (m_waveSamples >= k) return MRT_SUCCESS;
     const uint64_t slots = pixels * k;
     if (slots > 0xffffffffull) return fail(MRT_ERROR_INVALID_ARGUMENT, "frame too large for one wave");
-    // per slot: rayO, rayD, beta, L, hit (5 x 16 B), hitInst + 2 queues (3 x 4 B),
-    // shadow origin/dir/contribution (3 x 16 B)
-    const size_t bytes = size_t(slots) * (5 * 16 + 3 * 4 + 3 * 16) + 64;
+    const size_t bytes = size_t(slots) * kWaveBytesPerSlot + 64;
     MRT_TRY(m_wave.ensure(bytes));
     char* base = static_cast<char*>(m_wave.ptr);
     auto carve = [&](size_t n) {
@@ -867,10 +875,10 @@ mrtResult Engine::renderFrames(uint32_t count, mrtFrameInfo* info, bool defer) {
 }
 
 // Samples per pixel of one full wave at the current resolution (the wave
-// state holds at most 2^25 paths and 64 samples).
+// state holds at most m_maxWaveSlots paths and 64 samples).
 uint32_t Engine::waveCapacitySamples() const {
     const uint64_t pixels = std::max<uint64_t>(uint64_t(m_settings.width) * m_settings.height, 1);
-    return uint32_t(std::max<uint64_t>(1, std::min<uint64_t>(64, (uint64_t(1) << 25) / pixels)));
+    return uint32_t(std::max<uint64_t>(1, std::min<uint64_t>(64, m_maxWaveSlots / pixels)));
 }
 
 // Renders the queued samples with the frame parameters captured when the

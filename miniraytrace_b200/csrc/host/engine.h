@@ -114,6 +114,7 @@ private:
     DeviceBuffer m_packError;  // error word of the commit-time assembly kernels
     MrtWaveState m_waveState{};
     uint32_t m_waveSamples = 0;  // samples per pixel one wave holds
+    uint64_t m_maxWaveSlots = uint64_t(1) << 25;  // paths per wave, set from the GPU's memory
     void* m_pinned = nullptr;
     size_t m_pinnedBytes = 0;
 
