@@ -214,6 +214,7 @@ def reference_arm(args):
 
 def ours_arm(args):
     import miniraytrace_b200 as mrt
+    from miniraytrace_b200 import replicas
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -243,7 +244,7 @@ def ours_arm(args):
     ids = scene.apply(eng)
     commit = eng.commit()
     st0 = eng.stats()
-    eng.set_sample_stream(rank, world)
+    eng.set_sample_stream(*replicas.sample_stream(rank, world))
 
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")  # > 126 MB L2
     red = torch.empty((H, W, 4), dtype=torch.float64, device="cuda") if world > 1 else None
@@ -254,7 +255,7 @@ def ours_arm(args):
             # every rank's buffer holds its own cumulative samples; their sum on
             # rank 0 is the combined image of all ranks' sample streams
             eng.copy_accumulation_device(red.data_ptr(), red.numel() * 8, False)
-            dist.reduce(red, dst=0)
+            replicas.combine_accumulation(red, dist)
 
     for _ in range(args.warmup):
         flush.fill_(1)
@@ -288,10 +289,7 @@ def ours_arm(args):
     torch.cuda.synchronize()
     clocks = sampler.stop()
     step_ms = [a.elapsed_time(b) for a, b in ev]
-    total = torch.tensor([sum(step_ms)], dtype=torch.float64, device="cuda")
-    if dist:
-        dist.all_reduce(total, op=dist.ReduceOp.MAX)
-    total_ms = float(total.item())
+    total_ms = replicas.max_over_ranks(sum(step_ms), dist, "cuda")
     value = world * paths_per_step * args.steps / (total_ms / 1e3) / 1e6
 
     # roofline of the dominant kernel: the extend (closest-hit) stage, summed
@@ -327,12 +325,10 @@ def ours_arm(args):
             dt = time.perf_counter() - t0
             if k > 0:  # first one warms the host-side allocations
                 e2e_times.append(dt)
-        e2e_t = torch.tensor([float(np.mean(e2e_times))], dtype=torch.float64, device="cuda")
-        if dist:
-            dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
-        e2e = {"value": world * paths_per_step / float(e2e_t.item()) / 1e6, "unit": UNIT,
+        e2e_s = replicas.max_over_ranks(float(np.mean(e2e_times)), dist, "cuda")
+        e2e = {"value": world * paths_per_step / e2e_s / 1e6, "unit": UNIT,
                "h2d_bytes_per_step": int(np.mean(h2d)), "d2h_bytes_per_step": W * H * 16,
-               "seconds_per_step": float(e2e_t.item()),
+               "seconds_per_step": e2e_s,
                "breakdown": "mrtUpdateMesh(heightfield) + mrtSetEnvironment + mrtCommitScene (BVH rebuild, "
                             "packing, env CDF kernel, uploads) + 64 x mrtRenderFrame + RGBA32F readback"}
 

@@ -169,8 +169,7 @@ int orc_render_f32_sum64(void* s, const uint32_t* pixels, uint32_t npix, uint32_
 }
 
 // FP64 evaluation of the same sample streams; sums[3*i..] += L for each
-// frame in [frame0, frame0 + nframes). Sample f of the stream uses frame
-// index f * stride + offset when stride > 0.
+// frame index in [frame0, frame0 + nframes).
 int orc_render_f64(void* s, const uint32_t* pixels, uint32_t npix, uint32_t frame0, uint32_t nframes,
                    double* sums, int threads) {
     auto* o = static_cast<OracleScene*>(s);
