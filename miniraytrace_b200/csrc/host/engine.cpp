@@ -144,6 +144,7 @@ mrtResult Engine::init(const mrtEngineDesc& desc) {
     }
     m_validation = desc.enableValidation != 0;
     m_hostThreads = std::max(1u, std::thread::hardware_concurrency());
+    m_copyPool = std::make_unique<CopyPool>(std::min(5u, m_hostThreads - 1));
     int count = 0;
     const cudaError_t ce = cudaGetDeviceCount(&count);
     if (ce != cudaSuccess || count == 0)
@@ -978,8 +979,8 @@ mrtResult Engine::download(void* dst, const void* src, size_t bytes) {
     for (size_t c = 0; c < nChunks; ++c) {
         MRT_CUDA(cudaEventSynchronize(m_copyEvents[c % window]));
         const size_t off = c * chunk, len = std::min(chunk, bytes - off);
-        std::memcpy(static_cast<char*>(dst) + off, static_cast<const char*>(m_pinned) + off, len);
         if (issued < nChunks) MRT_TRY(issue(issued++));
+        m_copyPool->copy(static_cast<char*>(dst) + off, static_cast<const char*>(m_pinned) + off, len);
     }
     return MRT_SUCCESS;
 }

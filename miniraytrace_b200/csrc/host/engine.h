@@ -8,6 +8,7 @@
 
 #include <cstdint>
 #include <map>
+#include <memory>
 #include <vector>
 
 #include "../../../include/mrt_ext.h"
@@ -16,6 +17,7 @@
 #include "lbvh.h"
 #include "wide_bvh.h"
 #include "common.h"
+#include "copy_pool.h"
 #include "scene.h"
 
 namespace mrt {
@@ -117,6 +119,7 @@ private:
     uint64_t m_maxWaveSlots = uint64_t(1) << 25;  // paths per wave, set from the GPU's memory
     void* m_pinned = nullptr;
     size_t m_pinnedBytes = 0;
+    std::unique_ptr<CopyPool> m_copyPool;  // copies out of m_pinned on several threads
 
     // host-side packing state
     // One mesh on the device: its own copies of the vertex data, indices and
