@@ -222,6 +222,65 @@ def procedural_sky(w=2048, h=1024, sun_elev_deg=30.0, sun_azim_deg=40.0, sun_sig
 
 # ---- configurations -----------------------------------------------------------------
 
+def heightfield_rows(n=4096, rows=2443, amplitude=0.15, seed=7, extent=1.0):
+    """The first `rows` vertex rows (in z) of the n x n heightfield of
+    heightfield(n, ...): the same grid and fBm, cropped; 2 (n-1)(rows-1)
+    triangles."""
+    lin = np.linspace(-extent, extent, n, dtype=np.float64)
+    X, Z = np.meshgrid(lin, lin[:rows])
+    Y = amplitude * value_noise_fbm(X, Z, seed=seed)
+    pos = np.stack([X, Y, Z], -1).reshape(-1, 3).astype(np.float32)
+    dy_dx = np.gradient(Y, lin, axis=1)
+    dy_dz = np.gradient(Y, lin[:rows], axis=0)
+    nrm = np.stack([-dy_dx, np.ones_like(Y), -dy_dz], -1)
+    nrm /= np.linalg.norm(nrm, axis=-1, keepdims=True)
+    a = (np.arange(rows - 1)[:, None] * n + np.arange(n - 1)[None, :]).reshape(-1)
+    b, c, d = a + 1, a + n, a + n + 1
+    idx = np.stack([a, c, b, b, c, d], -1).reshape(-1).astype(np.uint32)
+    return pos, idx, nrm.reshape(-1, 3).astype(np.float32), Y
+
+
+def large(width=3840, height=2160, spp=1024, max_bounces=16, grid=4096, rows=2443, spheres=4096,
+          sky=(4096, 2048), seed=7) -> SceneSpec:
+    """C5, the largest run: the 4096^2 fBm heightfield cropped to 2 x 4095 x 2442
+    = 19,999,980 triangles, 4,096 config-2 icospheres (1,280 triangles each,
+    config-2 material mix) on it, a 4096x2048 sky, 3840x2160, depth 16."""
+    s = SceneSpec("large")
+    pos, idx, nrm, Y = heightfield_rows(grid, rows, 0.15, seed)
+    s.meshes.append(MeshSpec(pos, idx, nrm))
+    rng = np.random.default_rng(seed + 1000)
+    s.materials.append(dict(base_color=tuple(rng.uniform(0.1, 0.9, 3)), roughness=1.0))
+    s.instances.append((0, None, 0))
+    ipos, iidx, inrm = icosphere(3)
+    s.meshes.append(MeshSpec(ipos, iidx, inrm))
+    zmax = -1.0 + 2.0 * (rows - 1) / (grid - 1)
+    for k in range(spheres):
+        x = rng.uniform(-0.95, 0.95)
+        z = rng.uniform(-0.95, zmax - 0.05)
+        r = rng.uniform(0.02, 0.1)
+        gx = int(round((x + 1) / 2 * (grid - 1)))
+        gz = min(int(round((z + 1) / 2 * (grid - 1))), rows - 1)
+        y = float(Y[gz, gx]) + 0.5 * r
+        kind = rng.uniform()
+        if kind < 0.5:
+            m = dict(base_color=tuple(rng.uniform(0.1, 0.9, 3)), roughness=1.0)
+        elif kind < 0.8:
+            m = dict(base_color=tuple(rng.uniform(0.5, 1.0, 3)), metallic=1.0, roughness=float(rng.uniform(0.05, 0.8)))
+        else:
+            m = dict(base_color=(1.0, 1.0, 1.0), transmission=1.0, ior=1.5, roughness=0.05)
+        s.materials.append(m)
+        xf = np.array([[r, 0, 0, x], [0, r, 0, y], [0, 0, r, z]], np.float32)
+        s.instances.append((1, xf, len(s.materials) - 1))
+    s.environment = procedural_sky(*sky)
+    s.camera = dict(position=(0.0, 0.55, 2.1 + zmax - 1.0), target=(0.0, 0.0, zmax - 1.0), up=(0.0, 1.0, 0.0),
+                    fov_y_deg=45.0)
+    s.settings = dict(width=width, height=height, max_bounces=max_bounces, spp_limit=1 << 20,
+                      firefly_clamp=0.0, tonemap=abi.MRT_TONEMAP_LINEAR, denoise=False)
+    s.spp = spp
+    s.meta = dict(grid=grid, rows=rows, spheres=spheres, sky=list(sky), seed=seed)
+    return s
+
+
 def box_sphere(width=256, height=256, spp=16, max_bounces=8, firefly_clamp=0.0) -> SceneSpec:
     """C1: open box + GGX conductor UV sphere under a sun (see module doc)."""
     s = SceneSpec("box_sphere")
