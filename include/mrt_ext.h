@@ -107,6 +107,19 @@ MRT_API mrtResult mrtxSetSampleStream(mrtEngine*, uint32_t offset, uint32_t stri
 MRT_API mrtResult mrtxCopyAccumulationDevice(mrtEngine*, void* devPtr, size_t bytes,
                                              int32_t accumulate);
 
+/* Renders several engines' frames in one submission: engines[i] gets spp[i]
+ * more samples per pixel, as mrtxRenderFrames(engines[i], spp[i], ...) would
+ * give it (the same samples, bit for bit). Every engine commits and prepares
+ * first; then all engines' waves are issued, each on its own CUDA stream,
+ * before any is waited for, so jobs of uneven size overlap on the GPU. The
+ * engines may share a GPU. outInfos (optional, count entries with structSize
+ * set) receive each engine's state; frameMs is the time from the call's
+ * start to that engine's completion. An error stops further launches; engines
+ * already launched are still completed. Builds on the reference's per-frame
+ * submission (Renderer.cpp:773-843), which renders one engine at a time. */
+MRT_API mrtResult mrtxRenderBatch(mrtEngine* const* engines, const uint32_t* spp, uint32_t count,
+                                  mrtFrameInfo* outInfos);
+
 /* Host-side build of the acceleration structure the engine uses for a mesh,
  * for inspection and tests (no device needed): an 8-wide compressed BVH over
  * `count` boxes (6 floats each: lo xyz, hi xyz) with leaves of at most

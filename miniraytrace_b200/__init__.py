@@ -318,6 +318,21 @@ def build_env_cdf_no_alloc(dev_texels: int, width: int, height: int, dev_cdf: in
                                       C.c_void_p(dev_integral), C.c_void_p(stream)), "mrtxBuildEnvCdfNoAlloc")
 
 
+def render_batch(engines, spp):
+    """mrtxRenderBatch: engines[i] renders spp[i] more samples; all engines'
+    waves are issued before any is waited for. Returns each engine's frame
+    info (spp, converged, frameMs = call start to that engine's completion)."""
+    lib = load_library()
+    n = len(engines)
+    handles = (C.c_void_p * n)(*[e.h for e in engines])
+    counts = (C.c_uint32 * n)(*[int(k) for k in spp])
+    infos = (abi.FrameInfo * n)()
+    for i in range(n):
+        infos[i].structSize = C.sizeof(abi.FrameInfo)
+    _check(lib.mrtxRenderBatch(handles, counts, n, infos), "mrtxRenderBatch")
+    return [dict(spp=infos[i].spp, converged=bool(infos[i].converged), frameMs=infos[i].frameMs) for i in range(n)]
+
+
 def build_mesh_bvh(positions, indices, builder=abi.MRTX_BVH_HOST_SAH, max_leaf_prims=3, engine=None):
     """The engine's 8-wide BVH of a triangle mesh from one builder
     (abi.MRTX_BVH_*): (nodes as a WIDE_NODE_DTYPE array, triangle order).

@@ -173,6 +173,8 @@ FUNCTIONS = [
     ("mrtxCopyAccumulationDevice", C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, C.c_int32]),
     ("mrtxBuildWideBvh", C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p,
                                    C.POINTER(C.c_uint32)]),
+    ("mrtxRenderBatch", C.c_int, [C.POINTER(C.c_void_p), C.POINTER(C.c_uint32), C.c_uint32,
+                                  C.POINTER(FrameInfo)]),
     ("mrtxBuildMeshBvh", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.c_uint32,
                                    C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p, C.POINTER(C.c_uint32)]),
     ("mrtxBuildEnvCdfNoAlloc", C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p]),

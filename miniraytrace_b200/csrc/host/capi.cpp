@@ -291,6 +291,17 @@ MRT_API mrtResult mrtxBuildWideBvh(const float* aabbs, uint32_t count, uint32_t 
     });
 }
 
+MRT_API mrtResult mrtxRenderBatch(mrtEngine* const* engines, const uint32_t* spp, uint32_t count,
+                                  mrtFrameInfo* outInfos) {
+    if (count && (!engines || !spp)) return mrt::fail(MRT_ERROR_INVALID_ARGUMENT, "mrtxRenderBatch: null array");
+    std::vector<mrt::Engine*> list(count);
+    for (uint32_t i = 0; i < count; ++i) {
+        list[i] = unwrap(engines[i]);
+        if (!list[i]) return mrt::fail(MRT_ERROR_INVALID_HANDLE, "mrtxRenderBatch: null engine");
+    }
+    return guarded([&] { return mrt::Engine::renderBatch(list.data(), spp, count, outInfos); });
+}
+
 MRT_API mrtResult mrtxBuildMeshBvh(mrtEngine* engine, const float* positions, uint32_t vertexCount,
                                    const uint32_t* indices, uint32_t triangleCount, uint32_t builder,
                                    uint32_t maxLeafPrims, void* nodesOut, uint32_t nodeCapacity,

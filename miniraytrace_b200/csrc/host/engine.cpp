@@ -274,7 +274,12 @@ mrtResult Engine::allocateFrame() {
 // latency of one traversal.
 mrtResult Engine::ensureWave(uint32_t samples) {
     const uint64_t pixels = uint64_t(m_settings.width) * m_settings.height;
-    const uint64_t maxSlots = m_maxWaveSlots;
+    // at most half of the device memory free now (other engines may share
+    // the GPU), counting this engine's current wave allocation as free
+    size_t freeBytes = 0, totalBytes = 0;
+    MRT_CUDA(cudaMemGetInfo(&freeBytes, &totalBytes));
+    const uint64_t budget = (uint64_t(freeBytes) + m_wave.bytes) / 2 / kWaveBytesPerSlot;
+    const uint64_t maxSlots = std::max<uint64_t>(pixels, std::min<uint64_t>(m_maxWaveSlots, budget));
     uint32_t k = uint32_t(std::max<uint64_t>(1, std::min<uint64_t>(samples, maxSlots / std::max<uint64_t>(pixels, 1))));
     k = std::min<uint32_t>(k, 64);
     if (m_waveSamples >= k) return MRT_SUCCESS;
@@ -886,72 +891,133 @@ uint32_t Engine::waveCapacitySamples() const {
 // first of them was queued (the device scene cannot change meanwhile: every
 // commit that changes it resets the accumulation and drops the queue).
 mrtResult Engine::flushPending() {
-    if (m_pending == 0) return MRT_SUCCESS;
+    MRT_TRY(launchPending());
+    return completePending();
+}
+
+// Issues the queued samples' waves on this engine's stream and returns
+// without waiting (completePending waits and collects the statistics).
+mrtResult Engine::launchPending() {
+    if (m_pending == 0 || m_inFlight != 0) return MRT_SUCCESS;
     const uint32_t n = m_pending;
     m_pending = 0;
     m_stats.kernelLaunches = 0;
     m_stats.extendLaunches = 0;
-    {
-        MRT_TRY(guard(ensureWave(n)));
-        const MrtFrameParams p = m_pendingParams;
-        MRT_CUDA(cudaMemsetAsync(m_rayCounters.ptr, 0, 64, m_stream));
-        uint32_t launches = 0;
-        const uint32_t waves = (n + m_waveSamples - 1) / m_waveSamples;
-        const size_t perWave = size_t(6) * (p.maxBounces + 1);
-        while (m_stageEvents.size() < waves * perWave) {
-            cudaEvent_t ev;
-            MRT_CUDA(cudaEventCreate(&ev));
-            m_stageEvents.push_back(ev);
-        }
-        MRT_CUDA(cudaEventRecord(m_ev0, m_stream));
-        uint32_t wave = 0;
-        for (uint32_t done = 0; done < n; ++wave) {
-            const uint32_t k = std::min(n - done, m_waveSamples);
-            const cudaError_t le = mrtcu_wave(&p, &m_waveState, m_frameIndex + done, k, &launches,
-                                              m_stageEvents.data() + wave * perWave, m_stream);
-            if (le != cudaSuccess) return guard(fromCuda(le, "path tracing launch"));
-            done += k;
-        }
-        MRT_CUDA(cudaEventRecord(m_ev1, m_stream));
-        const cudaError_t se = cudaStreamSynchronize(m_stream);
-        if (se != cudaSuccess) return guard(fromCuda(se, "path tracing kernel"));
-        float ms = 0.0f;
-        MRT_CUDA(cudaEventElapsedTime(&ms, m_ev0, m_ev1));
-        m_stats.lastRenderMs = ms;
-        float ext = 0.0f, sha = 0.0f, shw = 0.0f;
-        for (uint32_t w = 0; w < waves; ++w)
-            for (uint32_t b = 0; b <= p.maxBounces; ++b) {
-                const cudaEvent_t* ev = m_stageEvents.data() + w * perWave + 6 * b;
-                float a = 0.0f, c = 0.0f, d = 0.0f;
-                MRT_CUDA(cudaEventElapsedTime(&a, ev[0], ev[1]));
-                MRT_CUDA(cudaEventElapsedTime(&c, ev[1], ev[2]));
-                MRT_CUDA(cudaEventElapsedTime(&d, ev[2], ev[3]));
-                ext += a;
-                sha += c;
-                shw += d;
-            }
-        m_stats.extendMs = ext;
-        m_stats.shadeMs = sha;
-        m_stats.shadowMs = shw;
-        m_stats.otherMs = ms - ext - sha - shw;
-        m_stats.lastRenderSpp = n;
-        m_stats.kernelLaunches = launches;
-        m_stats.extendLaunches = waves * (p.maxBounces + 1);
-        MRT_TRY(guard(checkErrorFlags()));
-        unsigned long long ctr[7];
-        MRT_CUDA(cudaMemcpy(ctr, m_rayCounters.ptr, sizeof(ctr), cudaMemcpyDeviceToHost));
-        m_stats.raysClosest = ctr[0];
-        m_stats.raysShadow = ctr[1];
-        m_stats.nodeFetches = ctr[2];
-        m_stats.triTests = ctr[3];
-        m_stats.surfaceHits = ctr[4];
-        m_stats.shadowNodeFetches = ctr[5];
-        m_stats.shadowTriTests = ctr[6];
-        m_stats.nodeBytes = sizeof(MrtWideNode);
-        m_stats.triBytes = 48;
-        m_frameIndex += n;
+    MRT_TRY(guard(ensureWave(n)));
+    const MrtFrameParams p = m_pendingParams;
+    MRT_CUDA(cudaMemsetAsync(m_rayCounters.ptr, 0, 64, m_stream));
+    uint32_t launches = 0;
+    const uint32_t waves = (n + m_waveSamples - 1) / m_waveSamples;
+    const size_t perWave = size_t(6) * (p.maxBounces + 1);
+    while (m_stageEvents.size() < waves * perWave) {
+        cudaEvent_t ev;
+        MRT_CUDA(cudaEventCreate(&ev));
+        m_stageEvents.push_back(ev);
     }
+    MRT_CUDA(cudaEventRecord(m_ev0, m_stream));
+    uint32_t wave = 0;
+    for (uint32_t done = 0; done < n; ++wave) {
+        const uint32_t k = std::min(n - done, m_waveSamples);
+        const cudaError_t le = mrtcu_wave(&p, &m_waveState, m_frameIndex + done, k, &launches,
+                                          m_stageEvents.data() + wave * perWave, m_stream);
+        if (le != cudaSuccess) return guard(fromCuda(le, "path tracing launch"));
+        done += k;
+    }
+    MRT_CUDA(cudaEventRecord(m_ev1, m_stream));
+    m_inFlight = n;
+    m_inFlightWaves = waves;
+    m_inFlightBounces = p.maxBounces + 1;
+    m_inFlightLaunches = launches;
     return MRT_SUCCESS;
+}
+
+mrtResult Engine::completePending() {
+    if (m_inFlight == 0) return MRT_SUCCESS;
+    const uint32_t n = m_inFlight, waves = m_inFlightWaves, bounces = m_inFlightBounces;
+    m_inFlight = 0;
+    const cudaError_t se = cudaStreamSynchronize(m_stream);
+    if (se != cudaSuccess) return guard(fromCuda(se, "path tracing kernel"));
+    float ms = 0.0f;
+    MRT_CUDA(cudaEventElapsedTime(&ms, m_ev0, m_ev1));
+    m_stats.lastRenderMs = ms;
+    const size_t perWave = size_t(6) * bounces;
+    float ext = 0.0f, sha = 0.0f, shw = 0.0f;
+    for (uint32_t w = 0; w < waves; ++w)
+        for (uint32_t b = 0; b < bounces; ++b) {
+            const cudaEvent_t* ev = m_stageEvents.data() + w * perWave + 6 * b;
+            float a = 0.0f, c = 0.0f, d = 0.0f;
+            MRT_CUDA(cudaEventElapsedTime(&a, ev[0], ev[1]));
+            MRT_CUDA(cudaEventElapsedTime(&c, ev[1], ev[2]));
+            MRT_CUDA(cudaEventElapsedTime(&d, ev[2], ev[3]));
+            ext += a;
+            sha += c;
+            shw += d;
+        }
+    m_stats.extendMs = ext;
+    m_stats.shadeMs = sha;
+    m_stats.shadowMs = shw;
+    m_stats.otherMs = ms - ext - sha - shw;
+    m_stats.lastRenderSpp = n;
+    m_stats.kernelLaunches = m_inFlightLaunches;
+    m_stats.extendLaunches = waves * bounces;
+    MRT_TRY(guard(checkErrorFlags()));
+    unsigned long long ctr[7];
+    MRT_CUDA(cudaMemcpy(ctr, m_rayCounters.ptr, sizeof(ctr), cudaMemcpyDeviceToHost));
+    m_stats.raysClosest = ctr[0];
+    m_stats.raysShadow = ctr[1];
+    m_stats.nodeFetches = ctr[2];
+    m_stats.triTests = ctr[3];
+    m_stats.surfaceHits = ctr[4];
+    m_stats.shadowNodeFetches = ctr[5];
+    m_stats.shadowTriTests = ctr[6];
+    m_stats.nodeBytes = sizeof(MrtWideNode);
+    m_stats.triBytes = 48;
+    m_frameIndex += n;
+    return MRT_SUCCESS;
+}
+
+// mrtxRenderBatch: every engine commits, queues its samples and sizes its
+// wave state first (allocations would stall the other streams), then all
+// engines' waves are issued, each on its own stream, before any is waited
+// for, so jobs of uneven size overlap on the GPU.
+mrtResult Engine::renderBatch(Engine* const* engines, const uint32_t* spp, uint32_t count, mrtFrameInfo* infos) {
+    const auto t0 = std::chrono::steady_clock::now();
+    for (uint32_t i = 0; i < count; ++i) {
+        Engine& e = *engines[i];
+        MRT_TRY(e.checkAlive());
+        MRT_TRY(e.flushPending());  // samples queued earlier render first, in order
+        MRT_TRY(e.commit(nullptr));
+        const uint32_t done = e.m_frameIndex;
+        const uint32_t n = done < e.m_settings.sppLimit ? std::min(spp[i], e.m_settings.sppLimit - done) : 0u;
+        if (n > 0) {
+            e.fillParams(e.m_pendingParams);
+            e.m_pending = n;
+            e.m_resolveExposure = std::exp2(e.m_settings.exposureEV);
+            e.m_resolveTonemap = e.m_settings.tonemap;
+            MRT_TRY(e.guard(e.ensureWave(n)));
+        }
+    }
+    mrtResult launchError = MRT_SUCCESS;
+    uint32_t launched = 0;
+    for (; launched < count && launchError == MRT_SUCCESS; ++launched) {
+        Engine& e = *engines[launched];
+        launchError = e.checkAlive();
+        if (launchError == MRT_SUCCESS) launchError = e.launchPending();
+    }
+    mrtResult result = launchError;
+    for (uint32_t i = 0; i < launched; ++i) {  // every launched engine is completed, even after an error
+        Engine& e = *engines[i];
+        mrtResult r = e.checkAlive();
+        if (r == MRT_SUCCESS) r = e.completePending();
+        if (result == MRT_SUCCESS) result = r;
+        if (infos && infos[i].structSize >= sizeof(mrtFrameInfo)) {
+            infos[i].spp = e.m_frameIndex + e.m_pending;
+            infos[i].converged = e.m_frameIndex + e.m_pending >= e.m_settings.sppLimit ? 1 : 0;
+            infos[i].denoised = 0;
+            infos[i].frameMs = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        }
+    }
+    return result;
 }
 
 // Device -> pinned staging -> caller memory, in chunks so the host copy of

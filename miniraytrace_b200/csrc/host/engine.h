@@ -51,6 +51,8 @@ public:
     mrtResult commit(mrtCommitStats* stats);
     mrtResult renderFrames(uint32_t count, mrtFrameInfo* info, bool defer = false);
     mrtResult flushPending();  // renders queued samples
+    // Several engines' samples issued together (one stream each), then waited for.
+    static mrtResult renderBatch(Engine* const* engines, const uint32_t* spp, uint32_t count, mrtFrameInfo* infos);
     mrtResult readFramebuffer(mrtPixelFormat fmt, void* dst, size_t dstSize);
 
     mrtResult traceRays(const mrtxRay* rays, uint32_t n, mrtxHit* hits);
@@ -77,6 +79,8 @@ private:
     mrtResult allocateFrame();
     mrtResult ensureWave(uint32_t samples);
     uint32_t waveCapacitySamples() const;
+    mrtResult launchPending();    // issues the queued samples' waves, no wait
+    mrtResult completePending();  // waits for them, statistics, error flags
     mrtResult up(DeviceBuffer& b, const void* src, size_t n);
     mrtResult sync(mrtCommitStats* stats);  // reference Renderer::syncScene
     mrtResult packMaterials();
@@ -147,6 +151,8 @@ private:
     // accumulation
     uint32_t m_frameIndex = 0;  // samples per pixel accumulated since reset
     uint32_t m_pending = 0;     // samples queued by mrtRenderFrame, not yet rendered
+    uint32_t m_inFlight = 0;    // samples issued by launchPending, not yet completed
+    uint32_t m_inFlightWaves = 0, m_inFlightBounces = 0, m_inFlightLaunches = 0;
     MrtFrameParams m_pendingParams{};
     uint32_t m_streamOffset = 0, m_streamStride = 1;
     float m_resolveExposure = 1.0f;

@@ -281,6 +281,29 @@ def large(width=3840, height=2160, spp=1024, max_bounces=16, grid=4096, rows=244
     return s
 
 
+def batch_jobs(count=16, seed=3, sky=(2048, 1024)) -> list:
+    """C3: `count` seeded variants of config 2 for one batched submission:
+    triangle counts log-uniform over 10k-2M (heightfield grid sized to the
+    count, 32 icospheres), resolution from {256^2, 512^2, 1280x720,
+    1920x1080}, 4-64 spp, depth 8-12. One sky is shared by all jobs."""
+    rng = np.random.default_rng(seed)
+    shared_sky = procedural_sky(*sky)
+    resolutions = [(256, 256), (512, 512), (1280, 720), (1920, 1080)]
+    jobs = []
+    for j in range(count):
+        tris = float(np.exp(rng.uniform(np.log(1e4), np.log(2e6))))
+        grid = int(round(np.sqrt(tris / 2.0))) + 1
+        w, h = resolutions[int(rng.integers(len(resolutions)))]
+        spp = int(rng.integers(4, 65))
+        depth = int(rng.integers(8, 13))
+        s = terrain(w, h, spp=spp, max_bounces=depth, grid=grid, spheres=32, sky=(8, 4), seed=int(seed * 100 + j))
+        s.environment = shared_sky
+        s.name = f"batch{j}"
+        s.meta.update(job=j, target_triangles=int(tris))
+        jobs.append(s)
+    return jobs
+
+
 def box_sphere(width=256, height=256, spp=16, max_bounces=8, firefly_clamp=0.0) -> SceneSpec:
     """C1: open box + GGX conductor UV sphere under a sun (see module doc)."""
     s = SceneSpec("box_sphere")
