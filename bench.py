@@ -53,7 +53,9 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--config", choices=["terrain", "box_sphere"], default="terrain")
+    ap.add_argument("--config", choices=["terrain", "box_sphere", "batch"], default="terrain",
+                    help="batch: the 16 uneven config-3 jobs in one mrtxRenderBatch submission per step "
+                         "(single GPU; reports aggregate Mpaths/s and per-job completion)")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -390,10 +392,94 @@ def ours_arm(args):
     return 0
 
 
+def batch_arm(args):
+    """Config 3: 16 seeded config-2 variants of uneven size, one
+    mrtxRenderBatch submission per step (every job's spp), on one GPU."""
+    import torch
+
+    import miniraytrace_b200 as mrt
+    from miniraytrace_b200 import build as mrt_build
+    from miniraytrace_b200 import scenes
+
+    if int(os.environ.get("RANK", "0")) != 0:
+        return 0  # single-GPU workload: other ranks have nothing to do
+    torch.cuda.set_device(0)
+    mrt_build.build()
+    jobs = scenes.batch_jobs()
+    engines = []
+    for sc in jobs:
+        e = mrt.Engine(sc.settings["width"], sc.settings["height"])
+        sc.apply(e)
+        e.commit()
+        engines.append(e)
+    spp = [sc.spp for sc in jobs]
+    paths = sum(sc.settings["width"] * sc.settings["height"] * sc.spp for sc in jobs)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    for _ in range(args.warmup):
+        flush.fill_(1)
+        mrt.render_batch(engines, spp)
+    torch.cuda.synchronize()
+    sampler = ClockSampler(0)
+    sampler.start()
+    time.sleep(0.3)
+    step_ms, completion, launches = [], [], 0
+    for k in range(args.steps):
+        flush.fill_(k & 0xFF)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        infos = mrt.render_batch(engines, spp)
+        b.record()
+        torch.cuda.synchronize()
+        step_ms.append(a.elapsed_time(b))
+        completion.append([i["frameMs"] for i in infos])
+        launches += sum(e.stats()["kernelLaunches"] for e in engines)
+    clocks = sampler.stop()
+    # the same jobs one after another, for comparison
+    seq_ms = []
+    for k in range(max(1, args.steps)):
+        flush.fill_(k & 0xFF)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for e, n in zip(engines, spp):
+            e.render_frames(n)
+        b.record()
+        torch.cuda.synchronize()
+        seq_ms.append(a.elapsed_time(b))
+    ms = float(np.mean(step_ms))
+    out = {
+        "metric": "aggregate Mpaths/s, 16-job batch", "value": paths / (ms / 1e3) / 1e6, "unit": "Mpaths/s",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "config 3: 16 seeded terrain variants, 10k-2M triangles (log-uniform) + 32 "
+                               "icospheres each, 256^2..1920x1080, 4-64 spp, depth 8-12, shared 2048x1024 sky",
+                   "paths_per_step": paths,
+                   "jobs": [dict(triangles=sc.triangle_count, width=sc.settings["width"],
+                                 height=sc.settings["height"], spp=sc.spp, depth=sc.settings["max_bounces"])
+                            for sc in jobs],
+                   "l2": "a 256 MiB buffer is written between timed steps"},
+        "per_job_completion_ms": [float(np.mean([c[j] for c in completion])) for j in range(len(jobs))],
+        "sequential_ms_per_step": float(np.mean(seq_ms)),
+        "gpu_launches": launches,
+        "clocks": clocks,
+    }
+    print(json.dumps(out), flush=True)
+    for e in engines:
+        e.close()
+    return 0
+
+
 def main():
     args = parse_args()
+    if args.impl == "reference" and args.config == "batch":
+        print(json.dumps({"impl": "reference", "unavailable": "the batched config-3 mode is timed on the GPU only; "
+                          "the reference arm times the terrain and box_sphere workloads"}), flush=True)
+        return 0
     if args.impl == "reference":
         return reference_arm(args)
+    if args.config == "batch":
+        return batch_arm(args)
     return ours_arm(args)
 
 

@@ -42,6 +42,12 @@ void DeviceBuffer::release() {
 
 namespace {
 
+// Jobs of one mrtxRenderBatch running on the GPU at once.
+#ifndef MRT_BATCH_WINDOW
+#define MRT_BATCH_WINDOW 4
+#endif
+constexpr uint32_t kBatchWindow = MRT_BATCH_WINDOW;
+
 // Path state per wave slot: rayO, rayD, beta, L, hit (5 x 16 B), hitInst +
 // two queues (3 x 4 B), shadow origin/dir/contribution (3 x 16 B).
 constexpr size_t kWaveBytesPerSlot = 5 * 16 + 3 * 4 + 3 * 16;
@@ -1002,6 +1008,16 @@ mrtResult Engine::renderBatch(Engine* const* engines, const uint32_t* spp, uint3
     for (; launched < count && launchError == MRT_SUCCESS; ++launched) {
         Engine& e = *engines[launched];
         launchError = e.checkAlive();
+        // at most kBatchWindow jobs run at once: job i waits on the GPU for
+        // job i - kBatchWindow, so a job fills its predecessor's last, short
+        // bounces without all jobs contending for SMs and L2
+        if (launchError == MRT_SUCCESS && launched >= kBatchWindow) {
+            Engine& prev = *engines[launched - kBatchWindow];
+            if (prev.m_inFlight) {
+                const cudaError_t we = cudaStreamWaitEvent(e.m_stream, prev.m_ev1, 0);
+                if (we != cudaSuccess) launchError = e.guard(fromCuda(we, "mrtxRenderBatch ordering"));
+            }
+        }
         if (launchError == MRT_SUCCESS) launchError = e.launchPending();
     }
     mrtResult result = launchError;
