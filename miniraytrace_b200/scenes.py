@@ -281,6 +281,47 @@ def large(width=3840, height=2160, spp=1024, max_bounces=16, grid=4096, rows=244
     return s
 
 
+def room(width=1920, height=1080, spp=64, max_bounces=12, grid=1024, seed=7, sky=(2048, 1024)) -> SceneSpec:
+    """C4: a closed 20 x 4 x 10 room (x, y, z) whose only opening is a 2 x 2
+    window in the z = 10 wall, facing the config-2 sky (its sun shines in
+    through it), with the config-2 heightfield scaled over the floor as
+    terrain, so most of the light is indirect. Diffuse walls (0.75) and
+    terrain (0.5); area-weighted terrain normals."""
+    s = SceneSpec("room")
+    x0, x1, y0, y1, z0, z1 = 0.0, 20.0, 0.0, 4.0, 0.0, 10.0
+    wx0, wx1, wy0, wy1 = 9.0, 11.0, 1.5, 3.5
+    faces = [
+        ((x0, y0, z0), (x1, y0, z0), (x1, y0, z1), (x0, y0, z1)),  # floor
+        ((x0, y1, z0), (x0, y1, z1), (x1, y1, z1), (x1, y1, z0)),  # ceiling
+        ((x0, y0, z0), (x0, y1, z0), (x1, y1, z0), (x1, y0, z0)),  # wall z = 0
+        ((x0, y0, z0), (x0, y0, z1), (x0, y1, z1), (x0, y1, z0)),  # wall x = 0
+        ((x1, y0, z0), (x1, y1, z0), (x1, y1, z1), (x1, y0, z1)),  # wall x = 20
+        # wall z = 10 around the window
+        ((x0, y0, z1), (wx0, y0, z1), (wx0, y1, z1), (x0, y1, z1)),
+        ((wx1, y0, z1), (x1, y0, z1), (x1, y1, z1), (wx1, y1, z1)),
+        ((wx0, y0, z1), (wx1, y0, z1), (wx1, wy0, z1), (wx0, wy0, z1)),
+        ((wx0, wy1, z1), (wx1, wy1, z1), (wx1, y1, z1), (wx0, y1, z1)),
+    ]
+    pos = np.concatenate([quad(*f)[0] for f in faces])
+    idx = np.concatenate([quad(*f)[1] + 4 * k for k, f in enumerate(faces)]).astype(np.uint32)
+    s.meshes.append(MeshSpec(pos, idx))
+    s.materials.append(dict(base_color=(0.75, 0.75, 0.75), roughness=1.0))
+    s.instances.append((0, None, 0))
+    hpos, hidx, _, _ = heightfield(grid, 0.15, seed)
+    hpos = hpos.astype(np.float64)
+    terrain_pos = np.stack([(hpos[:, 0] + 1.0) * 10.0, hpos[:, 1] * 2.0 + 0.35, (hpos[:, 2] + 1.0) * 5.0], 1)
+    s.meshes.append(MeshSpec(terrain_pos.astype(np.float32), hidx))
+    s.materials.append(dict(base_color=(0.5, 0.5, 0.5), roughness=1.0))
+    s.instances.append((1, None, 1))
+    s.environment = procedural_sky(*sky)
+    s.camera = dict(position=(2.0, 2.6, 1.5), target=(12.0, 1.0, 8.5), up=(0.0, 1.0, 0.0), fov_y_deg=60.0)
+    s.settings = dict(width=width, height=height, max_bounces=max_bounces, spp_limit=1 << 20,
+                      firefly_clamp=0.0, tonemap=abi.MRT_TONEMAP_LINEAR, denoise=False)
+    s.spp = spp
+    s.meta = dict(grid=grid, seed=seed, sky=list(sky))
+    return s
+
+
 def batch_jobs(count=16, seed=3, sky=(2048, 1024)) -> list:
     """C3: `count` seeded variants of config 2 for one batched submission:
     triangle counts log-uniform over 10k-2M (heightfield grid sized to the
