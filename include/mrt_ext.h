@@ -120,6 +120,42 @@ MRT_API mrtResult mrtxCopyAccumulationDevice(mrtEngine*, void* devPtr, size_t by
 MRT_API mrtResult mrtxRenderBatch(mrtEngine* const* engines, const uint32_t* spp, uint32_t count,
                                   mrtFrameInfo* outInfos);
 
+/* Radiance cache (no counterpart in the reference): a neural cache of
+ * outgoing radiance (multiresolution hash grid of position + spherical
+ * harmonics of the direction + surface features into a 5 x 64 ReLU MLP),
+ * trained online from full-length training paths. With `enabled`, rendered
+ * paths other than the training paths stop at their second surface vertex
+ * and take the cache's prediction there (biased, lower variance, fewer
+ * bounces). Bounds: the box the position encoding spans; a box with
+ * boundsHi <= boundsLo on any axis means the committed scene's bounds. */
+typedef struct mrtxRadianceCacheDesc {
+    size_t structSize;
+    int32_t enabled;
+    uint32_t trainingPaths;  /* full-length training paths per rendered sample (0: 65536) */
+    uint32_t stepsPerSample; /* Adam steps per rendered sample (0: 4) */
+    float learningRate;      /* 0: 1e-2 */
+    uint32_t seed;           /* parameter initialisation */
+    float boundsLo[3], boundsHi[3];
+} mrtxRadianceCacheDesc;
+MRT_API mrtResult mrtxSetRadianceCache(mrtEngine*, const mrtxRadianceCacheDesc* desc);
+
+/* The cache's prediction for `count` queries of 16 floats each (position
+ * xyz, outgoing direction xyz, normal xyz, roughness, albedo rgb, unused),
+ * host memory in and out (rgbOut: 3 floats per query). */
+MRT_API mrtResult mrtxRadianceCacheQuery(mrtEngine*, const float* features, uint32_t count, float* rgbOut);
+
+/* `steps` Adam steps on host-supplied samples (features as above, targets
+ * rgb); *lossOut (optional) receives the summed mean loss of the steps. */
+MRT_API mrtResult mrtxRadianceCacheTrain(mrtEngine*, const float* features, const float* targets, uint32_t count,
+                                         uint32_t steps, float* lossOut);
+
+/* Reads (gridOut, mlpOut) and then writes (gridIn, mlpIn) the cache's
+ * parameters; any pointer may be NULL. Grid: 16 x 2^19 x 2 floats; MLP:
+ * 6 x 64 x 64 floats (W0..W4 64 x 64, then the output rows). Writing resets
+ * the Adam state. */
+MRT_API mrtResult mrtxRadianceCacheParams(mrtEngine*, float* gridOut, float* mlpOut, const float* gridIn,
+                                          const float* mlpIn);
+
 /* Host-side build of the acceleration structure the engine uses for a mesh,
  * for inspection and tests (no device needed): an 8-wide compressed BVH over
  * `count` boxes (6 floats each: lo xyz, hi xyz) with leaves of at most

@@ -299,6 +299,40 @@ class Engine:
         _check(self.lib.mrtxBuildEnvCdf(self.h, _ptr(px), w, h, _ptr(cdf), C.byref(integ)), "mrtxBuildEnvCdf")
         return cdf, integ.value
 
+    def set_radiance_cache(self, enabled=True, training_paths=0, steps_per_sample=0, learning_rate=0.0, seed=1,
+                           bounds=None):
+        """mrtxSetRadianceCache; bounds = (lo xyz, hi xyz) or None for the scene's."""
+        d = abi.RadianceCacheDesc(enabled=1 if enabled else 0, trainingPaths=training_paths,
+                                  stepsPerSample=steps_per_sample, learningRate=learning_rate, seed=seed)
+        if bounds is not None:
+            d.boundsLo[:] = [float(v) for v in bounds[0]]
+            d.boundsHi[:] = [float(v) for v in bounds[1]]
+        _check(self.lib.mrtxSetRadianceCache(self.h, C.byref(d)), "mrtxSetRadianceCache")
+
+    def cache_query(self, features):
+        f = np.ascontiguousarray(np.asarray(features, np.float32).reshape(-1, 16))
+        out = np.empty((f.shape[0], 3), np.float32)
+        _check(self.lib.mrtxRadianceCacheQuery(self.h, _ptr(f), f.shape[0], _ptr(out)), "mrtxRadianceCacheQuery")
+        return out
+
+    def cache_train(self, features, targets, steps=1):
+        f = np.ascontiguousarray(np.asarray(features, np.float32).reshape(-1, 16))
+        t = np.ascontiguousarray(np.asarray(targets, np.float32).reshape(-1, 3))
+        loss = C.c_float()
+        _check(self.lib.mrtxRadianceCacheTrain(self.h, _ptr(f), _ptr(t), f.shape[0], steps, C.byref(loss)),
+               "mrtxRadianceCacheTrain")
+        return loss.value
+
+    def cache_params(self, grid=None, mlp=None):
+        """Returns (grid, mlp) as read, then writes the given arrays."""
+        g = np.empty(abi.CACHE_GRID_FLOATS, np.float32)
+        w = np.empty(abi.CACHE_MLP_FLOATS, np.float32)
+        gi = None if grid is None else np.ascontiguousarray(np.asarray(grid, np.float32).ravel())
+        wi = None if mlp is None else np.ascontiguousarray(np.asarray(mlp, np.float32).ravel())
+        _check(self.lib.mrtxRadianceCacheParams(self.h, _ptr(g), _ptr(w), _ptr(gi), _ptr(wi)),
+               "mrtxRadianceCacheParams")
+        return g, w
+
     def set_sample_stream(self, offset: int, stride: int):
         _check(self.lib.mrtxSetSampleStream(self.h, offset, stride), "mrtxSetSampleStream")
 

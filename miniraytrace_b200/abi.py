@@ -98,6 +98,12 @@ class FrameInfo(_Sized):
                 ("denoised", C.c_int32), ("frameMs", C.c_float)]
 
 
+class RadianceCacheDesc(_Sized):
+    _fields_ = [("structSize", C.c_size_t), ("enabled", C.c_int32), ("trainingPaths", C.c_uint32),
+                ("stepsPerSample", C.c_uint32), ("learningRate", C.c_float), ("seed", C.c_uint32),
+                ("boundsLo", C.c_float * 3), ("boundsHi", C.c_float * 3)]
+
+
 class CommitStats(_Sized):
     _fields_ = [("structSize", C.c_size_t), ("blasRebuilt", C.c_uint32), ("tlasRebuilt", C.c_int32),
                 ("commitMs", C.c_float)]
@@ -173,12 +179,21 @@ FUNCTIONS = [
     ("mrtxCopyAccumulationDevice", C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, C.c_int32]),
     ("mrtxBuildWideBvh", C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p,
                                    C.POINTER(C.c_uint32)]),
+    ("mrtxSetRadianceCache", C.c_int, [C.c_void_p, C.POINTER(RadianceCacheDesc)]),
+    ("mrtxRadianceCacheQuery", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]),
+    ("mrtxRadianceCacheTrain", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32,
+                                         C.POINTER(C.c_float)]),
+    ("mrtxRadianceCacheParams", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("mrtxRenderBatch", C.c_int, [C.POINTER(C.c_void_p), C.POINTER(C.c_uint32), C.c_uint32,
                                   C.POINTER(FrameInfo)]),
     ("mrtxBuildMeshBvh", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.c_uint32,
                                    C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p, C.POINTER(C.c_uint32)]),
     ("mrtxBuildEnvCdfNoAlloc", C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p]),
 ]
+
+# radiance cache sizes (floats)
+CACHE_GRID_FLOATS = 16 * (1 << 19) * 2
+CACHE_MLP_FLOATS = 6 * 64 * 64
 
 # mrtxBuildMeshBvh builders
 MRTX_BVH_HOST_SAH, MRTX_BVH_HOST_LBVH, MRTX_BVH_DEVICE_LBVH = 0, 1, 2

@@ -9,6 +9,16 @@
 
 #include "../common/device_types.h"
 
+// Radiance-cache parameters and training state on the device
+// (radiance_cache.cu): hash grid (16 x 2^19 x 2 floats) and MLP (6 x 64 x 64
+// floats), their gradients and Adam moments; position normalisation.
+typedef struct McacheParams {
+    float *grid, *mlp, *gGrid, *gMlp, *mGrid, *vGrid, *mMlp, *vMlp;
+    float lo[3], invExtent[3];
+    uint32_t step;
+    float lr;
+} McacheParams;
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -81,6 +91,15 @@ cudaError_t mrtcu_pack_triangles(const float4* pos, uint32_t nv, const uint32_t*
 cudaError_t mrtcu_rebase_nodes(const MrtWideNode* src, uint32_t n, uint32_t nodeBase, uint32_t triBase,
                                MrtWideNode* dst, cudaStream_t stream);
 cudaError_t mrtcu_fill_f4(float4* dst, size_t n, float4 value, cudaStream_t stream);
+
+// Radiance cache (radiance_cache.cu). Features: 16 floats per query
+// (position, outgoing direction, normal, roughness, albedo, unused).
+size_t mrtcu_rc_grid_floats(void);
+size_t mrtcu_rc_mlp_floats(void);
+cudaError_t mrtcu_rc_init(McacheParams C, uint32_t seed, cudaStream_t stream);
+cudaError_t mrtcu_rc_query(McacheParams C, const float* features, uint32_t n, float* out3, cudaStream_t stream);
+cudaError_t mrtcu_rc_train(McacheParams* C, const float* features, const float* targets, uint32_t n, uint32_t steps,
+                           uint32_t batch, float* lossOut, cudaStream_t stream);
 
 #ifdef __cplusplus
 }

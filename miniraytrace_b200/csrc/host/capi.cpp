@@ -291,6 +291,35 @@ MRT_API mrtResult mrtxBuildWideBvh(const float* aabbs, uint32_t count, uint32_t 
     });
 }
 
+MRT_API mrtResult mrtxSetRadianceCache(mrtEngine* e, const mrtxRadianceCacheDesc* desc) {
+    mrt::Engine* eng = unwrap(e);
+    if (!eng) return MRT_ERROR_INVALID_HANDLE;
+    if (!validStruct(desc)) return mrt::fail(MRT_ERROR_INVALID_ARGUMENT, "mrtxSetRadianceCache: bad descriptor");
+    return guarded([&] { return eng->setRadianceCache(*desc); });
+}
+
+MRT_API mrtResult mrtxRadianceCacheQuery(mrtEngine* e, const float* features, uint32_t count, float* rgbOut) {
+    mrt::Engine* eng = unwrap(e);
+    if (!eng) return MRT_ERROR_INVALID_HANDLE;
+    if (count && (!features || !rgbOut)) return mrt::fail(MRT_ERROR_INVALID_ARGUMENT, "mrtxRadianceCacheQuery: null");
+    return guarded([&] { return eng->cacheQuery(features, count, rgbOut); });
+}
+
+MRT_API mrtResult mrtxRadianceCacheTrain(mrtEngine* e, const float* features, const float* targets, uint32_t count,
+                                         uint32_t steps, float* lossOut) {
+    mrt::Engine* eng = unwrap(e);
+    if (!eng) return MRT_ERROR_INVALID_HANDLE;
+    if (count && (!features || !targets)) return mrt::fail(MRT_ERROR_INVALID_ARGUMENT, "mrtxRadianceCacheTrain: null");
+    return guarded([&] { return eng->cacheTrain(features, targets, count, steps, lossOut); });
+}
+
+MRT_API mrtResult mrtxRadianceCacheParams(mrtEngine* e, float* gridOut, float* mlpOut, const float* gridIn,
+                                          const float* mlpIn) {
+    mrt::Engine* eng = unwrap(e);
+    if (!eng) return MRT_ERROR_INVALID_HANDLE;
+    return guarded([&] { return eng->cacheParams(gridOut, mlpOut, gridIn, mlpIn); });
+}
+
 MRT_API mrtResult mrtxRenderBatch(mrtEngine* const* engines, const uint32_t* spp, uint32_t count,
                                   mrtFrameInfo* outInfos) {
     if (count && (!engines || !spp)) return mrt::fail(MRT_ERROR_INVALID_ARGUMENT, "mrtxRenderBatch: null array");

@@ -240,6 +240,7 @@ Engine::~Engine() {
                             &m_packError};
     for (DeviceBuffer* b : bufs) b->release();
     for (auto& [id, b] : m_blas) b.release();
+    m_cache.release();
     for (auto& t : m_texData) t.release();
     if (m_pinned) cudaFreeHost(m_pinned);
     for (auto& ev : m_copyEvents)
@@ -607,6 +608,15 @@ mrtResult Engine::packInstances() {
         ids.push_back(id);
         boxes.push_back(transformBox(it->second.bounds, in.o2w));
     }
+    for (int a = 0; a < 3; ++a) {
+        m_sceneLo[a] = 3.402823466e38f;
+        m_sceneHi[a] = -3.402823466e38f;
+    }
+    for (const Box3& b : boxes)
+        for (int a = 0; a < 3; ++a) {
+            m_sceneLo[a] = std::min(m_sceneLo[a], b.lo[a]);
+            m_sceneHi[a] = std::max(m_sceneHi[a], b.hi[a]);
+        }
     const auto tb = std::chrono::steady_clock::now();
     WideBvh tlas = collapseToWide(buildBvh(boxes, 1, 1), 1);
     m_stats.commitBvhMs += std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - tb).count();
@@ -1215,6 +1225,128 @@ mrtResult Engine::buildMeshBvhDevice(const V4f* pos, size_t nv, const uint32_t* 
     MRT_CUDA(cudaMemcpyAsync(out.primOrder.data(), m_bvhPrims.ptr, nt * sizeof(uint32_t), cudaMemcpyDeviceToHost,
                              m_stream));
     MRT_CUDA(cudaStreamSynchronize(m_stream));
+    return MRT_SUCCESS;
+}
+
+// ------------------------------------------------------------ radiance cache --
+
+void Engine::RadianceCache::release() {
+    for (DeviceBuffer* d : {&grid, &mlp, &gGrid, &gMlp, &mGrid, &vGrid, &mMlp, &vMlp, &in, &out, &loss}) d->release();
+    allocated = false;
+}
+
+// Position normalisation: the given box, else the committed scene's bounds,
+// else the unit cube.
+void Engine::cacheBounds() {
+    float lo[3], hi[3];
+    bool given = true, scene = true;
+    for (int a = 0; a < 3; ++a) {
+        given &= m_cache.hi[a] > m_cache.lo[a];
+        scene &= m_sceneHi[a] > m_sceneLo[a];
+    }
+    for (int a = 0; a < 3; ++a) {
+        lo[a] = given ? m_cache.lo[a] : scene ? m_sceneLo[a] : 0.0f;
+        hi[a] = given ? m_cache.hi[a] : scene ? m_sceneHi[a] : 1.0f;
+        m_cache.params.lo[a] = lo[a];
+        m_cache.params.invExtent[a] = hi[a] > lo[a] ? 1.0f / (hi[a] - lo[a]) : 1.0f;
+    }
+}
+
+mrtResult Engine::ensureCache() {
+    if (m_cache.allocated) return MRT_SUCCESS;
+    const size_t g = mrtcu_rc_grid_floats() * sizeof(float), w = mrtcu_rc_mlp_floats() * sizeof(float);
+    for (DeviceBuffer* d : {&m_cache.grid, &m_cache.gGrid, &m_cache.mGrid, &m_cache.vGrid}) MRT_TRY(d->ensure(g));
+    for (DeviceBuffer* d : {&m_cache.mlp, &m_cache.gMlp, &m_cache.mMlp, &m_cache.vMlp}) MRT_TRY(d->ensure(w));
+    MRT_TRY(m_cache.loss.ensure(16));
+    McacheParams& c = m_cache.params;
+    c.grid = m_cache.grid.as<float>();
+    c.mlp = m_cache.mlp.as<float>();
+    c.gGrid = m_cache.gGrid.as<float>();
+    c.gMlp = m_cache.gMlp.as<float>();
+    c.mGrid = m_cache.mGrid.as<float>();
+    c.vGrid = m_cache.vGrid.as<float>();
+    c.mMlp = m_cache.mMlp.as<float>();
+    c.vMlp = m_cache.vMlp.as<float>();
+    c.step = 0;
+    c.lr = m_cache.lr;
+    cacheBounds();
+    MRT_CUDA(mrtcu_rc_init(c, m_cache.seed, m_stream));
+    MRT_CUDA(cudaStreamSynchronize(m_stream));
+    m_cache.allocated = true;
+    return MRT_SUCCESS;
+}
+
+mrtResult Engine::setRadianceCache(const mrtxRadianceCacheDesc& d) {
+    MRT_TRY(checkAlive());
+    MRT_TRY(flushPending());
+    const bool reinit = m_cache.allocated && d.seed != m_cache.seed;
+    m_cache.trainingPaths = d.trainingPaths ? d.trainingPaths : 65536u;
+    m_cache.stepsPerSample = d.stepsPerSample ? d.stepsPerSample : 4u;
+    m_cache.lr = d.learningRate > 0.0f ? d.learningRate : 1e-2f;
+    m_cache.seed = d.seed;
+    for (int a = 0; a < 3; ++a) {
+        m_cache.lo[a] = d.boundsLo[a];
+        m_cache.hi[a] = d.boundsHi[a];
+    }
+    if (reinit) m_cache.release();
+    MRT_TRY(guard(ensureCache()));
+    m_cache.params.lr = m_cache.lr;
+    cacheBounds();
+    if (bool(d.enabled) != m_cache.enabled) resetAccumulation();  // a different estimator
+    m_cache.enabled = d.enabled != 0;
+    return MRT_SUCCESS;
+}
+
+mrtResult Engine::cacheQuery(const float* features, uint32_t n, float* rgb) {
+    MRT_TRY(checkAlive());
+    MRT_TRY(guard(ensureCache()));
+    if (n == 0) return MRT_SUCCESS;
+    MRT_TRY(up(m_cache.in, features, size_t(n) * 16 * sizeof(float)));
+    MRT_TRY(m_cache.out.ensure(size_t(n) * 3 * sizeof(float)));
+    MRT_CUDA(mrtcu_rc_query(m_cache.params, m_cache.in.as<float>(), n, m_cache.out.as<float>(), m_stream));
+    MRT_CUDA(cudaMemcpyAsync(rgb, m_cache.out.ptr, size_t(n) * 3 * sizeof(float), cudaMemcpyDeviceToHost, m_stream));
+    const cudaError_t e = cudaStreamSynchronize(m_stream);
+    if (e != cudaSuccess) return guard(fromCuda(e, "radiance cache query"));
+    return MRT_SUCCESS;
+}
+
+mrtResult Engine::cacheTrain(const float* features, const float* targets, uint32_t n, uint32_t steps, float* loss) {
+    MRT_TRY(checkAlive());
+    MRT_TRY(guard(ensureCache()));
+    if (n == 0 || steps == 0) return MRT_SUCCESS;
+    MRT_TRY(m_cache.in.ensure(size_t(n) * 19 * sizeof(float)));
+    float* din = m_cache.in.as<float>();
+    MRT_CUDA(cudaMemcpyAsync(din, features, size_t(n) * 16 * sizeof(float), cudaMemcpyHostToDevice, m_stream));
+    MRT_CUDA(cudaMemcpyAsync(din + size_t(n) * 16, targets, size_t(n) * 3 * sizeof(float), cudaMemcpyHostToDevice,
+                             m_stream));
+    MRT_CUDA(cudaMemsetAsync(m_cache.loss.ptr, 0, sizeof(float), m_stream));
+    MRT_CUDA(mrtcu_rc_train(&m_cache.params, din, din + size_t(n) * 16, n, steps, 65536u, m_cache.loss.as<float>(),
+                            m_stream));
+    float l = 0.0f;
+    MRT_CUDA(cudaMemcpyAsync(&l, m_cache.loss.ptr, sizeof(float), cudaMemcpyDeviceToHost, m_stream));
+    const cudaError_t e = cudaStreamSynchronize(m_stream);
+    if (e != cudaSuccess) return guard(fromCuda(e, "radiance cache training"));
+    if (loss) *loss = l;
+    return MRT_SUCCESS;
+}
+
+mrtResult Engine::cacheParams(float* gridOut, float* mlpOut, const float* gridIn, const float* mlpIn) {
+    MRT_TRY(checkAlive());
+    MRT_TRY(guard(ensureCache()));
+    const size_t g = mrtcu_rc_grid_floats() * sizeof(float), w = mrtcu_rc_mlp_floats() * sizeof(float);
+    if (gridOut) MRT_CUDA(cudaMemcpyAsync(gridOut, m_cache.grid.ptr, g, cudaMemcpyDeviceToHost, m_stream));
+    if (mlpOut) MRT_CUDA(cudaMemcpyAsync(mlpOut, m_cache.mlp.ptr, w, cudaMemcpyDeviceToHost, m_stream));
+    if (gridIn) MRT_CUDA(cudaMemcpyAsync(m_cache.grid.ptr, gridIn, g, cudaMemcpyHostToDevice, m_stream));
+    if (mlpIn) MRT_CUDA(cudaMemcpyAsync(m_cache.mlp.ptr, mlpIn, w, cudaMemcpyHostToDevice, m_stream));
+    if (gridIn || mlpIn) {
+        for (DeviceBuffer* d : {&m_cache.gGrid, &m_cache.mGrid, &m_cache.vGrid})
+            MRT_CUDA(cudaMemsetAsync(d->ptr, 0, g, m_stream));
+        for (DeviceBuffer* d : {&m_cache.gMlp, &m_cache.mMlp, &m_cache.vMlp})
+            MRT_CUDA(cudaMemsetAsync(d->ptr, 0, w, m_stream));
+        m_cache.params.step = 0;
+    }
+    const cudaError_t e = cudaStreamSynchronize(m_stream);
+    if (e != cudaSuccess) return guard(fromCuda(e, "radiance cache parameters"));
     return MRT_SUCCESS;
 }
 

@@ -13,6 +13,7 @@
 
 #include "../../../include/mrt_ext.h"
 #include "../common/device_types.h"
+#include "../cuda/device_api.h"
 #include "bvh_build.h"
 #include "lbvh.h"
 #include "wide_bvh.h"
@@ -64,6 +65,10 @@ public:
     mrtResult copyAccumulationDevice(void* dev, size_t bytes, bool accumulate);
     // 8-wide BVH of one triangle mesh built on this engine's GPU (LBVH
     // topology, SAH-optimal collapse), read back into `out`.
+    mrtResult setRadianceCache(const mrtxRadianceCacheDesc& d);
+    mrtResult cacheQuery(const float* features, uint32_t n, float* rgb);
+    mrtResult cacheTrain(const float* features, const float* targets, uint32_t n, uint32_t steps, float* loss);
+    mrtResult cacheParams(float* gridOut, float* mlpOut, const float* gridIn, const float* mlpIn);
     mrtResult buildMeshBvhDevice(const V4f* pos, size_t nv, const uint32_t* idx, size_t nt, uint32_t maxLeaf,
                                  WideBvh& out);
     // Device build from device positions/indices into the builder's own
@@ -118,6 +123,19 @@ private:
     DeviceBuffer m_wave;  // wavefront path state (one allocation, carved into MrtWaveState arrays)
     DeviceBuffer m_bvhPos, m_bvhIdx, m_bvhScratch, m_bvhNodes, m_bvhPrims;  // device BVH builder
     DeviceBuffer m_packError;  // error word of the commit-time assembly kernels
+
+    // radiance cache: parameters, gradients, Adam moments, query scratch
+    struct RadianceCache {
+        DeviceBuffer grid, mlp, gGrid, gMlp, mGrid, vGrid, mMlp, vMlp, in, out, loss;
+        McacheParams params{};
+        bool allocated = false, enabled = false;
+        uint32_t trainingPaths = 65536, stepsPerSample = 4, seed = 1;
+        float lr = 1e-2f;
+        float lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+        void release();
+    } m_cache;
+    mrtResult ensureCache();
+    void cacheBounds();
     MrtWaveState m_waveState{};
     uint32_t m_waveSamples = 0;  // samples per pixel one wave holds
     uint64_t m_maxWaveSlots = uint64_t(1) << 25;  // paths per wave, set from the GPU's memory
@@ -145,6 +163,7 @@ private:
     uint32_t m_nodeCount = 0, m_blasNodeCount = 0, m_triCount = 0, m_materialCount = 1;
     uint32_t m_tlasRoot = 0, m_instanceCount = 0, m_lightCount = 0;
     uint32_t m_envW = 0, m_envH = 0;
+    float m_sceneLo[3] = {0, 0, 0}, m_sceneHi[3] = {0, 0, 0};  // world bounds of the instances
     float m_envIntegralHost = 1.0f;
     bool m_hasEnv = false;
 
