@@ -131,11 +131,15 @@ MRT_API mrtResult mrtxRenderBatch(mrtEngine* const* engines, const uint32_t* spp
 typedef struct mrtxRadianceCacheDesc {
     size_t structSize;
     int32_t enabled;
-    uint32_t trainingPaths;  /* full-length training paths per rendered sample (0: 65536) */
-    uint32_t stepsPerSample; /* Adam steps per rendered sample (0: 4) */
+    uint32_t trainingPaths;  /* full-length training paths per rendered sample (0: a 32nd of the pixels) */
+    uint32_t stepsPerSample; /* Adam steps per rendered sample (0: 1) */
     float learningRate;      /* 0: 1e-2 */
     uint32_t seed;           /* parameter initialisation */
     float boundsLo[3], boundsHi[3];
+    uint32_t samplesPerUpdate; /* samples rendered between training rounds (0: 4) */
+    uint32_t trainingVertices; /* vertices of a training path that become training
+                                  samples, from the second surface vertex on (0: a
+                                  quarter of the bounce budget, at least 1) */
 } mrtxRadianceCacheDesc;
 MRT_API mrtResult mrtxSetRadianceCache(mrtEngine*, const mrtxRadianceCacheDesc* desc);
 

@@ -300,10 +300,11 @@ class Engine:
         return cdf, integ.value
 
     def set_radiance_cache(self, enabled=True, training_paths=0, steps_per_sample=0, learning_rate=0.0, seed=1,
-                           bounds=None):
+                           bounds=None, samples_per_update=0, training_vertices=0):
         """mrtxSetRadianceCache; bounds = (lo xyz, hi xyz) or None for the scene's."""
         d = abi.RadianceCacheDesc(enabled=1 if enabled else 0, trainingPaths=training_paths,
-                                  stepsPerSample=steps_per_sample, learningRate=learning_rate, seed=seed)
+                                  stepsPerSample=steps_per_sample, learningRate=learning_rate, seed=seed,
+                                  samplesPerUpdate=samples_per_update, trainingVertices=training_vertices)
         if bounds is not None:
             d.boundsLo[:] = [float(v) for v in bounds[0]]
             d.boundsHi[:] = [float(v) for v in bounds[1]]

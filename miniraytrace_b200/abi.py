@@ -101,7 +101,8 @@ class FrameInfo(_Sized):
 class RadianceCacheDesc(_Sized):
     _fields_ = [("structSize", C.c_size_t), ("enabled", C.c_int32), ("trainingPaths", C.c_uint32),
                 ("stepsPerSample", C.c_uint32), ("learningRate", C.c_float), ("seed", C.c_uint32),
-                ("boundsLo", C.c_float * 3), ("boundsHi", C.c_float * 3)]
+                ("boundsLo", C.c_float * 3), ("boundsHi", C.c_float * 3), ("samplesPerUpdate", C.c_uint32),
+                ("trainingVertices", C.c_uint32)]
 
 
 class CommitStats(_Sized):

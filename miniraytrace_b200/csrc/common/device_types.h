@@ -104,6 +104,26 @@ typedef struct MrtTexture {
 
 enum { MRT_FLAG_HAS_ENV = 1u, MRT_FLAG_ORTHO = 4u };
 
+// Radiance-cache mode of one wave (shade kernel's cache instantiation):
+// paths other than training paths stop at their second surface vertex and
+// append a query there (16 features; beta and the slot); training paths
+// continue and append a record at every vertex from the second on
+// (features; radiance gathered before the vertex and the slot; beta). A path
+// is a training path when hash(slot, sample base) % trainStride == 0.
+typedef struct MrtCacheArgs {
+    float* qFeat;
+    float4* qBeta;     // beta xyz, slot bits in w
+    uint32_t* qCount;
+    uint32_t qCap;
+    float* rFeat;
+    float4* rPrefix;   // radiance before the vertex xyz, slot bits in w
+    float4* rBeta;     // beta xyz
+    uint32_t* rCount;
+    uint32_t rCap;
+    uint32_t trainStride;
+    uint32_t recordBounces;  // training paths record their vertices 1..recordBounces
+} MrtCacheArgs;
+
 // Everything one path-tracing launch reads; passed by value as the kernel
 // parameter block (no constant-memory update, so launches stay
 // graph-capturable with new parameters).

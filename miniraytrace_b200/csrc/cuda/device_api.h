@@ -14,9 +14,12 @@
 // floats), their gradients and Adam moments; position normalisation.
 typedef struct McacheParams {
     float *grid, *mlp, *gGrid, *gMlp, *mGrid, *vGrid, *mMlp, *vMlp;
+    float* partial;          // per-block weight gradients of one step
+    uint32_t partialBlocks;  // blocks (of 64 samples) `partial` holds
     float lo[3], invExtent[3];
     uint32_t step;
     float lr;
+    uint32_t* status;        // device word: bit 0 set when a tensor-core wait gave up
 } McacheParams;
 
 #ifdef __cplusplus
@@ -30,7 +33,12 @@ extern "C" {
 // events per bounce; events 6b..6b+3 are recorded before extend, between
 // extend and shade, between shade and shadow, and after shadow of bounce b.
 cudaError_t mrtcu_wave(const MrtFrameParams* p, const MrtWaveState* s, uint32_t sampleBase, uint32_t samples,
-                       uint32_t* launches, const cudaEvent_t* stageEvents, cudaStream_t stream);
+                       uint32_t* launches, const cudaEvent_t* stageEvents, const MrtCacheArgs* cache,
+                       cudaStream_t stream);
+// With a cache, mrtcu_wave leaves the wave unfinalised: the cache's
+// predictions are added to the paths, then this accumulates the wave.
+cudaError_t mrtcu_wave_finalize(const MrtFrameParams* p, const MrtWaveState* s, uint32_t sampleBase,
+                                uint32_t samples, cudaStream_t stream);
 
 // Trace queries (closest hit / any hit) for n device-resident rays.
 cudaError_t mrtcu_trace_closest(const MrtFrameParams* p, const MrtQueryRay* rays, uint32_t n, MrtQueryHit* hits,
@@ -96,8 +104,16 @@ cudaError_t mrtcu_fill_f4(float4* dst, size_t n, float4 value, cudaStream_t stre
 // (position, outgoing direction, normal, roughness, albedo, unused).
 size_t mrtcu_rc_grid_floats(void);
 size_t mrtcu_rc_mlp_floats(void);
+size_t mrtcu_rc_partial_floats(uint32_t maxBatch);
 cudaError_t mrtcu_rc_init(McacheParams C, uint32_t seed, cudaStream_t stream);
 cudaError_t mrtcu_rc_query(McacheParams C, const float* features, uint32_t n, float* out3, cudaStream_t stream);
+// Cache mode of a wave: predictions for n queries added to the paths'
+// radiance (scratch3: 3 floats per query), and training targets of n
+// records (3 floats each).
+cudaError_t mrtcu_rc_apply_queries(McacheParams C, const float* qFeat, const float4* qBeta, uint32_t n,
+                                   uint32_t slots, float* scratch3, float4* L, cudaStream_t stream);
+cudaError_t mrtcu_rc_record_targets(const float4* prefix, const float4* beta, uint32_t n, uint32_t slots,
+                                    const float4* L, float* targets, cudaStream_t stream);
 cudaError_t mrtcu_rc_train(McacheParams* C, const float* features, const float* targets, uint32_t n, uint32_t steps,
                            uint32_t batch, float* lossOut, cudaStream_t stream);
 

@@ -254,7 +254,19 @@ __global__ void MRT_TRAV_BOUNDS waveExtendKernel(MrtFrameParams P, MrtWaveState 
 // (a shadow ray with its contribution is queued), BSDF sample, Russian
 // roulette, next ray queued. The draws from the path's pcg4d stream happen in
 // the reference's order; the counter lives in beta.w between bounces.
-__global__ void __launch_bounds__(128) waveShadeKernel(MrtFrameParams P, MrtWaveState S, WaveArgs A, uint32_t cur) {
+// Training-path selection of the cache mode (a slot hash, so training paths
+// spread over the image and change from wave to wave).
+MRT_DEV bool cacheTrainingPath(const MrtCacheArgs& K, uint32_t slot, uint32_t sampleBase) {
+    uint32_t x = slot * 0x9e3779b1u ^ (sampleBase + 1u) * 0x85ebca77u;
+    x ^= x >> 15;
+    x *= 0x2c1b3c6du;
+    x ^= x >> 12;
+    return x % K.trainStride == 0u;
+}
+
+template <bool kCache>
+__global__ void __launch_bounds__(128) waveShadeKernel(MrtFrameParams P, MrtWaveState S, WaveArgs A, uint32_t cur,
+                                                       MrtCacheArgs K) {
     const uint32_t* __restrict__ q = S.queue[cur];
     uint32_t* __restrict__ qn = S.queue[cur ^ 1u];
     const uint32_t n = S.counts[cur];
@@ -267,6 +279,9 @@ __global__ void __launch_bounds__(128) waveShadeKernel(MrtFrameParams P, MrtWave
         uint32_t slot = 0;
         float3 shOrig = f3(0.0f), shDir = f3(0.0f), shContrib = f3(0.0f);
         float shTMax = 0.0f;
+        bool cacheQuery = false, cacheRecord = false;  // cache mode only
+        float feat[13];
+        float3 cacheBeta = f3(0.0f), cachePrefix = f3(0.0f);
         if (valid) {
             slot = q[i];
             const float4 o4 = S.rayO[slot], d4 = S.rayD[slot], b4 = S.beta[slot], L4 = S.L[slot];
@@ -303,14 +318,26 @@ __global__ void __launch_bounds__(128) waveShadeKernel(MrtFrameParams P, MrtWave
                     if (mat.tex[4] >= 0) emission = emission * texRgb(P, mat.tex[4], s.uv);
                     if (maxComp(emission) > 0.0f && s.frontFace) L += beta * emission;
                     const Bsdf bsdf = makeBsdf(P, s);
+                    if (kCache && bounce >= 1u) {
+                        const float3 wo = -rd;
+                        const float f13[13] = {s.pos.x,    s.pos.y,    s.pos.z,    wo.x,
+                                               wo.y,       wo.z,       s.nShade.x, s.nShade.y,
+                                               s.nShade.z, bsdf.roughness, bsdf.baseColor.x, bsdf.baseColor.y,
+                                               bsdf.baseColor.z};
+                        for (int k = 0; k < 13; ++k) feat[k] = f13[k];
+                        cacheBeta = beta;
+                        cachePrefix = L;
+                        if (cacheTrainingPath(K, slot, A.sampleBase)) cacheRecord = bounce <= K.recordBounces;
+                        else cacheQuery = true;  // the cache stands for everything scattered from here on
+                    }
                     float3 Tn, Bn;
                     buildOnb(s.nShade, Tn, Bn);
                     const float3 nd = -rd;
                     float3 wo = f3(dot(nd, Tn), dot(nd, Bn), dot(nd, s.nShade));
                     if (wo.z < 1e-6f) wo.z = 1e-6f;
                     wo = normalize(wo);
-                    const LightSample ls = sampleOneLight(P, s.pos, rng);
-                    if (ls.valid && ls.pdf > 1e-9f) {
+                    const LightSample ls = cacheQuery ? LightSample{} : sampleOneLight(P, s.pos, rng);
+                    if (!cacheQuery && ls.valid && ls.pdf > 1e-9f) {
                         const float3 wi = f3(dot(ls.wi, Tn), dot(ls.wi, Bn), dot(ls.wi, s.nShade));
                         float3 f;
                         float bsdfPdf;
@@ -324,8 +351,8 @@ __global__ void __launch_bounds__(128) waveShadeKernel(MrtFrameParams P, MrtWave
                             shContrib = beta * f * fabsf(wi.z) * ls.radiance * w / ls.pdf;
                         }
                     }
-                    const BsdfSample bs = bsdfSample(bsdf, wo, rng);
-                    if (bs.valid) {
+                    const BsdfSample bs = cacheQuery ? BsdfSample{} : bsdfSample(bsdf, wo, rng);
+                    if (!cacheQuery && bs.valid) {
                         const float3 wiWorld = normalize(Tn * bs.wi.x + Bn * bs.wi.y + s.nShade * bs.wi.z);
                         beta *= bs.f * fabsf(bs.wi.z) / bs.pdf;
                         prevBsdfPdf = bs.pdf;
@@ -357,6 +384,23 @@ __global__ void __launch_bounds__(128) waveShadeKernel(MrtFrameParams P, MrtWave
             S.shO[si] = make_float4(shOrig.x, shOrig.y, shOrig.z, shTMax);
             S.shD[si] = make_float4(shDir.x, shDir.y, shDir.z, __uint_as_float(slot));
             S.shC[si] = make_float4(shContrib.x, shContrib.y, shContrib.z, 0.0f);
+        }
+        if (kCache) {
+            const uint32_t qi = warpAppend(K.qCount, cacheQuery);
+            if (cacheQuery && qi < K.qCap) {
+                float* f = K.qFeat + size_t(qi) * 16;
+                for (int k = 0; k < 13; ++k) f[k] = feat[k];
+                f[13] = f[14] = f[15] = 0.0f;
+                K.qBeta[qi] = make_float4(cacheBeta.x, cacheBeta.y, cacheBeta.z, __uint_as_float(slot));
+            }
+            const uint32_t ri = warpAppend(K.rCount, cacheRecord);
+            if (cacheRecord && ri < K.rCap) {
+                float* f = K.rFeat + size_t(ri) * 16;
+                for (int k = 0; k < 13; ++k) f[k] = feat[k];
+                f[13] = f[14] = f[15] = 0.0f;
+                K.rPrefix[ri] = make_float4(cachePrefix.x, cachePrefix.y, cachePrefix.z, __uint_as_float(slot));
+                K.rBeta[ri] = make_float4(cacheBeta.x, cacheBeta.y, cacheBeta.z, 0.0f);
+            }
         }
     }
     warpAddCounters(P.rayCounters, c);
@@ -496,16 +540,25 @@ int persistentBlocks(const void* kernel, int threads) {
 }
 }  // namespace
 
+extern "C" cudaError_t mrtcu_wave_finalize(const MrtFrameParams* p, const MrtWaveState* s, uint32_t sampleBase,
+                                           uint32_t samples, cudaStream_t stream) {
+    const uint32_t pixels = p->width * p->height;
+    if (pixels == 0 || samples == 0) return cudaSuccess;
+    WaveArgs A{pixels, pixels * samples, sampleBase, samples};
+    waveFinalizeKernel<<<(pixels + 255) / 256, 256, 0, stream>>>(*p, *s, A);
+    return cudaGetLastError();
+}
+
 extern "C" cudaError_t mrtcu_wave(const MrtFrameParams* p, const MrtWaveState* s, uint32_t sampleBase,
                                   uint32_t samples, uint32_t* launches, const cudaEvent_t* stageEvents,
-                                  cudaStream_t stream) {
+                                  const MrtCacheArgs* cache, cudaStream_t stream) {
     const uint32_t pixels = p->width * p->height;
     if (pixels == 0 || samples == 0) return cudaSuccess;
     if (uint64_t(pixels) * samples > s->capacity) return cudaErrorInvalidValue;
     static int gExtend = 0, gShade = 0, gShadow = 0;
     if (gExtend == 0) {
         gExtend = persistentBlocks(reinterpret_cast<const void*>(waveExtendKernel), MRT_TRAV_THREADS);
-        gShade = persistentBlocks(reinterpret_cast<const void*>(waveShadeKernel), 128);
+        gShade = persistentBlocks(reinterpret_cast<const void*>(waveShadeKernel<false>), 128);
         gShadow = persistentBlocks(reinterpret_cast<const void*>(waveShadowKernel), MRT_TRAV_THREADS);
     }
     WaveArgs A{pixels, pixels * samples, sampleBase, samples};
@@ -518,14 +571,17 @@ extern "C" cudaError_t mrtcu_wave(const MrtFrameParams* p, const MrtWaveState* s
         if (ev) cudaEventRecord(ev[0], stream);
         waveExtendKernel<<<gExtend, MRT_TRAV_THREADS, 0, stream>>>(*p, *s, cur);
         if (ev) cudaEventRecord(ev[1], stream);
-        waveShadeKernel<<<gShade, 128, 0, stream>>>(*p, *s, A, cur);
+        if (cache) waveShadeKernel<true><<<gShade, 128, 0, stream>>>(*p, *s, A, cur, *cache);
+        else waveShadeKernel<false><<<gShade, 128, 0, stream>>>(*p, *s, A, cur, MrtCacheArgs{});
         if (ev) cudaEventRecord(ev[2], stream);
         waveShadowKernel<<<gShadow, MRT_TRAV_THREADS, 0, stream>>>(*p, *s);
         if (ev) cudaEventRecord(ev[3], stream);
         n += 3;
     }
-    waveFinalizeKernel<<<(pixels + 255) / 256, 256, 0, stream>>>(*p, *s, A);
-    ++n;
+    if (!cache) {  // the cache mode finalises after applying the cache (mrtcu_wave_finalize)
+        waveFinalizeKernel<<<(pixels + 255) / 256, 256, 0, stream>>>(*p, *s, A);
+        ++n;
+    }
     if (launches) *launches += n;
     return cudaGetLastError();
 }

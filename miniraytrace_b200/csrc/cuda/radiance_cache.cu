@@ -13,10 +13,11 @@
 // Network: 5 hidden layers of 64 (W0..W4, 64 x 64, ReLU), output W5 (3 x 64
 // stored as 16 x 64, rows 3..15 unused). No other biases.
 //
-// All arithmetic is FP32 on the CUDA cores: at 64 queries per block the
-// 5 x 64 x 64 layers cost ~21k FMA per query, about a millisecond for the
-// two million queries of a 1080p frame; the weights are read from shared
-// memory as broadcasts and the activations from padded shared rows.
+// Inference runs on the tensor cores (tcgen05 MMAs with BF16 operands and
+// FP32 accumulators in tensor memory, below). Training keeps FP32 on the CUDA
+// cores: 64 samples per block, weights read from shared memory as broadcasts
+// and activations from padded shared rows.
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include "device_api.h"
@@ -26,7 +27,6 @@ namespace {
 constexpr int kLevels = 16;
 constexpr uint32_t kTableSize = 1u << 19;
 constexpr int kWidth = 64;
-constexpr int kPad = kWidth + 1;  // shared-memory row stride (no bank conflicts)
 constexpr int kLayers = 5;        // hidden layers
 constexpr int kOutRows = 16;
 constexpr int kBlock = 64;        // queries per block = threads per block
@@ -118,121 +118,373 @@ __device__ void encode(const McacheParams& C, const float* f, float* enc, Corner
     for (int k = 56; k < kWidth; ++k) enc[k] = 0.0f;
 }
 
-// Weight matrix `layer` (rows x 64, row-major) into shared memory.
+constexpr int kAct = 68;  // activation row stride in shared memory (float4 aligned, conflict-free)
+constexpr int kMlpFloats = (kLayers + 1) * kWidth * kWidth;
+
+// Weight matrix `layer` (rows x 64, row-major) into shared memory (stride 64).
 __device__ void loadWeights(const float* __restrict__ mlp, int layer, int rows, float* sW) {
-    const float* W = mlp + size_t(layer) * kWidth * kWidth;
-    for (int i = threadIdx.x; i < rows * kWidth; i += blockDim.x) sW[(i / kWidth) * kPad + (i % kWidth)] = W[i];
+    const float4* W = reinterpret_cast<const float4*>(mlp + size_t(layer) * kWidth * kWidth);
+    float4* d = reinterpret_cast<float4*>(sW);
+    for (int i = threadIdx.x; i < rows * kWidth / 4; i += blockDim.x) d[i] = W[i];
 }
 
-// out[t][j] = sum_k W[j][k] * in[t][k] for this thread's row t, j < rows;
-// ReLU when `relu`.
-__device__ void layerForward(const float* sW, const float* in, float* out, int rows, bool relu) {
-    const int t = threadIdx.x;
+// A 64-float row of shared memory into registers.
+__device__ __forceinline__ void loadRow(const float* row, float (&x)[kWidth]) {
+#pragma unroll
+    for (int m = 0; m < kWidth / 4; ++m) {
+        const float4 v = reinterpret_cast<const float4*>(row)[m];
+        x[4 * m] = v.x;
+        x[4 * m + 1] = v.y;
+        x[4 * m + 2] = v.z;
+        x[4 * m + 3] = v.w;
+    }
+}
+
+// out[j] = sum_k W[j][k] x[k] for j < rows (ReLU when `relu`): x in
+// registers, each weight row read as 16 broadcast 128-bit loads.
+__device__ __forceinline__ void denseForward(const float* sW, const float (&x)[kWidth], float* out, int rows,
+                                             bool relu) {
     for (int j = 0; j < rows; ++j) {
-        float acc = 0.0f;
-#pragma unroll 16
-        for (int k = 0; k < kWidth; ++k) acc = fmaf(sW[j * kPad + k], in[t * kPad + k], acc);
-        out[t * kPad + j] = relu ? fmaxf(acc, 0.0f) : acc;
+        const float4* w = reinterpret_cast<const float4*>(sW + j * kWidth);
+        float acc0 = 0.0f, acc1 = 0.0f;
+#pragma unroll
+        for (int m = 0; m < kWidth / 4; m += 2) {
+            const float4 v = w[m], u = w[m + 1];
+            acc0 = fmaf(v.x, x[4 * m], acc0);
+            acc1 = fmaf(v.y, x[4 * m + 1], acc1);
+            acc0 = fmaf(v.z, x[4 * m + 2], acc0);
+            acc1 = fmaf(v.w, x[4 * m + 3], acc1);
+            acc0 = fmaf(u.x, x[4 * m + 4], acc0);
+            acc1 = fmaf(u.y, x[4 * m + 5], acc1);
+            acc0 = fmaf(u.z, x[4 * m + 6], acc0);
+            acc1 = fmaf(u.w, x[4 * m + 7], acc1);
+        }
+        const float acc = acc0 + acc1;
+        out[j] = relu ? fmaxf(acc, 0.0f) : acc;
     }
 }
 
-// Inference: one query per thread, 64 per block. out3 (n x 3) = max(net, 0).
-__global__ void __launch_bounds__(kBlock) queryKernel(McacheParams C, const float* __restrict__ features, uint32_t n,
-                                                      float* __restrict__ out3) {
-    extern __shared__ float smem[];
-    float* sW = smem;                     // kWidth x kPad
-    float* a0 = sW + kWidth * kPad;       // kBlock x kPad
-    float* a1 = a0 + kBlock * kPad;
-    const uint32_t q = blockIdx.x * kBlock + threadIdx.x;
-    const bool valid = q < n;
-    float f[16];
-    for (int k = 0; k < 16; ++k) f[k] = valid ? features[size_t(q) * 16 + k] : 0.0f;
-    encode(C, f, a0 + threadIdx.x * kPad, nullptr);
-    float* in = a0;
-    float* out = a1;
-    for (int l = 0; l <= kLayers; ++l) {
-        __syncthreads();
-        loadWeights(C.mlp, l, l < kLayers ? kWidth : kOutRows, sW);
-        __syncthreads();
-        layerForward(sW, in, out, l < kLayers ? kWidth : 3, l < kLayers);
-        float* t = in;
-        in = out;
-        out = t;
+// ---------------------------------------------------------------- inference --
+// Inference on the tensor cores (tcgen05, kind::f16, BF16 operands, FP32
+// accumulation in tensor memory). A CTA of 128 threads takes tiles of 128
+// queries: thread r encodes query r into row r of the activation tile A
+// (128 x 64 BF16 in shared memory); per layer one thread issues four
+// 128 x N x 16 MMAs (N = 64, or 16 for the output layer whose rows 3..15
+// are zero) reading A and the layer's weights W (N x 64 BF16, shared memory)
+// into a 128 x N FP32 accumulator in tensor memory, commits them to an
+// mbarrier, and every thread reads its own row back (tensor-memory lane r),
+// applies the ReLU and writes it, as BF16, over its row of A for the next
+// layer. Weights are converted once per CTA; the CTA then loops over tiles.
+//
+// Shared-memory operand layout (no swizzle, K-major): the tile is a grid of
+// 8-row x 16-byte core matrices stored as 128 contiguous bytes; element
+// (row r, k) of an R x 64 operand sits at (r / 8) * 1024 + (k / 8) * 128 +
+// (r % 8) * 16 + (k % 8) * 2. In the matrix descriptor the leading byte
+// offset (between the two core matrices along K of one 16-wide K step) is
+// 128 and the stride byte offset (between 8-row groups) is 1024; K step s
+// starts 256 * s bytes in.
+
+constexpr int kTile = 128;                      // queries per tile = MMA M
+constexpr uint32_t kWBytes = kWidth * kWidth * 2;   // one hidden layer, BF16
+constexpr uint32_t kWOutBytes = kOutRows * kWidth * 2;
+constexpr uint32_t kWAllBytes = kLayers * kWBytes + kWOutBytes;
+constexpr uint32_t kABytes = kTile * kWidth * 2;
+constexpr uint32_t kTmemCols = 64;              // the accumulator: 128 lanes x 64 FP32 columns
+constexpr uint32_t kWaitLimit = 1u << 20;       // mbarrier polls before a tile gives up
+
+__device__ __forceinline__ uint32_t coreOffset(uint32_t r, uint32_t k) {
+    return (r >> 3) * 1024u + (k >> 3) * 128u + (r & 7u) * 16u + (k & 7u) * 2u;
+}
+
+__device__ __forceinline__ uint32_t smemAddr(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// Shared-memory matrix descriptor: start address, leading and stride byte
+// offsets (all >> 4), descriptor version 1 (bits 46-47), no swizzle.
+__device__ __forceinline__ uint64_t smemDesc(uint32_t addr) {
+    return uint64_t((addr & 0x3FFFFu) >> 4) | (uint64_t(128u >> 4) << 16) | (uint64_t(1024u >> 4) << 32) |
+           (uint64_t(1) << 46);
+}
+
+// Instruction descriptor of kind::f16: FP32 accumulator (bits 4-5 = 1),
+// A and B BF16 (bits 7-9, 10-12 = 1), both K-major, N >> 3 at bit 17,
+// M >> 4 at bit 24.
+__host__ __device__ constexpr uint32_t instrDesc(uint32_t m, uint32_t n) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((n >> 3) << 17) | ((m >> 4) << 24);
+}
+
+__device__ __forceinline__ void fenceAsyncShared() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void tcFenceBefore() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tcFenceAfter() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tcMma(uint32_t dTmem, uint64_t aDesc, uint64_t bDesc, uint32_t idesc, bool accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(dTmem),
+        "l"(aDesc), "l"(bDesc), "r"(idesc), "r"(uint32_t(accumulate))
+        : "memory");
+}
+
+__device__ __forceinline__ void tcCommit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+
+// Polls the mbarrier for the given phase parity at most kWaitLimit times.
+__device__ __forceinline__ bool waitParity(uint32_t bar, uint32_t parity) {
+    for (uint32_t i = 0; i < kWaitLimit; ++i) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.b32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (done) return true;
     }
-    if (valid)
-        for (int c = 0; c < 3; ++c) out3[size_t(q) * 3 + c] = fmaxf(in[threadIdx.x * kPad + c], 0.0f);
+    return false;
+}
+
+// 16 consecutive FP32 columns of this thread's tensor-memory lane.
+__device__ __forceinline__ void tmemLoad16(uint32_t taddr, float* v) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+          "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ void tmemWaitLoad() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+__device__ __forceinline__ uint32_t packBf16(float a, float b) {
+    const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);  // a in the low half
+    return *reinterpret_cast<const uint32_t*>(&h);
+}
+
+// 64 values (ReLU'd when `relu`) as row r of an operand tile.
+__device__ __forceinline__ void storeRow(uint8_t* tile, uint32_t r, const float* v, bool relu) {
+#pragma unroll
+    for (int c = 0; c < kWidth / 8; ++c) {
+        float x[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) x[i] = relu ? fmaxf(v[8 * c + i], 0.0f) : v[8 * c + i];
+        const uint4 w = make_uint4(packBf16(x[0], x[1]), packBf16(x[2], x[3]), packBf16(x[4], x[5]),
+                                   packBf16(x[6], x[7]));
+        *reinterpret_cast<uint4*>(tile + coreOffset(r, 8 * c)) = w;
+    }
+}
+
+__global__ void __launch_bounds__(kTile) tcQueryKernel(McacheParams C, const float* __restrict__ features,
+                                                       uint32_t n, float* __restrict__ out3) {
+    extern __shared__ __align__(1024) uint8_t smem[];
+    uint8_t* sW = smem;                 // W0..W4 (8 KiB each), W5 (2 KiB)
+    uint8_t* sA = smem + kWAllBytes;    // activation tile
+    uint64_t* bar = reinterpret_cast<uint64_t*>(sA + kABytes);
+    uint32_t* tmemSlot = reinterpret_cast<uint32_t*>(bar + 1);
+    const uint32_t t = threadIdx.x, warp = t >> 5;
+
+    // weights, FP32 row-major in global memory, to BF16 operand tiles
+    for (uint32_t i = t; i < uint32_t(kLayers * kWidth * kWidth + kOutRows * kWidth) / 2; i += kTile) {
+        const uint32_t e = 2 * i, layer = e / (kWidth * kWidth), rem = e % (kWidth * kWidth);
+        const uint32_t j = rem / kWidth, k = rem % kWidth;
+        const float2 w = reinterpret_cast<const float2*>(C.mlp)[i];
+        *reinterpret_cast<uint32_t*>(sW + layer * kWBytes + coreOffset(j, k)) = packBf16(w.x, w.y);
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smemAddr(tmemSlot)),
+                     "r"(kTmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (t == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smemAddr(bar)) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    fenceAsyncShared();
+    tcFenceBefore();
+    __syncthreads();
+    tcFenceAfter();
+    const uint32_t tmem = *tmemSlot;
+    const uint32_t barAddr = smemAddr(bar), aAddr = smemAddr(sA), wAddr = smemAddr(sW);
+    const uint32_t laneBase = tmem + ((warp * 32u) << 16);  // this warp's 32 lanes
+    uint32_t parity = 0;
+    bool ok = true;
+    for (uint32_t tile = blockIdx.x; ok && size_t(tile) * kTile < n; tile += gridDim.x) {
+        const uint32_t q = tile * kTile + t;
+        const bool valid = q < n;
+        float f[16];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const float4 v = valid ? reinterpret_cast<const float4*>(features)[size_t(q) * 4 + k]
+                                   : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            f[4 * k] = v.x;
+            f[4 * k + 1] = v.y;
+            f[4 * k + 2] = v.z;
+            f[4 * k + 3] = v.w;
+        }
+        float v[kWidth];
+        encode(C, f, v, nullptr);
+        storeRow(sA, t, v, false);
+        fenceAsyncShared();
+        tcFenceBefore();
+        __syncthreads();
+        for (int l = 0; l <= kLayers; ++l) {
+            const uint32_t rows = l < kLayers ? kWidth : kOutRows;
+            if (t == 0) {
+                tcFenceAfter();
+                const uint32_t idesc = instrDesc(kTile, rows);
+#pragma unroll
+                for (uint32_t s = 0; s < kWidth / 16; ++s)
+                    tcMma(tmem, smemDesc(aAddr + 256u * s), smemDesc(wAddr + uint32_t(l) * kWBytes + 256u * s), idesc,
+                          s > 0);
+                tcCommit(barAddr);
+            }
+            const bool done = waitParity(barAddr, parity);
+            parity ^= 1u;
+            if (!__syncthreads_and(done)) {
+                ok = false;
+                break;
+            }
+            tcFenceAfter();
+            if (l < kLayers) {
+#pragma unroll
+                for (int c = 0; c < kWidth / 16; ++c) tmemLoad16(laneBase + 16u * c, v + 16 * c);
+                tmemWaitLoad();
+                storeRow(sA, t, v, true);
+                fenceAsyncShared();
+                tcFenceBefore();
+                __syncthreads();
+            } else {
+                tmemLoad16(laneBase, v);
+                tmemWaitLoad();
+                tcFenceBefore();
+                if (valid)
+                    for (int c = 0; c < 3; ++c) out3[size_t(q) * 3 + c] = fmaxf(v[c], 0.0f);
+            }
+        }
+    }
+    tcFenceBefore();
+    __syncthreads();
+    tcFenceAfter();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
+    if (!ok && t == 0) atomicOr(C.status, 1u);
 }
 
 // One training step's forward + backward for 64 samples per block: loss =
 // mean over samples and channels of (y - t)^2 / (y^2 + 0.01), y held fixed in
-// the denominator. Weight gradients are reduced over the block's samples and
-// added to gMlp; grid gradients are scattered to the 8 corners of each level.
+// the denominator. Each block writes its weight gradients (summed over its
+// samples, 8 x 8 register tiles per thread) to partial[block]; the grid
+// gradients are scattered to the 8 corners of each level.
 __global__ void __launch_bounds__(kBlock) trainKernel(McacheParams C, const float* __restrict__ features,
-                                                      const float* __restrict__ targets, uint32_t n, float invBatch,
+                                                      const float* __restrict__ targets, uint32_t n, uint32_t first,
+                                                      uint32_t every, float invBatch, float* __restrict__ partial,
                                                       float* __restrict__ lossOut) {
-    extern __shared__ float smem[];
-    float* sW = smem;                            // kWidth x kPad
-    float* act = sW + kWidth * kPad;             // (kLayers + 1) x kBlock x kPad: enc, h1..h5
-    float* dA = act + (kLayers + 1) * kBlock * kPad;  // kBlock x kPad: gradient of the current layer's output
-    float* dB = dA + kBlock * kPad;
+    extern __shared__ float4 smem4[];
+    float* sW = reinterpret_cast<float*>(smem4);       // kWidth x kWidth
+    float* act = sW + kWidth * kWidth;                 // (kLayers + 1) x kBlock x kAct: enc, h1..h5
+    float* dA = act + (kLayers + 1) * kBlock * kAct;   // kBlock x kAct: gradient of the layer's output
+    float* dB = dA + kBlock * kAct;
     const int t = threadIdx.x;
-    const uint32_t s = blockIdx.x * kBlock + t;
-    const bool valid = s < n;
+    const uint32_t j = blockIdx.x * kBlock + t;  // the step's j-th sample is record first + j * every
+    const bool valid = j < n;
+    const size_t s = size_t(first) + size_t(j) * every;
     float f[16];
-    for (int k = 0; k < 16; ++k) f[k] = valid ? features[size_t(s) * 16 + k] : 0.0f;
+    for (int k = 0; k < 16; ++k) f[k] = valid ? features[s * 16 + k] : 0.0f;
     Corners corners;
-    encode(C, f, act + t * kPad, &corners);
+    encode(C, f, act + t * kAct, &corners);
+    float x[kWidth];
     for (int l = 0; l <= kLayers; ++l) {
         __syncthreads();
         loadWeights(C.mlp, l, l < kLayers ? kWidth : kOutRows, sW);
         __syncthreads();
-        float* out = l < kLayers ? act + (l + 1) * kBlock * kPad : dA;  // the output goes to dA first
-        layerForward(sW, act + l * kBlock * kPad, out, l < kLayers ? kWidth : 3, l < kLayers);
+        loadRow(act + (l * kBlock + t) * kAct, x);
+        float* out = l < kLayers ? act + ((l + 1) * kBlock + t) * kAct : dA + t * kAct;
+        denseForward(sW, x, out, l < kLayers ? kWidth : 3, l < kLayers);
     }
-    // output gradient (3 channels), zero for padding samples
+    // output gradient (3 channels; zero for padding samples and channels)
     float loss = 0.0f;
     for (int c = 0; c < kWidth; ++c) {
         float g = 0.0f;
         if (c < 3 && valid) {
-            const float y = dA[t * kPad + c], tg = targets[size_t(s) * 3 + c];
+            const float y = dA[t * kAct + c], tg = targets[s * 3 + c];
             const float den = y * y + 0.01f;
             loss += (y - tg) * (y - tg) / den;
             g = 2.0f * (y - tg) / den * invBatch;
         }
-        dA[t * kPad + c] = g;
+        dA[t * kAct + c] = g;
     }
     if (lossOut && valid) atomicAdd(lossOut, loss * invBatch);
-    // backward through W5 .. W0
+    float* myPartial = partial + size_t(blockIdx.x) * kMlpFloats;
+    const int jt = t / 8, kt = t % 8;  // this thread's 8 x 8 tile of a weight gradient
     for (int l = kLayers; l >= 0; --l) {
         const int rows = l < kLayers ? kWidth : 3;
         __syncthreads();
         loadWeights(C.mlp, l, l < kLayers ? kWidth : kOutRows, sW);
         __syncthreads();
-        // weight gradient: gW[j][k] = sum_t dA[t][j] * in[t][k]
-        const float* in = act + l * kBlock * kPad;
-        float* gW = C.gMlp + size_t(l) * kWidth * kWidth;
-        for (int e = t; e < rows * kWidth; e += kBlock) {
-            const int j = e / kWidth, k = e % kWidth;
-            float acc = 0.0f;
-            for (int r = 0; r < kBlock; ++r) acc = fmaf(dA[r * kPad + j], in[r * kPad + k], acc);
-            atomicAdd(gW + e, acc);
+        const float* in = act + l * kBlock * kAct;
+        // weight gradient tile: g[j][k] = sum_r dA[r][j] in[r][k]
+        float g[8][8];
+#pragma unroll
+        for (int a = 0; a < 8; ++a)
+#pragma unroll
+            for (int b = 0; b < 8; ++b) g[a][b] = 0.0f;
+        if (8 * jt < rows) {
+            for (int r = 0; r < kBlock; ++r) {
+                const float4 d0 = reinterpret_cast<const float4*>(dA + r * kAct + 8 * jt)[0];
+                const float4 d1 = reinterpret_cast<const float4*>(dA + r * kAct + 8 * jt)[1];
+                const float4 i0 = reinterpret_cast<const float4*>(in + r * kAct + 8 * kt)[0];
+                const float4 i1 = reinterpret_cast<const float4*>(in + r * kAct + 8 * kt)[1];
+                const float dv[8] = {d0.x, d0.y, d0.z, d0.w, d1.x, d1.y, d1.z, d1.w};
+                const float iv[8] = {i0.x, i0.y, i0.z, i0.w, i1.x, i1.y, i1.z, i1.w};
+#pragma unroll
+                for (int a = 0; a < 8; ++a)
+#pragma unroll
+                    for (int b = 0; b < 8; ++b) g[a][b] = fmaf(dv[a], iv[b], g[a][b]);
+            }
         }
-        // input gradient: dB[t][k] = sum_j W[j][k] * dA[t][j], through the ReLU of `in` (hidden inputs)
-        for (int k = 0; k < kWidth; ++k) {
-            float acc = 0.0f;
-            for (int j = 0; j < rows; ++j) acc = fmaf(sW[j * kPad + k], dA[t * kPad + j], acc);
-            if (l > 0 && in[t * kPad + k] <= 0.0f) acc = 0.0f;
-            dB[t * kPad + k] = acc;
+        float* gOut = myPartial + size_t(l) * kWidth * kWidth;
+#pragma unroll
+        for (int a = 0; a < 8; ++a) {
+            float4* o = reinterpret_cast<float4*>(gOut + (8 * jt + a) * kWidth + 8 * kt);
+            o[0] = make_float4(g[a][0], g[a][1], g[a][2], g[a][3]);
+            o[1] = make_float4(g[a][4], g[a][5], g[a][6], g[a][7]);
         }
+        // input gradient of this thread's sample: dB[t][k] = sum_j W[j][k] dA[t][j],
+        // through the ReLU of the layer input (hidden layers only)
+        float acc[kWidth];
+#pragma unroll
+        for (int k = 0; k < kWidth; ++k) acc[k] = 0.0f;
+        for (int j = 0; j < rows; ++j) {
+            const float dj = dA[t * kAct + j];
+            const float4* w = reinterpret_cast<const float4*>(sW + j * kWidth);
+#pragma unroll
+            for (int m = 0; m < kWidth / 4; ++m) {
+                const float4 v = w[m];
+                acc[4 * m] = fmaf(v.x, dj, acc[4 * m]);
+                acc[4 * m + 1] = fmaf(v.y, dj, acc[4 * m + 1]);
+                acc[4 * m + 2] = fmaf(v.z, dj, acc[4 * m + 2]);
+                acc[4 * m + 3] = fmaf(v.w, dj, acc[4 * m + 3]);
+            }
+        }
+        float xin[kWidth];
+        loadRow(in + t * kAct, xin);
+#pragma unroll
+        for (int k = 0; k < kWidth; ++k)
+            dB[t * kAct + k] = (l > 0 && xin[k] <= 0.0f) ? 0.0f : acc[k];
         __syncthreads();
-        float* x = dA;
+        float* sw = dA;
         dA = dB;
-        dB = x;
+        dB = sw;
     }
     // dA holds the encoding gradient: scatter the grid part
     if (valid) {
         for (int l = 0; l < kLevels; ++l) {
-            const float g0 = dA[t * kPad + 2 * l], g1 = dA[t * kPad + 2 * l + 1];
+            const float g0 = dA[t * kAct + 2 * l], g1 = dA[t * kAct + 2 * l + 1];
             if (g0 == 0.0f && g1 == 0.0f) continue;
             for (int c = 0; c < 8; ++c) {
                 const uint32_t i = corners.idx[l][c];
@@ -244,11 +496,25 @@ __global__ void __launch_bounds__(kBlock) trainKernel(McacheParams C, const floa
     }
 }
 
-// Adam on every parameter; gradients are cleared for the next step.
+// gMlp[i] = sum over blocks of partial[b][i] (rows the output layer leaves
+// unwritten are zero in every partial).
+__global__ void reducePartialsKernel(const float* __restrict__ partial, uint32_t blocks, float* __restrict__ gMlp) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < kMlpFloats; i += gridDim.x * blockDim.x) {
+        float acc = 0.0f;
+        for (uint32_t b = 0; b < blocks; ++b) acc += partial[size_t(b) * kMlpFloats + i];
+        gMlp[i] = acc;
+    }
+}
+
+// Adam; gradients are cleared for the next step. With `lazy`, entries that
+// got no gradient this step are left as they are (their moments and values
+// do not decay), which the hash grid needs: a step touches a few of its
+// 16.8 M entries.
 __global__ void adamKernel(float* __restrict__ p, float* __restrict__ g, float* __restrict__ m, float* __restrict__ v,
-                           size_t n, float lr, float b1, float b2, float eps, float c1, float c2) {
+                           size_t n, float lr, float b1, float b2, float eps, float c1, float c2, bool lazy) {
     for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x) {
         const float gi = g[i];
+        if (lazy && gi == 0.0f) continue;
         g[i] = 0.0f;
         const float mi = b1 * m[i] + (1.0f - b1) * gi;
         const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
@@ -259,7 +525,7 @@ __global__ void adamKernel(float* __restrict__ p, float* __restrict__ g, float* 
 }
 
 // Deterministic initial values: grid uniform in [-1e-4, 1e-4], weights
-// uniform in +-sqrt(6 / (fan_in + fan_out)).
+// uniform in +-sqrt(6 / (fan_in + fan_out)), unused output rows zero.
 __device__ float hashUniform(uint32_t i, uint32_t seed) {
     uint32_t x = i * 747796405u + seed * 2891336453u + 1u;
     x ^= x >> 16;
@@ -271,7 +537,7 @@ __device__ float hashUniform(uint32_t i, uint32_t seed) {
 }
 
 __global__ void initKernel(float* __restrict__ grid, size_t gridN, float* __restrict__ mlp, uint32_t seed) {
-    const size_t total = gridN + size_t(kLayers + 1) * kWidth * kWidth;
+    const size_t total = gridN + size_t(kMlpFloats);
     for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < total; i += size_t(gridDim.x) * blockDim.x) {
         if (i < gridN) {
             grid[i] = 1e-4f * hashUniform(uint32_t(i), seed);
@@ -285,8 +551,40 @@ __global__ void initKernel(float* __restrict__ grid, size_t gridN, float* __rest
     }
 }
 
-size_t smemQuery() { return sizeof(float) * (kWidth * kPad + 2 * kBlock * kPad); }
-size_t smemTrain() { return sizeof(float) * (kWidth * kPad + (kLayers + 1 + 2) * kBlock * kPad); }
+// L[slot] += beta * prediction for every query of the wave.
+__global__ void applyQueriesKernel(const float* __restrict__ out3, const float4* __restrict__ qBeta, uint32_t n,
+                                   uint32_t slots, float4* __restrict__ L) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float4 b = qBeta[i];
+        const uint32_t slot = __float_as_uint(b.w);
+        if (slot >= slots) continue;
+        float4 l = L[slot];
+        l.x += b.x * out3[3 * size_t(i)];
+        l.y += b.y * out3[3 * size_t(i) + 1];
+        l.z += b.z * out3[3 * size_t(i) + 2];
+        L[slot] = l;
+    }
+}
+
+// Training target of a recorded vertex: the radiance its path gathered from
+// the vertex on, divided by the throughput that reached the vertex.
+__global__ void recordTargetsKernel(const float4* __restrict__ prefix, const float4* __restrict__ beta, uint32_t n,
+                                    uint32_t slots, const float4* __restrict__ L, float* __restrict__ targets) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float4 pre = prefix[i], b = beta[i];
+        const uint32_t slot = __float_as_uint(pre.w);
+        const float4 l = slot < slots ? L[slot] : pre;
+        const float d[3] = {l.x - pre.x, l.y - pre.y, l.z - pre.z};
+        const float bb[3] = {b.x, b.y, b.z};
+        for (int c = 0; c < 3; ++c) {
+            const float t = bb[c] > 1e-6f ? d[c] / bb[c] : 0.0f;
+            targets[3 * size_t(i) + c] = fminf(fmaxf(t, 0.0f), 1e3f);
+        }
+    }
+}
+
+size_t smemQuery() { return kWAllBytes + kABytes + 16; }
+size_t smemTrain() { return sizeof(float) * (kWidth * kWidth + (kLayers + 1 + 2) * kBlock * kAct); }
 
 unsigned gridFor(size_t n) {
     const size_t b = (n + 255) / 256;
@@ -296,12 +594,16 @@ unsigned gridFor(size_t n) {
 }  // namespace
 
 extern "C" size_t mrtcu_rc_grid_floats() { return size_t(kLevels) * kTableSize * 2; }
-extern "C" size_t mrtcu_rc_mlp_floats() { return size_t(kLayers + 1) * kWidth * kWidth; }
+extern "C" size_t mrtcu_rc_mlp_floats() { return size_t(kMlpFloats); }
+extern "C" size_t mrtcu_rc_partial_floats(uint32_t maxBatch) {
+    return size_t((maxBatch + kBlock - 1) / kBlock) * kMlpFloats;
+}
 
 extern "C" cudaError_t mrtcu_rc_init(McacheParams C, uint32_t seed, cudaStream_t stream) {
     const size_t gridN = mrtcu_rc_grid_floats(), mlpN = mrtcu_rc_mlp_floats();
     initKernel<<<gridFor(gridN + mlpN), 256, 0, stream>>>(C.grid, gridN, C.mlp, seed);
-    cudaError_t e;
+    cudaError_t e = cudaMemsetAsync(C.status, 0, sizeof(uint32_t), stream);
+    if (e != cudaSuccess) return e;
     for (float* p : {C.gGrid, C.mGrid, C.vGrid})
         if ((e = cudaMemsetAsync(p, 0, gridN * sizeof(float), stream)) != cudaSuccess) return e;
     for (float* p : {C.gMlp, C.mMlp, C.vMlp})
@@ -312,33 +614,62 @@ extern "C" cudaError_t mrtcu_rc_init(McacheParams C, uint32_t seed, cudaStream_t
 extern "C" cudaError_t mrtcu_rc_query(McacheParams C, const float* features, uint32_t n, float* out3,
                                       cudaStream_t stream) {
     if (n == 0) return cudaSuccess;
-    cudaError_t e = cudaFuncSetAttribute(queryKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smemQuery()));
+    cudaError_t e = cudaFuncSetAttribute(tcQueryKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smemQuery()));
     if (e != cudaSuccess) return e;
-    queryKernel<<<(n + kBlock - 1) / kBlock, kBlock, smemQuery(), stream>>>(C, features, n, out3);
+    // Persistent CTAs: at most 3 fit an SM by shared memory (59 KiB each), so
+    // their tensor memory (64 columns each) never exceeds the SM's 512.
+    int sms = 148;
+    int dev = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const uint32_t tiles = (n + kTile - 1) / kTile;
+    const uint32_t ctas = tiles < uint32_t(sms) * 3u ? tiles : uint32_t(sms) * 3u;
+    tcQueryKernel<<<ctas, kTile, smemQuery(), stream>>>(C, features, n, out3);
     return cudaGetLastError();
 }
 
-// `steps` Adam steps; step k trains on samples [k*batch, (k+1)*batch) modulo n.
+// `steps` Adam steps on batches of up to `batch` of the n samples.
 extern "C" cudaError_t mrtcu_rc_train(McacheParams* C, const float* features, const float* targets, uint32_t n,
                                       uint32_t steps, uint32_t batch, float* lossOut, cudaStream_t stream) {
     if (n == 0 || steps == 0) return cudaSuccess;
     cudaError_t e = cudaFuncSetAttribute(trainKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smemTrain()));
     if (e != cudaSuccess) return e;
     batch = batch < n ? batch : n;
+    batch = batch < C->partialBlocks * kBlock ? batch : C->partialBlocks * kBlock;
     const size_t gridN = mrtcu_rc_grid_floats(), mlpN = mrtcu_rc_mlp_floats();
+    // Step k trains on every `every`-th sample from sample k mod every: each
+    // batch spreads over all of the samples (they arrive ordered by bounce
+    // and by pixel), and consecutive steps take disjoint batches.
+    const uint32_t every = (n + batch - 1) / batch;
     for (uint32_t k = 0; k < steps; ++k) {
-        const uint32_t first = uint32_t((uint64_t(k) * batch) % n);
-        const uint32_t count = first + batch <= n ? batch : n - first;
-        trainKernel<<<(count + kBlock - 1) / kBlock, kBlock, smemTrain(), stream>>>(
-            *C, features + size_t(first) * 16, targets + size_t(first) * 3, count, 1.0f / (3.0f * float(count)),
-            lossOut);
+        const uint32_t first = k % every;
+        const uint32_t count = (n - first + every - 1) / every;  // <= batch
+        const uint32_t blocks = (count + kBlock - 1) / kBlock;
+        trainKernel<<<blocks, kBlock, smemTrain(), stream>>>(*C, features, targets, count, first, every,
+                                                              1.0f / (3.0f * float(count)), C->partial, lossOut);
+        reducePartialsKernel<<<gridFor(kMlpFloats), 256, 0, stream>>>(C->partial, blocks, C->gMlp);
         ++C->step;
         const float b1 = 0.9f, b2 = 0.99f;
         const float c1 = 1.0f / (1.0f - powf(b1, float(C->step))), c2 = 1.0f / (1.0f - powf(b2, float(C->step)));
         adamKernel<<<gridFor(gridN), 256, 0, stream>>>(C->grid, C->gGrid, C->mGrid, C->vGrid, gridN, C->lr, b1, b2,
-                                                       1e-10f, c1, c2);
+                                                       1e-10f, c1, c2, true);
         adamKernel<<<gridFor(mlpN), 256, 0, stream>>>(C->mlp, C->gMlp, C->mMlp, C->vMlp, mlpN, C->lr, b1, b2,
-                                                      1e-10f, c1, c2);
+                                                      1e-10f, c1, c2, false);
     }
+    return cudaGetLastError();
+}
+
+extern "C" cudaError_t mrtcu_rc_apply_queries(McacheParams C, const float* qFeat, const float4* qBeta, uint32_t n,
+                                              uint32_t slots, float* scratch3, float4* L, cudaStream_t stream) {
+    if (n == 0) return cudaSuccess;
+    const cudaError_t e = mrtcu_rc_query(C, qFeat, n, scratch3, stream);
+    if (e != cudaSuccess) return e;
+    applyQueriesKernel<<<gridFor(n), 256, 0, stream>>>(scratch3, qBeta, n, slots, L);
+    return cudaGetLastError();
+}
+
+extern "C" cudaError_t mrtcu_rc_record_targets(const float4* prefix, const float4* beta, uint32_t n, uint32_t slots,
+                                               const float4* L, float* targets, cudaStream_t stream) {
+    if (n == 0) return cudaSuccess;
+    recordTargetsKernel<<<gridFor(n), 256, 0, stream>>>(prefix, beta, n, slots, L, targets);
     return cudaGetLastError();
 }

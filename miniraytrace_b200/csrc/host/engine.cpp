@@ -48,6 +48,9 @@ namespace {
 #endif
 constexpr uint32_t kBatchWindow = MRT_BATCH_WINDOW;
 
+// Largest batch of one radiance-cache training step.
+constexpr uint32_t kCacheMaxBatch = 65536;
+
 // Path state per wave slot: rayO, rayD, beta, L, hit (5 x 16 B), hitInst +
 // two queues (3 x 4 B), shadow origin/dir/contribution (3 x 16 B).
 constexpr size_t kWaveBytesPerSlot = 5 * 16 + 3 * 4 + 3 * 16;
@@ -923,7 +926,10 @@ mrtResult Engine::launchPending() {
     const MrtFrameParams p = m_pendingParams;
     MRT_CUDA(cudaMemsetAsync(m_rayCounters.ptr, 0, 64, m_stream));
     uint32_t launches = 0;
-    const uint32_t waves = (n + m_waveSamples - 1) / m_waveSamples;
+    // the cache mode renders waves of a few samples and trains after each
+    const uint32_t waveCap = m_cache.enabled ? std::min(m_waveSamples, m_cache.samplesPerUpdate) : m_waveSamples;
+    if (m_cache.enabled) MRT_TRY(guard(cacheWaveBuffers(waveCap, p.maxBounces)));
+    const uint32_t waves = (n + waveCap - 1) / waveCap;
     const size_t perWave = size_t(6) * (p.maxBounces + 1);
     while (m_stageEvents.size() < waves * perWave) {
         cudaEvent_t ev;
@@ -933,10 +939,13 @@ mrtResult Engine::launchPending() {
     MRT_CUDA(cudaEventRecord(m_ev0, m_stream));
     uint32_t wave = 0;
     for (uint32_t done = 0; done < n; ++wave) {
-        const uint32_t k = std::min(n - done, m_waveSamples);
+        const uint32_t k = std::min(n - done, waveCap);
+        if (m_cache.enabled) MRT_CUDA(cudaMemsetAsync(m_cache.counts.ptr, 0, 8, m_stream));
         const cudaError_t le = mrtcu_wave(&p, &m_waveState, m_frameIndex + done, k, &launches,
-                                          m_stageEvents.data() + wave * perWave, m_stream);
+                                          m_stageEvents.data() + wave * perWave,
+                                          m_cache.enabled ? &m_cache.args : nullptr, m_stream);
         if (le != cudaSuccess) return guard(fromCuda(le, "path tracing launch"));
+        if (m_cache.enabled) MRT_TRY(guard(cacheWave(p, m_frameIndex + done, k)));
         done += k;
     }
     MRT_CUDA(cudaEventRecord(m_ev1, m_stream));
@@ -1231,7 +1240,9 @@ mrtResult Engine::buildMeshBvhDevice(const V4f* pos, size_t nv, const uint32_t* 
 // ------------------------------------------------------------ radiance cache --
 
 void Engine::RadianceCache::release() {
-    for (DeviceBuffer* d : {&grid, &mlp, &gGrid, &gMlp, &mGrid, &vGrid, &mMlp, &vMlp, &in, &out, &loss}) d->release();
+    for (DeviceBuffer* d : {&grid, &mlp, &gGrid, &gMlp, &mGrid, &vGrid, &mMlp, &vMlp, &in, &out, &loss, &partial, &qFeat,
+                            &qBeta, &rFeat, &rPrefix, &rBeta, &rTarget, &counts, &scratch})
+        d->release();
     allocated = false;
 }
 
@@ -1258,7 +1269,11 @@ mrtResult Engine::ensureCache() {
     for (DeviceBuffer* d : {&m_cache.grid, &m_cache.gGrid, &m_cache.mGrid, &m_cache.vGrid}) MRT_TRY(d->ensure(g));
     for (DeviceBuffer* d : {&m_cache.mlp, &m_cache.gMlp, &m_cache.mMlp, &m_cache.vMlp}) MRT_TRY(d->ensure(w));
     MRT_TRY(m_cache.loss.ensure(16));
+    MRT_TRY(m_cache.partial.ensure(mrtcu_rc_partial_floats(kCacheMaxBatch) * sizeof(float)));
     McacheParams& c = m_cache.params;
+    c.partial = m_cache.partial.as<float>();
+    c.status = m_cache.loss.as<uint32_t>() + 1;  // the loss buffer's second word
+    c.partialBlocks = uint32_t((kCacheMaxBatch + 63) / 64);
     c.grid = m_cache.grid.as<float>();
     c.mlp = m_cache.mlp.as<float>();
     c.gGrid = m_cache.gGrid.as<float>();
@@ -1280,8 +1295,10 @@ mrtResult Engine::setRadianceCache(const mrtxRadianceCacheDesc& d) {
     MRT_TRY(checkAlive());
     MRT_TRY(flushPending());
     const bool reinit = m_cache.allocated && d.seed != m_cache.seed;
-    m_cache.trainingPaths = d.trainingPaths ? d.trainingPaths : 65536u;
-    m_cache.stepsPerSample = d.stepsPerSample ? d.stepsPerSample : 4u;
+    m_cache.trainingPaths = d.trainingPaths;  // 0: a 32nd of the pixels (cacheWaveBuffers)
+    m_cache.stepsPerSample = d.stepsPerSample ? d.stepsPerSample : 1u;
+    m_cache.samplesPerUpdate = d.samplesPerUpdate ? std::min(d.samplesPerUpdate, 64u) : 4u;
+    m_cache.trainingVertices = d.trainingVertices;
     m_cache.lr = d.learningRate > 0.0f ? d.learningRate : 1e-2f;
     m_cache.seed = d.seed;
     for (int a = 0; a < 3; ++a) {
@@ -1305,9 +1322,11 @@ mrtResult Engine::cacheQuery(const float* features, uint32_t n, float* rgb) {
     MRT_TRY(m_cache.out.ensure(size_t(n) * 3 * sizeof(float)));
     MRT_CUDA(mrtcu_rc_query(m_cache.params, m_cache.in.as<float>(), n, m_cache.out.as<float>(), m_stream));
     MRT_CUDA(cudaMemcpyAsync(rgb, m_cache.out.ptr, size_t(n) * 3 * sizeof(float), cudaMemcpyDeviceToHost, m_stream));
+    uint32_t status = 0;
+    MRT_CUDA(cudaMemcpyAsync(&status, m_cache.params.status, sizeof(status), cudaMemcpyDeviceToHost, m_stream));
     const cudaError_t e = cudaStreamSynchronize(m_stream);
     if (e != cudaSuccess) return guard(fromCuda(e, "radiance cache query"));
-    return MRT_SUCCESS;
+    return cacheStatus(status);
 }
 
 mrtResult Engine::cacheTrain(const float* features, const float* targets, uint32_t n, uint32_t steps, float* loss) {
@@ -1347,6 +1366,73 @@ mrtResult Engine::cacheParams(float* gridOut, float* mlpOut, const float* gridIn
     }
     const cudaError_t e = cudaStreamSynchronize(m_stream);
     if (e != cudaSuccess) return guard(fromCuda(e, "radiance cache parameters"));
+    return MRT_SUCCESS;
+}
+
+// A query kernel whose tensor-core wait gave up leaves bit 0 of the status
+// word set (its outputs are incomplete).
+mrtResult Engine::cacheStatus(uint32_t status) {
+    if (status & 1u) return fail(MRT_ERROR_UNKNOWN, "radiance cache: a tensor-core wait timed out");
+    return MRT_SUCCESS;
+}
+
+// Query and record buffers of one cache-mode wave of `samples` samples.
+mrtResult Engine::cacheWaveBuffers(uint32_t samples, uint32_t maxBounces) {
+    MRT_TRY(ensureCache());
+    const uint64_t pixels = uint64_t(m_settings.width) * m_settings.height;
+    const uint64_t q = pixels * samples;
+    const uint64_t training = m_cache.trainingPaths ? m_cache.trainingPaths : std::max<uint64_t>(1024, pixels / 32);
+    const uint32_t stride = uint32_t(std::max<uint64_t>(1, pixels / training));
+    // A vertex k bounces in sees maxBounces - k more bounces; the queried
+    // vertex (k = 1) sees maxBounces - 1. Deeper vertices' targets miss the
+    // energy of the bounces cut off at the budget, so only the first few
+    // vertices train the cache.
+    const uint32_t vertices = m_cache.trainingVertices ? m_cache.trainingVertices
+                                                       : std::max(1u, maxBounces / 4u);
+    const uint64_t r = std::min<uint64_t>(q, (pixels / stride + 1024) * samples * std::min(vertices, std::max(1u, maxBounces)));
+    MRT_TRY(m_cache.qFeat.ensure(q * 16 * sizeof(float)));
+    MRT_TRY(m_cache.qBeta.ensure(q * sizeof(float4)));
+    MRT_TRY(m_cache.scratch.ensure(q * 3 * sizeof(float)));
+    MRT_TRY(m_cache.rFeat.ensure(r * 16 * sizeof(float)));
+    MRT_TRY(m_cache.rPrefix.ensure(r * sizeof(float4)));
+    MRT_TRY(m_cache.rBeta.ensure(r * sizeof(float4)));
+    MRT_TRY(m_cache.rTarget.ensure(r * 3 * sizeof(float)));
+    MRT_TRY(m_cache.counts.ensure(16));
+    MrtCacheArgs& K = m_cache.args;
+    K.qFeat = m_cache.qFeat.as<float>();
+    K.qBeta = m_cache.qBeta.as<float4>();
+    K.qCount = m_cache.counts.as<uint32_t>();
+    K.qCap = uint32_t(q);
+    K.rFeat = m_cache.rFeat.as<float>();
+    K.rPrefix = m_cache.rPrefix.as<float4>();
+    K.rBeta = m_cache.rBeta.as<float4>();
+    K.rCount = m_cache.counts.as<uint32_t>() + 1;
+    K.rCap = uint32_t(r);
+    K.trainStride = stride;
+    K.recordBounces = vertices;
+    cacheBounds();
+    return MRT_SUCCESS;
+}
+
+// After a cache-mode wave's bounces: the cache's predictions join the
+// stopped paths, the training paths' vertices become training samples, the
+// cache trains on them, and the wave is accumulated.
+mrtResult Engine::cacheWave(const MrtFrameParams& p, uint32_t sampleBase, uint32_t samples) {
+    uint32_t counts[2] = {0, 0}, status = 0;
+    MRT_CUDA(cudaMemcpyAsync(counts, m_cache.counts.ptr, sizeof(counts), cudaMemcpyDeviceToHost, m_stream));
+    MRT_CUDA(cudaMemcpyAsync(&status, m_cache.params.status, sizeof(status), cudaMemcpyDeviceToHost, m_stream));
+    MRT_CUDA(cudaStreamSynchronize(m_stream));
+    MRT_TRY(cacheStatus(status));  // the previous wave's queries
+    const MrtCacheArgs& K = m_cache.args;
+    const uint32_t nq = std::min(counts[0], K.qCap), nr = std::min(counts[1], K.rCap);
+    const uint32_t slots = p.width * p.height * samples;
+    MRT_CUDA(mrtcu_rc_apply_queries(m_cache.params, K.qFeat, K.qBeta, nq, slots, m_cache.scratch.as<float>(),
+                                    m_waveState.L, m_stream));
+    MRT_CUDA(mrtcu_rc_record_targets(K.rPrefix, K.rBeta, nr, slots, m_waveState.L, m_cache.rTarget.as<float>(),
+                                     m_stream));
+    MRT_CUDA(mrtcu_rc_train(&m_cache.params, K.rFeat, m_cache.rTarget.as<float>(), nr,
+                            m_cache.stepsPerSample * samples, 16384u, nullptr, m_stream));
+    MRT_CUDA(mrtcu_wave_finalize(&p, &m_waveState, sampleBase, samples, m_stream));
     return MRT_SUCCESS;
 }
 

@@ -126,16 +126,21 @@ private:
 
     // radiance cache: parameters, gradients, Adam moments, query scratch
     struct RadianceCache {
-        DeviceBuffer grid, mlp, gGrid, gMlp, mGrid, vGrid, mMlp, vMlp, in, out, loss;
+        DeviceBuffer grid, mlp, gGrid, gMlp, mGrid, vGrid, mMlp, vMlp, in, out, loss, partial;
+        DeviceBuffer qFeat, qBeta, rFeat, rPrefix, rBeta, rTarget, counts, scratch;  // per-wave queries/records
+        MrtCacheArgs args{};
         McacheParams params{};
         bool allocated = false, enabled = false;
-        uint32_t trainingPaths = 65536, stepsPerSample = 4, seed = 1;
+        uint32_t trainingPaths = 0, stepsPerSample = 1, seed = 1, samplesPerUpdate = 4, trainingVertices = 0;
         float lr = 1e-2f;
         float lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
         void release();
     } m_cache;
     mrtResult ensureCache();
     void cacheBounds();
+    mrtResult cacheWaveBuffers(uint32_t samples, uint32_t maxBounces);
+    mrtResult cacheStatus(uint32_t status);
+    mrtResult cacheWave(const MrtFrameParams& p, uint32_t sampleBase, uint32_t samples);
     MrtWaveState m_waveState{};
     uint32_t m_waveSamples = 0;  // samples per pixel one wave holds
     uint64_t m_maxWaveSlots = uint64_t(1) << 25;  // paths per wave, set from the GPU's memory
