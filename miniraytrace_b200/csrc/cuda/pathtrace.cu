@@ -14,11 +14,14 @@
 //   - traversal is the watertight two-level walk of trace.cuh;
 //   - the first-hit AOV buffers of the reference are not produced (they only
 //     feed an optional OIDN denoiser and are not readable through the ABI).
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include "device_api.h"
 #include "shade.cuh"
 #include "trace.cuh"
+
+namespace cg = cooperative_groups;
 
 namespace {
 
@@ -106,6 +109,15 @@ MRT_DEV void warpAddCounters(unsigned long long* ctr, const uint32_t (&c)[kCtrCo
 
 // Warp-aggregated queue append: every lane of the warp must call it; lanes
 // with pred get consecutive indices from one atomicAdd on *count.
+// Index of this thread's entry in a list that every thread of the current
+// coalesced group appends one entry to (one atomic per group).
+MRT_DEV uint32_t coalescedAppend(uint32_t* count) {
+    const cg::coalesced_group g = cg::coalesced_threads();
+    uint32_t base = 0;
+    if (g.thread_rank() == 0) base = atomicAdd(count, g.size());
+    return g.shfl(base, 0) + g.thread_rank();
+}
+
 MRT_DEV uint32_t warpAppend(uint32_t* count, bool pred) {
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t mask = __ballot_sync(0xffffffffu, pred);
@@ -254,14 +266,25 @@ __global__ void MRT_TRAV_BOUNDS waveExtendKernel(MrtFrameParams P, MrtWaveState 
 // (a shadow ray with its contribution is queued), BSDF sample, Russian
 // roulette, next ray queued. The draws from the path's pcg4d stream happen in
 // the reference's order; the counter lives in beta.w between bounces.
-// Training-path selection of the cache mode (a slot hash, so training paths
-// spread over the image and change from wave to wave).
-MRT_DEV bool cacheTrainingPath(const MrtCacheArgs& K, uint32_t slot, uint32_t sampleBase) {
-    uint32_t x = slot * 0x9e3779b1u ^ (sampleBase + 1u) * 0x85ebca77u;
+// Training-path selection of the cache mode: whether the path of (pixel,
+// frame index) is a training path, a hash of both, so training paths spread
+// over the image and every sample (of every sample stream) picks its own.
+MRT_DEV bool cacheTrainingPath(const MrtCacheArgs& K, uint32_t pixel, uint32_t frame) {
+    uint32_t x = pixel * 0x9e3779b1u ^ (frame + 1u) * 0x85ebca77u;
     x ^= x >> 15;
     x *= 0x2c1b3c6du;
     x ^= x >> 12;
     return x % K.trainStride == 0u;
+}
+
+// The 16 cache input features of a surface vertex: position, outgoing
+// direction, shading normal, roughness, base colour, zero padding.
+MRT_DEV void writeCacheFeatures(float* out, const Surface& s, float3 wo, const Bsdf& bsdf) {
+    float4* f = reinterpret_cast<float4*>(out);
+    f[0] = make_float4(s.pos.x, s.pos.y, s.pos.z, wo.x);
+    f[1] = make_float4(wo.y, wo.z, s.nShade.x, s.nShade.y);
+    f[2] = make_float4(s.nShade.z, bsdf.roughness, bsdf.baseColor.x, bsdf.baseColor.y);
+    f[3] = make_float4(bsdf.baseColor.z, 0.0f, 0.0f, 0.0f);
 }
 
 template <bool kCache>
@@ -279,9 +302,7 @@ __global__ void __launch_bounds__(128) waveShadeKernel(MrtFrameParams P, MrtWave
         uint32_t slot = 0;
         float3 shOrig = f3(0.0f), shDir = f3(0.0f), shContrib = f3(0.0f);
         float shTMax = 0.0f;
-        bool cacheQuery = false, cacheRecord = false;  // cache mode only
-        float feat[13];
-        float3 cacheBeta = f3(0.0f), cachePrefix = f3(0.0f);
+        bool cacheQuery = false;  // cache mode: the path stops here and takes the cache's prediction
         if (valid) {
             slot = q[i];
             const float4 o4 = S.rayO[slot], d4 = S.rayD[slot], b4 = S.beta[slot], L4 = S.L[slot];
@@ -319,16 +340,28 @@ __global__ void __launch_bounds__(128) waveShadeKernel(MrtFrameParams P, MrtWave
                     if (maxComp(emission) > 0.0f && s.frontFace) L += beta * emission;
                     const Bsdf bsdf = makeBsdf(P, s);
                     if (kCache && bounce >= 1u) {
-                        const float3 wo = -rd;
-                        const float f13[13] = {s.pos.x,    s.pos.y,    s.pos.z,    wo.x,
-                                               wo.y,       wo.z,       s.nShade.x, s.nShade.y,
-                                               s.nShade.z, bsdf.roughness, bsdf.baseColor.x, bsdf.baseColor.y,
-                                               bsdf.baseColor.z};
-                        for (int k = 0; k < 13; ++k) feat[k] = f13[k];
-                        cacheBeta = beta;
-                        cachePrefix = L;
-                        if (cacheTrainingPath(K, slot, A.sampleBase)) cacheRecord = bounce <= K.recordBounces;
-                        else cacheQuery = true;  // the cache stands for everything scattered from here on
+                        // A query (the cache stands for everything scattered
+                        // from here on) or, on a training path's first
+                        // vertices, a training record; its features are
+                        // written out here.
+                        // (Queries and records append in separate branches: a
+                        // coalesced group then shares one list.)
+                        cacheQuery = !cacheTrainingPath(K, pixel, frameOf(P, A, slot));
+                        const float4 b4 = make_float4(beta.x, beta.y, beta.z, __uint_as_float(slot));
+                        if (cacheQuery) {
+                            const uint32_t idx = coalescedAppend(K.qCount);
+                            if (idx < K.qCap) {
+                                writeCacheFeatures(K.qFeat + size_t(idx) * 16, s, -rd, bsdf);
+                                K.qBeta[idx] = b4;
+                            }
+                        } else if (bounce <= K.recordBounces) {
+                            const uint32_t idx = coalescedAppend(K.rCount);
+                            if (idx < K.rCap) {
+                                writeCacheFeatures(K.rFeat + size_t(idx) * 16, s, -rd, bsdf);
+                                K.rPrefix[idx] = make_float4(L.x, L.y, L.z, __uint_as_float(slot));
+                                K.rBeta[idx] = b4;
+                            }
+                        }
                     }
                     float3 Tn, Bn;
                     buildOnb(s.nShade, Tn, Bn);
@@ -384,23 +417,6 @@ __global__ void __launch_bounds__(128) waveShadeKernel(MrtFrameParams P, MrtWave
             S.shO[si] = make_float4(shOrig.x, shOrig.y, shOrig.z, shTMax);
             S.shD[si] = make_float4(shDir.x, shDir.y, shDir.z, __uint_as_float(slot));
             S.shC[si] = make_float4(shContrib.x, shContrib.y, shContrib.z, 0.0f);
-        }
-        if (kCache) {
-            const uint32_t qi = warpAppend(K.qCount, cacheQuery);
-            if (cacheQuery && qi < K.qCap) {
-                float* f = K.qFeat + size_t(qi) * 16;
-                for (int k = 0; k < 13; ++k) f[k] = feat[k];
-                f[13] = f[14] = f[15] = 0.0f;
-                K.qBeta[qi] = make_float4(cacheBeta.x, cacheBeta.y, cacheBeta.z, __uint_as_float(slot));
-            }
-            const uint32_t ri = warpAppend(K.rCount, cacheRecord);
-            if (cacheRecord && ri < K.rCap) {
-                float* f = K.rFeat + size_t(ri) * 16;
-                for (int k = 0; k < 13; ++k) f[k] = feat[k];
-                f[13] = f[14] = f[15] = 0.0f;
-                K.rPrefix[ri] = make_float4(cachePrefix.x, cachePrefix.y, cachePrefix.z, __uint_as_float(slot));
-                K.rBeta[ri] = make_float4(cacheBeta.x, cacheBeta.y, cacheBeta.z, 0.0f);
-            }
         }
     }
     warpAddCounters(P.rayCounters, c);

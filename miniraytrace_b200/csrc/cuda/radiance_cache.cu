@@ -191,6 +191,7 @@ constexpr uint32_t kWAllBytes = kLayers * kWBytes + kWOutBytes;
 constexpr uint32_t kABytes = kTile * kWidth * 2;
 constexpr uint32_t kTmemCols = 64;              // the accumulator: 128 lanes x 64 FP32 columns
 constexpr uint32_t kWaitLimit = 1u << 20;       // mbarrier polls before a tile gives up
+constexpr bool kRenderClamp = true;             // rendering takes max(prediction, 0)
 
 __device__ __forceinline__ uint32_t coreOffset(uint32_t r, uint32_t k) {
     return (r >> 3) * 1024u + (k >> 3) * 128u + (r & 7u) * 16u + (k & 7u) * 2u;
@@ -279,7 +280,7 @@ __device__ __forceinline__ void storeRow(uint8_t* tile, uint32_t r, const float*
 }
 
 __global__ void __launch_bounds__(kTile) tcQueryKernel(McacheParams C, const float* __restrict__ features,
-                                                       uint32_t n, float* __restrict__ out3) {
+                                                       uint32_t n, float* __restrict__ out3, bool clampOut) {
     extern __shared__ __align__(1024) uint8_t smem[];
     uint8_t* sW = smem;                 // W0..W4 (8 KiB each), W5 (2 KiB)
     uint8_t* sA = smem + kWAllBytes;    // activation tile
@@ -363,7 +364,7 @@ __global__ void __launch_bounds__(kTile) tcQueryKernel(McacheParams C, const flo
                 tmemWaitLoad();
                 tcFenceBefore();
                 if (valid)
-                    for (int c = 0; c < 3; ++c) out3[size_t(q) * 3 + c] = fmaxf(v[c], 0.0f);
+                    for (int c = 0; c < 3; ++c) out3[size_t(q) * 3 + c] = clampOut ? fmaxf(v[c], 0.0f) : v[c];
             }
         }
     }
@@ -611,8 +612,8 @@ extern "C" cudaError_t mrtcu_rc_init(McacheParams C, uint32_t seed, cudaStream_t
     return cudaGetLastError();
 }
 
-extern "C" cudaError_t mrtcu_rc_query(McacheParams C, const float* features, uint32_t n, float* out3,
-                                      cudaStream_t stream) {
+static cudaError_t launchQuery(const McacheParams& C, const float* features, uint32_t n, float* out3, bool clampOut,
+                               cudaStream_t stream) {
     if (n == 0) return cudaSuccess;
     cudaError_t e = cudaFuncSetAttribute(tcQueryKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smemQuery()));
     if (e != cudaSuccess) return e;
@@ -623,8 +624,13 @@ extern "C" cudaError_t mrtcu_rc_query(McacheParams C, const float* features, uin
     if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const uint32_t tiles = (n + kTile - 1) / kTile;
     const uint32_t ctas = tiles < uint32_t(sms) * 3u ? tiles : uint32_t(sms) * 3u;
-    tcQueryKernel<<<ctas, kTile, smemQuery(), stream>>>(C, features, n, out3);
+    tcQueryKernel<<<ctas, kTile, smemQuery(), stream>>>(C, features, n, out3, clampOut);
     return cudaGetLastError();
+}
+
+extern "C" cudaError_t mrtcu_rc_query(McacheParams C, const float* features, uint32_t n, float* out3,
+                                      cudaStream_t stream) {
+    return launchQuery(C, features, n, out3, true, stream);
 }
 
 // `steps` Adam steps on batches of up to `batch` of the n samples.
@@ -661,7 +667,7 @@ extern "C" cudaError_t mrtcu_rc_train(McacheParams* C, const float* features, co
 extern "C" cudaError_t mrtcu_rc_apply_queries(McacheParams C, const float* qFeat, const float4* qBeta, uint32_t n,
                                               uint32_t slots, float* scratch3, float4* L, cudaStream_t stream) {
     if (n == 0) return cudaSuccess;
-    const cudaError_t e = mrtcu_rc_query(C, qFeat, n, scratch3, stream);
+    const cudaError_t e = launchQuery(C, qFeat, n, scratch3, kRenderClamp, stream);
     if (e != cudaSuccess) return e;
     applyQueriesKernel<<<gridFor(n), 256, 0, stream>>>(scratch3, qBeta, n, slots, L);
     return cudaGetLastError();

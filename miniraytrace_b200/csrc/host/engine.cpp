@@ -1430,8 +1430,13 @@ mrtResult Engine::cacheWave(const MrtFrameParams& p, uint32_t sampleBase, uint32
                                     m_waveState.L, m_stream));
     MRT_CUDA(mrtcu_rc_record_targets(K.rPrefix, K.rBeta, nr, slots, m_waveState.L, m_cache.rTarget.as<float>(),
                                      m_stream));
-    MRT_CUDA(mrtcu_rc_train(&m_cache.params, K.rFeat, m_cache.rTarget.as<float>(), nr,
-                            m_cache.stepsPerSample * samples, 16384u, nullptr, m_stream));
+    // Batches of up to 16,384 records, smaller when the wave has fewer than
+    // steps x 16,384: the steps then take disjoint batches, so no record
+    // trains the cache twice (re-used noisy targets get memorised).
+    const uint32_t steps = m_cache.stepsPerSample * samples;
+    const uint32_t batch = std::max(64u, std::min(16384u, nr / std::max(1u, steps)));
+    MRT_CUDA(mrtcu_rc_train(&m_cache.params, K.rFeat, m_cache.rTarget.as<float>(), nr, steps, batch, nullptr,
+                            m_stream));
     MRT_CUDA(mrtcu_wave_finalize(&p, &m_waveState, sampleBase, samples, m_stream));
     return MRT_SUCCESS;
 }
