@@ -53,10 +53,12 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--config", choices=["terrain", "box_sphere", "batch", "room"], default="terrain",
+    ap.add_argument("--config", choices=["terrain", "box_sphere", "batch", "room", "cache"], default="terrain",
                     help="batch: the 16 uneven config-3 jobs in one mrtxRenderBatch submission per step "
                          "(single GPU; reports aggregate Mpaths/s and per-job completion); "
-                         "room: time to relMSE 1e-3 on config 4")
+                         "room: time to relMSE 1e-3 on config 4, plain and radiance-cached; "
+                         "cache: config 4 rendered with the radiance cache, 4 spp per step, reporting the "
+                         "cache's inference and training kernels")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -146,6 +148,14 @@ def measured_peaks():
         d = json.loads(p.read_text())
         return float(d["hbm_gbs"]), "measured"
     return 6650.0, "fallback"
+
+
+def measured_bf16_tflops():
+    """Burst bf16 dense TFLOP/s measured on this GPU pool (fallback 1590)."""
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        return float(json.loads(p.read_text())["bf16_tflops"])
+    return 1590.0
 
 
 def ncu_dram_bytes_per_ray(config):
@@ -483,15 +493,24 @@ def converge(engine, ref, target, chunk, limit):
     end). Device time is the engines' CUDA-event render time; the readback
     and the relMSE between chunks are not counted."""
     spp, device_ms, curve = 0, 0.0, []
+    cache = {"cacheQueryMs": 0.0, "cacheTrainMs": 0.0, "cacheQueries": 0, "cacheRecords": 0, "cacheSteps": 0}
     err = float("inf")
     while err > target and spp < limit:
         engine.render_frames(chunk)
         spp += chunk
-        device_ms += engine.stats()["lastRenderMs"]
+        st = engine.stats()
+        device_ms += st["lastRenderMs"]
+        for k in cache:
+            cache[k] += st[k]
         err = rel_mse(engine.read_framebuffer()[..., :3].astype(np.float64), ref)
         if spp & (spp - 1) == 0 or err <= target:
             curve.append((spp, round(device_ms, 1), err))
-    return spp, device_ms / 1e3, err <= target, curve
+    return spp, device_ms / 1e3, err <= target, curve, cache
+
+
+# FLOPs of one radiance-cache query: 5 hidden 64 x 64 layers and the 16 x 64
+# output layer as the tensor cores compute it, 2 FLOPs per multiply-add.
+CACHE_QUERY_FLOPS = 2 * (5 * 64 * 64 + 16 * 64)
 
 
 def room_arm(args):
@@ -528,9 +547,19 @@ def room_arm(args):
         e.commit()
         if mode == "cached":
             e.set_radiance_cache(enabled=True)
-        spp, secs, reached, curve = converge(e, R, TARGET, chunk, REF_SPP // 4)
+        spp, secs, reached, curve, cache = converge(e, R, TARGET, chunk, REF_SPP // 4)
         arms[mode] = {"spp_to_target": spp if reached else None, "seconds": secs if reached else None,
                       "ms_per_spp": secs * 1e3 / spp, "curve_spp_ms_relmse": curve}
+        if mode == "cached" and cache["cacheQueryMs"] > 0:
+            peak = measured_bf16_tflops()
+            tflops = cache["cacheQueries"] * CACHE_QUERY_FLOPS / (cache["cacheQueryMs"] * 1e-3) / 1e12
+            arms[mode]["cache_kernels"] = {
+                "inference_ms": round(cache["cacheQueryMs"], 2), "queries": cache["cacheQueries"],
+                "gqueries_per_s": cache["cacheQueries"] / (cache["cacheQueryMs"] * 1e-3) / 1e9,
+                "inference_tflops": tflops, "inference_frac_of_measured_bf16": tflops / peak if peak else None,
+                "training_ms": round(cache["cacheTrainMs"], 2), "training_records": cache["cacheRecords"],
+                "training_steps": cache["cacheSteps"],
+                "share_of_render_time": (cache["cacheQueryMs"] + cache["cacheTrainMs"]) / (secs * 1e3)}
         e.close()
     clocks = sampler.stop()
     plain_s, cached_s = arms["plain"]["seconds"], arms["cached"]["seconds"]
@@ -552,9 +581,63 @@ def room_arm(args):
     return 0
 
 
+def cache_arm(args):
+    """The config-4 room in the radiance-cache mode: W untimed steps, then K
+    steps of 4 samples per pixel (one training round each). Reports the
+    device time of the cache's inference (tensor-core query kernel and the
+    application of its predictions) and training, from CUDA events the engine
+    records around them on its stream, and inference against the tensor
+    roofline."""
+    import torch
+
+    import miniraytrace_b200 as mrt
+    from miniraytrace_b200 import build as mrt_build
+    from miniraytrace_b200 import scenes
+
+    if int(os.environ.get("RANK", "0")) != 0:
+        return 0
+    torch.cuda.set_device(0)
+    mrt_build.build()
+    W, H = (int(x) for x in args.resolution.split("x")) if args.resolution else (1920, 1080)
+    s = scenes.room(W, H)
+    e = mrt.Engine(W, H)
+    s.apply(e)
+    e.commit()
+    e.set_radiance_cache(enabled=True)
+    for _ in range(args.warmup):
+        e.render_frames(4)
+    tot = {"lastRenderMs": 0.0, "cacheQueryMs": 0.0, "cacheTrainMs": 0.0, "cacheQueries": 0, "cacheRecords": 0,
+           "cacheSteps": 0}
+    for _ in range(args.steps):
+        e.render_frames(4)
+        st = e.stats()
+        for k in tot:
+            tot[k] += st[k]
+    e.close()
+    peak = measured_bf16_tflops()
+    qps = tot["cacheQueries"] / (tot["cacheQueryMs"] * 1e-3)
+    tflops = qps * CACHE_QUERY_FLOPS / 1e12
+    out = {
+        "metric": "radiance-cache inference throughput (config 4)", "value": qps / 1e9, "unit": "Gqueries/s",
+        "higher_is_better": True, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "dtype": "bf16 operands, f32 accumulation", "data": "synthetic",
+        "config": {"workload": f"config 4 room, {W}x{H}, 4 spp per step, queries at the second vertex"},
+        "roofline": {"bound": "tensor", "achieved": tflops, "peak": peak, "unit": "TFLOP/s", "frac": tflops / peak,
+                     "note": "measured bf16 burst peak; the kernel is bound by its hash-grid gathers"},
+        "inference_ms_per_step": tot["cacheQueryMs"] / args.steps,
+        "queries_per_step": tot["cacheQueries"] / args.steps,
+        "training_ms_per_step": tot["cacheTrainMs"] / args.steps,
+        "training_records_per_step": tot["cacheRecords"] / args.steps,
+        "adam_steps_per_step": tot["cacheSteps"] / args.steps,
+        "render_ms_per_step": tot["lastRenderMs"] / args.steps,
+    }
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def main():
     args = parse_args()
-    if args.impl == "reference" and args.config in ("batch", "room"):
+    if args.impl == "reference" and args.config in ("batch", "room", "cache"):
         print(json.dumps({"impl": "reference", "unavailable": "the batched config-3 mode is timed on the GPU only; "
                           "the reference arm times the terrain and box_sphere workloads"}), flush=True)
         return 0
@@ -564,6 +647,8 @@ def main():
         return batch_arm(args)
     if args.config == "room":
         return room_arm(args)
+    if args.config == "cache":
+        return cache_arm(args)
     return ours_arm(args)
 
 

@@ -86,6 +86,12 @@ typedef struct mrtxStats {
     /* device time of the last render call per wavefront stage (CUDA events) */
     float extendMs, shadeMs, shadowMs, otherMs;
     uint32_t extendLaunches; /* closest-hit (extend) kernel launches of the last render call */
+    /* radiance-cache mode, last render call: device time of the cache's
+     * inference (queries and their application to the paths) and of its
+     * training (targets, steps, Adam), with their counts */
+    float cacheQueryMs, cacheTrainMs;
+    uint64_t cacheQueries, cacheRecords;
+    uint32_t cacheSteps;
 } mrtxStats;
 MRT_API mrtResult mrtxGetStats(mrtEngine*, mrtxStats* out);
 

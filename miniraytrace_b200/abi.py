@@ -130,7 +130,9 @@ class Stats(_Sized):
                 ("triTests", C.c_uint64), ("surfaceHits", C.c_uint64), ("commitH2DBytes", C.c_uint64),
                 ("shadowNodeFetches", C.c_uint64), ("shadowTriTests", C.c_uint64), ("nodeBytes", C.c_uint32),
                 ("triBytes", C.c_uint32), ("extendMs", C.c_float), ("shadeMs", C.c_float), ("shadowMs", C.c_float),
-                ("otherMs", C.c_float), ("extendLaunches", C.c_uint32)]
+                ("otherMs", C.c_float), ("extendLaunches", C.c_uint32), ("cacheQueryMs", C.c_float),
+                ("cacheTrainMs", C.c_float), ("cacheQueries", C.c_uint64), ("cacheRecords", C.c_uint64),
+                ("cacheSteps", C.c_uint32)]
 
 
 LOG_FN = C.CFUNCTYPE(None, C.c_int, C.c_char_p, C.c_void_p)

@@ -69,40 +69,47 @@ struct Corners {
 };
 
 // Encoding of one query into enc[0..63]; corner indices and weights kept
-// for the backward pass when `corners` is given.
-__device__ void encode(const McacheParams& C, const float* f, float* enc, Corners* corners) {
+// for the backward pass when `corners` is given. Levels are visited kGroup at
+// a time (their 8 kGroup gathers can be in flight together).
+template <int kGroup = 1>
+__device__ __forceinline__ void encode(const McacheParams& C, const float* f, float* enc, Corners* corners) {
     float p[3];
     for (int a = 0; a < 3; ++a) {
         const float u = (f[a] - C.lo[a]) * C.invExtent[a];
         p[a] = fminf(fmaxf(u, 0.0f), 1.0f);
     }
-    for (int l = 0; l < kLevels; ++l) {
-        const float s = levelScale(l);
-        const uint32_t res = uint32_t(ceilf(s));
-        float fr[3];
-        uint32_t b[3];
-        for (int a = 0; a < 3; ++a) {
-            const float x = p[a] * s;
-            const float fl = fminf(floorf(x), float(res - 1));
-            b[a] = uint32_t(fl);
-            fr[a] = x - fl;
-        }
-        float e0 = 0.0f, e1 = 0.0f;
-        for (int c = 0; c < 8; ++c) {
-            const uint32_t cx = b[0] + (c & 1), cy = b[1] + ((c >> 1) & 1), cz = b[2] + ((c >> 2) & 1);
-            const float w = ((c & 1) ? fr[0] : 1.0f - fr[0]) * ((c & 2) ? fr[1] : 1.0f - fr[1]) *
-                            ((c & 4) ? fr[2] : 1.0f - fr[2]);
-            const uint32_t i = uint32_t(l) * kTableSize + gridIndex(cx, cy, cz, res);
-            const float2 g = reinterpret_cast<const float2*>(C.grid)[i];
-            e0 += w * g.x;
-            e1 += w * g.y;
-            if (corners) {
-                corners->idx[l][c] = i;
-                corners->w[l][c] = w;
+    for (int l0 = 0; l0 < kLevels; l0 += kGroup) {
+#pragma unroll
+        for (int g = 0; g < kGroup; ++g) {
+            const int l = l0 + g;
+            const float s = levelScale(l);
+            const uint32_t res = uint32_t(ceilf(s));
+            float fr[3];
+            uint32_t b[3];
+            for (int a = 0; a < 3; ++a) {
+                const float x = p[a] * s;
+                const float fl = fminf(floorf(x), float(res - 1));
+                b[a] = uint32_t(fl);
+                fr[a] = x - fl;
             }
+            float e0 = 0.0f, e1 = 0.0f;
+#pragma unroll
+            for (int c = 0; c < 8; ++c) {
+                const uint32_t cx = b[0] + (c & 1), cy = b[1] + ((c >> 1) & 1), cz = b[2] + ((c >> 2) & 1);
+                const float w = ((c & 1) ? fr[0] : 1.0f - fr[0]) * ((c & 2) ? fr[1] : 1.0f - fr[1]) *
+                                ((c & 4) ? fr[2] : 1.0f - fr[2]);
+                const uint32_t i = uint32_t(l) * kTableSize + gridIndex(cx, cy, cz, res);
+                const float2 gv = reinterpret_cast<const float2*>(C.grid)[i];
+                e0 += w * gv.x;
+                e1 += w * gv.y;
+                if (corners) {
+                    corners->idx[l][c] = i;
+                    corners->w[l][c] = w;
+                }
+            }
+            enc[2 * l] = e0;
+            enc[2 * l + 1] = e1;
         }
-        enc[2 * l] = e0;
-        enc[2 * l + 1] = e1;
     }
     float d[3] = {f[3], f[4], f[5]};
     const float dl = rsqrtf(fmaxf(d[0] * d[0] + d[1] * d[1] + d[2] * d[2], 1e-20f));
@@ -189,7 +196,13 @@ constexpr uint32_t kWBytes = kWidth * kWidth * 2;   // one hidden layer, BF16
 constexpr uint32_t kWOutBytes = kOutRows * kWidth * 2;
 constexpr uint32_t kWAllBytes = kLayers * kWBytes + kWOutBytes;
 constexpr uint32_t kABytes = kTile * kWidth * 2;
-constexpr uint32_t kTmemCols = 64;              // the accumulator: 128 lanes x 64 FP32 columns
+constexpr uint32_t kTmemCols = 64;              // one accumulator: 128 lanes x 64 FP32 columns
+// Tiles a query CTA works on at once. One: the kernel is bound by the
+// encoding's hash-grid gathers, and on 2M random queries two groups per CTA
+// (twice the warps in flight) took 1.67 ms against 0.92 ms for one, as did
+// gathering four levels at a time (1.09 ms): more gathers in flight evict
+// each other from L1.
+constexpr uint32_t kQueryGroups = 1;
 constexpr uint32_t kWaitLimit = 1u << 20;       // mbarrier polls before a tile gives up
 constexpr bool kRenderClamp = true;             // rendering takes max(prediction, 0)
 
@@ -279,17 +292,38 @@ __device__ __forceinline__ void storeRow(uint8_t* tile, uint32_t r, const float*
     }
 }
 
-__global__ void __launch_bounds__(kTile) tcQueryKernel(McacheParams C, const float* __restrict__ features,
-                                                       uint32_t n, float* __restrict__ out3, bool clampOut) {
+// AND of `v` over the 128 threads of named barrier `id` (a barrier too).
+__device__ __forceinline__ bool groupAnd(bool v, uint32_t id) {
+    uint32_t out;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\tsetp.ne.u32 q, %1, 0;\n\tbar.red.and.pred p, %2, 128, q;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(out)
+        : "r"(uint32_t(v)), "r"(id)
+        : "memory");
+    return out != 0;
+}
+
+__device__ __forceinline__ void groupSync(uint32_t id) { asm volatile("bar.sync %0, 128;" ::"r"(id) : "memory"); }
+
+// kGroups independent groups of 128 threads share the CTA's weights; group h
+// owns activation tile h, mbarrier h, named barrier 1 + h and tensor-memory
+// columns [64 h, 64 h + 64), and walks tiles blockIdx.x * kGroups + h,
+// stepping by gridDim.x * kGroups. (Warp w of the CTA reaches tensor-memory
+// lanes 32 (w % 4) .. 32 (w % 4) + 31, so every group covers all 128 lanes.)
+__global__ void __launch_bounds__(kTile* kQueryGroups, 3) tcQueryKernel(McacheParams C, const float* __restrict__ features,
+                                                                     uint32_t n, float* __restrict__ out3,
+                                                                     bool clampOut) {
     extern __shared__ __align__(1024) uint8_t smem[];
-    uint8_t* sW = smem;                 // W0..W4 (8 KiB each), W5 (2 KiB)
-    uint8_t* sA = smem + kWAllBytes;    // activation tile
-    uint64_t* bar = reinterpret_cast<uint64_t*>(sA + kABytes);
-    uint32_t* tmemSlot = reinterpret_cast<uint32_t*>(bar + 1);
+    uint8_t* sW = smem;  // W0..W4 (8 KiB each), W5 (2 KiB)
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kWAllBytes + kQueryGroups * kABytes);
+    uint32_t* tmemSlot = reinterpret_cast<uint32_t*>(bars + kQueryGroups);
     const uint32_t t = threadIdx.x, warp = t >> 5;
+    const uint32_t h = t / kTile, r = t % kTile;  // group, row of its tile
+    uint8_t* sA = smem + kWAllBytes + h * kABytes;
 
     // weights, FP32 row-major in global memory, to BF16 operand tiles
-    for (uint32_t i = t; i < uint32_t(kLayers * kWidth * kWidth + kOutRows * kWidth) / 2; i += kTile) {
+    for (uint32_t i = t; i < uint32_t(kLayers * kWidth * kWidth + kOutRows * kWidth) / 2; i += blockDim.x) {
         const uint32_t e = 2 * i, layer = e / (kWidth * kWidth), rem = e % (kWidth * kWidth);
         const uint32_t j = rem / kWidth, k = rem % kWidth;
         const float2 w = reinterpret_cast<const float2*>(C.mlp)[i];
@@ -297,25 +331,27 @@ __global__ void __launch_bounds__(kTile) tcQueryKernel(McacheParams C, const flo
     }
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smemAddr(tmemSlot)),
-                     "r"(kTmemCols)
+                     "r"(kTmemCols * kQueryGroups)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
-    if (t == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smemAddr(bar)) : "memory");
+    if (r == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smemAddr(bars + h)) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     fenceAsyncShared();
     tcFenceBefore();
     __syncthreads();
     tcFenceAfter();
-    const uint32_t tmem = *tmemSlot;
-    const uint32_t barAddr = smemAddr(bar), aAddr = smemAddr(sA), wAddr = smemAddr(sW);
-    const uint32_t laneBase = tmem + ((warp * 32u) << 16);  // this warp's 32 lanes
+    const uint32_t tmem = *tmemSlot + kTmemCols * h;                 // this group's columns
+    const uint32_t barAddr = smemAddr(bars + h), aAddr = smemAddr(sA), wAddr = smemAddr(sW);
+    const uint32_t laneBase = tmem + (((warp % 4u) * 32u) << 16);     // this warp's 32 lanes
+    const uint32_t barId = 1u + h;
     uint32_t parity = 0;
     bool ok = true;
-    for (uint32_t tile = blockIdx.x; ok && size_t(tile) * kTile < n; tile += gridDim.x) {
-        const uint32_t q = tile * kTile + t;
+    for (uint32_t tile = blockIdx.x * kQueryGroups + h; ok && size_t(tile) * kTile < n;
+         tile += gridDim.x * kQueryGroups) {
+        const uint32_t q = tile * kTile + r;
         const bool valid = q < n;
         float f[16];
 #pragma unroll
@@ -328,14 +364,14 @@ __global__ void __launch_bounds__(kTile) tcQueryKernel(McacheParams C, const flo
             f[4 * k + 3] = v.w;
         }
         float v[kWidth];
-        encode(C, f, v, nullptr);
-        storeRow(sA, t, v, false);
+        encode<1>(C, f, v, nullptr);
+        storeRow(sA, r, v, false);
         fenceAsyncShared();
         tcFenceBefore();
-        __syncthreads();
+        groupSync(barId);
         for (int l = 0; l <= kLayers; ++l) {
             const uint32_t rows = l < kLayers ? kWidth : kOutRows;
-            if (t == 0) {
+            if (r == 0) {
                 tcFenceAfter();
                 const uint32_t idesc = instrDesc(kTile, rows);
 #pragma unroll
@@ -346,7 +382,7 @@ __global__ void __launch_bounds__(kTile) tcQueryKernel(McacheParams C, const flo
             }
             const bool done = waitParity(barAddr, parity);
             parity ^= 1u;
-            if (!__syncthreads_and(done)) {
+            if (!groupAnd(done, barId)) {
                 ok = false;
                 break;
             }
@@ -355,10 +391,10 @@ __global__ void __launch_bounds__(kTile) tcQueryKernel(McacheParams C, const flo
 #pragma unroll
                 for (int c = 0; c < kWidth / 16; ++c) tmemLoad16(laneBase + 16u * c, v + 16 * c);
                 tmemWaitLoad();
-                storeRow(sA, t, v, true);
+                storeRow(sA, r, v, true);
                 fenceAsyncShared();
                 tcFenceBefore();
-                __syncthreads();
+                groupSync(barId);
             } else {
                 tmemLoad16(laneBase, v);
                 tmemWaitLoad();
@@ -372,8 +408,10 @@ __global__ void __launch_bounds__(kTile) tcQueryKernel(McacheParams C, const flo
     __syncthreads();
     tcFenceAfter();
     if (warp == 0)
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
-    if (!ok && t == 0) atomicOr(C.status, 1u);
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(*tmemSlot),
+                     "r"(kTmemCols * kQueryGroups)
+                     : "memory");
+    if (!ok && r == 0) atomicOr(C.status, 1u);
 }
 
 // One training step's forward + backward for 64 samples per block: loss =
@@ -584,7 +622,7 @@ __global__ void recordTargetsKernel(const float4* __restrict__ prefix, const flo
     }
 }
 
-size_t smemQuery() { return kWAllBytes + kABytes + 16; }
+size_t smemQuery() { return kWAllBytes + kQueryGroups * kABytes + 8 * kQueryGroups + 16; }
 size_t smemTrain() { return sizeof(float) * (kWidth * kWidth + (kLayers + 1 + 2) * kBlock * kAct); }
 
 unsigned gridFor(size_t n) {
@@ -617,14 +655,16 @@ static cudaError_t launchQuery(const McacheParams& C, const float* features, uin
     if (n == 0) return cudaSuccess;
     cudaError_t e = cudaFuncSetAttribute(tcQueryKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smemQuery()));
     if (e != cudaSuccess) return e;
-    // Persistent CTAs: at most 3 fit an SM by shared memory (59 KiB each), so
-    // their tensor memory (64 columns each) never exceeds the SM's 512.
+    // Persistent CTAs: at most 3 fit an SM by shared memory (58 KiB each with
+    // one group, 74 KiB with two), so their tensor memory (64 columns a
+    // group) never exceeds the SM's 512.
     int sms = 148;
     int dev = 0;
     if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const uint32_t tiles = (n + kTile - 1) / kTile;
-    const uint32_t ctas = tiles < uint32_t(sms) * 3u ? tiles : uint32_t(sms) * 3u;
-    tcQueryKernel<<<ctas, kTile, smemQuery(), stream>>>(C, features, n, out3, clampOut);
+    const uint32_t groups = (n + kTile - 1) / kTile;
+    const uint32_t want = (groups + kQueryGroups - 1) / kQueryGroups;
+    const uint32_t ctas = want < uint32_t(sms) * 3u ? want : uint32_t(sms) * 3u;
+    tcQueryKernel<<<ctas, kTile * kQueryGroups, smemQuery(), stream>>>(C, features, n, out3, clampOut);
     return cudaGetLastError();
 }
 

@@ -250,6 +250,8 @@ Engine::~Engine() {
         if (ev) cudaEventDestroy(ev);
     for (auto& ev : m_stageEvents)
         if (ev) cudaEventDestroy(ev);
+    for (auto& ev : m_cacheEvents)
+        if (ev) cudaEventDestroy(ev);
     if (m_ev0) cudaEventDestroy(m_ev0);
     if (m_ev1) cudaEventDestroy(m_ev1);
     if (m_stream) cudaStreamDestroy(m_stream);
@@ -936,6 +938,13 @@ mrtResult Engine::launchPending() {
         MRT_CUDA(cudaEventCreate(&ev));
         m_stageEvents.push_back(ev);
     }
+    while (m_cache.enabled && m_cacheEvents.size() < size_t(3) * waves) {
+        cudaEvent_t ev;
+        MRT_CUDA(cudaEventCreate(&ev));
+        m_cacheEvents.push_back(ev);
+    }
+    m_cacheQueries = m_cacheRecords = 0;
+    m_cacheSteps = 0;
     MRT_CUDA(cudaEventRecord(m_ev0, m_stream));
     uint32_t wave = 0;
     for (uint32_t done = 0; done < n; ++wave) {
@@ -945,7 +954,7 @@ mrtResult Engine::launchPending() {
                                           m_stageEvents.data() + wave * perWave,
                                           m_cache.enabled ? &m_cache.args : nullptr, m_stream);
         if (le != cudaSuccess) return guard(fromCuda(le, "path tracing launch"));
-        if (m_cache.enabled) MRT_TRY(guard(cacheWave(p, m_frameIndex + done, k)));
+        if (m_cache.enabled) MRT_TRY(guard(cacheWave(p, m_frameIndex + done, k, m_cacheEvents.data() + 3 * wave)));
         done += k;
     }
     MRT_CUDA(cudaEventRecord(m_ev1, m_stream));
@@ -953,6 +962,7 @@ mrtResult Engine::launchPending() {
     m_inFlightWaves = waves;
     m_inFlightBounces = p.maxBounces + 1;
     m_inFlightLaunches = launches;
+    m_inFlightCache = m_cache.enabled;
     return MRT_SUCCESS;
 }
 
@@ -985,6 +995,19 @@ mrtResult Engine::completePending() {
     m_stats.lastRenderSpp = n;
     m_stats.kernelLaunches = m_inFlightLaunches;
     m_stats.extendLaunches = waves * bounces;
+    m_stats.cacheQueryMs = m_stats.cacheTrainMs = 0.0f;
+    if (m_inFlightCache)
+        for (uint32_t w = 0; w < waves; ++w) {
+            const cudaEvent_t* ev = m_cacheEvents.data() + 3 * w;
+            float q = 0.0f, t = 0.0f;
+            MRT_CUDA(cudaEventElapsedTime(&q, ev[0], ev[1]));
+            MRT_CUDA(cudaEventElapsedTime(&t, ev[1], ev[2]));
+            m_stats.cacheQueryMs += q;
+            m_stats.cacheTrainMs += t;
+        }
+    m_stats.cacheQueries = m_inFlightCache ? m_cacheQueries : 0;
+    m_stats.cacheRecords = m_inFlightCache ? m_cacheRecords : 0;
+    m_stats.cacheSteps = m_inFlightCache ? m_cacheSteps : 0;
     MRT_TRY(guard(checkErrorFlags()));
     unsigned long long ctr[7];
     MRT_CUDA(cudaMemcpy(ctr, m_rayCounters.ptr, sizeof(ctr), cudaMemcpyDeviceToHost));
@@ -1417,7 +1440,7 @@ mrtResult Engine::cacheWaveBuffers(uint32_t samples, uint32_t maxBounces) {
 // After a cache-mode wave's bounces: the cache's predictions join the
 // stopped paths, the training paths' vertices become training samples, the
 // cache trains on them, and the wave is accumulated.
-mrtResult Engine::cacheWave(const MrtFrameParams& p, uint32_t sampleBase, uint32_t samples) {
+mrtResult Engine::cacheWave(const MrtFrameParams& p, uint32_t sampleBase, uint32_t samples, const cudaEvent_t* ev) {
     uint32_t counts[2] = {0, 0}, status = 0;
     MRT_CUDA(cudaMemcpyAsync(counts, m_cache.counts.ptr, sizeof(counts), cudaMemcpyDeviceToHost, m_stream));
     MRT_CUDA(cudaMemcpyAsync(&status, m_cache.params.status, sizeof(status), cudaMemcpyDeviceToHost, m_stream));
@@ -1426,8 +1449,10 @@ mrtResult Engine::cacheWave(const MrtFrameParams& p, uint32_t sampleBase, uint32
     const MrtCacheArgs& K = m_cache.args;
     const uint32_t nq = std::min(counts[0], K.qCap), nr = std::min(counts[1], K.rCap);
     const uint32_t slots = p.width * p.height * samples;
+    MRT_CUDA(cudaEventRecord(ev[0], m_stream));
     MRT_CUDA(mrtcu_rc_apply_queries(m_cache.params, K.qFeat, K.qBeta, nq, slots, m_cache.scratch.as<float>(),
                                     m_waveState.L, m_stream));
+    MRT_CUDA(cudaEventRecord(ev[1], m_stream));
     MRT_CUDA(mrtcu_rc_record_targets(K.rPrefix, K.rBeta, nr, slots, m_waveState.L, m_cache.rTarget.as<float>(),
                                      m_stream));
     // Batches of up to 16,384 records, smaller when the wave has fewer than
@@ -1437,6 +1462,10 @@ mrtResult Engine::cacheWave(const MrtFrameParams& p, uint32_t sampleBase, uint32
     const uint32_t batch = std::max(64u, std::min(16384u, nr / std::max(1u, steps)));
     MRT_CUDA(mrtcu_rc_train(&m_cache.params, K.rFeat, m_cache.rTarget.as<float>(), nr, steps, batch, nullptr,
                             m_stream));
+    MRT_CUDA(cudaEventRecord(ev[2], m_stream));
+    m_cacheQueries += nq;
+    m_cacheRecords += nr;
+    m_cacheSteps += nr ? steps : 0;
     MRT_CUDA(mrtcu_wave_finalize(&p, &m_waveState, sampleBase, samples, m_stream));
     return MRT_SUCCESS;
 }

@@ -104,6 +104,9 @@ private:
     cudaEvent_t m_ev0 = nullptr, m_ev1 = nullptr;
     std::vector<cudaEvent_t> m_copyEvents;
     std::vector<cudaEvent_t> m_stageEvents;  // 6 per bounce per wave of one render call
+    std::vector<cudaEvent_t> m_cacheEvents;  // cache mode: 3 per wave (inference, training)
+    uint64_t m_cacheQueries = 0, m_cacheRecords = 0;  // of the render call in flight
+    uint32_t m_cacheSteps = 0;
     bool m_lost = false;
     bool m_validation = false;
     unsigned m_hostThreads = 1;
@@ -140,7 +143,7 @@ private:
     void cacheBounds();
     mrtResult cacheWaveBuffers(uint32_t samples, uint32_t maxBounces);
     mrtResult cacheStatus(uint32_t status);
-    mrtResult cacheWave(const MrtFrameParams& p, uint32_t sampleBase, uint32_t samples);
+    mrtResult cacheWave(const MrtFrameParams& p, uint32_t sampleBase, uint32_t samples, const cudaEvent_t* ev);
     MrtWaveState m_waveState{};
     uint32_t m_waveSamples = 0;  // samples per pixel one wave holds
     uint64_t m_maxWaveSlots = uint64_t(1) << 25;  // paths per wave, set from the GPU's memory
@@ -177,6 +180,7 @@ private:
     uint32_t m_pending = 0;     // samples queued by mrtRenderFrame, not yet rendered
     uint32_t m_inFlight = 0;    // samples issued by launchPending, not yet completed
     uint32_t m_inFlightWaves = 0, m_inFlightBounces = 0, m_inFlightLaunches = 0;
+    bool m_inFlightCache = false;  // the render call in flight uses the radiance cache
     MrtFrameParams m_pendingParams{};
     uint32_t m_streamOffset = 0, m_streamStride = 1;
     float m_resolveExposure = 1.0f;
