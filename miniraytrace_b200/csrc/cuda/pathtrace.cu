@@ -571,10 +571,15 @@ extern "C" cudaError_t mrtcu_wave(const MrtFrameParams* p, const MrtWaveState* s
     const uint32_t pixels = p->width * p->height;
     if (pixels == 0 || samples == 0) return cudaSuccess;
     if (uint64_t(pixels) * samples > s->capacity) return cudaErrorInvalidValue;
-    static int gExtend = 0, gShade = 0, gShadow = 0;
+    // Grids of exactly the resident blocks of each kernel (the cache-mode
+    // shade kernel uses more registers, so fewer of its blocks fit an SM; a
+    // grid sized for the other variant would leave a second, serial wave of
+    // blocks).
+    static int gExtend = 0, gShade = 0, gShadeCache = 0, gShadow = 0;
     if (gExtend == 0) {
         gExtend = persistentBlocks(reinterpret_cast<const void*>(waveExtendKernel), MRT_TRAV_THREADS);
         gShade = persistentBlocks(reinterpret_cast<const void*>(waveShadeKernel<false>), 128);
+        gShadeCache = persistentBlocks(reinterpret_cast<const void*>(waveShadeKernel<true>), 128);
         gShadow = persistentBlocks(reinterpret_cast<const void*>(waveShadowKernel), MRT_TRAV_THREADS);
     }
     WaveArgs A{pixels, pixels * samples, sampleBase, samples};
@@ -587,7 +592,7 @@ extern "C" cudaError_t mrtcu_wave(const MrtFrameParams* p, const MrtWaveState* s
         if (ev) cudaEventRecord(ev[0], stream);
         waveExtendKernel<<<gExtend, MRT_TRAV_THREADS, 0, stream>>>(*p, *s, cur);
         if (ev) cudaEventRecord(ev[1], stream);
-        if (cache) waveShadeKernel<true><<<gShade, 128, 0, stream>>>(*p, *s, A, cur, *cache);
+        if (cache) waveShadeKernel<true><<<gShadeCache, 128, 0, stream>>>(*p, *s, A, cur, *cache);
         else waveShadeKernel<false><<<gShade, 128, 0, stream>>>(*p, *s, A, cur, MrtCacheArgs{});
         if (ev) cudaEventRecord(ev[2], stream);
         waveShadowKernel<<<gShadow, MRT_TRAV_THREADS, 0, stream>>>(*p, *s);
