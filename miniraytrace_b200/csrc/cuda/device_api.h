@@ -15,7 +15,7 @@
 typedef struct McacheParams {
     float *grid, *mlp, *gGrid, *gMlp, *mGrid, *vGrid, *mMlp, *vMlp;
     float* partial;          // per-block weight gradients of one step
-    uint32_t partialBlocks;  // blocks (of 64 samples) `partial` holds
+    uint32_t partialBlocks;  // training CTAs' partial gradients `partial` holds
     float lo[3], invExtent[3];
     uint32_t step;
     float lr;
@@ -104,6 +104,7 @@ cudaError_t mrtcu_fill_f4(float4* dst, size_t n, float4 value, cudaStream_t stre
 // (position, outgoing direction, normal, roughness, albedo, unused).
 size_t mrtcu_rc_grid_floats(void);
 size_t mrtcu_rc_mlp_floats(void);
+uint32_t mrtcu_rc_partial_blocks(uint32_t maxBatch);
 size_t mrtcu_rc_partial_floats(uint32_t maxBatch);
 cudaError_t mrtcu_rc_init(McacheParams C, uint32_t seed, cudaStream_t stream);
 cudaError_t mrtcu_rc_query(McacheParams C, const float* features, uint32_t n, float* out3, cudaStream_t stream);

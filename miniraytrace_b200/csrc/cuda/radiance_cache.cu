@@ -29,7 +29,6 @@ constexpr uint32_t kTableSize = 1u << 19;
 constexpr int kWidth = 64;
 constexpr int kLayers = 5;        // hidden layers
 constexpr int kOutRows = 16;
-constexpr int kBlock = 64;        // queries per block = threads per block
 // Grid scale of level l: 16 * 2^(7 l / 15), 16 -> 2048 in 16 geometric
 // steps, as float literals so any other implementation can use the same values.
 __constant__ float kLevelScale[kLevels] = {16.0f, 22.110605239868164f, 30.554931640625f, 42.2242546081543f, 58.35023880004883f, 80.63494873046875f, 111.43047332763672f, 153.98719787597656f, 212.79690551757812f, 294.0667724609375f, 406.3746643066406f, 561.5744018554688f, 776.046875f, 1072.42919921875f, 1482.003662109375f, 2048.0f};
@@ -125,51 +124,7 @@ __device__ __forceinline__ void encode(const McacheParams& C, const float* f, fl
     for (int k = 56; k < kWidth; ++k) enc[k] = 0.0f;
 }
 
-constexpr int kAct = 68;  // activation row stride in shared memory (float4 aligned, conflict-free)
 constexpr int kMlpFloats = (kLayers + 1) * kWidth * kWidth;
-
-// Weight matrix `layer` (rows x 64, row-major) into shared memory (stride 64).
-__device__ void loadWeights(const float* __restrict__ mlp, int layer, int rows, float* sW) {
-    const float4* W = reinterpret_cast<const float4*>(mlp + size_t(layer) * kWidth * kWidth);
-    float4* d = reinterpret_cast<float4*>(sW);
-    for (int i = threadIdx.x; i < rows * kWidth / 4; i += blockDim.x) d[i] = W[i];
-}
-
-// A 64-float row of shared memory into registers.
-__device__ __forceinline__ void loadRow(const float* row, float (&x)[kWidth]) {
-#pragma unroll
-    for (int m = 0; m < kWidth / 4; ++m) {
-        const float4 v = reinterpret_cast<const float4*>(row)[m];
-        x[4 * m] = v.x;
-        x[4 * m + 1] = v.y;
-        x[4 * m + 2] = v.z;
-        x[4 * m + 3] = v.w;
-    }
-}
-
-// out[j] = sum_k W[j][k] x[k] for j < rows (ReLU when `relu`): x in
-// registers, each weight row read as 16 broadcast 128-bit loads.
-__device__ __forceinline__ void denseForward(const float* sW, const float (&x)[kWidth], float* out, int rows,
-                                             bool relu) {
-    for (int j = 0; j < rows; ++j) {
-        const float4* w = reinterpret_cast<const float4*>(sW + j * kWidth);
-        float acc0 = 0.0f, acc1 = 0.0f;
-#pragma unroll
-        for (int m = 0; m < kWidth / 4; m += 2) {
-            const float4 v = w[m], u = w[m + 1];
-            acc0 = fmaf(v.x, x[4 * m], acc0);
-            acc1 = fmaf(v.y, x[4 * m + 1], acc1);
-            acc0 = fmaf(v.z, x[4 * m + 2], acc0);
-            acc1 = fmaf(v.w, x[4 * m + 3], acc1);
-            acc0 = fmaf(u.x, x[4 * m + 4], acc0);
-            acc1 = fmaf(u.y, x[4 * m + 5], acc1);
-            acc0 = fmaf(u.z, x[4 * m + 6], acc0);
-            acc1 = fmaf(u.w, x[4 * m + 7], acc1);
-        }
-        const float acc = acc0 + acc1;
-        out[j] = relu ? fmaxf(acc, 0.0f) : acc;
-    }
-}
 
 // ---------------------------------------------------------------- inference --
 // Inference on the tensor cores (tcgen05, kind::f16, BF16 operands, FP32
@@ -214,18 +169,32 @@ __device__ __forceinline__ uint32_t smemAddr(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
 
-// Shared-memory matrix descriptor: start address, leading and stride byte
-// offsets (all >> 4), descriptor version 1 (bits 46-47), no swizzle.
-__device__ __forceinline__ uint64_t smemDesc(uint32_t addr) {
-    return uint64_t((addr & 0x3FFFFu) >> 4) | (uint64_t(128u >> 4) << 16) | (uint64_t(1024u >> 4) << 32) |
+// Shared-memory matrix descriptor: start address, leading byte offset (the
+// stride between core matrices along K), stride byte offset (between core
+// matrices along M or N), all >> 4; descriptor version 1 (bits 46-47); no
+// swizzle.
+__device__ __forceinline__ uint64_t smemDesc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+    return uint64_t((addr & 0x3FFFFu) >> 4) | (uint64_t(lbo >> 4) << 16) | (uint64_t(sbo >> 4) << 32) |
            (uint64_t(1) << 46);
 }
 
+// An operand tile of the layout above read K-major: K runs along a row (the
+// activations of a record, the inputs of a weight row).
+__device__ __forceinline__ uint64_t descK(uint32_t addr) { return smemDesc(addr, 128u, 1024u); }
+
+// The same tile read MN-major, i.e. transposed: its rows become the K
+// dimension. Element (row r, column c) sits at (r / 8) * 1024 + (r % 8) * 16
+// + (c / 8) * 128 + (c % 8) * 2, which is the MN-major canonical layout with
+// M/N index c (8-element core-matrix rows, blocks 128 bytes apart) and K
+// index r (blocks of 8 rows 1024 bytes apart).
+__device__ __forceinline__ uint64_t descMN(uint32_t addr) { return smemDesc(addr, 1024u, 128u); }
+
 // Instruction descriptor of kind::f16: FP32 accumulator (bits 4-5 = 1),
-// A and B BF16 (bits 7-9, 10-12 = 1), both K-major, N >> 3 at bit 17,
-// M >> 4 at bit 24.
-__host__ __device__ constexpr uint32_t instrDesc(uint32_t m, uint32_t n) {
-    return (1u << 4) | (1u << 7) | (1u << 10) | ((n >> 3) << 17) | ((m >> 4) << 24);
+// A and B BF16 (bits 7-9, 10-12 = 1), A and B major-ness (bits 15, 16: 0 K,
+// 1 MN), N >> 3 at bit 17, M >> 4 at bit 24.
+__host__ __device__ constexpr uint32_t instrDesc(uint32_t m, uint32_t n, bool aMN = false, bool bMN = false) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | (uint32_t(aMN) << 15) | (uint32_t(bMN) << 16) | ((n >> 3) << 17) |
+           ((m >> 4) << 24);
 }
 
 __device__ __forceinline__ void fenceAsyncShared() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
@@ -292,6 +261,31 @@ __device__ __forceinline__ void storeRow(uint8_t* tile, uint32_t r, const float*
     }
 }
 
+// The weights, FP32 row-major in global memory, as BF16 operand tiles:
+// W0..W4 (64 x 64, 8 KiB each), then W5 (16 x 64, 2 KiB).
+__device__ void loadWeightTiles(const float* __restrict__ mlp, uint8_t* sW) {
+    for (uint32_t i = threadIdx.x; i < uint32_t(kLayers * kWidth * kWidth + kOutRows * kWidth) / 2; i += blockDim.x) {
+        const uint32_t e = 2 * i, layer = e / (kWidth * kWidth), rem = e % (kWidth * kWidth);
+        const uint32_t j = rem / kWidth, k = rem % kWidth;
+        const float2 w = reinterpret_cast<const float2*>(mlp)[i];
+        *reinterpret_cast<uint32_t*>(sW + layer * kWBytes + coreOffset(j, k)) = packBf16(w.x, w.y);
+    }
+}
+
+// Row r of an operand tile as 64 floats.
+__device__ __forceinline__ void loadRowBf16(const uint8_t* tile, uint32_t r, float* v) {
+#pragma unroll
+    for (int c = 0; c < kWidth / 8; ++c) {
+        const uint4 w = *reinterpret_cast<const uint4*>(tile + coreOffset(r, 8 * c));
+        const uint32_t u[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            v[8 * c + 2 * i] = __uint_as_float(u[i] << 16);
+            v[8 * c + 2 * i + 1] = __uint_as_float(u[i] & 0xFFFF0000u);
+        }
+    }
+}
+
 // AND of `v` over the 128 threads of named barrier `id` (a barrier too).
 __device__ __forceinline__ bool groupAnd(bool v, uint32_t id) {
     uint32_t out;
@@ -322,13 +316,7 @@ __global__ void __launch_bounds__(kTile* kQueryGroups, 3) tcQueryKernel(McachePa
     const uint32_t h = t / kTile, r = t % kTile;  // group, row of its tile
     uint8_t* sA = smem + kWAllBytes + h * kABytes;
 
-    // weights, FP32 row-major in global memory, to BF16 operand tiles
-    for (uint32_t i = t; i < uint32_t(kLayers * kWidth * kWidth + kOutRows * kWidth) / 2; i += blockDim.x) {
-        const uint32_t e = 2 * i, layer = e / (kWidth * kWidth), rem = e % (kWidth * kWidth);
-        const uint32_t j = rem / kWidth, k = rem % kWidth;
-        const float2 w = reinterpret_cast<const float2*>(C.mlp)[i];
-        *reinterpret_cast<uint32_t*>(sW + layer * kWBytes + coreOffset(j, k)) = packBf16(w.x, w.y);
-    }
+    loadWeightTiles(C.mlp, sW);
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smemAddr(tmemSlot)),
                      "r"(kTmemCols * kQueryGroups)
@@ -376,8 +364,7 @@ __global__ void __launch_bounds__(kTile* kQueryGroups, 3) tcQueryKernel(McachePa
                 const uint32_t idesc = instrDesc(kTile, rows);
 #pragma unroll
                 for (uint32_t s = 0; s < kWidth / 16; ++s)
-                    tcMma(tmem, smemDesc(aAddr + 256u * s), smemDesc(wAddr + uint32_t(l) * kWBytes + 256u * s), idesc,
-                          s > 0);
+                    tcMma(tmem, descK(aAddr + 256u * s), descK(wAddr + uint32_t(l) * kWBytes + 256u * s), idesc, s > 0);
                 tcCommit(barAddr);
             }
             const bool done = waitParity(barAddr, parity);
@@ -414,125 +401,205 @@ __global__ void __launch_bounds__(kTile* kQueryGroups, 3) tcQueryKernel(McachePa
     if (!ok && r == 0) atomicOr(C.status, 1u);
 }
 
-// One training step's forward + backward for 64 samples per block: loss =
-// mean over samples and channels of (y - t)^2 / (y^2 + 0.01), y held fixed in
-// the denominator. Each block writes its weight gradients (summed over its
-// samples, 8 x 8 register tiles per thread) to partial[block]; the grid
-// gradients are scattered to the 8 corners of each level.
-__global__ void __launch_bounds__(kBlock) trainKernel(McacheParams C, const float* __restrict__ features,
-                                                      const float* __restrict__ targets, uint32_t n, uint32_t first,
-                                                      uint32_t every, float invBatch, float* __restrict__ partial,
-                                                      float* __restrict__ lossOut) {
-    extern __shared__ float4 smem4[];
-    float* sW = reinterpret_cast<float*>(smem4);       // kWidth x kWidth
-    float* act = sW + kWidth * kWidth;                 // (kLayers + 1) x kBlock x kAct: enc, h1..h5
-    float* dA = act + (kLayers + 1) * kBlock * kAct;   // kBlock x kAct: gradient of the layer's output
-    float* dB = dA + kBlock * kAct;
-    const int t = threadIdx.x;
-    const uint32_t j = blockIdx.x * kBlock + t;  // the step's j-th sample is record first + j * every
-    const bool valid = j < n;
-    const size_t s = size_t(first) + size_t(j) * every;
-    float f[16];
-    for (int k = 0; k < 16; ++k) f[k] = valid ? features[s * 16 + k] : 0.0f;
-    Corners corners;
-    encode(C, f, act + t * kAct, &corners);
-    float x[kWidth];
-    for (int l = 0; l <= kLayers; ++l) {
-        __syncthreads();
-        loadWeights(C.mlp, l, l < kLayers ? kWidth : kOutRows, sW);
-        __syncthreads();
-        loadRow(act + (l * kBlock + t) * kAct, x);
-        float* out = l < kLayers ? act + ((l + 1) * kBlock + t) * kAct : dA + t * kAct;
-        denseForward(sW, x, out, l < kLayers ? kWidth : 3, l < kLayers);
+// ----------------------------------------------------------------- training --
+// One training step on the tensor cores. A CTA of 128 threads takes tiles of
+// 128 records (the step's j-th record is record first + j * every): thread r
+// encodes record r into row r of A0 and the forward pass keeps every layer's
+// input A0..A5 (BF16 tiles); the loss gradient of the mean relative L2 loss
+// (y - t)^2 / (y^2 + 0.01) over records and channels (y held fixed in the
+// denominator) becomes dZ5, and per layer l = 5..0 one thread issues
+//   dW_l (64 x 64, rows beyond the layer's outputs zero) = dZ_l^T A_l:
+//       M = 128 (rows 64..127 are unused), N = 64, K = 128 records, A = the
+//       dZ tile read MN-major, B = the A_l tile read MN-major;
+//   dA_l (128 x 64) = dZ_l W_l: M = 128, N = 64, K = the layer's outputs,
+//       A = the dZ tile K-major, B = the W_l tile read MN-major;
+// then every thread reads its dA row, masks it with the ReLU of A_l into
+// dZ_{l-1} (BF16) or, for l = 0, scatters the encoding gradient into the
+// hash-grid gradient at the 8 corners of each level. Threads 0..63 read dW_l
+// rows from tensor memory into this CTA's partial weight gradient (FP32).
+// Operands are BF16 with FP32 accumulation, as in inference.
+constexpr uint32_t kDzSlack = 2048;  // read by the dW MMA's unused rows 64..127, kept zero
+
+size_t smemTrain() { return kWAllBytes + (kLayers + 1) * kABytes + kABytes + kDzSlack + 16; }
+
+__global__ void __launch_bounds__(kTile, 1) tcTrainKernel(McacheParams C, const float* __restrict__ features,
+                                                          const float* __restrict__ targets, uint32_t n,
+                                                          uint32_t first, uint32_t every, float invBatch,
+                                                          float* __restrict__ partial, float* __restrict__ lossOut) {
+    extern __shared__ __align__(1024) uint8_t smem[];
+    uint8_t* sW = smem;                                  // W0..W5
+    uint8_t* sAct = smem + kWAllBytes;                   // A0 (encoding) .. A5, kABytes each
+    uint8_t* sDz = sAct + (kLayers + 1) * kABytes;       // dZ tile, then kDzSlack zero bytes
+    uint64_t* bar = reinterpret_cast<uint64_t*>(sDz + kABytes + kDzSlack);
+    uint32_t* tmemSlot = reinterpret_cast<uint32_t*>(bar + 1);
+    const uint32_t t = threadIdx.x, warp = t >> 5;
+
+    loadWeightTiles(C.mlp, sW);
+    for (uint32_t i = t; i < kDzSlack / 16; i += kTile)
+        reinterpret_cast<uint4*>(sDz + kABytes)[i] = make_uint4(0u, 0u, 0u, 0u);
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smemAddr(tmemSlot)),
+                     "r"(2u * kTmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
-    // output gradient (3 channels; zero for padding samples and channels)
-    float loss = 0.0f;
-    for (int c = 0; c < kWidth; ++c) {
-        float g = 0.0f;
-        if (c < 3 && valid) {
-            const float y = dA[t * kAct + c], tg = targets[s * 3 + c];
-            const float den = y * y + 0.01f;
-            loss += (y - tg) * (y - tg) / den;
-            g = 2.0f * (y - tg) / den * invBatch;
-        }
-        dA[t * kAct + c] = g;
+    if (t == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smemAddr(bar)) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    if (lossOut && valid) atomicAdd(lossOut, loss * invBatch);
+    fenceAsyncShared();
+    tcFenceBefore();
+    __syncthreads();
+    tcFenceAfter();
+    const uint32_t tmem = *tmemSlot;
+    const uint32_t accA = tmem, accW = tmem + kTmemCols;   // forward / input gradient, weight gradient
+    const uint32_t lane = (warp * 32u) << 16;             // this warp's 32 tensor-memory lanes
+    const uint32_t barAddr = smemAddr(bar), wAddr = smemAddr(sW), actAddr = smemAddr(sAct), dzAddr = smemAddr(sDz);
     float* myPartial = partial + size_t(blockIdx.x) * kMlpFloats;
-    const int jt = t / 8, kt = t % 8;  // this thread's 8 x 8 tile of a weight gradient
-    for (int l = kLayers; l >= 0; --l) {
-        const int rows = l < kLayers ? kWidth : 3;
+    uint32_t parity = 0;
+    bool ok = true, firstTile = true;
+    const uint32_t tiles = (n + kTile - 1) / kTile;
+    for (uint32_t tile = blockIdx.x; ok && tile < tiles; tile += gridDim.x) {
+        const uint32_t j = tile * kTile + t;
+        const bool valid = j < n;
+        const size_t rec = size_t(first) + size_t(j) * every;
+        float f[16];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const float4 v = valid ? reinterpret_cast<const float4*>(features)[rec * 4 + k]
+                                   : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            f[4 * k] = v.x;
+            f[4 * k + 1] = v.y;
+            f[4 * k + 2] = v.z;
+            f[4 * k + 3] = v.w;
+        }
+        Corners corners;
+        float v[kWidth];
+        encode(C, f, v, &corners);
+        storeRow(sAct, t, v, false);
+        fenceAsyncShared();
+        tcFenceBefore();
         __syncthreads();
-        loadWeights(C.mlp, l, l < kLayers ? kWidth : kOutRows, sW);
-        __syncthreads();
-        const float* in = act + l * kBlock * kAct;
-        // weight gradient tile: g[j][k] = sum_r dA[r][j] in[r][k]
-        float g[8][8];
+        // forward
+        for (int l = 0; ok && l <= kLayers; ++l) {
+            if (t == 0) {
+                tcFenceAfter();
+                const uint32_t idesc = instrDesc(kTile, l < kLayers ? kWidth : kOutRows);
 #pragma unroll
-        for (int a = 0; a < 8; ++a)
-#pragma unroll
-            for (int b = 0; b < 8; ++b) g[a][b] = 0.0f;
-        if (8 * jt < rows) {
-            for (int r = 0; r < kBlock; ++r) {
-                const float4 d0 = reinterpret_cast<const float4*>(dA + r * kAct + 8 * jt)[0];
-                const float4 d1 = reinterpret_cast<const float4*>(dA + r * kAct + 8 * jt)[1];
-                const float4 i0 = reinterpret_cast<const float4*>(in + r * kAct + 8 * kt)[0];
-                const float4 i1 = reinterpret_cast<const float4*>(in + r * kAct + 8 * kt)[1];
-                const float dv[8] = {d0.x, d0.y, d0.z, d0.w, d1.x, d1.y, d1.z, d1.w};
-                const float iv[8] = {i0.x, i0.y, i0.z, i0.w, i1.x, i1.y, i1.z, i1.w};
-#pragma unroll
-                for (int a = 0; a < 8; ++a)
-#pragma unroll
-                    for (int b = 0; b < 8; ++b) g[a][b] = fmaf(dv[a], iv[b], g[a][b]);
+                for (uint32_t s = 0; s < kWidth / 16; ++s)
+                    tcMma(accA, descK(actAddr + uint32_t(l) * kABytes + 256u * s),
+                          descK(wAddr + uint32_t(l) * kWBytes + 256u * s), idesc, s > 0);
+                tcCommit(barAddr);
             }
-        }
-        float* gOut = myPartial + size_t(l) * kWidth * kWidth;
+            const bool done = waitParity(barAddr, parity);
+            parity ^= 1u;
+            ok = __syncthreads_and(done) != 0;
+            if (!ok) break;
+            tcFenceAfter();
+            if (l < kLayers) {
 #pragma unroll
-        for (int a = 0; a < 8; ++a) {
-            float4* o = reinterpret_cast<float4*>(gOut + (8 * jt + a) * kWidth + 8 * kt);
-            o[0] = make_float4(g[a][0], g[a][1], g[a][2], g[a][3]);
-            o[1] = make_float4(g[a][4], g[a][5], g[a][6], g[a][7]);
-        }
-        // input gradient of this thread's sample: dB[t][k] = sum_j W[j][k] dA[t][j],
-        // through the ReLU of the layer input (hidden layers only)
-        float acc[kWidth];
-#pragma unroll
-        for (int k = 0; k < kWidth; ++k) acc[k] = 0.0f;
-        for (int j = 0; j < rows; ++j) {
-            const float dj = dA[t * kAct + j];
-            const float4* w = reinterpret_cast<const float4*>(sW + j * kWidth);
-#pragma unroll
-            for (int m = 0; m < kWidth / 4; ++m) {
-                const float4 v = w[m];
-                acc[4 * m] = fmaf(v.x, dj, acc[4 * m]);
-                acc[4 * m + 1] = fmaf(v.y, dj, acc[4 * m + 1]);
-                acc[4 * m + 2] = fmaf(v.z, dj, acc[4 * m + 2]);
-                acc[4 * m + 3] = fmaf(v.w, dj, acc[4 * m + 3]);
+                for (int c = 0; c < kWidth / 16; ++c) tmemLoad16(accA + lane + 16u * c, v + 16 * c);
+                tmemWaitLoad();
+                storeRow(sAct + uint32_t(l + 1) * kABytes, t, v, true);
+                fenceAsyncShared();
+            } else {
+                tmemLoad16(accA + lane, v);
+                tmemWaitLoad();
             }
+            tcFenceBefore();
+            __syncthreads();
         }
-        float xin[kWidth];
-        loadRow(in + t * kAct, xin);
+        if (!ok) break;
+        // output gradient: dZ5 (channels 0..2; the rest and padding records zero)
+        float g[kWidth];
+        float loss = 0.0f;
 #pragma unroll
-        for (int k = 0; k < kWidth; ++k)
-            dB[t * kAct + k] = (l > 0 && xin[k] <= 0.0f) ? 0.0f : acc[k];
+        for (int c = 0; c < kWidth; ++c) g[c] = 0.0f;
+        if (valid)
+            for (int c = 0; c < 3; ++c) {
+                const float y = v[c], tg = targets[rec * 3 + c];
+                const float den = y * y + 0.01f;
+                loss += (y - tg) * (y - tg) / den;
+                g[c] = 2.0f * (y - tg) / den * invBatch;
+            }
+        if (lossOut && valid) atomicAdd(lossOut, loss * invBatch);
+        storeRow(sDz, t, g, false);
+        fenceAsyncShared();
+        tcFenceBefore();
         __syncthreads();
-        float* sw = dA;
-        dA = dB;
-        dB = sw;
+        // backward
+        for (int l = kLayers; ok && l >= 0; --l) {
+            const uint32_t outs = l < kLayers ? kWidth : kOutRows;  // K of the input-gradient MMA
+            if (t == 0) {
+                tcFenceAfter();
+                const uint32_t idescW = instrDesc(kTile, kWidth, true, true);
+#pragma unroll
+                for (uint32_t s = 0; s < kTile / 16; ++s)
+                    tcMma(accW, descMN(dzAddr + 2048u * s), descMN(actAddr + uint32_t(l) * kABytes + 2048u * s),
+                          idescW, s > 0);
+                const uint32_t idescA = instrDesc(kTile, kWidth, false, true);
+                for (uint32_t s = 0; s < outs / 16; ++s)
+                    tcMma(accA, descK(dzAddr + 256u * s), descMN(wAddr + uint32_t(l) * kWBytes + 2048u * s), idescA,
+                          s > 0);
+                tcCommit(barAddr);
+            }
+            const bool done = waitParity(barAddr, parity);
+            parity ^= 1u;
+            ok = __syncthreads_and(done) != 0;
+            if (!ok) break;
+            tcFenceAfter();
+            if (warp < 2) {  // dW rows 0..63: lanes 0..63
+                float w[kWidth];
+#pragma unroll
+                for (int c = 0; c < kWidth / 16; ++c) tmemLoad16(accW + lane + 16u * c, w + 16 * c);
+                tmemWaitLoad();
+                float4* o = reinterpret_cast<float4*>(myPartial + size_t(l) * kWidth * kWidth + size_t(t) * kWidth);
+#pragma unroll
+                for (int c = 0; c < kWidth / 4; ++c) {
+                    float4 a = make_float4(w[4 * c], w[4 * c + 1], w[4 * c + 2], w[4 * c + 3]);
+                    if (!firstTile) {
+                        const float4 b = o[c];
+                        a.x += b.x;
+                        a.y += b.y;
+                        a.z += b.z;
+                        a.w += b.w;
+                    }
+                    o[c] = a;
+                }
+            }
+#pragma unroll
+            for (int c = 0; c < kWidth / 16; ++c) tmemLoad16(accA + lane + 16u * c, g + 16 * c);
+            tmemWaitLoad();
+            if (l > 0) {
+                loadRowBf16(sAct + uint32_t(l) * kABytes, t, v);  // A_l = ReLU(Z_{l-1})
+#pragma unroll
+                for (int c = 0; c < kWidth; ++c) g[c] = v[c] > 0.0f ? g[c] : 0.0f;
+                storeRow(sDz, t, g, false);
+                fenceAsyncShared();
+            } else if (valid) {
+                for (int lv = 0; lv < kLevels; ++lv) {
+                    const float g0 = g[2 * lv], g1 = g[2 * lv + 1];
+                    if (g0 == 0.0f && g1 == 0.0f) continue;
+                    for (int c = 0; c < 8; ++c) {
+                        const uint32_t i = corners.idx[lv][c];
+                        const float w = corners.w[lv][c];
+                        atomicAdd(C.gGrid + 2 * size_t(i), w * g0);
+                        atomicAdd(C.gGrid + 2 * size_t(i) + 1, w * g1);
+                    }
+                }
+            }
+            tcFenceBefore();
+            __syncthreads();
+        }
+        firstTile = false;
     }
-    // dA holds the encoding gradient: scatter the grid part
-    if (valid) {
-        for (int l = 0; l < kLevels; ++l) {
-            const float g0 = dA[t * kAct + 2 * l], g1 = dA[t * kAct + 2 * l + 1];
-            if (g0 == 0.0f && g1 == 0.0f) continue;
-            for (int c = 0; c < 8; ++c) {
-                const uint32_t i = corners.idx[l][c];
-                const float w = corners.w[l][c];
-                atomicAdd(C.gGrid + 2 * size_t(i), w * g0);
-                atomicAdd(C.gGrid + 2 * size_t(i) + 1, w * g1);
-            }
-        }
-    }
+    tcFenceBefore();
+    __syncthreads();
+    tcFenceAfter();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2u * kTmemCols)
+                     : "memory");
+    if (!ok && t == 0) atomicOr(C.status, 1u);
 }
 
 // gMlp[i] = sum over blocks of partial[b][i] (rows the output layer leaves
@@ -623,7 +690,6 @@ __global__ void recordTargetsKernel(const float4* __restrict__ prefix, const flo
 }
 
 size_t smemQuery() { return kWAllBytes + kQueryGroups * kABytes + 8 * kQueryGroups + 16; }
-size_t smemTrain() { return sizeof(float) * (kWidth * kWidth + (kLayers + 1 + 2) * kBlock * kAct); }
 
 unsigned gridFor(size_t n) {
     const size_t b = (n + 255) / 256;
@@ -634,8 +700,14 @@ unsigned gridFor(size_t n) {
 
 extern "C" size_t mrtcu_rc_grid_floats() { return size_t(kLevels) * kTableSize * 2; }
 extern "C" size_t mrtcu_rc_mlp_floats() { return size_t(kMlpFloats); }
+// Training CTAs (one per SM at most, each writing its own partial weight
+// gradient) for batches of up to maxBatch records.
+extern "C" uint32_t mrtcu_rc_partial_blocks(uint32_t maxBatch) {
+    const uint32_t tiles = (maxBatch + kTile - 1) / kTile;
+    return tiles < 512u ? tiles : 512u;
+}
 extern "C" size_t mrtcu_rc_partial_floats(uint32_t maxBatch) {
-    return size_t((maxBatch + kBlock - 1) / kBlock) * kMlpFloats;
+    return size_t(mrtcu_rc_partial_blocks(maxBatch)) * kMlpFloats;
 }
 
 extern "C" cudaError_t mrtcu_rc_init(McacheParams C, uint32_t seed, cudaStream_t stream) {
@@ -677,10 +749,13 @@ extern "C" cudaError_t mrtcu_rc_query(McacheParams C, const float* features, uin
 extern "C" cudaError_t mrtcu_rc_train(McacheParams* C, const float* features, const float* targets, uint32_t n,
                                       uint32_t steps, uint32_t batch, float* lossOut, cudaStream_t stream) {
     if (n == 0 || steps == 0) return cudaSuccess;
-    cudaError_t e = cudaFuncSetAttribute(trainKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smemTrain()));
+    cudaError_t e = cudaFuncSetAttribute(tcTrainKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smemTrain()));
     if (e != cudaSuccess) return e;
+    int sms = 148, dev = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    // one CTA per SM at most (shared memory), each with its own partial
+    const uint32_t maxCtas = uint32_t(sms) < C->partialBlocks ? uint32_t(sms) : C->partialBlocks;
     batch = batch < n ? batch : n;
-    batch = batch < C->partialBlocks * kBlock ? batch : C->partialBlocks * kBlock;
     const size_t gridN = mrtcu_rc_grid_floats(), mlpN = mrtcu_rc_mlp_floats();
     // Step k trains on every `every`-th sample from sample k mod every: each
     // batch spreads over all of the samples (they arrive ordered by bounce
@@ -689,8 +764,9 @@ extern "C" cudaError_t mrtcu_rc_train(McacheParams* C, const float* features, co
     for (uint32_t k = 0; k < steps; ++k) {
         const uint32_t first = k % every;
         const uint32_t count = (n - first + every - 1) / every;  // <= batch
-        const uint32_t blocks = (count + kBlock - 1) / kBlock;
-        trainKernel<<<blocks, kBlock, smemTrain(), stream>>>(*C, features, targets, count, first, every,
+        const uint32_t tiles = (count + kTile - 1) / kTile;
+        const uint32_t blocks = tiles < maxCtas ? tiles : maxCtas;
+        tcTrainKernel<<<blocks, kTile, smemTrain(), stream>>>(*C, features, targets, count, first, every,
                                                               1.0f / (3.0f * float(count)), C->partial, lossOut);
         reducePartialsKernel<<<gridFor(kMlpFloats), 256, 0, stream>>>(C->partial, blocks, C->gMlp);
         ++C->step;

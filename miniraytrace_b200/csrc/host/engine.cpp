@@ -1296,7 +1296,7 @@ mrtResult Engine::ensureCache() {
     McacheParams& c = m_cache.params;
     c.partial = m_cache.partial.as<float>();
     c.status = m_cache.loss.as<uint32_t>() + 1;  // the loss buffer's second word
-    c.partialBlocks = uint32_t((kCacheMaxBatch + 63) / 64);
+    c.partialBlocks = mrtcu_rc_partial_blocks(kCacheMaxBatch);
     c.grid = m_cache.grid.as<float>();
     c.mlp = m_cache.mlp.as<float>();
     c.gGrid = m_cache.gGrid.as<float>();

@@ -10,8 +10,10 @@ relative + 2e-4 absolute (FP32 sums in another order, device rsqrt), all
 within 1e-2 relative + 2e-3 absolute (the odd hidden activation whose FP32
 sum lands on the other side of a BF16 rounding boundary moves by one BF16
 step), and all within 3e-2 of the output scale of the FP32 network.
-Training is FP32: gradients compared by sign where they are above 1e-3 of
-their layer's largest."""
+Training runs on the tensor cores too (BF16 activations, weights and
+back-propagated gradients, FP32 sums): one Adam step is compared by sign
+with gradients from numpy doing the same roundings, where they are above
+1e-3 of their layer's largest."""
 import numpy as np
 import pytest
 
@@ -114,17 +116,22 @@ def forward_bf16(enc, mlp):
 
 
 def gradients(F, targets, grid, mlp, lo, hi):
-    """Gradients of the mean relative L2 loss (denominator held fixed)."""
+    """Gradients of the mean relative L2 loss (denominator held fixed) as the
+    tensor-core training step forms them: the encoding, weights, hidden
+    activations and each back-propagated gradient rounded to BF16."""
     enc, corners = encode(F, grid, lo, hi)
-    y, hs = forward(enc, mlp)
-    W = mlp.reshape(6, 64, 64).astype(np.float64)
+    W = bf16(mlp).reshape(6, 64, 64)
+    hs = [bf16(enc)]
+    for l in range(5):
+        hs.append(bf16(np.maximum(hs[-1] @ W[l].T, 0.0)))
+    y = hs[5] @ W[5][:3].T
     n = F.shape[0]
-    d = 2.0 * (y - targets) / (y * y + 0.01) / (3.0 * n)
+    dz = bf16(2.0 * (y - targets) / (y * y + 0.01) / (3.0 * n))
     gW = np.zeros((6, 64, 64))
-    gW[5][:3] = d.T @ hs[5]
-    delta = d @ W[5][:3]
+    gW[5][:3] = dz.T @ hs[5]
+    delta = dz @ W[5][:3]
     for l in range(4, -1, -1):
-        delta = delta * (hs[l + 1] > 0)
+        delta = bf16(delta * (hs[l + 1] > 0))
         gW[l] = delta.T @ hs[l]
         delta = delta @ W[l]
     gG = np.zeros(grid.size)
