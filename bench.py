@@ -369,6 +369,7 @@ def ours_arm(args):
                        "accumulation": "fp64"},
             "gpu_launches": launches,
             "kernel_ms_per_launch": float(np.mean(kernel_ms)),
+            "step_ms": [round(x, 2) for x in step_ms],
             "mrays_per_s": world * rays / launch_s / 1e6,
             "rays_per_path": rays / paths_per_step,
             "commit_ms": commit["commitMs"],

@@ -6,6 +6,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <atomic>
 #include <future>
 #include <thread>
 
@@ -130,7 +131,30 @@ Box3 transformBox(const Box3& b, const float m[12]) {
 // Upload that counts the bytes a commit moves host-to-device.
 mrtResult Engine::up(DeviceBuffer& b, const void* src, size_t n) {
     m_stats.commitH2DBytes += n;
-    return b.upload(src, n, m_stream);
+    if (n < kStageChunk) return b.upload(src, n, m_stream);
+    MRT_TRY(b.ensure(n));
+    return uploadStaged(b.ptr, src, n);
+}
+
+// Host -> pinned staging -> device for large uploads: the copy pool's
+// threads fill one 4 MB pinned slot while the DMA out of the previous slots
+// runs (a copy straight from pageable memory moves ~10 GB/s; this one is
+// bound by the host threads' copy).
+mrtResult Engine::uploadStaged(void* dst, const void* src, size_t n) {
+    if (!m_stage) {
+        MRT_CUDA(cudaMallocHost(&m_stage, kStageChunk * kStageSlots));
+        for (auto& ev : m_stageCopyEvents) MRT_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    }
+    for (size_t c = 0, off = 0; off < n; ++c, off += kStageChunk) {
+        const size_t len = std::min(kStageChunk, n - off), slot = c % kStageSlots;
+        char* stage = static_cast<char*>(m_stage) + slot * kStageChunk;
+        if (m_stageUsed[slot]) MRT_CUDA(cudaEventSynchronize(m_stageCopyEvents[slot]));
+        m_copyPool->copy(stage, static_cast<const char*>(src) + off, len);
+        MRT_CUDA(cudaMemcpyAsync(static_cast<char*>(dst) + off, stage, len, cudaMemcpyHostToDevice, m_stream));
+        MRT_CUDA(cudaEventRecord(m_stageCopyEvents[slot], m_stream));
+        m_stageUsed[slot] = true;
+    }
+    return MRT_SUCCESS;
 }
 
 // ------------------------------------------------------------- lifecycle --
@@ -246,6 +270,9 @@ Engine::~Engine() {
     m_cache.release();
     for (auto& t : m_texData) t.release();
     if (m_pinned) cudaFreeHost(m_pinned);
+    if (m_stage) cudaFreeHost(m_stage);
+    for (auto& ev : m_stageCopyEvents)
+        if (ev) cudaEventDestroy(ev);
     for (auto& ev : m_copyEvents)
         if (ev) cudaEventDestroy(ev);
     for (auto& ev : m_stageEvents)
@@ -396,7 +423,8 @@ mrtResult Engine::sync(mrtCommitStats* stats) {
     m_stats.commitH2DBytes = 0;
     if (dirty & DirtyTextures) MRT_TRY(uploadTextures());
     if (dirty & DirtyMaterials) MRT_TRY(packMaterials());
-    if (dirty & DirtyGeometry) MRT_TRY(packGeometry(rebuilt));
+    const bool tangents = (dirty & (DirtyGeometry | DirtyInstances | DirtyMaterials)) && ensureTangents();
+    if ((dirty & DirtyGeometry) || tangents) MRT_TRY(packGeometry(rebuilt));
     const bool tlas = (dirty & (DirtyGeometry | DirtyInstances | DirtyMaterials)) != 0;
     if (tlas) MRT_TRY(packInstances());
     if (dirty & DirtyEnv) MRT_TRY(packEnvironment());
@@ -412,6 +440,35 @@ mrtResult Engine::sync(mrtCommitStats* stats) {
         stats->commitMs = ms;
     }
     return MRT_SUCCESS;
+}
+
+// Tangents for every mesh with uvs that an instance draws with a material
+// naming a normal texture, computed once per vertex data (on host threads,
+// a mesh at a time). Returns whether any were computed (their meshes' device
+// tangents and the global attribute arrays need refreshing).
+bool Engine::ensureTangents() {
+    auto& meshes = m_scene.meshes();
+    std::vector<MeshData*> todo;
+    for (const auto& [iid, in] : m_scene.instances()) {
+        const auto mt = m_scene.materials().find(in.material);
+        if (mt == m_scene.materials().end() || mt->second.tex[3] == MRT_INVALID_ID) continue;
+        auto it = meshes.find(in.mesh);
+        if (it == meshes.end() || it->second.uvs.empty() || it->second.tangentsDone) continue;
+        it->second.tangentsDone = true;  // (an instance list may name a mesh twice)
+        todo.push_back(&it->second);
+    }
+    std::atomic<size_t> next{0};
+    auto work = [&] {
+        for (size_t k; (k = next.fetch_add(1)) < todo.size();) {
+            Scene::computeTangents(*todo[k]);
+            todo[k]->tangentsPending = true;
+        }
+    };
+    std::vector<std::thread> pool;
+    for (size_t t = 1; t < std::min<size_t>(todo.size(), m_hostThreads); ++t) pool.emplace_back(work);
+    work();
+    for (auto& t : pool) t.join();
+    return !todo.empty();
 }
 
 // reference Renderer.cpp:510-550 (clamps, default material at index 0, texture
@@ -519,7 +576,15 @@ mrtResult Engine::packGeometry(uint32_t& rebuilt) {
         if (mesh.blasDirty || !m_blas.count(id)) changed.push_back(id);
 
     const auto tu = std::chrono::steady_clock::now();
-    for (uint32_t id : changed) MRT_TRY(uploadMesh(meshes[id], m_blas[id]));
+    for (uint32_t id : changed) {
+        MRT_TRY(uploadMesh(meshes[id], m_blas[id]));
+        meshes[id].tangentsPending = false;
+    }
+    for (auto& [id, mesh] : meshes) {  // tangents computed since the mesh's upload
+        if (!mesh.tangentsPending) continue;
+        mesh.tangentsPending = false;
+        MRT_TRY(up(m_blas[id].tangents, mesh.tangents.data(), mesh.tangents.size() * sizeof(V4f)));
+    }
     m_stats.commitUploadMs += std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - tu).count();
 
     const auto tb = std::chrono::steady_clock::now();

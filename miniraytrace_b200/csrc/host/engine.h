@@ -149,6 +149,13 @@ private:
     uint64_t m_maxWaveSlots = uint64_t(1) << 25;  // paths per wave, set from the GPU's memory
     void* m_pinned = nullptr;
     size_t m_pinnedBytes = 0;
+    // upload staging: kStageSlots pinned slots of kStageChunk bytes, each
+    // with the event of its last DMA
+    static constexpr size_t kStageChunk = size_t(4) << 20, kStageSlots = 4;
+    void* m_stage = nullptr;
+    cudaEvent_t m_stageCopyEvents[kStageSlots] = {};
+    bool m_stageUsed[kStageSlots] = {};
+    mrtResult uploadStaged(void* dst, const void* src, size_t n);
     std::unique_ptr<CopyPool> m_copyPool;  // copies out of m_pinned on several threads
 
     // host-side packing state
@@ -165,6 +172,7 @@ private:
         size_t deviceBytes() const;
     };
     mrtResult uploadMesh(const MeshData& m, Blas& b);
+    bool ensureTangents();
     mrtResult buildBlasOnDevice(Blas& b);
     std::map<uint32_t, Blas> m_blas;
     std::map<uint32_t, uint32_t> m_materialIndex;

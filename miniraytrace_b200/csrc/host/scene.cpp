@@ -1,12 +1,35 @@
 // Scene store implementation (semantics: reference core/src/scene/Scene.cpp).
 #include "scene.h"
 
+#include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
+#include <thread>
+#include <vector>
 
 namespace mrt {
 
 namespace {
+
+// fn(begin, end) over [0, n): on up to 8 threads when n is large (the work
+// items are independent), else on the calling thread.
+template <class Fn>
+void parallelRanges(size_t n, Fn&& fn) {
+    const size_t kMinPerThread = size_t(1) << 18;
+    const size_t threads = std::min<size_t>({8, std::max(1u, std::thread::hardware_concurrency()),
+                                             (n + kMinPerThread - 1) / kMinPerThread});
+    if (threads <= 1) {
+        fn(size_t(0), n);
+        return;
+    }
+    std::vector<std::thread> pool;
+    const size_t step = (n + threads - 1) / threads;
+    for (size_t t = 1; t < threads; ++t)
+        pool.emplace_back([&, t] { fn(std::min(n, t * step), std::min(n, (t + 1) * step)); });
+    fn(size_t(0), std::min(n, step));
+    for (auto& th : pool) th.join();
+}
 
 inline void sub3(const V4f& a, const V4f& b, float r[3]) {
     r[0] = a.x - b.x;
@@ -48,9 +71,11 @@ void computeNormals(MeshData& m) {
     }
 }
 
+}  // namespace
+
 // Per-vertex tangents from UV gradients, Gram-Schmidt against the normal,
 // handedness in w (reference Scene.cpp:31-60).
-void computeTangents(MeshData& m) {
+void Scene::computeTangents(MeshData& m) {
     if (m.uvs.empty()) return;
     const size_t nv = m.positions.size();
     std::vector<float> tan(nv * 3, 0.0f), bit(nv * 3, 0.0f);
@@ -96,6 +121,8 @@ void computeTangents(MeshData& m) {
     }
 }
 
+namespace {
+
 void rowsToXf(const float* r, float out[12]) { std::memcpy(out, r, 12 * sizeof(float)); }
 
 MaterialData toMaterial(const mrtMaterialDesc& d) {
@@ -132,25 +159,27 @@ LightData toLight(const mrtLightDesc& d) {
 }  // namespace
 
 void Scene::copyMesh(const mrtMeshDesc& d, MeshData& out) {
-    out.positions.resize(d.vertexCount);
-    for (uint32_t i = 0; i < d.vertexCount; ++i)
-        out.positions[i] = V4f{d.positions[i * 3], d.positions[i * 3 + 1], d.positions[i * 3 + 2], 0.0f};
-    out.indices.assign(d.indices, d.indices + d.indexCount);
-    if (d.normals) {
-        out.normals.resize(d.vertexCount);
-        for (uint32_t i = 0; i < d.vertexCount; ++i)
-            out.normals[i] = V4f{d.normals[i * 3], d.normals[i * 3 + 1], d.normals[i * 3 + 2], 0.0f};
-    } else {
-        computeNormals(out);
-    }
-    if (d.uvs) {
-        out.uvs.resize(d.vertexCount);
-        for (uint32_t i = 0; i < d.vertexCount; ++i) out.uvs[i] = V2f{d.uvs[i * 2], d.uvs[i * 2 + 1]};
-        computeTangents(out);
-    } else {
-        out.uvs.clear();
-        out.tangents.clear();
-    }
+    const size_t nv = d.vertexCount;
+    out.positions.resize(nv);
+    out.indices.resize(d.indexCount);
+    if (d.normals) out.normals.resize(nv);
+    if (d.uvs) out.uvs.resize(nv);
+    else out.uvs.clear();
+    // element-wise copies: independent of the order, split over threads
+    parallelRanges(nv, [&](size_t b, size_t e) {
+        for (size_t i = b; i < e; ++i) {
+            out.positions[i] = V4f{d.positions[i * 3], d.positions[i * 3 + 1], d.positions[i * 3 + 2], 0.0f};
+            if (d.normals) out.normals[i] = V4f{d.normals[i * 3], d.normals[i * 3 + 1], d.normals[i * 3 + 2], 0.0f};
+            if (d.uvs) out.uvs[i] = V2f{d.uvs[i * 2], d.uvs[i * 2 + 1]};
+        }
+    });
+    parallelRanges(d.indexCount, [&](size_t b, size_t e) {
+        std::memcpy(out.indices.data() + b, d.indices + b, (e - b) * sizeof(uint32_t));
+    });
+    if (!d.normals) computeNormals(out);  // ordered sums: sequential
+    out.tangents.clear();  // computed at commit when a normal map needs them
+    out.tangentsDone = false;
+    out.tangentsPending = false;
     out.blasDirty = true;
 }
 
@@ -161,9 +190,13 @@ namespace {
 // buffer there); here such a mesh is rejected instead.
 bool meshDescUsable(const mrtMeshDesc& d) {
     if (!d.positions || !d.indices || d.indexCount % 3 != 0) return false;
-    for (uint32_t i = 0; i < d.indexCount; ++i)
-        if (d.indices[i] >= d.vertexCount) return false;
-    return true;
+    std::atomic<bool> ok{true};
+    parallelRanges(d.indexCount, [&](size_t b, size_t e) {
+        uint32_t mx = 0;
+        for (size_t i = b; i < e; ++i) mx = std::max(mx, d.indices[i]);
+        if (e > b && mx >= d.vertexCount) ok = false;
+    });
+    return ok;
 }
 }  // namespace
 
@@ -300,7 +333,9 @@ void Scene::setEnvironment(const mrtTextureDesc& d, float rotation, float intens
     m_env.height = d.height;
     m_env.format = MRT_TEX_RGBA32F;
     const size_t bytes = size_t(d.width) * d.height * 16;
-    m_env.data.assign(static_cast<const uint8_t*>(d.pixels), static_cast<const uint8_t*>(d.pixels) + bytes);
+    m_env.data.resize(bytes);
+    const uint8_t* src = static_cast<const uint8_t*>(d.pixels);
+    parallelRanges(bytes / 16, [&](size_t b, size_t e) { std::memcpy(m_env.data.data() + 16 * b, src + 16 * b, 16 * (e - b)); });
     m_envValid = true;
     m_envRotation = rotation;
     m_envIntensity = intensity;

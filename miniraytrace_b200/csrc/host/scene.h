@@ -42,9 +42,11 @@ struct MeshData {
     std::vector<V4f> positions;  // w = 0
     std::vector<V4f> normals;    // w = 0
     std::vector<V2f> uvs;        // empty when none
-    std::vector<V4f> tangents;   // w = handedness; empty when no uvs
+    std::vector<V4f> tangents;   // w = handedness; empty until computed (needs uvs)
     std::vector<uint32_t> indices;
     bool blasDirty = true;
+    bool tangentsDone = false;     // tangents computed for the current vertex data
+    bool tangentsPending = false;  // computed, not yet on the device
 };
 
 struct InstanceData {
@@ -95,6 +97,11 @@ struct CameraExData {  // explicit frustum (SceneTypes.hpp:129-135 defaults)
 class Scene {
 public:
     uint32_t addMesh(const mrtMeshDesc& d);
+    // Per-vertex tangents from UV gradients (reference Scene.cpp:31-60). The
+    // reference computes them whenever a mesh with uvs is stored; they are
+    // read only by normal mapping, so here the commit computes them, once per
+    // vertex data, for meshes drawn with a normal-mapped material.
+    static void computeTangents(MeshData& m);
     void updateMesh(uint32_t id, const mrtMeshDesc& d);
     void removeMesh(uint32_t id);
 
