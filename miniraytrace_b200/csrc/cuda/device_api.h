@@ -65,6 +65,10 @@ cudaError_t mrtcu_env_cdf_noalloc(unsigned char* scratch, const float4* texels, 
 // RGBA32F readback conversion: out[i] = (sum / count, 1) with the pixel's
 // own sample count; spp == 0 (nothing accumulated since the last reset)
 // gives (0, 0, 0, 1) as the reference does (Renderer.cpp:904).
+// Reads `count` 16-byte words at buf `reps` times with loads cached in L2
+// only, from every SM (a bandwidth probe); *sink is written only for a value
+// a zero-filled buffer never yields.
+cudaError_t mrtcu_l2_read_probe(const void* buf, size_t count, uint32_t reps, uint32_t* sink, cudaStream_t stream);
 cudaError_t mrtcu_readback_rgba32f(const double* accum, size_t npix, uint32_t spp, float4* out,
                                    cudaStream_t stream);
 

@@ -191,6 +191,29 @@ extern "C" cudaError_t mrtcu_env_cdf_noalloc(unsigned char* scratch, const float
     return mrtcu_env_cdf(texels, sinTheta, w, h, cdf, rowSums, rowInv, integral, stream);
 }
 
+namespace {
+// Every block strides over the whole buffer, `reps` times; loads bypass L1
+// (ld.global.cg), so a buffer smaller than L2 is served by L2.
+__global__ void l2ReadProbeKernel(const uint4* __restrict__ buf, size_t count, uint32_t reps, uint32_t* sink) {
+    const size_t stride = size_t(gridDim.x) * blockDim.x;
+    uint32_t acc = 0;
+    for (uint32_t r = 0; r < reps; ++r)
+        for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < count; i += stride) {
+            const uint4 v = __ldcg(buf + i);
+            acc ^= v.x ^ v.y ^ v.z ^ v.w;
+        }
+    if (acc == 0x9e3779b9u) *sink = acc;
+}
+}  // namespace
+
+extern "C" cudaError_t mrtcu_l2_read_probe(const void* buf, size_t count, uint32_t reps, uint32_t* sink,
+                                           cudaStream_t stream) {
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    l2ReadProbeKernel<<<sms * 8, 256, 0, stream>>>(static_cast<const uint4*>(buf), count, reps, sink);
+    return cudaGetLastError();
+}
+
 extern "C" cudaError_t mrtcu_readback_rgba32f(const double* accum, size_t npix, uint32_t spp, float4* out,
                                               cudaStream_t stream) {
     if (npix == 0) return cudaSuccess;

@@ -107,8 +107,6 @@ MRT_DEV void warpAddCounters(unsigned long long* ctr, const uint32_t (&c)[kCtrCo
     }
 }
 
-// Warp-aggregated queue append: every lane of the warp must call it; lanes
-// with pred get consecutive indices from one atomicAdd on *count.
 // Index of this thread's entry in a list that every thread of the current
 // coalesced group appends one entry to (one atomic per group).
 MRT_DEV uint32_t coalescedAppend(uint32_t* count) {
@@ -116,17 +114,6 @@ MRT_DEV uint32_t coalescedAppend(uint32_t* count) {
     uint32_t base = 0;
     if (g.thread_rank() == 0) base = atomicAdd(count, g.size());
     return g.shfl(base, 0) + g.thread_rank();
-}
-
-MRT_DEV uint32_t warpAppend(uint32_t* count, bool pred) {
-    const uint32_t lane = threadIdx.x & 31;
-    const uint32_t mask = __ballot_sync(0xffffffffu, pred);
-    if (mask == 0) return 0xffffffffu;
-    const int leader = __ffs(mask) - 1;
-    uint32_t base = 0;
-    if (int(lane) == leader) base = atomicAdd(count, uint32_t(__popc(mask)));
-    base = __shfl_sync(0xffffffffu, base, leader);
-    return pred ? base + uint32_t(__popc(mask & ((1u << lane) - 1u))) : 0xffffffffu;
 }
 
 struct WaveArgs {

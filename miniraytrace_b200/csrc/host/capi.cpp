@@ -242,6 +242,12 @@ MRT_API mrtResult mrtxReadAccumulation(mrtEngine* e, double* dst, size_t dstSize
     return guarded([&] { return eng->readAccumulation(dst, dstSize, outSpp); });
 }
 
+MRT_API mrtResult mrtxMeasureL2Bandwidth(mrtEngine* e, float* outGBs) {
+    mrt::Engine* eng = unwrap(e);
+    if (!eng || !outGBs) return MRT_ERROR_INVALID_ARGUMENT;
+    return guarded([&] { return eng->measureL2Bandwidth(outGBs); });
+}
+
 MRT_API mrtResult mrtxGetStats(mrtEngine* e, mrtxStats* out) {
     mrt::Engine* eng = unwrap(e);
     if (!eng || !validStruct(out)) return MRT_ERROR_INVALID_ARGUMENT;

@@ -1233,6 +1233,33 @@ mrtResult Engine::readAccumulation(double* dst, size_t dstSize, uint32_t* spp) {
     return MRT_SUCCESS;
 }
 
+// L2 read bandwidth of this engine's GPU: a 32 MiB zero-filled buffer (well
+// inside the 126 MB L2) read 32 times by every SM with L2-only loads, timed
+// with events on the engine's stream after one warm-up pass. The buffer is
+// released before returning.
+mrtResult Engine::measureL2Bandwidth(float* gbs) {
+    MRT_TRY(checkAlive());
+    MRT_TRY(flushPending());
+    const size_t bytes = size_t(32) << 20;
+    const uint32_t reps = 32;
+    DeviceBuffer buf, sink;
+    MRT_TRY(buf.ensure(bytes));
+    MRT_TRY(sink.ensure(16));
+    MRT_CUDA(cudaMemsetAsync(buf.ptr, 0, bytes, m_stream));
+    MRT_CUDA(mrtcu_l2_read_probe(buf.ptr, bytes / 16, 2, sink.as<uint32_t>(), m_stream));
+    MRT_CUDA(cudaEventRecord(m_ev0, m_stream));
+    MRT_CUDA(mrtcu_l2_read_probe(buf.ptr, bytes / 16, reps, sink.as<uint32_t>(), m_stream));
+    MRT_CUDA(cudaEventRecord(m_ev1, m_stream));
+    const cudaError_t e = cudaStreamSynchronize(m_stream);
+    if (e != cudaSuccess) return guard(fromCuda(e, "L2 bandwidth probe"));
+    float ms = 0.0f;
+    MRT_CUDA(cudaEventElapsedTime(&ms, m_ev0, m_ev1));
+    *gbs = float(double(bytes) * reps / (double(ms) * 1e-3) / 1e9);
+    buf.release();
+    sink.release();
+    return MRT_SUCCESS;
+}
+
 mrtResult Engine::getStats(mrtxStats* out) const {
     mrtxStats s = m_stats;
     s.structSize = sizeof(mrtxStats);

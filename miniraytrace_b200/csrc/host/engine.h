@@ -60,6 +60,7 @@ public:
     mrtResult traceShadowRays(const mrtxRay* rays, uint32_t n, uint32_t* occluded);
     mrtResult readAccumulation(double* dst, size_t dstSize, uint32_t* spp);
     mrtResult getStats(mrtxStats* out) const;
+    mrtResult measureL2Bandwidth(float* gbs);
     mrtResult buildEnvCdf(const float* rgba, uint32_t w, uint32_t h, float* cdf, float* integral);
     mrtResult setSampleStream(uint32_t offset, uint32_t stride);
     mrtResult copyAccumulationDevice(void* dev, size_t bytes, bool accumulate);

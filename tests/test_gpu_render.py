@@ -526,3 +526,15 @@ def test_incremental_geometry_commit_matches_fresh_engine(gpu):
     assert np.array_equal(ha["prim"], hb["prim"]) and np.array_equal(ha["t"], hb["t"])
     a.close()
     b.close()
+
+
+def test_l2_bandwidth_probe(gpu):
+    """mrtxMeasureL2Bandwidth returns a plausible L2 read bandwidth (above a
+    tenth of the HBM copy rate, below 100 TB/s) and frees its buffer."""
+    e = gpu.Engine(16, 16)
+    base = e.stats()["deviceBytes"]
+    g = e.measure_l2_bandwidth()
+    assert 600.0 < g < 100000.0, g
+    assert e.stats()["deviceBytes"] == base
+    e.close()
+
