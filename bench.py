@@ -53,12 +53,14 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--config", choices=["terrain", "box_sphere", "batch", "room", "cache"], default="terrain",
+    ap.add_argument("--config", choices=["terrain", "box_sphere", "batch", "room", "cache", "large"],
+                    default="terrain",
                     help="batch: the 16 uneven config-3 jobs in one mrtxRenderBatch submission per step "
                          "(single GPU; reports aggregate Mpaths/s and per-job completion); "
                          "room: time to relMSE 1e-3 on config 4, plain and radiance-cached; "
                          "cache: config 4 rendered with the radiance cache, 4 spp per step, reporting the "
-                         "cache's inference and training kernels")
+                         "cache's inference and training kernels; large: config 5 (25.2 M triangles, 3840x2160, "
+                         "depth 16), 16 spp per step, no CPU baseline")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -72,6 +74,8 @@ def make_scene(name):
     from miniraytrace_b200 import scenes
     if name == "terrain":
         return scenes.terrain()
+    if name == "large":
+        return scenes.large(spp=16)  # 16 of config 5's 1024 spp per step: one 2^27-path wave at 4K
     return scenes.box_sphere(1920, 1080, spp=16)
 
 
@@ -81,6 +85,10 @@ def workload_desc(scene):
         return (f"terrain {st['width']}x{st['height']}, {scene.spp} spp/step, max bounces {st['max_bounces']}, "
                 f"{scene.triangle_count:,} triangles (1024^2 fBm heightfield + 256 x 1280-triangle icosphere "
                 f"instances), 2048x1024 procedural sky, env importance sampling + MIS")
+    if scene.name == "large":
+        return (f"config 5: {st['width']}x{st['height']}, {scene.spp} spp/step (of 1024), max bounces "
+                f"{st['max_bounces']}, {scene.triangle_count:,} triangles (4096^2 fBm heightfield cropped to "
+                f"19,999,980 triangles + 4,096 x 1280-triangle icosphere instances), 4096x2048 sky, one camera")
     return f"box_sphere {st['width']}x{st['height']}, {scene.spp} spp/step, sun light"
 
 
@@ -344,12 +352,12 @@ def ours_arm(args):
                "h2d_bytes_per_step": int(np.mean(h2d)), "d2h_bytes_per_step": W * H * 16,
                "seconds_per_step": e2e_s,
                "breakdown": "mrtUpdateMesh(heightfield) + mrtSetEnvironment + mrtCommitScene (BVH rebuild, "
-                            "packing, env CDF kernel, uploads) + 64 x mrtRenderFrame + RGBA32F readback"}
+                            "packing, env CDF kernel, uploads) + %d x mrtRenderFrame + RGBA32F readback" % spp}
 
     out = None
     if rank == 0:
         cpu = None
-        if world == 1 and not args.no_cpu_baseline:
+        if world == 1 and not args.no_cpu_baseline and args.config != "large":
             threads = os.cpu_count() or 1
             o, rng, n, _ = cpu_sample_rate(scene, args.cpu_seconds, threads, "port")
             r = run_cpu_sample(o, rng, n, W * H, threads, 7)
@@ -357,7 +365,8 @@ def ours_arm(args):
                    "sample": f"{n} uniformly drawn pixels x 1 spp of the same workload (oracle FP32, "
                              f"{threads} threads)"}
         out = {
-            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "metric": METRIC if args.config != "large" else "Mpaths/s at 3840x2160 (config 5)",
+            "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": workload_desc(scene), "width": W, "height": H, "spp_per_step": spp,
@@ -646,8 +655,8 @@ def cache_arm(args):
 
 def main():
     args = parse_args()
-    if args.impl == "reference" and args.config in ("batch", "room", "cache"):
-        print(json.dumps({"impl": "reference", "unavailable": "the batched config-3 mode is timed on the GPU only; "
+    if args.impl == "reference" and args.config in ("batch", "room", "cache", "large"):
+        print(json.dumps({"impl": "reference", "unavailable": f"the {args.config} mode is timed on the GPU only; "
                           "the reference arm times the terrain and box_sphere workloads"}), flush=True)
         return 0
     if args.impl == "reference":
