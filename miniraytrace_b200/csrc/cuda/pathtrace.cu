@@ -276,7 +276,7 @@ MRT_DEV void writeCacheFeatures(float* out, const Surface& s, float3 wo, const B
     f[3] = make_float4(bsdf.baseColor.z, 0.0f, 0.0f, 0.0f);
 }
 
-constexpr uint32_t kShadeBlock = 128;
+constexpr uint32_t kShadeBlock = 256;
 
 // Appends to two lists at once, one atomic per list per block (a per-warp
 // atomic on the same counter serialised in L2: 4.2 M a bounce at 1080p x 64
