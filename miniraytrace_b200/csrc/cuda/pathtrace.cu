@@ -15,6 +15,8 @@
 //   - the first-hit AOV buffers of the reference are not produced (they only
 //     feed an optional OIDN denoiser and are not readable through the ABI).
 #include <cooperative_groups.h>
+#include <map>
+#include <mutex>
 #include <cuda_runtime.h>
 
 #include "device_api.h"
@@ -574,6 +576,33 @@ int persistentBlocks(const void* kernel, int threads) {
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kernel, threads, 0);
     return sms * (perSm > 0 ? perSm : 1);
 }
+// Grids of exactly the resident blocks of each wavefront kernel on a device
+// (the cache-mode shade kernel uses more registers, so fewer of its blocks
+// fit an SM; a grid sized for the other variant would leave a second, serial
+// wave of blocks). Computed once per device, on first use with it current.
+struct WaveGrids {
+    int extend, shade, shadeCache, shadow;
+};
+
+const WaveGrids& waveGrids() {
+    static std::mutex mutex;
+    static std::map<int, WaveGrids> grids;  // nodes never move: references stay valid
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lock(mutex);
+    auto it = grids.find(dev);
+    if (it == grids.end())
+        it = grids.emplace(dev, WaveGrids{persistentBlocks(reinterpret_cast<const void*>(waveExtendKernel),
+                                                           MRT_TRAV_THREADS),
+                                          persistentBlocks(reinterpret_cast<const void*>(waveShadeKernel<false>),
+                                                           kShadeBlock),
+                                          persistentBlocks(reinterpret_cast<const void*>(waveShadeKernel<true>),
+                                                           kShadeBlock),
+                                          persistentBlocks(reinterpret_cast<const void*>(waveShadowKernel),
+                                                           MRT_TRAV_THREADS)})
+                 .first;
+    return it->second;
+}
 }  // namespace
 
 extern "C" cudaError_t mrtcu_wave_finalize(const MrtFrameParams* p, const MrtWaveState* s, uint32_t sampleBase,
@@ -591,17 +620,8 @@ extern "C" cudaError_t mrtcu_wave(const MrtFrameParams* p, const MrtWaveState* s
     const uint32_t pixels = p->width * p->height;
     if (pixels == 0 || samples == 0) return cudaSuccess;
     if (uint64_t(pixels) * samples > s->capacity) return cudaErrorInvalidValue;
-    // Grids of exactly the resident blocks of each kernel (the cache-mode
-    // shade kernel uses more registers, so fewer of its blocks fit an SM; a
-    // grid sized for the other variant would leave a second, serial wave of
-    // blocks).
-    static int gExtend = 0, gShade = 0, gShadeCache = 0, gShadow = 0;
-    if (gExtend == 0) {
-        gExtend = persistentBlocks(reinterpret_cast<const void*>(waveExtendKernel), MRT_TRAV_THREADS);
-        gShade = persistentBlocks(reinterpret_cast<const void*>(waveShadeKernel<false>), kShadeBlock);
-        gShadeCache = persistentBlocks(reinterpret_cast<const void*>(waveShadeKernel<true>), kShadeBlock);
-        gShadow = persistentBlocks(reinterpret_cast<const void*>(waveShadowKernel), MRT_TRAV_THREADS);
-    }
+    const WaveGrids& g = waveGrids();
+    const int gExtend = g.extend, gShade = g.shade, gShadeCache = g.shadeCache, gShadow = g.shadow;
     WaveArgs A{pixels, pixels * samples, sampleBase, samples};
     uint32_t n = 0;
     waveInitKernel<<<(A.slots + 255) / 256, 256, 0, stream>>>(*p, *s, A);
