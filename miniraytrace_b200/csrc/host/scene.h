@@ -2,8 +2,9 @@
 // store (core/include/mrt/Scene.hpp:39-125, core/src/scene/Scene.cpp):
 //   - every add deep-copies the caller's arrays; ids are monotone, shared by
 //     all object kinds, and 0 is never valid;
-//   - meshes get area-weighted normals when none are supplied and tangents
-//     when UVs are supplied;
+//   - meshes get area-weighted normals when none are supplied; tangents
+//     (for meshes with UVs) are computed by the engine's commit for meshes
+//     an instance draws with a normal-mapped material (computeTangents);
 //   - textures live in slots that are recycled after removal, with a
 //     generation counter that tells the engine to re-upload a slot;
 //   - every mutation sets dirty bits that the engine's commit consumes.
