@@ -214,7 +214,7 @@ mrtResult Engine::init(const mrtEngineDesc& desc) {
     if (prop.major != 10)
         return fail(MRT_ERROR_SHADER_LOAD, std::string("GPU ") + prop.name + " (sm_" + std::to_string(prop.major) +
                                                std::to_string(prop.minor) +
-                                               ") cannot run this build's kernels, which are compiled for sm_100a only.");
+                                               ") cannot run this library's kernels, which are compiled for sm_100a only.");
     MRT_CUDA(cudaStreamCreateWithFlags(&m_stream, cudaStreamNonBlocking));
     MRT_CUDA(cudaEventCreate(&m_ev0));
     MRT_CUDA(cudaEventCreate(&m_ev1));
