@@ -13,10 +13,10 @@
 // Network: 5 hidden layers of 64 (W0..W4, 64 x 64, ReLU), output W5 (3 x 64
 // stored as 16 x 64, rows 3..15 unused). No other biases.
 //
-// Inference runs on the tensor cores (tcgen05 MMAs with BF16 operands and
-// FP32 accumulators in tensor memory, below). Training keeps FP32 on the CUDA
-// cores: 64 samples per block, weights read from shared memory as broadcasts
-// and activations from padded shared rows.
+// Inference and training run on the tensor cores (tcgen05 MMAs with BF16
+// operands and FP32 accumulators in tensor memory, below); the hash-grid
+// encoding, the ReLU masks, the loss gradient and Adam run on the CUDA cores
+// in FP32, and the parameters are kept in FP32.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
