@@ -1243,6 +1243,13 @@ mrtResult Engine::measureL2Bandwidth(float* gbs) {
     const size_t bytes = size_t(32) << 20;
     const uint32_t reps = 32;
     DeviceBuffer buf, sink;
+    struct ReleaseOnExit {  // DeviceBuffer frees nothing by itself
+        DeviceBuffer &a, &b;
+        ~ReleaseOnExit() {
+            a.release();
+            b.release();
+        }
+    } releaseOnExit{buf, sink};
     MRT_TRY(buf.ensure(bytes));
     MRT_TRY(sink.ensure(16));
     MRT_CUDA(cudaMemsetAsync(buf.ptr, 0, bytes, m_stream));
@@ -1255,8 +1262,6 @@ mrtResult Engine::measureL2Bandwidth(float* gbs) {
     float ms = 0.0f;
     MRT_CUDA(cudaEventElapsedTime(&ms, m_ev0, m_ev1));
     *gbs = float(double(bytes) * reps / (double(ms) * 1e-3) / 1e9);
-    buf.release();
-    sink.release();
     return MRT_SUCCESS;
 }
 
