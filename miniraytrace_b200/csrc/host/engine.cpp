@@ -713,9 +713,13 @@ mrtResult Engine::packInstances() {
         // instance count outgrew the reserved TLAS room: grow, keeping the BLAS part
         DeviceBuffer bigger;
         MRT_TRY(bigger.ensure(need + need / 2));
-        MRT_CUDA(cudaMemcpyAsync(bigger.ptr, m_nodes.ptr, size_t(m_tlasRoot) * sizeof(MrtWideNode),
-                                 cudaMemcpyDeviceToDevice, m_stream));
-        MRT_CUDA(cudaStreamSynchronize(m_stream));
+        cudaError_t e = cudaMemcpyAsync(bigger.ptr, m_nodes.ptr, size_t(m_tlasRoot) * sizeof(MrtWideNode),
+                                        cudaMemcpyDeviceToDevice, m_stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(m_stream);
+        if (e != cudaSuccess) {
+            bigger.release();
+            return fromCuda(e, "growing the node buffer for the TLAS");
+        }
         m_nodes.release();
         m_nodes = bigger;
     }
