@@ -1,5 +1,5 @@
 // Host-side checks of the scene store (compiled and run by
-// tests/test_scene_host_cpu.py, no GPU needed): a mesh large enough for the
+// tests/test_host_cpu.py, no GPU needed): a mesh large enough for the
 // threaded copy and index check is stored element for element; an index
 // past the vertex count anywhere in the array rejects the mesh; tangents are
 // not computed when the mesh is stored, and computing them twice gives the
