@@ -118,6 +118,7 @@ MRT_DEV uint32_t coalescedAppend(uint32_t* count) {
     return g.shfl(base, 0) + g.thread_rank();
 }
 
+// Slot layout of a wave: slot = pixel * samples + sample (sample-minor).
 struct WaveArgs {
     uint32_t pixels;      // W * H
     uint32_t slots;       // pixels * samples of this wave
@@ -126,7 +127,7 @@ struct WaveArgs {
 };
 
 MRT_DEV uint32_t frameOf(const MrtFrameParams& P, const WaveArgs& A, uint32_t slot) {
-    return P.streamOffset + (A.sampleBase + slot / A.pixels) * P.streamStride;
+    return P.streamOffset + (A.sampleBase + slot % A.samples) * P.streamStride;
 }
 
 // Camera rays of every slot of the wave (pathtrace.comp:101-130).
@@ -139,7 +140,7 @@ __global__ void __launch_bounds__(256) waveInitKernel(MrtFrameParams P, MrtWaveS
         S.counts[4] = 0;  // extend fetch counter (kExtendHead) of bounce 0
     }
     if (slot >= A.slots) return;
-    const uint32_t pixel = slot % A.pixels;
+    const uint32_t pixel = slot / A.samples;
     const uint32_t px = pixel % P.width, py = pixel / P.width;
     Rng rng{px, py, frameOf(P, A, slot), 0u};
     const float2 jitter = rng2(rng);
@@ -329,7 +330,7 @@ __global__ void __launch_bounds__(kShadeBlock) waveShadeKernel(MrtFrameParams P,
             slot = q[i];
             const float4 o4 = S.rayO[slot], d4 = S.rayD[slot], b4 = S.beta[slot], L4 = S.L[slot];
             const float4 h4 = S.hit[slot];
-            const uint32_t pixel = slot % A.pixels;
+            const uint32_t pixel = slot / A.samples;
             Rng rng{pixel % P.width, pixel / P.width, frameOf(P, A, slot), __float_as_uint(b4.w)};
             const uint32_t bounce = __float_as_uint(d4.w);
             float3 ro = f3(o4), rd = f3(d4), beta = f3(b4), L = f3(L4);
@@ -501,7 +502,7 @@ __global__ void __launch_bounds__(256) waveFinalizeKernel(MrtFrameParams P, MrtW
     if (pixel >= A.pixels) return;
     double sx = 0.0, sy = 0.0, sz = 0.0;
     for (uint32_t s = 0; s < A.samples; ++s) {
-        const float4 l4 = S.L[s * A.pixels + pixel];
+        const float4 l4 = S.L[size_t(pixel) * A.samples + s];
         float3 L = f3(l4);
         if (P.fireflyClamp > 0.0f) {
             const float m = maxComp(L);

@@ -1,4 +1,4 @@
-"""Rendering with the radiance cache (config 4's room at small sizes).
+"""Rendering with the radiance cache (config 4's room at reduced sizes).
 Switching the cache on or off starts a new accumulation; with it off the
 path tracer is the plain one, bit for bit. With it on, the image is finite
 and opaque, its mean stays within 5 % of a converged plain image (the cache
@@ -40,7 +40,11 @@ def test_cache_toggle_keeps_the_plain_path(gpu):
 
 
 def test_cached_render_beats_plain_at_equal_samples(gpu):
-    w, h, spp = 160, 90, 64
+    # 320x180: about 1,800 training paths a sample. At 160x90 (1,024) the
+    # cache's early bias after a 64-spp warm-up moved between 1 % and 7 % from
+    # run to run (its gradient sums use float atomics, so training is not
+    # bit-reproducible); at this size it stayed within 0.5 %.
+    w, h, spp = 320, 180, 64
     s = scenes.room(w, h)
     ref = gpu.Engine(w, h)
     s.apply(ref)
