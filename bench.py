@@ -61,7 +61,8 @@ def parse_args():
                          "cache: config 4 rendered with the radiance cache, 4 spp per step, reporting the "
                          "cache's inference and training kernels; large: config 5 (25.2 M triangles, 3840x2160, "
                          "depth 16), 16 spp per step, no CPU baseline")
-    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--e2e-steps", type=int, default=4,
+                    help="end-to-end steps averaged (wall-clock: host jitter of up to ~25 ms a step was seen)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--spp", type=int, default=0, help="samples per pixel per step (0 = the workload's 64)")
