@@ -163,7 +163,8 @@ typedef struct MrtFrameParams {
 // A wave renders `spp` samples of every pixel: slot = pixel * spp + s, so
 // the samples of a pixel sit in neighbouring lanes (their paths start at one
 // surface point and traverse similar nodes: 8.7% faster on the 1080p terrain
-// than slot = s * pixels + pixel).
+// than slot = s * pixels + pixel; ordering the pixels in 8x8 tiles instead
+// of rows changed nothing).
 // Each bounce runs extend (closest hit of the queued rays), shade (surface,
 // NEE sample, BSDF sample, Russian roulette; appends the continuing paths to
 // the other queue and the shadow rays to the shadow queue) and shadow
