@@ -403,8 +403,8 @@ def ours_arm(args):
                             "kernel": "waveExtendKernel (closest hit), all launches of a step",
                             "peak_source": "measured in this process (mrtxMeasureL2Bandwidth): every SM re-reads a "
                                            "32 MiB buffer with L2-only loads, 32 passes, CUDA events",
-                            "note": "the extend kernel is bound by instruction issue (ncu: 77% of issue slots "
-                                    "busy, 9.2 threads per warp instruction), not by L2"},
+                            "note": "the extend kernel is bound by instruction issue (ncu, bounce 1 of a 4-spp frame: "
+                                    "80% of issue slots busy, 10.0 threads per warp instruction), not by L2"},
             "rays_closest_per_step": c["raysClosest"],
             "per_ray": {"closest_nodes": c["nodeFetches"] / max(1, c["raysClosest"]),
                         "closest_tris": c["triTests"] / max(1, c["raysClosest"]),
