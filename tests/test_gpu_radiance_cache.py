@@ -1,5 +1,5 @@
-"""Radiance cache network on the GPU against a numpy implementation of the
-same network: hash-grid + spherical-harmonics encoding and 5 x 64 ReLU MLP
+"""Radiance cache network on the GPU against the oracle's numpy restatement
+of the same network (oracle/radiance_cache.py): hash-grid + spherical-harmonics encoding and 5 x 64 ReLU MLP
 outputs, the direction of one Adam step (its first step moves every
 parameter by +-learning rate, opposite to the gradient's sign), and that
 training fits a smooth function. Inference runs on the tensor cores with
@@ -18,128 +18,17 @@ import numpy as np
 import pytest
 
 from miniraytrace_b200 import abi
+from oracle.radiance_cache import encode, forward, forward_bf16, gradients_bf16
 
 pytestmark = pytest.mark.gpu
 
-LEVELS, T = 16, 1 << 19
-SCALES = np.array([16.0 * 2.0 ** (l * 7.0 / 15.0) for l in range(LEVELS)], np.float32)
 LR = 1e-2
-
-
-def grid_index(x, y, z, res):
-    if (res + 1) ** 3 <= T:
-        return x + (res + 1) * (y + (res + 1) * z)
-    return ((x * np.uint64(1)) ^ (y * np.uint64(2654435761)) ^ (z * np.uint64(805459861))) & np.uint64(T - 1)
-
-
-def sh4(d):
-    x, y, z = d[:, 0], d[:, 1], d[:, 2]
-    xx, yy, zz = x * x, y * y, z * z
-    return np.stack([
-        np.full_like(x, 0.28209479177387814), -0.48860251190291987 * y, 0.48860251190291987 * z,
-        -0.48860251190291987 * x, 1.0925484305920792 * x * y, -1.0925484305920792 * y * z,
-        0.94617469575755997 * zz - 0.31539156525251999, -1.0925484305920792 * x * z,
-        0.54627421529603959 * (xx - yy), 0.59004358992664352 * y * (-3 * xx + yy), 2.8906114426405538 * x * y * z,
-        0.45704579946446572 * y * (1 - 5 * zz), 0.3731763325901154 * z * (5 * zz - 3),
-        0.45704579946446572 * x * (1 - 5 * zz), 1.4453057213202769 * z * (xx - yy),
-        0.59004358992664352 * x * (-xx + 3 * yy)], 1)
-
-
-def encode(F, grid, lo, hi):
-    """(n, 64) encoding and, per level, the 8 corner indices and weights."""
-    n = F.shape[0]
-    inv = (np.float32(1.0) / (hi - lo)).astype(np.float32)
-    p = np.clip((F[:, :3] - lo) * inv, 0, 1).astype(np.float32)
-    enc = np.zeros((n, 64), np.float64)
-    g2 = grid.reshape(-1, 2).astype(np.float64)
-    corners = []
-    for l in range(LEVELS):
-        s = SCALES[l]
-        res = int(np.ceil(s))
-        x = (p * s).astype(np.float32)
-        fl = np.minimum(np.floor(x), np.float32(res - 1))
-        b = fl.astype(np.uint64)
-        fr = (x - fl).astype(np.float64)
-        lvl = []
-        for c in range(8):
-            o = [(c >> a) & 1 for a in range(3)]
-            w = np.ones(n)
-            for a in range(3):
-                w = w * (fr[:, a] if o[a] else 1 - fr[:, a])
-            idx = np.uint64(l * T) + grid_index(b[:, 0] + np.uint64(o[0]), b[:, 1] + np.uint64(o[1]),
-                                                b[:, 2] + np.uint64(o[2]), res)
-            idx = idx.astype(np.int64)
-            enc[:, 2 * l] += w * g2[idx, 0]
-            enc[:, 2 * l + 1] += w * g2[idx, 1]
-            lvl.append((idx, w))
-        corners.append(lvl)
-    d = F[:, 3:6].astype(np.float64)
-    d = d / np.sqrt(np.maximum((d * d).sum(1, keepdims=True), 1e-20))
-    enc[:, 32:48] = sh4(d)
-    enc[:, 48:51] = 0.5 * F[:, 6:9] + 0.5
-    enc[:, 51] = F[:, 9]
-    enc[:, 52:55] = F[:, 10:13]
-    enc[:, 55] = 1.0
-    return enc, corners
-
-
-def forward(enc, mlp):
-    W = mlp.reshape(6, 64, 64).astype(np.float64)
-    hs = [enc]
-    h = enc
-    for l in range(5):
-        h = np.maximum(h @ W[l].T, 0.0)
-        hs.append(h)
-    return h @ W[5][:3].T, hs
-
-
-def bf16(x):
-    """Round to the nearest BF16 (ties to even), returned as float64."""
-    b = np.asarray(x, np.float64).astype(np.float32).view(np.uint32).astype(np.uint64)
-    b = ((b + 0x7FFF + ((b >> 16) & 1)) >> 16) << 16
-    return b.astype(np.uint32).view(np.float32).astype(np.float64)
 
 
 def assert_bf16_close(out, ref, msg=""):
     near = np.isclose(out, ref, rtol=5e-3, atol=2e-4)
     assert near.mean() >= 0.999, (msg, near.size - near.sum())
     np.testing.assert_allclose(out, ref, rtol=1e-2, atol=2e-3, err_msg=msg)
-
-
-def forward_bf16(enc, mlp):
-    """The tensor-core inference: BF16 operands, FP32 (here FP64) sums."""
-    W = bf16(mlp).reshape(6, 64, 64)
-    h = bf16(enc)
-    for l in range(5):
-        h = bf16(np.maximum(h @ W[l].T, 0.0))
-    return np.maximum(h @ W[5][:3].T, 0.0)
-
-
-def gradients(F, targets, grid, mlp, lo, hi):
-    """Gradients of the mean relative L2 loss (denominator held fixed) as the
-    tensor-core training step forms them: the encoding, weights, hidden
-    activations and each back-propagated gradient rounded to BF16."""
-    enc, corners = encode(F, grid, lo, hi)
-    W = bf16(mlp).reshape(6, 64, 64)
-    hs = [bf16(enc)]
-    for l in range(5):
-        hs.append(bf16(np.maximum(hs[-1] @ W[l].T, 0.0)))
-    y = hs[5] @ W[5][:3].T
-    n = F.shape[0]
-    dz = bf16(2.0 * (y - targets) / (y * y + 0.01) / (3.0 * n))
-    gW = np.zeros((6, 64, 64))
-    gW[5][:3] = dz.T @ hs[5]
-    delta = dz @ W[5][:3]
-    for l in range(4, -1, -1):
-        delta = bf16(delta * (hs[l + 1] > 0))
-        gW[l] = delta.T @ hs[l]
-        delta = delta @ W[l]
-    gG = np.zeros(grid.size)
-    for l in range(LEVELS):
-        for idx, w in corners[l]:
-            np.add.at(gG, 2 * idx, w * delta[:, 2 * l])
-            np.add.at(gG, 2 * idx + 1, w * delta[:, 2 * l + 1])
-    return gW.ravel(), gG
 
 
 def random_features(rng, n, lo, hi):
@@ -208,7 +97,7 @@ def test_one_adam_step_follows_numpy_gradients(engine):
     targets = rng.uniform(0, 2, (256, 3)).astype(np.float32)
     engine.cache_train(F, targets, steps=1)
     grid1, mlp1 = engine.cache_params()
-    gW, gG = gradients(F, targets.astype(np.float64), grid, mlp, LO, HI)
+    gW, gG = gradients_bf16(F, targets.astype(np.float64), grid, mlp, LO, HI)
     for name, p0, p1, g in (("mlp", mlp, mlp1, gW), ("grid", grid, grid1, gG)):
         step = p1.astype(np.float64) - p0
         big = np.abs(g) > 1e-3 * np.abs(g).max()
