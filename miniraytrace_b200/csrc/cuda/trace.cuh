@@ -16,9 +16,11 @@
 //   - a conservative slab test: box planes are exact reals on a power-of-two
 //     grid and every rounding of the slab arithmetic is covered by a margin
 //     derived per node (see slabAxis), so no child box the ray really
-//     enters is culled (the reference's exact-comparison slab test
-//     occasionally drops a hit or an occluder whose point lies on its leaf
-//     box's face);
+//     enters is culled (the reference's exact-comparison slab test,
+//     intersect.glsl:10-18, has no such margin);
+//   - every instance is traced: TLAS leaves hold one instance each (the
+//     reference can build a 2-instance TLAS leaf, Bvh.cpp:104, and then
+//     enters only its first instance, intersect.glsl:116-121, 150-152);
 //   - stacks are bounded and an overflow sets an error flag instead of
 //     writing out of bounds; node, triangle and instance indices are checked.
 #pragma once

@@ -58,6 +58,7 @@ def load():
             "orc_readback_f32": (None, [vp, u32, u32, vp]), "orc_resolve_rgba8": (None, [vp, u32, f32, u32, vp]),
             "orc_pcg4d": (None, [vp, u32, vp]), "orc_stats": (None, [vp, vp]),
             "orc_set_bruteforce": (None, [vp, i32]),
+            "orc_set_all_leaf_instances": (None, [vp, i32]), "orc_unwalked_instances": (u32, [vp]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(lib, name)
@@ -206,6 +207,17 @@ class OracleScene:
         triangle (1 = reference Moeller-Trumbore test, 2 = watertight test
         with the hit reported by the reference formula, 0 = BVH walk)."""
         self.lib.orc_set_bruteforce(self.h, int(mode))
+
+    def set_all_leaf_instances(self, on: bool):
+        """True: a TLAS leaf enters every instance it holds. False (default,
+        the reference): only its first (intersect.glsl:116-121, 150-152), so
+        the second instance of a 2-instance TLAS leaf, which Bvh.cpp:104 makes
+        when SAH prefers it, is never traced."""
+        self.lib.orc_set_all_leaf_instances(self.h, 1 if on else 0)
+
+    def unwalked_instances(self) -> int:
+        """After commit(): instances the reference traversal never enters."""
+        return int(self.lib.orc_unwalked_instances(self.h))
 
     def render_f32(self, frame0, nframes, pixels=None, threads=8, accum=None):
         """Reference-order FP32 accumulation; returns (npix, 4) float32."""

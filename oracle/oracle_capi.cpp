@@ -22,6 +22,7 @@ struct OracleScene {
     std::unique_ptr<Packed> packed;
     Globals globals{};
     int bruteForce = 0;  // 1: brute force with the reference test, 2: with the watertight test
+    bool allLeafInstances = false;  // Tracer::allLeafInstances
 };
 
 template <class Fn>
@@ -105,6 +106,24 @@ void orc_set_settings(void* s, const mrtRenderSettings* d) {
 // triangle instead of walking the BVH.
 void orc_set_bruteforce(void* s, int mode) { static_cast<OracleScene*>(s)->bruteForce = mode; }
 
+// 1: walk every instance of a TLAS leaf; 0 (default): only its first, as the
+// reference shaders do (intersect.glsl:116-121, 150-152).
+void orc_set_all_leaf_instances(void* s, int on) { static_cast<OracleScene*>(s)->allLeafInstances = on != 0; }
+
+// After orc_commit: how many instances the reference traversal never enters
+// (those after the first of a multi-instance TLAS leaf, Bvh.cpp:104).
+uint32_t orc_unwalked_instances(void* s) {
+    auto* o = static_cast<OracleScene*>(s);
+    if (!o->packed) return 0;
+    const Packed& P = *o->packed;
+    uint32_t n = 0;
+    for (size_t i = P.tlasRoot; i < P.nodes.size(); ++i) {
+        const uint32_t count = P.nodes[i].packed >> 2;
+        if (count > 1) n += count - 1;
+    }
+    return n;
+}
+
 // Pack the scene (BVH builds, CDF). Returns the number of BVH nodes.
 uint32_t orc_commit(void* s) {
     auto* o = static_cast<OracleScene*>(s);
@@ -124,6 +143,7 @@ int orc_render_f32(void* s, const uint32_t* pixels, uint32_t npix, uint32_t fram
     const Globals& g = o->globals;
     const uint32_t total = pixels ? npix : g.width * g.height;
     Tracer<float> tr{*o->packed, g};
+    tr.allLeafInstances = o->allLeafInstances;
     parallelFor(total, threads, [&](uint32_t i) {
         const uint32_t p = pixels ? pixels[i] : i;
         const uint32_t px = p % g.width, py = p / g.width;
@@ -152,6 +172,7 @@ int orc_render_f32_sum64(void* s, const uint32_t* pixels, uint32_t npix, uint32_
     const Globals& g = o->globals;
     const uint32_t total = pixels ? npix : g.width * g.height;
     Tracer<float> tr{*o->packed, g};
+    tr.allLeafInstances = o->allLeafInstances;
     tr.bruteForce = o->bruteForce != 0;
     tr.watertight = o->bruteForce == 2;
     parallelFor(total, threads, [&](uint32_t i) {
@@ -177,6 +198,7 @@ int orc_render_f64(void* s, const uint32_t* pixels, uint32_t npix, uint32_t fram
     const Globals& g = o->globals;
     const uint32_t total = pixels ? npix : g.width * g.height;
     Tracer<double> tr{*o->packed, g};
+    tr.allLeafInstances = o->allLeafInstances;
     parallelFor(total, threads, [&](uint32_t i) {
         const uint32_t p = pixels ? pixels[i] : i;
         const uint32_t px = p % g.width, py = p / g.width;
@@ -197,6 +219,7 @@ int orc_trace(void* s, const RayIn* rays, uint32_t n, HitOut* out, int threads) 
     if (!o->packed) return -1;
     const Packed& P = *o->packed;
     Tracer<float> tr{P, o->globals};
+    tr.allLeafInstances = o->allLeafInstances;
     parallelFor(n, threads, [&](uint32_t i) {
         Ray<float> r;
         r.origin = V3f(rays[i].o[0], rays[i].o[1], rays[i].o[2]);
@@ -221,6 +244,7 @@ int orc_trace_shadow(void* s, const RayIn* rays, uint32_t n, uint32_t* occluded,
     auto* o = static_cast<OracleScene*>(s);
     if (!o->packed) return -1;
     Tracer<float> tr{*o->packed, o->globals};
+    tr.allLeafInstances = o->allLeafInstances;
     parallelFor(n, threads, [&](uint32_t i) {
         Ray<float> r;
         r.origin = V3f(rays[i].o[0], rays[i].o[1], rays[i].o[2]);

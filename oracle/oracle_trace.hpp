@@ -146,6 +146,13 @@ template <class T> struct Tracer {
     const Globals& g;
     bool bruteForce = false;  // diagnostic: closest hit by testing every triangle
     bool watertight = false;  // diagnostic: brute force decides with the watertight test
+    // Off (the reference): a TLAS leaf enters only instances[leftOrPrim]
+    // (intersect.glsl:116-121, 150-152), although Bvh.cpp:104 makes a
+    // 2-instance TLAS leaf when SAH prefers it (count <= 2 * maxLeafSize 1);
+    // the second instance of such a leaf is never traversed. On: every
+    // instance of the leaf is entered, which is what the 1-instance TLAS
+    // leaves the reference intends (Bvh.hpp:36) would give.
+    bool allLeafInstances = false;
 
     // intersect.glsl:10-18
     T intersectAabb(const BvhNode& n, V3<T> o, V3<T> invDir, T tMax) const {
@@ -231,9 +238,12 @@ template <class T> struct Tracer {
                 stack[sp++] = farC;
                 stack[sp++] = nearC;
             } else {
-                const GpuInstance& in = P.instances[n.leftOrPrim];
-                const V3<T> oObj = wToO(in, ray.origin, true), dObj = wToO(in, ray.dir, false);
-                traverseBlas(in.blasRoot, n.leftOrPrim, oObj, dObj, tMax, hit);
+                const uint32_t walked = allLeafInstances ? count : 1u;
+                for (uint32_t k = 0; k < walked; ++k) {
+                    const GpuInstance& in = P.instances[n.leftOrPrim + k];
+                    const V3<T> oObj = wToO(in, ray.origin, true), dObj = wToO(in, ray.dir, false);
+                    traverseBlas(in.blasRoot, n.leftOrPrim + k, oObj, dObj, tMax, hit);
+                }
             }
         }
         return hit;
@@ -341,23 +351,26 @@ template <class T> struct Tracer {
                 stack[sp++] = n.leftOrPrim;
                 stack[sp++] = n.leftOrPrim + 1;
             } else {
-                const GpuInstance& in = P.instances[n.leftOrPrim];
-                const V3<T> oObj = wToO(in, ray.origin, true), dObj = wToO(in, ray.dir, false);
-                const V3<T> invObj = V3<T>(T(1)) / dObj;
-                uint32_t bstack[64];
-                int bsp = 0;
-                bstack[bsp++] = in.blasRoot;
-                while (bsp > 0) {
-                    const BvhNode& bn = P.nodes[bstack[--bsp]];
-                    if (intersectAabb(bn, oObj, invObj, tMax) >= tMax) continue;
-                    const uint32_t bcnt = bn.packed >> 2;
-                    if (bcnt == 0) {
-                        bstack[bsp++] = bn.leftOrPrim;
-                        bstack[bsp++] = bn.leftOrPrim + 1;
-                    } else {
-                        for (uint32_t i = 0; i < bcnt; ++i) {
-                            V2<T> b;
-                            if (intersectTriangle(bn.leftOrPrim + i, oObj, dObj, tMax, b) > T(0)) return true;
+                const uint32_t walked = allLeafInstances ? count : 1u;
+                for (uint32_t k = 0; k < walked; ++k) {
+                    const GpuInstance& in = P.instances[n.leftOrPrim + k];
+                    const V3<T> oObj = wToO(in, ray.origin, true), dObj = wToO(in, ray.dir, false);
+                    const V3<T> invObj = V3<T>(T(1)) / dObj;
+                    uint32_t bstack[64];
+                    int bsp = 0;
+                    bstack[bsp++] = in.blasRoot;
+                    while (bsp > 0) {
+                        const BvhNode& bn = P.nodes[bstack[--bsp]];
+                        if (intersectAabb(bn, oObj, invObj, tMax) >= tMax) continue;
+                        const uint32_t bcnt = bn.packed >> 2;
+                        if (bcnt == 0) {
+                            bstack[bsp++] = bn.leftOrPrim;
+                            bstack[bsp++] = bn.leftOrPrim + 1;
+                        } else {
+                            for (uint32_t i = 0; i < bcnt; ++i) {
+                                V2<T> b;
+                                if (intersectTriangle(bn.leftOrPrim + i, oObj, dObj, tMax, b) > T(0)) return true;
+                            }
                         }
                     }
                 }

@@ -147,3 +147,62 @@ def test_readback_and_resolve_semantics(oracle_lib):
     rgba8 = oracle_lib.resolve_rgba8(acc, 0.0, 0)
     assert rgba8[0, 3] == 255 and rgba8[0, 0] == 255  # mean 1.0 -> white
     assert (rgba8[1, :3] == 0).all()
+
+
+def test_tlas_two_instance_leaf_enters_only_the_first(oracle_lib):
+    """The reference's TLAS keeps at most one instance per leaf only while
+    SAH prefers a split: Bvh.cpp:104 makes a leaf of up to 2 * maxLeafSize
+    (= 2 for the TLAS) primitives when no split is cheaper, and its closest-
+    hit and shadow walks (intersect.glsl:116-121, 150-152) enter only
+    instances[leftOrPrim] of a TLAS leaf. Pinned here on the room scene,
+    whose wall box holds the heightfield's box: the reference builder itself
+    makes the 2-instance root leaf, the oracle's faithful walk never sees the
+    heightfield, and the oracle's all-instance walk agrees with brute force."""
+    from miniraytrace_b200 import scenes
+    s = scenes.room(48, 27, grid=64)
+    boxes = np.stack([np.concatenate([m.positions.min(0), m.positions.max(0)]) for m in s.meshes]).astype(np.float32)
+    nodes, order = oracle_lib.bvh_build(boxes, 1)
+    assert len(nodes) == 1 and int(nodes[0]["packed"]) >> 2 == 2
+    if oracle_lib.load_ref_bvh() is not None:
+        r_nodes, r_order = oracle_lib.bvh_build(boxes, 1, use_reference=True)
+        assert r_nodes.tobytes() == nodes.tobytes() and np.array_equal(r_order, order)
+
+    o = oracle_lib.OracleScene(48, 27)
+    s.apply(o)
+    o.commit()
+    assert o.unwalked_instances() == 1
+    rng = np.random.default_rng(1)
+    cam = np.float32(s.camera["position"])
+    tg = np.stack([rng.uniform(0, 20, 2000), rng.uniform(0, 4, 2000), rng.uniform(0, 10, 2000)], 1)
+    d = (tg - cam) / np.linalg.norm(tg - cam, axis=1, keepdims=True)
+    org, d = np.tile(cam, (len(d), 1)), d.astype(np.float32)
+    bf, _, mb = o.trace_bruteforce(org, d)
+    ok = (bf["hit"] == 1) & (mb >= 1e-5)
+    walk = o.trace_rays(org, d)
+    # brute force sees both instances; the faithful walk only the walls, so
+    # every ray brute force sends into the heightfield comes back with a
+    # farther wall hit
+    assert len(np.unique(bf["instance"][ok])) == 2
+    on_terrain = ok & (bf["t"] < walk["t"] * (1 - 1e-4))
+    assert on_terrain.sum() > 300
+    assert len(np.unique(bf["instance"][on_terrain])) == 1
+    assert len(np.unique(walk["instance"][ok])) == 1
+    # shadow rays from just above the floor, up to below the ceiling: only the
+    # heightfield (y in [0.05, 0.65]) lies in the way
+    p = np.stack([rng.uniform(1, 19, 500), np.full(500, 0.01), rng.uniform(1, 9, 500)], 1).astype(np.float32)
+    up = np.tile(np.float32([0, 1, 0]), (500, 1))
+    assert (o.trace_shadow_rays(p, up, t_max=1.0) == 0).all()
+
+    o.set_all_leaf_instances(True)
+    walk = o.trace_rays(org, d)
+    assert np.array_equal(walk["hit"][ok], bf["hit"][ok])
+    np.testing.assert_allclose(walk["t"][ok], bf["t"][ok], rtol=1e-4)
+    assert (o.trace_shadow_rays(p, up, t_max=1.0) == 1).all()
+    o.close()
+
+    b = scenes.box_sphere()
+    o = oracle_lib.OracleScene(64, 64)
+    b.apply(o)
+    o.commit()
+    assert o.unwalked_instances() == 0
+    o.close()
