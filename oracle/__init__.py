@@ -203,9 +203,11 @@ class OracleScene:
         return self.lib.orc_commit(self.h)
 
     def set_bruteforce(self, mode: int):
-        """Diagnostic: closest hits of render_f32_sum64 by testing every
-        triangle (1 = reference Moeller-Trumbore test, 2 = watertight test
-        with the hit reported by the reference formula, 0 = BVH walk)."""
+        """Diagnostic: closest and shadow hits of the render calls
+        (render_f32, render_f64, render_f32_sum64) by testing every triangle
+        of every instance (1 = reference Moeller-Trumbore test, 2 = watertight
+        test with the hit reported by the reference formula, 0 = BVH walk).
+        trace_rays and trace_shadow_rays always walk the BVH."""
         self.lib.orc_set_bruteforce(self.h, int(mode))
 
     def set_all_leaf_instances(self, on: bool):

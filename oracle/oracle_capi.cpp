@@ -144,6 +144,8 @@ int orc_render_f32(void* s, const uint32_t* pixels, uint32_t npix, uint32_t fram
     const uint32_t total = pixels ? npix : g.width * g.height;
     Tracer<float> tr{*o->packed, g};
     tr.allLeafInstances = o->allLeafInstances;
+    tr.bruteForce = o->bruteForce != 0;
+    tr.watertight = o->bruteForce == 2;
     parallelFor(total, threads, [&](uint32_t i) {
         const uint32_t p = pixels ? pixels[i] : i;
         const uint32_t px = p % g.width, py = p / g.width;
@@ -199,6 +201,8 @@ int orc_render_f64(void* s, const uint32_t* pixels, uint32_t npix, uint32_t fram
     const uint32_t total = pixels ? npix : g.width * g.height;
     Tracer<double> tr{*o->packed, g};
     tr.allLeafInstances = o->allLeafInstances;
+    tr.bruteForce = o->bruteForce != 0;
+    tr.watertight = o->bruteForce == 2;
     parallelFor(total, threads, [&](uint32_t i) {
         const uint32_t p = pixels ? pixels[i] : i;
         const uint32_t px = p % g.width, py = p / g.width;

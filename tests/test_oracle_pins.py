@@ -7,6 +7,9 @@
 - The reference's BVH tests (topology, traversal == brute force, degenerate
   inputs: bvh_tests.cpp:91-188) are restated against the oracle.
 - pcg4d golden vectors; environment-CDF fixture and properties.
+- The reference's 2-instance TLAS leaves, of which its traversal enters
+  only the first instance, and the oracle's switches around them (walk every
+  leaf instance; brute force), on the room and an instanced terrain.
 """
 from pathlib import Path
 
@@ -206,3 +209,30 @@ def test_tlas_two_instance_leaf_enters_only_the_first(oracle_lib):
     o.commit()
     assert o.unwalked_instances() == 0
     o.close()
+
+
+def test_walk_modes_on_an_instanced_terrain(oracle_lib):
+    """The oracle's three ways to find hits, on a small instanced terrain
+    (48^2 heightfield, 24 icospheres) whose reference TLAS holds one
+    2-instance leaf: the faithful walk differs from brute force in some
+    pixels; entering every leaf instance gives brute force's image bit for
+    bit; the switches act on render_f32 and render_f64 alike."""
+    from miniraytrace_b200 import scenes
+    s = scenes.terrain(width=48, height=32, spp=2, grid=48, spheres=24, sky=(64, 32))
+    o = oracle_lib.OracleScene(48, 32)
+    s.apply(o)
+    o.commit()
+    assert o.unwalked_instances() == 1
+    faithful = o.render_f32(0, 2)
+    o.set_all_leaf_instances(True)
+    every = o.render_f32(0, 2)
+    every64 = o.render_f64(0, 2)
+    o.set_all_leaf_instances(False)
+    o.set_bruteforce(2)
+    brute = o.render_f32(0, 2)
+    brute64 = o.render_f64(0, 2)
+    o.close()
+    assert np.array_equal(every, brute)
+    assert np.allclose(every64, brute64, rtol=1e-12, atol=0)
+    differ = ~np.all(faithful == brute, axis=-1)
+    assert 0 < differ.sum() < 0.02 * differ.size
