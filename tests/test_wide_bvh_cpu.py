@@ -256,3 +256,27 @@ def test_mesh_builder_rejects_bad_input(mrt_lib):
         mrt.build_mesh_bvh(pos, idx + 100, 1)
     with pytest.raises(mrt.MrtError):
         mrt.build_mesh_bvh(pos, idx, 2)  # device builder without an engine
+
+
+def test_instance_tree_has_one_instance_per_leaf():
+    """The engine's TLAS (binary build with leaf size 1, collapsed with one
+    primitive per leaf) puts every instance in a leaf of its own, even for
+    nested and coincident boxes, where the reference's build makes
+    2-instance leaves (Bvh.cpp:104) whose second instance its traversal
+    never enters (intersect.glsl:116-121): the room's wall box holding the
+    heightfield's, and a random set of nested, overlapping and equal boxes."""
+    from miniraytrace_b200 import scenes
+    s = scenes.room(48, 27, grid=64)
+    room = np.stack([np.concatenate([m.positions.min(0), m.positions.max(0)]) for m in s.meshes])
+    rng = np.random.default_rng(11)
+    c = rng.uniform(-5, 5, (300, 3))
+    r = rng.exponential(1.0, (300, 1)) * rng.uniform(0.2, 1.0, (300, 3))
+    boxes = np.concatenate([c - r, c + r], 1)
+    boxes[100:120] = boxes[0]                  # equal boxes
+    boxes[120:140, :3] = boxes[0, :3] - 1.0    # boxes holding box 0
+    boxes[120:140, 3:] = boxes[0, 3:] + 1.0
+    for b in (room, boxes):
+        nodes, order = mrt.build_wide_bvh(b.astype(np.float32), max_leaf_prims=1)
+        per_leaf = [ref[1] for nd in nodes for _, kind, ref in children(nd) if kind == "leaf"]
+        assert per_leaf and all(n == 1 for n in per_leaf)
+        assert sorted(subtree_prims(nodes, order, 0)) == list(range(len(b)))
