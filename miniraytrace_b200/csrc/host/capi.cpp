@@ -238,19 +238,22 @@ MRT_API mrtResult mrtxTraceShadowRays(mrtEngine* e, const mrtxRay* rays, uint32_
 
 MRT_API mrtResult mrtxReadAccumulation(mrtEngine* e, double* dst, size_t dstSize, uint32_t* outSpp) {
     mrt::Engine* eng = unwrap(e);
-    if (!eng || !dst) return MRT_ERROR_INVALID_ARGUMENT;
+    if (!eng) return MRT_ERROR_INVALID_HANDLE;
+    if (!dst) return mrt::fail(MRT_ERROR_INVALID_ARGUMENT, "mrtxReadAccumulation: null destination");
     return guarded([&] { return eng->readAccumulation(dst, dstSize, outSpp); });
 }
 
 MRT_API mrtResult mrtxMeasureL2Bandwidth(mrtEngine* e, float* outGBs) {
     mrt::Engine* eng = unwrap(e);
-    if (!eng || !outGBs) return MRT_ERROR_INVALID_ARGUMENT;
+    if (!eng) return MRT_ERROR_INVALID_HANDLE;
+    if (!outGBs) return mrt::fail(MRT_ERROR_INVALID_ARGUMENT, "mrtxMeasureL2Bandwidth: null output");
     return guarded([&] { return eng->measureL2Bandwidth(outGBs); });
 }
 
 MRT_API mrtResult mrtxGetStats(mrtEngine* e, mrtxStats* out) {
     mrt::Engine* eng = unwrap(e);
-    if (!eng || !validStruct(out)) return MRT_ERROR_INVALID_ARGUMENT;
+    if (!eng) return MRT_ERROR_INVALID_HANDLE;
+    if (!validStruct(out)) return mrt::fail(MRT_ERROR_INVALID_ARGUMENT, "mrtxGetStats: bad mrtxStats");
     return guarded([&] {
         const mrtResult r = eng->flushPending();
         return r != MRT_SUCCESS ? r : eng->getStats(out);

@@ -123,6 +123,9 @@ def test_null_and_short_struct_handling(mrt_lib):
     lib.mrtResetAccumulation(None)
     assert lib.mrtxRenderFrames(None, 1, None) == abi.MRT_ERROR_INVALID_HANDLE
     assert lib.mrtxTraceRays(None, None, 0, None) == abi.MRT_ERROR_INVALID_HANDLE
+    assert lib.mrtxReadAccumulation(None, None, 0, None) == abi.MRT_ERROR_INVALID_HANDLE
+    assert lib.mrtxMeasureL2Bandwidth(None, None) == abi.MRT_ERROR_INVALID_HANDLE
+    assert lib.mrtxGetStats(None, None) == abi.MRT_ERROR_INVALID_HANDLE
     assert lib.mrtGetLastErrorMessage() is not None
 
 
