@@ -231,8 +231,11 @@ MRT_API mrtResult mrtxBuildMeshBvh(mrtEngine* engine, const float* positions, ui
  * work runs on that GPU and is asynchronous: results are complete when
  * `stream` reaches the point of this call. The first call on each GPU does
  * a one-time set-up (it looks up the scratch array's device address with
- * cudaGetSymbolAddress and loads the kernels); make that first call before
- * any stream capture. The scratch is shared by every call on a GPU: calls
+ * cudaGetSymbolAddress and loads the kernels). After it, a call only
+ * launches kernels on `stream`: the sin(theta) table travels in their
+ * parameters, so the call does not wait for `stream` and keeps no reference
+ * to host memory once it returns. Capturing calls into a CUDA graph is not
+ * tested. The scratch is shared by every call on a GPU: calls
  * that overlap in time (other threads, other streams) race and corrupt
  * each other's results, so serialise them. Nothing in the scratch has to
  * be cleared between calls. */

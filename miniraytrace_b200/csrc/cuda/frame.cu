@@ -3,6 +3,8 @@
 // the FP64 add used to combine replicas.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <cstring>
 #include <mutex>
 
 #include "../../../include/mrt_ext.h"
@@ -160,6 +162,20 @@ constexpr int kNoAllocMaxDevices = 64;
 __device__ __align__(256) unsigned char g_envCdfScratch[size_t(kNoAllocMaxRows) * 16];
 std::mutex g_scratchMutex;
 unsigned char* g_scratchAddr[kNoAllocMaxDevices] = {};
+
+// The sin(theta) table reaches the scratch as kernel parameters, 1,000 rows
+// a launch (4,008 bytes with the pointer: within the 4 KiB parameter
+// limit), so a call neither waits for its stream, as a copy from pageable
+// host memory would, nor refers to the caller's memory once it returns.
+constexpr uint32_t kSinChunk = 1000;
+struct SinChunk {
+    uint32_t first, count;
+    float v[kSinChunk];
+};
+__global__ void sinChunkKernel(float* dst, SinChunk c) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < c.count) dst[c.first + i] = c.v[i];
+}
 }  // namespace
 
 extern "C" cudaError_t mrtcu_env_cdf_noalloc_setup(int device, unsigned char** scratch) {
@@ -174,6 +190,7 @@ extern "C" cudaError_t mrtcu_env_cdf_noalloc_setup(int device, unsigned char** s
         if ((e = cudaFuncGetAttributes(&fa, envCdfRowsKernel)) != cudaSuccess) return e;
         if ((e = cudaFuncGetAttributes(&fa, envCdfNormalizeKernel)) != cudaSuccess) return e;
         if ((e = cudaFuncGetAttributes(&fa, envCdfMarginalKernel)) != cudaSuccess) return e;
+        if ((e = cudaFuncGetAttributes(&fa, sinChunkKernel)) != cudaSuccess) return e;
         g_scratchAddr[device] = static_cast<unsigned char*>(addr);
     }
     *scratch = g_scratchAddr[device];
@@ -186,8 +203,15 @@ extern "C" cudaError_t mrtcu_env_cdf_noalloc(unsigned char* scratch, const float
     double* rowSums = reinterpret_cast<double*>(scratch);
     float* sinTheta = reinterpret_cast<float*>(scratch + size_t(kNoAllocMaxRows) * 8);
     float* rowInv = reinterpret_cast<float*>(scratch + size_t(kNoAllocMaxRows) * 12);
-    const cudaError_t e = cudaMemcpyAsync(sinTheta, hostSinTheta, size_t(h) * sizeof(float), cudaMemcpyHostToDevice, stream);
-    if (e != cudaSuccess) return e;
+    for (uint32_t first = 0; first < h; first += kSinChunk) {
+        SinChunk c{};
+        c.first = first;
+        c.count = std::min(kSinChunk, h - first);
+        std::memcpy(c.v, hostSinTheta + first, c.count * sizeof(float));
+        sinChunkKernel<<<(c.count + 255) / 256, 256, 0, stream>>>(sinTheta, c);
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
     return mrtcu_env_cdf(texels, sinTheta, w, h, cdf, rowSums, rowInv, integral, stream);
 }
 

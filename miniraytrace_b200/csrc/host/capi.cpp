@@ -378,7 +378,7 @@ MRT_API mrtResult mrtxBuildMeshBvh(mrtEngine* engine, const float* positions, ui
 // Allocation-free CDF: device pointers in and out, scratch in the static
 // device array of csrc/cuda/frame.cu. The sin(theta) table is the one
 // Engine::runEnvCdf builds (same float expression), held on this thread's
-// stack and copied into the scratch.
+// stack and handed to the device as kernel parameters.
 MRT_API mrtResult mrtxBuildEnvCdfNoAlloc(const float* devTexels, uint32_t w, uint32_t h, float* devCdfOut,
                                          float* devIntegralOut, void* stream) {
     if (!devTexels || !devCdfOut || !devIntegralOut || w == 0 || h == 0)

@@ -49,7 +49,8 @@ def test_scratch_reuse_across_sizes_and_default_stream(gpu):
     """A smaller map after a larger one: stale scratch rows must not leak."""
     import torch
     e = gpu.Engine(16, 16)
-    for w, h in ((512, 4096), (300, 100), (300, 100)):
+    # heights at, just past and below the 1,000-row parameter chunks
+    for w, h in ((512, 4096), (300, 100), (300, 100), (64, 1000), (64, 1001), (96, 2000)):
         sky = scenes.procedural_sky(w, h, sun_azim_deg=float(w % 90))
         ref_cdf, ref_integ = e.build_env_cdf(sky)
         tex, cdf, integ = device_buffers(torch, sky)
