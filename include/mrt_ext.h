@@ -220,25 +220,27 @@ MRT_API mrtResult mrtxBuildMeshBvh(mrtEngine* engine, const float* positions, ui
  * library, so maps are limited to MRTX_ENV_CDF_NOALLOC_MAX_HEIGHT rows
  * (any width); a taller map fails with MRT_ERROR_INVALID_ARGUMENT.
  *
- *   devTexels       w*h RGBA32F texels (16 bytes each), device memory
- *   devCdfOut       w*h + h floats, device memory: the same layout and
- *                   values mrtxBuildEnvCdf returns in cdfOut
- *   devIntegralOut  one float, device memory
+ *   devTexels       w*h RGBA32F texels (16 bytes each), device memory,
+ *                   16-byte aligned (read as 16-byte vectors)
+ *   devCdfOut       w*h + h floats, device memory, 4-byte aligned: the
+ *                   same layout and values mrtxBuildEnvCdf returns in cdfOut
+ *   devIntegralOut  one float, device memory, 4-byte aligned
  *   stream          a cudaStream_t on the GPU that owns devTexels, or NULL
  *                   for that GPU's legacy default stream
  *
  * All three pointers must be device (or managed) memory of one GPU; the
  * work runs on that GPU and is asynchronous: results are complete when
  * `stream` reaches the point of this call. The first call on each GPU does
- * a one-time set-up (it looks up the scratch array's device address with
- * cudaGetSymbolAddress and loads the kernels). After it, a call only
- * launches kernels on `stream`: the sin(theta) table travels in their
- * parameters, so the call does not wait for `stream` and keeps no reference
- * to host memory once it returns. Capturing calls into a CUDA graph is not
- * tested. The scratch is shared by every call on a GPU: calls
- * that overlap in time (other threads, other streams) race and corrupt
- * each other's results, so serialise them. Nothing in the scratch has to
- * be cleared between calls. */
+ * a one-time set-up (it loads the kernels), so make that first call before
+ * any stream capture. Every call looks up the scratch array's device
+ * address with cudaGetSymbolAddress (no allocation), so a device reset
+ * between calls leaves no stale address behind. A call then only launches
+ * kernels on `stream`: the sin(theta) table travels in their parameters,
+ * so the call does not wait for `stream` and keeps no reference to host
+ * memory once it returns. The scratch is shared by every call on a GPU:
+ * calls that overlap in time (other threads, other streams) race and
+ * corrupt each other's results, so serialise them. Nothing in the scratch
+ * has to be cleared between calls. */
 MRT_API mrtResult mrtxBuildEnvCdfNoAlloc(const float* devTexels, uint32_t w, uint32_t h, float* devCdfOut,
                                          float* devIntegralOut, void* stream);
 

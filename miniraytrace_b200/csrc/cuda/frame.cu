@@ -160,40 +160,46 @@ namespace {
 constexpr uint32_t kNoAllocMaxRows = MRTX_ENV_CDF_NOALLOC_MAX_HEIGHT;
 constexpr int kNoAllocMaxDevices = 64;
 __device__ __align__(256) unsigned char g_envCdfScratch[size_t(kNoAllocMaxRows) * 16];
-std::mutex g_scratchMutex;
-unsigned char* g_scratchAddr[kNoAllocMaxDevices] = {};
+std::mutex g_loadMutex;
+bool g_kernelsLoaded[kNoAllocMaxDevices] = {};
 
 // The sin(theta) table reaches the scratch as kernel parameters, 1,000 rows
-// a launch (4,008 bytes with the pointer: within the 4 KiB parameter
-// limit), so a call neither waits for its stream, as a copy from pageable
-// host memory would, nor refers to the caller's memory once it returns.
+// a launch (4,016 bytes with the destination pointer: within the 4 KiB
+// parameter limit), so a call neither waits for its stream, as a copy from
+// pageable host memory would, nor refers to the caller's memory once it
+// returns.
 constexpr uint32_t kSinChunk = 1000;
 struct SinChunk {
     uint32_t first, count;
     float v[kSinChunk];
 };
+static_assert(sizeof(SinChunk) + sizeof(float*) <= 4096, "kernel parameters above 4 KiB");
 __global__ void sinChunkKernel(float* dst, SinChunk c) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < c.count) dst[c.first + i] = c.v[i];
 }
 }  // namespace
 
+// The scratch array's device address on the current device. It is looked up
+// on every call (the lookup allocates nothing once the module is loaded), so
+// a context that was torn down and created again (cudaDeviceReset) never
+// sees a stale address. The kernels are loaded once per device, so later
+// calls load no code.
 extern "C" cudaError_t mrtcu_env_cdf_noalloc_setup(int device, unsigned char** scratch) {
     if (device < 0 || device >= kNoAllocMaxDevices) return cudaErrorInvalidDevice;
-    std::lock_guard<std::mutex> lock(g_scratchMutex);
-    if (!g_scratchAddr[device]) {
-        void* addr = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&addr, g_envCdfScratch);
-        if (e != cudaSuccess) return e;
-        // load the three kernels now, so later calls load no code either
+    void* addr = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&addr, g_envCdfScratch);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lock(g_loadMutex);
+    if (!g_kernelsLoaded[device]) {
         cudaFuncAttributes fa;
         if ((e = cudaFuncGetAttributes(&fa, envCdfRowsKernel)) != cudaSuccess) return e;
         if ((e = cudaFuncGetAttributes(&fa, envCdfNormalizeKernel)) != cudaSuccess) return e;
         if ((e = cudaFuncGetAttributes(&fa, envCdfMarginalKernel)) != cudaSuccess) return e;
         if ((e = cudaFuncGetAttributes(&fa, sinChunkKernel)) != cudaSuccess) return e;
-        g_scratchAddr[device] = static_cast<unsigned char*>(addr);
+        g_kernelsLoaded[device] = true;
     }
-    *scratch = g_scratchAddr[device];
+    *scratch = static_cast<unsigned char*>(addr);
     return cudaSuccess;
 }
 

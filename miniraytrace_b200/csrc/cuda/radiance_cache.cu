@@ -398,6 +398,11 @@ __global__ void __launch_bounds__(kTile* kQueryGroups, 3) tcQueryKernel(McachePa
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(*tmemSlot),
                      "r"(kTmemCols * kQueryGroups)
                      : "memory");
+    // A wait that gave up is fatal for the cache, not a retryable error: the
+    // MMA it waited for may still be writing the tensor-memory columns freed
+    // above, and a later CTA on this SM may be given them. The engine
+    // therefore discards every output of the launch (and the accumulation
+    // holding them) and never launches the cache kernels again.
     if (!ok && r == 0) atomicOr(C.status, 1u);
 }
 
@@ -599,6 +604,8 @@ __global__ void __launch_bounds__(kTile, 1) tcTrainKernel(McacheParams C, const 
     if (warp == 0)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2u * kTmemCols)
                      : "memory");
+    // Fatal for the cache, as in the query kernel: the engine discards the
+    // launch's results and runs no cache kernel again.
     if (!ok && t == 0) atomicOr(C.status, 1u);
 }
 

@@ -387,6 +387,14 @@ MRT_API mrtResult mrtxBuildEnvCdfNoAlloc(const float* devTexels, uint32_t w, uin
         return mrt::fail(MRT_ERROR_INVALID_ARGUMENT, "mrtxBuildEnvCdfNoAlloc: height " + std::to_string(h) +
                                                          " exceeds the maximum of " +
                                                          std::to_string(MRTX_ENV_CDF_NOALLOC_MAX_HEIGHT) + " rows");
+    // The row kernel reads texels as 16-byte vectors and the outputs are
+    // written as floats: a pointer carved out of a caller's pool at a finer
+    // offset would fault on the device (a sticky error that ends the
+    // caller's context), so it is refused here, before anything launches.
+    if (reinterpret_cast<uintptr_t>(devTexels) % 16 != 0 || reinterpret_cast<uintptr_t>(devCdfOut) % 4 != 0 ||
+        reinterpret_cast<uintptr_t>(devIntegralOut) % 4 != 0)
+        return mrt::fail(MRT_ERROR_INVALID_ARGUMENT,
+                         "mrtxBuildEnvCdfNoAlloc: devTexels must be 16-byte aligned and the outputs 4-byte aligned");
     int device = -1;
     for (const void* ptr : {static_cast<const void*>(devTexels), static_cast<const void*>(devCdfOut),
                             static_cast<const void*>(devIntegralOut)}) {

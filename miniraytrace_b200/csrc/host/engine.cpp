@@ -1090,6 +1090,11 @@ mrtResult Engine::completePending() {
     m_stats.nodeBytes = sizeof(MrtWideNode);
     m_stats.triBytes = 48;
     m_frameIndex += n;
+    if (m_inFlightCache) {  // the last wave's cache kernels (earlier waves were checked between waves)
+        uint32_t status = 0;
+        MRT_CUDA(cudaMemcpy(&status, m_cache.params.status, sizeof(status), cudaMemcpyDeviceToHost));
+        MRT_TRY(cacheStatus(status));
+    }
     return MRT_SUCCESS;
 }
 
@@ -1418,6 +1423,7 @@ mrtResult Engine::ensureCache() {
 mrtResult Engine::setRadianceCache(const mrtxRadianceCacheDesc& d) {
     MRT_TRY(checkAlive());
     MRT_TRY(flushPending());
+    if (m_cache.failed && d.enabled) return cacheStatus(0);
     const bool reinit = m_cache.allocated && d.seed != m_cache.seed;
     m_cache.trainingPaths = d.trainingPaths;  // 0: a 32nd of the pixels (cacheWaveBuffers)
     m_cache.stepsPerSample = d.stepsPerSample ? d.stepsPerSample : 1u;
@@ -1440,6 +1446,7 @@ mrtResult Engine::setRadianceCache(const mrtxRadianceCacheDesc& d) {
 
 mrtResult Engine::cacheQuery(const float* features, uint32_t n, float* rgb) {
     MRT_TRY(checkAlive());
+    MRT_TRY(cacheStatus(0));
     MRT_TRY(guard(ensureCache()));
     if (n == 0) return MRT_SUCCESS;
     MRT_TRY(up(m_cache.in, features, size_t(n) * 16 * sizeof(float)));
@@ -1455,6 +1462,7 @@ mrtResult Engine::cacheQuery(const float* features, uint32_t n, float* rgb) {
 
 mrtResult Engine::cacheTrain(const float* features, const float* targets, uint32_t n, uint32_t steps, float* loss) {
     MRT_TRY(checkAlive());
+    MRT_TRY(cacheStatus(0));
     MRT_TRY(guard(ensureCache()));
     if (n == 0 || steps == 0) return MRT_SUCCESS;
     MRT_TRY(m_cache.in.ensure(size_t(n) * 19 * sizeof(float)));
@@ -1493,10 +1501,21 @@ mrtResult Engine::cacheParams(float* gridOut, float* mlpOut, const float* gridIn
     return MRT_SUCCESS;
 }
 
-// A query kernel whose tensor-core wait gave up leaves bit 0 of the status
-// word set (its outputs are incomplete).
+// A cache kernel whose tensor-core wait gave up leaves bit 0 of the status
+// word set. That is fatal for the cache: the MMA it waited for may still
+// have been writing tensor memory when the CTA freed it, so every output of
+// the launch is suspect. The accumulation (which may hold its predictions)
+// is discarded, the cache mode is switched off, and every later cache call
+// of this engine fails.
 mrtResult Engine::cacheStatus(uint32_t status) {
-    if (status & 1u) return fail(MRT_ERROR_UNKNOWN, "radiance cache: a tensor-core wait timed out");
+    if (status & 1u) {
+        m_cache.failed = true;
+        m_cache.enabled = false;
+        resetAccumulation();
+    }
+    if (m_cache.failed)
+        return fail(MRT_ERROR_UNKNOWN, "radiance cache: a tensor-core wait timed out; the cache is disabled and "
+                                       "the accumulation was discarded");
     return MRT_SUCCESS;
 }
 

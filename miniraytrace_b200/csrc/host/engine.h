@@ -135,6 +135,11 @@ private:
         MrtCacheArgs args{};
         McacheParams params{};
         bool allocated = false, enabled = false;
+        // Set once a tensor-core wait of a cache kernel gave up: that MMA may
+        // still have been writing tensor memory when its CTA freed it, so no
+        // cache output of the launch is trusted and no cache kernel runs again
+        // in this engine.
+        bool failed = false;
         uint32_t trainingPaths = 0, stepsPerSample = 1, seed = 1, samplesPerUpdate = 4, trainingVertices = 0;
         float lr = 1e-2f;
         float lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};

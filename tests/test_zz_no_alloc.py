@@ -77,3 +77,27 @@ def test_rejects_oversized_and_host_inputs(gpu):
         gpu.build_env_cdf_no_alloc(host.ctypes.data, 4, 4, cdf.data_ptr(), integ.data_ptr())
     assert err.value.code == abi.MRT_ERROR_INVALID_ARGUMENT
     assert "device memory" in str(err.value)
+
+
+def test_rejects_misaligned_pointers_before_launching(gpu):
+    """A texel pointer carved from a pool at a 4-byte offset would fault on
+    the device's 16-byte loads; the call refuses it on the host instead, and
+    the context stays usable for a correct call afterwards."""
+    import torch
+    w, h = 64, 32
+    sky = scenes.procedural_sky(w, h)
+    tex, cdf, integ = device_buffers(torch, sky)
+    big = torch.zeros((h * w * 4 + 4,), dtype=torch.float32, device="cuda")
+    for args in ((big.data_ptr() + 4, cdf.data_ptr(), integ.data_ptr()),
+                 (tex.data_ptr(), cdf.data_ptr() + 2, integ.data_ptr()),
+                 (tex.data_ptr(), cdf.data_ptr(), integ.data_ptr() + 1)):
+        with pytest.raises(gpu.MrtError) as err:
+            gpu.build_env_cdf_no_alloc(args[0], w, h, args[1], args[2])
+        assert err.value.code == abi.MRT_ERROR_INVALID_ARGUMENT
+        assert "aligned" in str(err.value)
+    e = gpu.Engine(16, 16)
+    ref_cdf, _ = e.build_env_cdf(sky)
+    e.close()
+    gpu.build_env_cdf_no_alloc(tex.data_ptr(), w, h, cdf.data_ptr(), integ.data_ptr(), 0)
+    torch.cuda.synchronize()
+    assert np.array_equal(cdf.cpu().numpy(), ref_cdf)
