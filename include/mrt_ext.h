@@ -113,6 +113,27 @@ MRT_API mrtResult mrtxBuildEnvCdf(mrtEngine*, const float* rgba, uint32_t w, uin
  * is the reference stream (reference pathtrace.comp:105). Resets accumulation. */
 MRT_API mrtResult mrtxSetSampleStream(mrtEngine*, uint32_t offset, uint32_t stride);
 
+/* Node visits one ray's traversal may make before it gives up (0 restores
+ * the default, 2^22, which a well-formed BVH never approaches). A ray that
+ * gives up, overflows its traversal stack or meets an out-of-range scene
+ * index makes the call that traced it fail with MRT_ERROR_UNKNOWN instead of
+ * hanging or returning a silently wrong image; a render call then resets
+ * the accumulation (its samples are not kept) and the engine stays usable.
+ * The reference has no counterpart: its shader loops until its stack
+ * empties (intersect.glsl:48-125) and every device error aborts the process
+ * (core/src/gpu/GpuContext.hpp:22-31). */
+MRT_API mrtResult mrtxSetTraversalBudget(mrtEngine*, uint32_t maxVisits);
+
+/* Test hook for allocation failures: after this call the next
+ * `succeedFirst` device or pinned-host allocations of the library succeed
+ * and every later one fails as MRT_ERROR_OUT_OF_MEMORY, in every engine of
+ * the process; succeedFirst < 0 turns the injection off. A call that meets
+ * the failure returns MRT_ERROR_OUT_OF_MEMORY and leaves the engine usable:
+ * the scene stays dirty, so the next commit redoes the work. Nothing is
+ * done to the GPU. The reference maps std::bad_alloc the same way
+ * (capi/src/capi.cpp:116-120) but has no injection. */
+MRT_API mrtResult mrtxInjectAllocationFailure(int32_t succeedFirst);
+
 /* Copy the FP64 accumulation buffer (layout as mrtxReadAccumulation) to a
  * device pointer on this engine's GPU, or add a device buffer of the same
  * layout into it (accumulate != 0). Used to reduce replicas' samples. */

@@ -343,6 +343,11 @@ class Engine:
     def set_sample_stream(self, offset: int, stride: int):
         _check(self.lib.mrtxSetSampleStream(self.h, offset, stride), "mrtxSetSampleStream")
 
+    def set_traversal_budget(self, max_visits: int):
+        """mrtxSetTraversalBudget: node visits per ray before the traversal
+        gives up and the call fails (0 = the default, 2^22)."""
+        _check(self.lib.mrtxSetTraversalBudget(self.h, max_visits), "mrtxSetTraversalBudget")
+
     def copy_accumulation_device(self, dev_ptr: int, nbytes: int, accumulate: bool):
         _check(self.lib.mrtxCopyAccumulationDevice(self.h, C.c_void_p(dev_ptr), nbytes, 1 if accumulate else 0),
                "mrtxCopyAccumulationDevice")
@@ -357,6 +362,13 @@ def build_env_cdf_no_alloc(dev_texels: int, width: int, height: int, dev_cdf: in
     lib = load_library()
     _check(lib.mrtxBuildEnvCdfNoAlloc(C.c_void_p(dev_texels), width, height, C.c_void_p(dev_cdf),
                                       C.c_void_p(dev_integral), C.c_void_p(stream)), "mrtxBuildEnvCdfNoAlloc")
+
+
+def inject_allocation_failure(succeed_first: int):
+    """mrtxInjectAllocationFailure: the next `succeed_first` device or
+    pinned-host allocations succeed, later ones fail as out of memory;
+    a negative value turns the injection off."""
+    _check(load_library().mrtxInjectAllocationFailure(succeed_first), "mrtxInjectAllocationFailure")
 
 
 def render_batch(engines, spp):

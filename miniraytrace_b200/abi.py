@@ -180,6 +180,8 @@ FUNCTIONS = [
     ("mrtxBuildEnvCdf", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p,
                                   C.POINTER(C.c_float)]),
     ("mrtxSetSampleStream", C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32]),
+    ("mrtxSetTraversalBudget", C.c_int, [C.c_void_p, C.c_uint32]),
+    ("mrtxInjectAllocationFailure", C.c_int, [C.c_int32]),
     ("mrtxCopyAccumulationDevice", C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, C.c_int32]),
     ("mrtxBuildWideBvh", C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p,
                                    C.POINTER(C.c_uint32)]),

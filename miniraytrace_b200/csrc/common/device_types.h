@@ -104,6 +104,8 @@ typedef struct MrtTexture {
 
 enum { MRT_FLAG_HAS_ENV = 1u, MRT_FLAG_ORTHO = 4u };
 
+#define MRT_DEFAULT_MAX_VISITS (1u << 22)
+
 // Radiance-cache mode of one wave (shade kernel's cache instantiation):
 // paths other than training paths stop at their second surface vertex and
 // append a query there (16 features; beta and the slot); training paths
@@ -140,6 +142,15 @@ typedef struct MrtFrameParams {
     // offset 0, stride 1, pathtrace.comp:105).
     uint32_t streamOffset, streamStride;
     uint32_t nodeCount, instanceCount, triCount, materialCount;
+    // Node visits one traversal may make before it gives up and sets bit 0
+    // of errorFlags. A well-formed BVH never gets near the default
+    // (MRT_DEFAULT_MAX_VISITS); the bound only turns a malformed tree into
+    // an error instead of an endless loop.
+    uint32_t maxVisits, pad0;
+    // sRGB decode of an 8-bit channel value k, (k / 255) -> linear, 256
+    // entries built on the host (the decode is a double-precision power;
+    // the table keeps it off the GPU and gives the same bits).
+    const float* srgbLut;
     // scene arrays (device pointers)
     const MrtWideNode* nodes;  // 8-wide BVH: every BLAS, then the TLAS
     const float4* triVerts;

@@ -63,7 +63,7 @@ MRT_DEV Surface makeSurface(const MrtFrameParams& P, float3 rayDir, const HitRec
         const float3 tanH = b0 * f3(ta) + b1 * f3(tb) + b2 * f3(tc);
         const float tanW = b0 * ta.w + b1 * tb.w + b2 * tc.w;
         const float3 tangent = normalize(xformDir(in->o2w, tanH));
-        const float4 tx = sampleBilinear(P.textures[m.tex[3]], s.uv.x, s.uv.y);
+        const float4 tx = sampleBilinear(P.textures[m.tex[3]], P.srgbLut, s.uv.x, s.uv.y);
         const float3 tn = f3(tx.x, tx.y, tx.z) * 2.0f - f3(1.0f);
         const float3 bitan = cross(nShade, tangent) * tanW;
         nShade = normalize(tangent * tn.x + bitan * tn.y + nShade * tn.z);
@@ -75,7 +75,7 @@ MRT_DEV Surface makeSurface(const MrtFrameParams& P, float3 rayDir, const HitRec
 }
 
 MRT_DEV float3 texRgb(const MrtFrameParams& P, int slot, float2 uv) {
-    const float4 c = sampleBilinear(P.textures[slot], uv.x, uv.y);
+    const float4 c = sampleBilinear(P.textures[slot], P.srgbLut, uv.x, uv.y);
     return f3(c.x, c.y, c.z);
 }
 

@@ -50,39 +50,35 @@ MRT_DEV void buildOnb(float3 n, float3& t, float3& b) {
 }
 
 // ---- textures: bilinear, LOD 0, REPEAT in u and v -----------------------------------
-// sRGB decode of an 8-bit channel: c <= 0.04045 ? c / 12.92 :
-// ((c + 0.055) / 1.055)^2.4 with the power taken in double and rounded.
-MRT_DEV float srgbToLinear(float c) {
-    return c <= 0.04045f ? c / 12.92f : float(pow(double((c + 0.055f) / 1.055f), 2.4));
-}
-MRT_DEV float4 texelFetch(const MrtTexture& t, uint32_t x, uint32_t y) {
+// An 8-bit channel k decodes to k / 255; sRGB textures then go through
+// c <= 0.04045 ? c / 12.92 : ((c + 0.055) / 1.055)^2.4, which is looked up
+// in the 256-entry table the engine builds on the host (srgbLut).
+MRT_DEV float4 texelFetch(const MrtTexture& t, const float* __restrict__ srgbLut, uint32_t x, uint32_t y) {
     const size_t i = size_t(y) * t.width + x;
     if (t.format == MRT_DTEX_RGBA32F) return ldg4(reinterpret_cast<const float4*>(t.texels) + i);
     const uint32_t p = __ldg(reinterpret_cast<const uint32_t*>(t.texels) + i);
-    float4 c = make_float4(float(p & 255u) / 255.0f, float((p >> 8) & 255u) / 255.0f,
-                           float((p >> 16) & 255u) / 255.0f, float(p >> 24) / 255.0f);
-    if (t.format == MRT_DTEX_RGBA8_SRGB) {
-        c.x = srgbToLinear(c.x);
-        c.y = srgbToLinear(c.y);
-        c.z = srgbToLinear(c.z);
-    }
-    return c;
+    if (t.format == MRT_DTEX_RGBA8_SRGB)
+        return make_float4(__ldg(srgbLut + (p & 255u)), __ldg(srgbLut + ((p >> 8) & 255u)),
+                           __ldg(srgbLut + ((p >> 16) & 255u)), float(p >> 24) / 255.0f);
+    return make_float4(float(p & 255u) / 255.0f, float((p >> 8) & 255u) / 255.0f, float((p >> 16) & 255u) / 255.0f,
+                       float(p >> 24) / 255.0f);
 }
+// floor(f) mod n for an integral f (REPEAT addressing): a 32-bit remainder
+// while f fits an int; beyond that fmodf, whose result is exact, gives the
+// same residue.
 MRT_DEV uint32_t wrapIndex(float f, uint32_t n) {
-    // floor(f) mod n, for |f| well inside the int range
-    long long i = (long long)f;
-    long long m = i % (long long)n;
-    return uint32_t(m < 0 ? m + n : m);
+    const int m = fabsf(f) < 2147483648.0f ? int(f) % int(n) : int(fmodf(f, float(n)));
+    return uint32_t(m < 0 ? m + int(n) : m);
 }
-MRT_DEV float4 sampleBilinear(const MrtTexture& t, float u, float v) {
+MRT_DEV float4 sampleBilinear(const MrtTexture& t, const float* __restrict__ srgbLut, float u, float v) {
     if (t.texels == nullptr) return make_float4(1.0f, 1.0f, 1.0f, 1.0f);
     const float fx = u * float(t.width) - 0.5f, fy = v * float(t.height) - 0.5f;
     const float x0f = floorf(fx), y0f = floorf(fy);
     const float ax = fx - x0f, ay = fy - y0f;
     const uint32_t x0 = wrapIndex(x0f, t.width), x1 = x0 + 1 == t.width ? 0 : x0 + 1;
     const uint32_t y0 = wrapIndex(y0f, t.height), y1 = y0 + 1 == t.height ? 0 : y0 + 1;
-    const float4 t00 = texelFetch(t, x0, y0), t10 = texelFetch(t, x1, y0);
-    const float4 t01 = texelFetch(t, x0, y1), t11 = texelFetch(t, x1, y1);
+    const float4 t00 = texelFetch(t, srgbLut, x0, y0), t10 = texelFetch(t, srgbLut, x1, y0);
+    const float4 t01 = texelFetch(t, srgbLut, x0, y1), t11 = texelFetch(t, srgbLut, x1, y1);
     const float w00 = (1.0f - ax) * (1.0f - ay), w10 = ax * (1.0f - ay), w01 = (1.0f - ax) * ay, w11 = ax * ay;
     return make_float4(w00 * t00.x + w10 * t10.x + w01 * t01.x + w11 * t11.x,
                        w00 * t00.y + w10 * t10.y + w01 * t01.y + w11 * t11.y,

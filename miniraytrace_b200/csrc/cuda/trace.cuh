@@ -29,10 +29,6 @@
 #include "vec.cuh"
 
 #define MRT_EPS_RAY 1e-4f
-// Upper bound on node visits of one traversal. A well-formed BVH never gets
-// near it; it only turns a malformed tree into an error flag instead of an
-// endless loop.
-#define MRT_MAX_VISITS (1u << 22)
 
 struct TraceRay {
     float3 o, d;
@@ -77,10 +73,23 @@ MRT_DEV float3 safeInv(float3 d) {
               d.z != 0.0f ? 1.0f / d.z : copysignf(big, d.z));
 }
 
+// a * b - c * d by Kahan's algorithm: w = c d rounded, e = w - c d exactly
+// (one FMA), result = (a b - w) + e. Its error is at most 2 ulp (Jeannerod,
+// Louvet and Muller, Math. Comp. 2013), so the sign is exact and the result
+// is zero exactly when a b = c d. Single precision throughout.
+MRT_DEV float diffOfProducts(float a, float b, float c, float d) {
+    const float w = __fmul_rn(c, d);
+    const float e = __fmaf_rn(-c, d, w);
+    const float f = __fmaf_rn(a, b, -w);
+    return __fadd_rn(f, e);
+}
+
 // Watertight test (Woop et al. 2013). Accepts t in (1e-4, tMax); both faces.
 // The edge functions use explicit round-to-nearest products with no fused
 // multiply-add, so an edge shared by two triangles evaluates to exactly
-// opposite values from both sides.
+// opposite values from both sides. When one of them rounds to zero they are
+// re-evaluated with correctly signed differences of products, so a ray on
+// an edge is decided by the exact sign of every edge function.
 MRT_DEV bool hitTriangle(const float4* __restrict__ tv, uint32_t tri, float3 o, const Shear& s, float tMax, float& tOut,
                          float& uOut, float& vOut) {
     const float4 p0 = ldg4(tv + 3 * tri), p1 = ldg4(tv + 3 * tri + 1), p2 = ldg4(tv + 3 * tri + 2);
@@ -95,10 +104,10 @@ MRT_DEV bool hitTriangle(const float4* __restrict__ tv, uint32_t tri, float3 o, 
     float U = __fsub_rn(__fmul_rn(Cx, By), __fmul_rn(Cy, Bx));
     float V = __fsub_rn(__fmul_rn(Ax, Cy), __fmul_rn(Ay, Cx));
     float W = __fsub_rn(__fmul_rn(Bx, Ay), __fmul_rn(By, Ax));
-    if (U == 0.0f || V == 0.0f || W == 0.0f) {  // exact fallback on an edge
-        U = float(double(Cx) * double(By) - double(Cy) * double(Bx));
-        V = float(double(Ax) * double(Cy) - double(Ay) * double(Cx));
-        W = float(double(Bx) * double(Ay) - double(By) * double(Ax));
+    if (U == 0.0f || V == 0.0f || W == 0.0f) {  // exactly signed fallback on an edge
+        U = diffOfProducts(Cx, By, Cy, Bx);
+        V = diffOfProducts(Ax, Cy, Ay, Cx);
+        W = diffOfProducts(Bx, Ay, By, Ax);
     }
     if ((U < 0.0f || V < 0.0f || W < 0.0f) && (U > 0.0f || V > 0.0f || W > 0.0f)) return false;
     const float det = U + V + W;
@@ -384,7 +393,7 @@ MRT_DEV int travNodeStep(const MrtFrameParams& P, WideTrav& T, WideStack& stack,
             continue;
         }
         if (T.g.nodeBits & 0xff000000u) {
-            if (++T.visits > MRT_MAX_VISITS) {
+            if (++T.visits > P.maxVisits) {
                 T.ok = false;
                 return kTravDone;
             }

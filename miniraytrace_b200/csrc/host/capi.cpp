@@ -273,6 +273,17 @@ MRT_API mrtResult mrtxSetSampleStream(mrtEngine* e, uint32_t offset, uint32_t st
     return guarded([&] { return eng->setSampleStream(offset, stride); });
 }
 
+MRT_API mrtResult mrtxSetTraversalBudget(mrtEngine* e, uint32_t maxVisits) {
+    mrt::Engine* eng = unwrap(e);
+    if (!eng) return MRT_ERROR_INVALID_HANDLE;
+    return guarded([&] { return eng->setTraversalBudget(maxVisits); });
+}
+
+MRT_API mrtResult mrtxInjectAllocationFailure(int32_t succeedFirst) {
+    mrt::setAllocationFailureInjection(succeedFirst);
+    return MRT_SUCCESS;
+}
+
 MRT_API mrtResult mrtxCopyAccumulationDevice(mrtEngine* e, void* devPtr, size_t bytes, int32_t accumulate) {
     mrt::Engine* eng = unwrap(e);
     if (!eng) return MRT_ERROR_INVALID_HANDLE;

@@ -32,6 +32,13 @@ mrtResult fail(mrtResult code, const std::string& msg);
 mrtResult fromCuda(cudaError_t e, const char* what);
 bool isStickyCudaError(cudaError_t e);
 
+// Allocation-failure injection for tests (mrtxInjectAllocationFailure):
+// with a budget n >= 0, the next n device or pinned-host allocations
+// succeed and every later one fails as out of memory, until the budget is
+// set back to -1. allocationFailureInjected() is asked at each allocation.
+void setAllocationFailureInjection(int64_t succeedFirst);
+bool allocationFailureInjected();
+
 }  // namespace mrt
 
 // Evaluate a CUDA call; on failure record it and return the mapped result

@@ -3,6 +3,7 @@
 #include "engine.h"
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstring>
@@ -16,6 +17,21 @@ namespace mrt {
 
 // ---------------------------------------------------------------- buffers --
 
+namespace {
+std::atomic<int64_t> g_allocBudget{-1};  // -1: no injected failures
+}
+
+void setAllocationFailureInjection(int64_t succeedFirst) { g_allocBudget.store(succeedFirst < 0 ? -1 : succeedFirst); }
+
+bool allocationFailureInjected() {
+    int64_t v = g_allocBudget.load();
+    while (v >= 0) {
+        if (v == 0) return true;
+        if (g_allocBudget.compare_exchange_weak(v, v - 1)) return false;
+    }
+    return false;
+}
+
 mrtResult DeviceBuffer::ensure(size_t n) {
     n = std::max<size_t>(n, 16);
     if (ptr && bytes >= n) return MRT_SUCCESS;
@@ -24,6 +40,7 @@ mrtResult DeviceBuffer::ensure(size_t n) {
     if (ptr) cudaFree(ptr);
     ptr = nullptr;
     bytes = 0;
+    if (allocationFailureInjected()) return fromCuda(cudaErrorMemoryAllocation, "cudaMalloc (injected failure)");
     MRT_CUDA(cudaMalloc(&ptr, cap));
     bytes = cap;
     return MRT_SUCCESS;
@@ -142,6 +159,7 @@ mrtResult Engine::up(DeviceBuffer& b, const void* src, size_t n) {
 // bound by the host threads' copy).
 mrtResult Engine::uploadStaged(void* dst, const void* src, size_t n) {
     if (!m_stage) {
+        if (allocationFailureInjected()) return fromCuda(cudaErrorMemoryAllocation, "cudaMallocHost (injected failure)");
         MRT_CUDA(cudaMallocHost(&m_stage, kStageChunk * kStageSlots));
         for (auto& ev : m_stageCopyEvents) MRT_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
     }
@@ -232,6 +250,15 @@ mrtResult Engine::init(const mrtEngineDesc& desc) {
     std::vector<MrtTexture> table(MRT_MAX_TEXTURES);
     std::memset(table.data(), 0, table.size() * sizeof(MrtTexture));
     MRT_TRY(m_texTable.upload(table.data(), table.size() * sizeof(MrtTexture), m_stream));
+    // sRGB decode of the 256 channel values, with the same expression as the
+    // sampler's format conversion in the CPU evaluation of the shaders
+    // (power in double, rounded to float); the kernels look it up
+    float lut[256];
+    for (int k = 0; k < 256; ++k) {
+        const float c = float(k) / 255.0f;
+        lut[k] = c <= 0.04045f ? c / 12.92f : float(std::pow(double((c + 0.055f) / 1.055f), 2.4));
+    }
+    MRT_TRY(m_srgbLut.upload(lut, sizeof(lut), m_stream));
     m_texGeneration.assign(MRT_MAX_TEXTURES, 0);
     const float black[4] = {0, 0, 0, 1};
     MRT_TRY(m_envTexels.upload(black, sizeof(black), m_stream));
@@ -299,11 +326,11 @@ mrtResult Engine::guard(mrtResult r) {
 
 mrtResult Engine::allocateFrame() {
     const size_t pixels = size_t(m_settings.width) * m_settings.height;
+    m_waveSamples = 0;  // wave slots depend on the frame size
     MRT_TRY(m_accum.ensure(pixels * 32));
     MRT_CUDA(cudaMemsetAsync(m_accum.ptr, 0, pixels * 32, m_stream));
     MRT_TRY(m_out32.ensure(pixels * 16));
     MRT_TRY(m_out8.ensure(pixels * 4));
-    m_waveSamples = 0;  // wave slots depend on the frame size
     return MRT_SUCCESS;
 }
 
@@ -325,6 +352,11 @@ mrtResult Engine::ensureWave(uint32_t samples) {
     const uint64_t slots = pixels * k;
     if (slots > 0xffffffffull) return fail(MRT_ERROR_INVALID_ARGUMENT, "frame too large for one wave");
     const size_t bytes = size_t(slots) * kWaveBytesPerSlot + 64;
+    // growing frees the old allocation first: forget the carved pointers
+    // before, so a failed allocation leaves no wave state that points into
+    // freed memory (the next call allocates again)
+    m_waveSamples = 0;
+    m_waveState = MrtWaveState{};
     MRT_TRY(m_wave.ensure(bytes));
     char* base = static_cast<char*>(m_wave.ptr);
     auto carve = [&](size_t n) {
@@ -912,6 +944,8 @@ void Engine::fillParams(MrtFrameParams& p) const {
     p.instanceCount = m_instanceCount;
     p.triCount = m_triCount;
     p.materialCount = m_materialCount;
+    p.maxVisits = m_maxVisits ? m_maxVisits : MRT_DEFAULT_MAX_VISITS;
+    p.srgbLut = m_srgbLut.as<float>();
     p.nodes = m_nodes.as<MrtWideNode>();
     p.triVerts = m_triVerts.as<float4>();
     p.triIndex = m_triIndex.as<uint4>();
@@ -929,16 +963,31 @@ void Engine::fillParams(MrtFrameParams& p) const {
     p.rayCounters = m_rayCounters.as<unsigned long long>();
 }
 
+// A traversal that gave up (stack overflow, visit budget spent) or met an
+// out-of-range scene index leaves a bit in the error word. Its rays may have
+// missed geometry, so the call that launched them fails; for a render the
+// caller's accumulation is reset (the samples are not kept), and the engine
+// stays usable.
 mrtResult Engine::checkErrorFlags() {
     uint32_t flags = 0;
     MRT_CUDA(cudaMemcpyAsync(&flags, m_flags.ptr, sizeof(flags), cudaMemcpyDeviceToHost, m_stream));
     MRT_CUDA(cudaStreamSynchronize(m_stream));
     if (flags) {
         MRT_CUDA(cudaMemsetAsync(m_flags.ptr, 0, sizeof(uint32_t), m_stream));
-        log(LogLevel::Warn, std::string("traversal problem in at least one ray (flags ") + std::to_string(flags) +
-                                "): " + ((flags & 1u) ? "stack or visit budget exhausted " : "") +
-                                ((flags & 2u) ? "out-of-range scene index " : "") + "- affected rays may miss geometry");
+        MRT_CUDA(cudaStreamSynchronize(m_stream));
+        return fail(MRT_ERROR_UNKNOWN, std::string("traversal problem in at least one ray (flags ") +
+                                           std::to_string(flags) + "): " +
+                                           ((flags & 1u) ? "stack or node-visit budget exhausted " : "") +
+                                           ((flags & 2u) ? "out-of-range scene index " : "") +
+                                           "- affected rays may have missed geometry");
     }
+    return MRT_SUCCESS;
+}
+
+mrtResult Engine::setTraversalBudget(uint32_t maxVisits) {
+    MRT_TRY(checkAlive());
+    MRT_TRY(flushPending());
+    m_maxVisits = maxVisits;
     return MRT_SUCCESS;
 }
 
@@ -1077,7 +1126,10 @@ mrtResult Engine::completePending() {
     m_stats.cacheQueries = m_inFlightCache ? m_cacheQueries : 0;
     m_stats.cacheRecords = m_inFlightCache ? m_cacheRecords : 0;
     m_stats.cacheSteps = m_inFlightCache ? m_cacheSteps : 0;
-    MRT_TRY(guard(checkErrorFlags()));
+    if (const mrtResult fr = checkErrorFlags(); fr != MRT_SUCCESS) {
+        resetAccumulation();
+        return guard(fr);
+    }
     unsigned long long ctr[7];
     MRT_CUDA(cudaMemcpy(ctr, m_rayCounters.ptr, sizeof(ctr), cudaMemcpyDeviceToHost));
     m_stats.raysClosest = ctr[0];
@@ -1159,6 +1211,7 @@ mrtResult Engine::download(void* dst, const void* src, size_t bytes) {
         if (m_pinned) cudaFreeHost(m_pinned);
         m_pinned = nullptr;
         m_pinnedBytes = 0;
+        if (allocationFailureInjected()) return fromCuda(cudaErrorMemoryAllocation, "cudaMallocHost (injected failure)");
         MRT_CUDA(cudaMallocHost(&m_pinned, bytes));
         m_pinnedBytes = bytes;
     }

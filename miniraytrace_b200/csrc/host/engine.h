@@ -63,6 +63,7 @@ public:
     mrtResult measureL2Bandwidth(float* gbs);
     mrtResult buildEnvCdf(const float* rgba, uint32_t w, uint32_t h, float* cdf, float* integral);
     mrtResult setSampleStream(uint32_t offset, uint32_t stride);
+    mrtResult setTraversalBudget(uint32_t maxVisits);
     mrtResult copyAccumulationDevice(void* dev, size_t bytes, bool accumulate);
     // 8-wide BVH of one triangle mesh built on this engine's GPU (LBVH
     // topology, SAH-optimal collapse), read back into `out`.
@@ -120,6 +121,8 @@ private:
     DeviceBuffer m_instances, m_materials, m_lights;
     DeviceBuffer m_envTexels, m_envCdf, m_envSin, m_envRowSums, m_envIntegral;
     DeviceBuffer m_texTable;
+    DeviceBuffer m_srgbLut;  // 256 floats: sRGB decode of k / 255
+    uint32_t m_maxVisits = 0;  // traversal visit budget (0: the kernels' default)
     DeviceBuffer m_texData[MRT_MAX_TEXTURES];
     std::vector<uint32_t> m_texGeneration;
     // device frame state

@@ -57,6 +57,7 @@ def load():
             "orc_bvh_build": (u32, [vp, u32, u32, vp, vp]), "orc_env_cdf": (f32, [vp, u32, u32, vp]),
             "orc_readback_f32": (None, [vp, u32, u32, vp]), "orc_resolve_rgba8": (None, [vp, u32, f32, u32, vp]),
             "orc_pcg4d": (None, [vp, u32, vp]), "orc_stats": (None, [vp, vp]),
+            "orc_diff_of_products": (None, [vp, u32, vp]),
             "orc_set_bruteforce": (None, [vp, i32]),
             "orc_set_all_leaf_instances": (None, [vp, i32]), "orc_unwalked_instances": (u32, [vp]),
         }
@@ -66,6 +67,15 @@ def load():
             fn.argtypes = args
         _lib = lib
     return _lib
+
+
+def diff_of_products(abcd):
+    """float32 a*b - c*d by Kahan's FMA algorithm, as the watertight test's
+    edge fallback computes it; abcd is (N, 4)."""
+    x = np.ascontiguousarray(np.asarray(abcd, np.float32).reshape(-1, 4))
+    out = np.empty(x.shape[0], np.float32)
+    load().orc_diff_of_products(x.ctypes.data, x.shape[0], out.ctypes.data)
+    return out
 
 
 def load_ref_bvh():

@@ -382,6 +382,13 @@ void orc_pcg4d(const uint32_t* in, uint32_t n, uint32_t* out) {
     }
 }
 
+// Kahan's a * b - c * d in single precision, as the watertight test's edge
+// fallback evaluates it (4 floats per entry in, 1 out).
+void orc_diff_of_products(const float* abcd, uint32_t n, float* out) {
+    for (uint32_t i = 0; i < n; ++i)
+        out[i] = Tracer<float>::diffOfProducts(abcd[4 * i], abcd[4 * i + 1], abcd[4 * i + 2], abcd[4 * i + 3]);
+}
+
 // Scene statistics after orc_commit: nodes, triangles, instances, tlasRoot,
 // max BLAS depth (root = 1).
 void orc_stats(void* s, uint32_t* out5) {

@@ -297,6 +297,15 @@ template <class T> struct Tracer {
         }
         return hit;
     }
+    // a * b - c * d by Kahan's algorithm (rounded product, its exact error by
+    // one fused multiply-add, then the sum): within 2 ulp (Jeannerod, Louvet
+    // and Muller 2013), so its sign is exact.
+    static T diffOfProducts(T a, T b, T c, T d) {
+        const T w = c * d;
+        const T e = std::fma(-c, d, w);
+        const T f = std::fma(a, b, -w);
+        return f + e;
+    }
     // Woop, Benthin and Wald 2013 watertight test (diagnostic twin of the
     // GPU kernel's decision), t in (1e-4, tMax).
     T intersectWatertight(uint32_t tri, V3<T> o, V3<T> d, T tMax, V2<T>& bary) const {
@@ -312,10 +321,10 @@ template <class T> struct Tracer {
         const T Bx = B[kx] - sx * B[kz], By = B[ky] - sy * B[kz];
         const T Cx = Cc[kx] - sx * Cc[kz], Cy = Cc[ky] - sy * Cc[kz];
         T U = Cx * By - Cy * Bx, V = Ax * Cy - Ay * Cx, W = Bx * Ay - By * Ax;
-        if (U == T(0) || V == T(0) || W == T(0)) {
-            U = T(double(Cx) * double(By) - double(Cy) * double(Bx));
-            V = T(double(Ax) * double(Cy) - double(Ay) * double(Cx));
-            W = T(double(Bx) * double(Ay) - double(By) * double(Ax));
+        if (U == T(0) || V == T(0) || W == T(0)) {  // exactly signed edge functions
+            U = diffOfProducts(Cx, By, Cy, Bx);
+            V = diffOfProducts(Ax, Cy, Ay, Cx);
+            W = diffOfProducts(Bx, Ay, By, Ax);
         }
         if ((U < T(0) || V < T(0) || W < T(0)) && (U > T(0) || V > T(0) || W > T(0))) return T(-1);
         const T det = U + V + W;
