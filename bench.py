@@ -63,6 +63,9 @@ def parse_args():
                          "depth 16), 16 spp per step, no CPU baseline")
     ap.add_argument("--e2e-steps", type=int, default=4,
                     help="end-to-end steps averaged (wall-clock: host jitter of up to ~25 ms a step was seen)")
+    ap.add_argument("--interactive-frames", type=int, default=48,
+                    help="frames of the plug-in's loop (mrtCommitScene, mrtRenderFrame, RGBA32F readback every "
+                         "frame) timed for e2e_interactive (0 = skip)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--spp", type=int, default=0, help="samples per pixel per step (0 = the workload's 64)")
@@ -355,6 +358,38 @@ def ours_arm(args):
                "breakdown": "mrtUpdateMesh(heightfield) + mrtSetEnvironment + mrtCommitScene (BVH rebuild, "
                             "packing, env CDF kernel, uploads) + %d x mrtRenderFrame + RGBA32F readback" % spp}
 
+    # The plug-in's own loop (reference rhino/MiniRaytrace.Rhino/Session/
+    # RenderSession.cs:203-209): mrtCommitScene, one mrtRenderFrame, and the
+    # frame callback's mrtReadFramebuffer(RGBA32F) into host memory, every
+    # frame; wall-clock timed, so each frame's sample is rendered (and read)
+    # inside the loop.
+    interactive = None
+    if args.interactive_frames > 0:
+        host_img = np.empty((H, W, 4), np.float32)
+        eng.commit()
+        for _ in range(3):
+            eng.commit()
+            eng.render_frame()
+            eng.read_framebuffer(mrt.MRT_PIXEL_RGBA32F_LINEAR, out=host_img)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        dev_ms = []
+        t0 = time.perf_counter()
+        for _ in range(args.interactive_frames):
+            eng.commit()
+            eng.render_frame()
+            eng.read_framebuffer(mrt.MRT_PIXEL_RGBA32F_LINEAR, out=host_img)
+            dev_ms.append(eng.stats()["lastRenderMs"])
+        dt = replicas.max_over_ranks(time.perf_counter() - t0, dist, "cuda")
+        interactive = {
+            "value": world * W * H * args.interactive_frames / dt / 1e6, "unit": UNIT,
+            "frames": args.interactive_frames, "ms_per_frame": dt * 1e3 / args.interactive_frames,
+            "render_device_ms_per_frame": float(np.mean(dev_ms)),
+            "h2d_bytes_per_step": 0, "d2h_bytes_per_step": W * H * 16,
+            "loop": "mrtCommitScene + mrtRenderFrame (1 spp) + mrtReadFramebuffer(RGBA32F) into host memory, "
+                    "per frame (the plug-in's render loop), wall-clock"}
+
     out = None
     if rank == 0:
         cpu = None
@@ -412,6 +447,7 @@ def ours_arm(args):
                         "shadow_tris": c["shadowTriTests"] / max(1, c["raysShadow"])},
             "clocks": clocks,
             "e2e": e2e,
+            "e2e_interactive": interactive,
             "cpu_baseline": cpu,
         }
         print(json.dumps(out), flush=True)

@@ -48,6 +48,14 @@ typedef struct mrtxHit {
  * 88-125 `traceRay`) for `count` rays; commits pending scene changes first. */
 MRT_API mrtResult mrtxTraceRays(mrtEngine*, const mrtxRay* rays, uint32_t count, mrtxHit* hits);
 
+/* mrtxTraceRays through the renderer's own closest-hit stage: the rays
+ * take the place of a wave's paths and one launch of the wavefront's extend
+ * kernel (persistent warps that refill finished lanes, warp-batched
+ * triangle tests) traces them, exactly as it traces path segments. Each
+ * ray's tMax is ignored (path rays are traced to 1e30). Same output as
+ * mrtxTraceRays; for checking the kernel a render uses. */
+MRT_API mrtResult mrtxTraceRaysWavefront(mrtEngine*, const mrtxRay* rays, uint32_t count, mrtxHit* hits);
+
 /* Any-hit traversal (reference intersect.glsl:128-178 `traceShadowRay`):
  * occluded[i] = 1 when ray i hits anything in (1e-4, tMax), else 0. */
 MRT_API mrtResult mrtxTraceShadowRays(mrtEngine*, const mrtxRay* rays, uint32_t count,
@@ -192,6 +200,30 @@ MRT_API mrtResult mrtxRadianceCacheTrain(mrtEngine*, const float* features, cons
  * the Adam state. */
 MRT_API mrtResult mrtxRadianceCacheParams(mrtEngine*, float* gridOut, float* mlpOut, const float* gridIn,
                                           const float* mlpIn);
+
+/* Averaging of the cache's weights for inference (Polyak averaging): every
+ * training step blends the new parameters into a moving average with
+ * weight 1 - d, d = min(decay, (1 + k) / (10 + k)) at step k, and every
+ * query (rendering and mrtxRadianceCacheQuery) reads the average. The
+ * online training's constant learning rate makes the live weights wander
+ * from one step to the next; the average does not. decay in [0, 1); 0
+ * switches averaging off (queries read the live weights). Default 0.99.
+ * Writing parameters (mrtxRadianceCacheParams) restarts the average at
+ * them. */
+MRT_API mrtResult mrtxSetRadianceCacheAveraging(mrtEngine*, float decay);
+
+/* The gradients the cache's training step computes for one batch, read
+ * back without taking the step: the tensor-core forward and backward pass
+ * over all `count` samples (features and targets as in
+ * mrtxRadianceCacheTrain) gives the gradient of the mean loss over samples
+ * and channels with respect to the hash grid (gridGradOut, layout as the
+ * grid in mrtxRadianceCacheParams; entries no sample touches are exactly 0)
+ * and the MLP (mlpGradOut, layout as the weights); *lossOut receives the
+ * mean loss. Any output may be NULL. The parameters and the optimizer's
+ * state are unchanged. For checking the training kernels against a CPU
+ * evaluation of the same network. */
+MRT_API mrtResult mrtxRadianceCacheGradients(mrtEngine*, const float* features, const float* targets, uint32_t count,
+                                             float* gridGradOut, float* mlpGradOut, float* lossOut);
 
 /* Host-side build of the acceleration structure the engine uses for a mesh,
  * for inspection and tests (no device needed): an 8-wide compressed BVH over

@@ -268,10 +268,13 @@ class Engine:
         self.lib.mrtResetAccumulation(self.h)
 
     # -- extensions
-    def trace_rays(self, origins, dirs, t_max=1e30):
+    def trace_rays(self, origins, dirs, t_max=1e30, wavefront=False):
+        """Closest hits (mrtxTraceRays); wavefront=True traces them with the
+        renderer's extend kernel (mrtxTraceRaysWavefront, tMax ignored)."""
         rays = make_rays(origins, dirs, t_max)
         hits = np.zeros(rays.shape[0], dtype=abi.HIT_DTYPE)
-        _check(self.lib.mrtxTraceRays(self.h, _ptr(rays), rays.shape[0], _ptr(hits)), "mrtxTraceRays")
+        fn = self.lib.mrtxTraceRaysWavefront if wavefront else self.lib.mrtxTraceRays
+        _check(fn(self.h, _ptr(rays), rays.shape[0], _ptr(hits)), "mrtxTraceRays")
         return hits
 
     def trace_shadow_rays(self, origins, dirs, t_max=1e30):
@@ -329,6 +332,23 @@ class Engine:
         _check(self.lib.mrtxRadianceCacheTrain(self.h, _ptr(f), _ptr(t), f.shape[0], steps, C.byref(loss)),
                "mrtxRadianceCacheTrain")
         return loss.value
+
+    def set_cache_averaging(self, decay: float):
+        """mrtxSetRadianceCacheAveraging: moving-average decay of the weights
+        queries read (0 = queries read the live weights)."""
+        _check(self.lib.mrtxSetRadianceCacheAveraging(self.h, float(decay)), "mrtxSetRadianceCacheAveraging")
+
+    def cache_gradients(self, features, targets):
+        """mrtxRadianceCacheGradients: (grid gradient, MLP gradient, mean
+        loss) of one batch, without an optimizer step."""
+        f = np.ascontiguousarray(np.asarray(features, np.float32).reshape(-1, 16))
+        t = np.ascontiguousarray(np.asarray(targets, np.float32).reshape(-1, 3))
+        g = np.empty(abi.CACHE_GRID_FLOATS, np.float32)
+        w = np.empty(abi.CACHE_MLP_FLOATS, np.float32)
+        loss = C.c_float()
+        _check(self.lib.mrtxRadianceCacheGradients(self.h, _ptr(f), _ptr(t), f.shape[0], _ptr(g), _ptr(w),
+                                                   C.byref(loss)), "mrtxRadianceCacheGradients")
+        return g, w, loss.value
 
     def cache_params(self, grid=None, mlp=None):
         """Returns (grid, mlp) as read, then writes the given arrays."""

@@ -181,6 +181,10 @@ FUNCTIONS = [
                                   C.POINTER(C.c_float)]),
     ("mrtxSetSampleStream", C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32]),
     ("mrtxSetTraversalBudget", C.c_int, [C.c_void_p, C.c_uint32]),
+    ("mrtxTraceRaysWavefront", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]),
+    ("mrtxSetRadianceCacheAveraging", C.c_int, [C.c_void_p, C.c_float]),
+    ("mrtxRadianceCacheGradients", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p,
+                                             C.c_void_p]),
     ("mrtxInjectAllocationFailure", C.c_int, [C.c_int32]),
     ("mrtxCopyAccumulationDevice", C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, C.c_int32]),
     ("mrtxBuildWideBvh", C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p,

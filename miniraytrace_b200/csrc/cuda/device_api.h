@@ -14,6 +14,12 @@
 // floats), their gradients and Adam moments; position normalisation.
 typedef struct McacheParams {
     float *grid, *mlp, *gGrid, *gMlp, *mGrid, *vGrid, *mMlp, *vMlp;
+    // Exponential moving average of the parameters (Polyak averaging),
+    // updated by every Adam step where the parameter changed; NULL = none.
+    // Step k blends with weight 1 - d, d = min(emaDecay, (1 + k) / (10 + k)),
+    // so early on the average follows the fast-changing weights closely.
+    float *emaGrid, *emaMlp;
+    float emaDecay;
     float* partial;          // per-block weight gradients of one step
     uint32_t partialBlocks;  // training CTAs' partial gradients `partial` holds
     float lo[3], invExtent[3];
@@ -43,6 +49,11 @@ cudaError_t mrtcu_wave_finalize(const MrtFrameParams* p, const MrtWaveState* s, 
 // Trace queries (closest hit / any hit) for n device-resident rays.
 cudaError_t mrtcu_trace_closest(const MrtFrameParams* p, const MrtQueryRay* rays, uint32_t n, MrtQueryHit* hits,
                                 cudaStream_t stream);
+// The same closest-hit queries through the wavefront's extend kernel (the
+// rays occupy wave slots 0..n-1; n <= s->capacity; tMax of the rays ignored:
+// the extend stage traces to 1e30).
+cudaError_t mrtcu_trace_closest_wave(const MrtFrameParams* p, const MrtWaveState* s, const MrtQueryRay* rays,
+                                     uint32_t n, MrtQueryHit* hits, cudaStream_t stream);
 cudaError_t mrtcu_trace_any(const MrtFrameParams* p, const MrtQueryRay* rays, uint32_t n, uint32_t* occluded,
                             cudaStream_t stream);
 
@@ -121,6 +132,10 @@ cudaError_t mrtcu_rc_record_targets(const float4* prefix, const float4* beta, ui
                                     const float4* L, float* targets, cudaStream_t stream);
 cudaError_t mrtcu_rc_train(McacheParams* C, const float* features, const float* targets, uint32_t n, uint32_t steps,
                            uint32_t batch, float* lossOut, cudaStream_t stream);
+// Gradients of the mean loss over n samples (no optimizer step): the MLP's
+// into C->gMlp, the hash grid's into C->gGrid.
+cudaError_t mrtcu_rc_gradients(McacheParams* C, const float* features, const float* targets, uint32_t n,
+                               float* lossOut, cudaStream_t stream);
 
 #ifdef __cplusplus
 }

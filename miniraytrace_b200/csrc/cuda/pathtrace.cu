@@ -524,6 +524,48 @@ __global__ void __launch_bounds__(256) waveFinalizeKernel(MrtFrameParams P, MrtW
     }
 }
 
+// Query rays through the wavefront's own closest-hit stage: the rays become
+// wave slots 0..n-1 on queue 0 (bounce 0, tMax 1e30 as every path ray), the
+// extend kernel runs as in a render, and its hit records are converted to
+// query hits. This checks the persistent, refilling, warp-batched kernel the
+// renderer times, not a one-ray-per-thread twin of it.
+__global__ void queryToWaveKernel(const MrtQueryRay* __restrict__ rays, uint32_t n, MrtWaveState S) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) {
+        S.counts[0] = n;
+        S.counts[kExtendHead] = 0;
+    }
+    if (i >= n) return;
+    const MrtQueryRay r = rays[i];
+    S.rayO[i] = make_float4(r.origin[0], r.origin[1], r.origin[2], 0.0f);
+    S.rayD[i] = make_float4(r.dir[0], r.dir[1], r.dir[2], __uint_as_float(0u));
+    S.queue[0][i] = i;
+}
+
+__global__ void waveToQueryKernel(MrtFrameParams P, MrtWaveState S, uint32_t n, MrtQueryHit* __restrict__ hits) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 h = S.hit[i];
+    const uint32_t tri = __float_as_uint(h.w);
+    MrtQueryHit out;
+    out.pad[0] = out.pad[1] = 0;
+    if (tri != 0xffffffffu && tri < P.triCount) {
+        out.t = h.x;
+        out.instance = P.instances[S.hitInst[i]].userId;
+        out.prim = ldg4u(P.triIndex + tri).w;
+        out.hit = 1;
+        out.u = h.y;
+        out.v = h.z;
+    } else {
+        out.t = 1e30f;
+        out.instance = 0;
+        out.prim = 0;
+        out.hit = 0;
+        out.u = out.v = 0.0f;
+    }
+    hits[i] = out;
+}
+
 __global__ void traceClosestKernel(MrtFrameParams P, const MrtQueryRay* __restrict__ rays, uint32_t n,
                                    MrtQueryHit* __restrict__ hits) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -652,6 +694,18 @@ extern "C" cudaError_t mrtcu_trace_closest(const MrtFrameParams* p, const MrtQue
                                            MrtQueryHit* hits, cudaStream_t stream) {
     if (n == 0) return cudaSuccess;
     traceClosestKernel<<<(n + 127) / 128, 128, 0, stream>>>(*p, rays, n, hits);
+    return cudaGetLastError();
+}
+
+extern "C" cudaError_t mrtcu_trace_closest_wave(const MrtFrameParams* p, const MrtWaveState* s,
+                                                const MrtQueryRay* rays, uint32_t n, MrtQueryHit* hits,
+                                                cudaStream_t stream) {
+    if (n == 0) return cudaSuccess;
+    if (n > s->capacity) return cudaErrorInvalidValue;
+    const WaveGrids& g = waveGrids();
+    queryToWaveKernel<<<(n + 255) / 256, 256, 0, stream>>>(rays, n, *s);
+    waveExtendKernel<<<g.extend, MRT_TRAV_THREADS, 0, stream>>>(*p, *s, 0u);
+    waveToQueryKernel<<<(n + 255) / 256, 256, 0, stream>>>(*p, *s, n, hits);
     return cudaGetLastError();
 }
 

@@ -623,8 +623,12 @@ __global__ void reducePartialsKernel(const float* __restrict__ partial, uint32_t
 // got no gradient this step are left as they are (their moments and values
 // do not decay), which the hash grid needs: a step touches a few of its
 // 16.8 M entries.
+// One Adam step (lazy: entries with a zero gradient, untouched by the
+// batch, keep their parameter and moments); with `ema`, the moving average
+// of each changed parameter takes the new value with weight 1 - emaDecay.
 __global__ void adamKernel(float* __restrict__ p, float* __restrict__ g, float* __restrict__ m, float* __restrict__ v,
-                           size_t n, float lr, float b1, float b2, float eps, float c1, float c2, bool lazy) {
+                           size_t n, float lr, float b1, float b2, float eps, float c1, float c2, bool lazy,
+                           float* __restrict__ ema, float emaDecay) {
     for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x) {
         const float gi = g[i];
         if (lazy && gi == 0.0f) continue;
@@ -633,7 +637,9 @@ __global__ void adamKernel(float* __restrict__ p, float* __restrict__ g, float* 
         const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
         m[i] = mi;
         v[i] = vi;
-        p[i] -= lr * (mi * c1) / (sqrtf(vi * c2) + eps);
+        const float pi = p[i] - lr * (mi * c1) / (sqrtf(vi * c2) + eps);
+        p[i] = pi;
+        if (ema) ema[i] = emaDecay * ema[i] + (1.0f - emaDecay) * pi;
     }
 }
 
@@ -722,6 +728,12 @@ extern "C" cudaError_t mrtcu_rc_init(McacheParams C, uint32_t seed, cudaStream_t
     initKernel<<<gridFor(gridN + mlpN), 256, 0, stream>>>(C.grid, gridN, C.mlp, seed);
     cudaError_t e = cudaMemsetAsync(C.status, 0, sizeof(uint32_t), stream);
     if (e != cudaSuccess) return e;
+    if (C.emaGrid && (e = cudaMemcpyAsync(C.emaGrid, C.grid, gridN * sizeof(float), cudaMemcpyDeviceToDevice,
+                                          stream)) != cudaSuccess)
+        return e;
+    if (C.emaMlp && (e = cudaMemcpyAsync(C.emaMlp, C.mlp, mlpN * sizeof(float), cudaMemcpyDeviceToDevice,
+                                         stream)) != cudaSuccess)
+        return e;
     for (float* p : {C.gGrid, C.mGrid, C.vGrid})
         if ((e = cudaMemsetAsync(p, 0, gridN * sizeof(float), stream)) != cudaSuccess) return e;
     for (float* p : {C.gMlp, C.mMlp, C.vMlp})
@@ -779,11 +791,36 @@ extern "C" cudaError_t mrtcu_rc_train(McacheParams* C, const float* features, co
         ++C->step;
         const float b1 = 0.9f, b2 = 0.99f;
         const float c1 = 1.0f / (1.0f - powf(b1, float(C->step))), c2 = 1.0f / (1.0f - powf(b2, float(C->step)));
+        const float st = float(C->step);
+        const float d = fminf(C->emaDecay, (1.0f + st) / (10.0f + st));
         adamKernel<<<gridFor(gridN), 256, 0, stream>>>(C->grid, C->gGrid, C->mGrid, C->vGrid, gridN, C->lr, b1, b2,
-                                                       1e-10f, c1, c2, true);
+                                                       1e-10f, c1, c2, true, C->emaGrid, d);
         adamKernel<<<gridFor(mlpN), 256, 0, stream>>>(C->mlp, C->gMlp, C->mMlp, C->vMlp, mlpN, C->lr, b1, b2,
-                                                      1e-10f, c1, c2, false);
+                                                      1e-10f, c1, c2, false, C->emaMlp, d);
     }
+    return cudaGetLastError();
+}
+
+// The gradients of one batch without an optimizer step: the training
+// kernel's forward and backward pass over all n samples (the mean loss over
+// samples and channels), the per-CTA weight gradients summed into C->gMlp,
+// the hash-grid gradient scattered into C->gGrid (cleared first). The
+// parameters and the Adam moments are not touched; the caller clears gGrid
+// afterwards so no later Adam step consumes it.
+extern "C" cudaError_t mrtcu_rc_gradients(McacheParams* C, const float* features, const float* targets, uint32_t n,
+                                          float* lossOut, cudaStream_t stream) {
+    if (n == 0) return cudaSuccess;
+    cudaError_t e = cudaFuncSetAttribute(tcTrainKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smemTrain()));
+    if (e != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(C->gGrid, 0, mrtcu_rc_grid_floats() * sizeof(float), stream)) != cudaSuccess) return e;
+    int sms = 148, dev = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const uint32_t maxCtas = uint32_t(sms) < C->partialBlocks ? uint32_t(sms) : C->partialBlocks;
+    const uint32_t tiles = (n + kTile - 1) / kTile;
+    const uint32_t blocks = tiles < maxCtas ? tiles : maxCtas;
+    tcTrainKernel<<<blocks, kTile, smemTrain(), stream>>>(*C, features, targets, n, 0u, 1u, 1.0f / (3.0f * float(n)),
+                                                          C->partial, lossOut);
+    reducePartialsKernel<<<gridFor(kMlpFloats), 256, 0, stream>>>(C->partial, blocks, C->gMlp);
     return cudaGetLastError();
 }
 

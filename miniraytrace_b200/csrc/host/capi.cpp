@@ -229,6 +229,13 @@ MRT_API mrtResult mrtxTraceRays(mrtEngine* e, const mrtxRay* rays, uint32_t coun
     return guarded([&] { return eng->traceRays(rays, count, hits); });
 }
 
+MRT_API mrtResult mrtxTraceRaysWavefront(mrtEngine* e, const mrtxRay* rays, uint32_t count, mrtxHit* hits) {
+    mrt::Engine* eng = unwrap(e);
+    if (!eng) return MRT_ERROR_INVALID_HANDLE;
+    if (count && (!rays || !hits)) return mrt::fail(MRT_ERROR_INVALID_ARGUMENT, "mrtxTraceRaysWavefront: null pointer");
+    return guarded([&] { return eng->traceRaysWavefront(rays, count, hits); });
+}
+
 MRT_API mrtResult mrtxTraceShadowRays(mrtEngine* e, const mrtxRay* rays, uint32_t count, uint32_t* occluded) {
     mrt::Engine* eng = unwrap(e);
     if (!eng) return MRT_ERROR_INVALID_HANDLE;
@@ -331,6 +338,21 @@ MRT_API mrtResult mrtxRadianceCacheTrain(mrtEngine* e, const float* features, co
     if (!eng) return MRT_ERROR_INVALID_HANDLE;
     if (count && (!features || !targets)) return mrt::fail(MRT_ERROR_INVALID_ARGUMENT, "mrtxRadianceCacheTrain: null");
     return guarded([&] { return eng->cacheTrain(features, targets, count, steps, lossOut); });
+}
+
+MRT_API mrtResult mrtxRadianceCacheGradients(mrtEngine* e, const float* features, const float* targets,
+                                             uint32_t count, float* gridGradOut, float* mlpGradOut, float* lossOut) {
+    mrt::Engine* eng = unwrap(e);
+    if (!eng) return MRT_ERROR_INVALID_HANDLE;
+    if (count && (!features || !targets))
+        return mrt::fail(MRT_ERROR_INVALID_ARGUMENT, "mrtxRadianceCacheGradients: null samples");
+    return guarded([&] { return eng->cacheGradients(features, targets, count, gridGradOut, mlpGradOut, lossOut); });
+}
+
+MRT_API mrtResult mrtxSetRadianceCacheAveraging(mrtEngine* e, float decay) {
+    mrt::Engine* eng = unwrap(e);
+    if (!eng) return MRT_ERROR_INVALID_HANDLE;
+    return guarded([&] { return eng->setCacheAveraging(decay); });
 }
 
 MRT_API mrtResult mrtxRadianceCacheParams(mrtEngine* e, float* gridOut, float* mlpOut, const float* gridIn,

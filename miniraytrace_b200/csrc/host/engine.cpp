@@ -1009,12 +1009,20 @@ mrtResult Engine::renderFrames(uint32_t count, mrtFrameInfo* info, bool defer) {
         m_resolveExposure = std::exp2(m_settings.exposureEV);
         m_resolveTonemap = m_settings.tonemap;
     }
-    if (m_pending > 0 && (!defer || m_pending >= waveCapacitySamples())) MRT_TRY(flushPending());
+    const bool flush = m_pending > 0 && (!defer || m_pending >= waveCapacitySamples());
+    if (flush) MRT_TRY(flushPending());
     if (info && info->structSize >= sizeof(mrtFrameInfo)) {
         info->spp = m_frameIndex + m_pending;
         info->converged = m_frameIndex + m_pending >= m_settings.sppLimit ? 1 : 0;
         info->denoised = 0;
-        info->frameMs = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        // A call that rendered reports its wall time, as the reference times
+        // its render call (Renderer.cpp:774, 837-841). A queued frame has not
+        // been rendered yet: it reports the device time of one sample of the
+        // last rendered wave, what the frame will cost (0 before any wave).
+        const float wall = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        info->frameMs = (flush || n == 0 || m_stats.lastRenderSpp == 0)
+                            ? wall
+                            : m_stats.lastRenderMs / float(m_stats.lastRenderSpp);
     }
     return MRT_SUCCESS;
 }
@@ -1270,6 +1278,33 @@ mrtResult Engine::traceRays(const mrtxRay* rays, uint32_t n, mrtxHit* hits) {
     return guard(checkErrorFlags());
 }
 
+// Closest hits through the renderer's own extend kernel, in chunks of the
+// wave state's capacity (the rays take the place of a wave's paths; no
+// render is in flight, and the next render initialises its wave anew). Ray
+// counters are off, so render statistics stay those of the last render.
+mrtResult Engine::traceRaysWavefront(const mrtxRay* rays, uint32_t n, mrtxHit* hits) {
+    MRT_TRY(flushPending());
+    MRT_TRY(commit(nullptr));
+    if (n == 0) return MRT_SUCCESS;
+    MRT_TRY(guard(ensureWave(64)));
+    MrtFrameParams p;
+    fillParams(p);
+    p.rayCounters = nullptr;
+    const uint32_t chunk = m_waveState.capacity;
+    if (chunk == 0) return fail(MRT_ERROR_UNKNOWN, "no wave state for wavefront trace queries");
+    MRT_TRY(m_queryRays.upload(rays, size_t(n) * sizeof(mrtxRay), m_stream));
+    MRT_TRY(m_queryOut.ensure(size_t(n) * sizeof(mrtxHit)));
+    for (uint32_t first = 0; first < n; first += chunk) {
+        const uint32_t k = std::min(chunk, n - first);
+        MRT_CUDA(mrtcu_trace_closest_wave(&p, &m_waveState, m_queryRays.as<MrtQueryRay>() + first, k,
+                                          m_queryOut.as<MrtQueryHit>() + first, m_stream));
+    }
+    MRT_CUDA(cudaMemcpyAsync(hits, m_queryOut.ptr, size_t(n) * sizeof(mrtxHit), cudaMemcpyDeviceToHost, m_stream));
+    const cudaError_t se = cudaStreamSynchronize(m_stream);
+    if (se != cudaSuccess) return guard(fromCuda(se, "wavefront trace query kernel"));
+    return guard(checkErrorFlags());
+}
+
 mrtResult Engine::traceShadowRays(const mrtxRay* rays, uint32_t n, uint32_t* occluded) {
     MRT_TRY(flushPending());
     MRT_TRY(commit(nullptr));
@@ -1423,7 +1458,7 @@ mrtResult Engine::buildMeshBvhDevice(const V4f* pos, size_t nv, const uint32_t* 
 
 void Engine::RadianceCache::release() {
     for (DeviceBuffer* d : {&grid, &mlp, &gGrid, &gMlp, &mGrid, &vGrid, &mMlp, &vMlp, &in, &out, &loss, &partial, &qFeat,
-                            &qBeta, &rFeat, &rPrefix, &rBeta, &rTarget, &counts, &scratch})
+                            &qBeta, &rFeat, &rPrefix, &rBeta, &rTarget, &counts, &scratch, &emaGrid, &emaMlp})
         d->release();
     allocated = false;
 }
@@ -1448,8 +1483,10 @@ void Engine::cacheBounds() {
 mrtResult Engine::ensureCache() {
     if (m_cache.allocated) return MRT_SUCCESS;
     const size_t g = mrtcu_rc_grid_floats() * sizeof(float), w = mrtcu_rc_mlp_floats() * sizeof(float);
-    for (DeviceBuffer* d : {&m_cache.grid, &m_cache.gGrid, &m_cache.mGrid, &m_cache.vGrid}) MRT_TRY(d->ensure(g));
-    for (DeviceBuffer* d : {&m_cache.mlp, &m_cache.gMlp, &m_cache.mMlp, &m_cache.vMlp}) MRT_TRY(d->ensure(w));
+    for (DeviceBuffer* d : {&m_cache.grid, &m_cache.gGrid, &m_cache.mGrid, &m_cache.vGrid, &m_cache.emaGrid})
+        MRT_TRY(d->ensure(g));
+    for (DeviceBuffer* d : {&m_cache.mlp, &m_cache.gMlp, &m_cache.mMlp, &m_cache.vMlp, &m_cache.emaMlp})
+        MRT_TRY(d->ensure(w));
     MRT_TRY(m_cache.loss.ensure(16));
     MRT_TRY(m_cache.partial.ensure(mrtcu_rc_partial_floats(kCacheMaxBatch) * sizeof(float)));
     McacheParams& c = m_cache.params;
@@ -1464,6 +1501,9 @@ mrtResult Engine::ensureCache() {
     c.vGrid = m_cache.vGrid.as<float>();
     c.mMlp = m_cache.mMlp.as<float>();
     c.vMlp = m_cache.vMlp.as<float>();
+    c.emaGrid = m_cache.emaDecay > 0.0f ? m_cache.emaGrid.as<float>() : nullptr;
+    c.emaMlp = m_cache.emaDecay > 0.0f ? m_cache.emaMlp.as<float>() : nullptr;
+    c.emaDecay = m_cache.emaDecay;
     c.step = 0;
     c.lr = m_cache.lr;
     cacheBounds();
@@ -1504,7 +1544,7 @@ mrtResult Engine::cacheQuery(const float* features, uint32_t n, float* rgb) {
     if (n == 0) return MRT_SUCCESS;
     MRT_TRY(up(m_cache.in, features, size_t(n) * 16 * sizeof(float)));
     MRT_TRY(m_cache.out.ensure(size_t(n) * 3 * sizeof(float)));
-    MRT_CUDA(mrtcu_rc_query(m_cache.params, m_cache.in.as<float>(), n, m_cache.out.as<float>(), m_stream));
+    MRT_CUDA(mrtcu_rc_query(inferenceParams(), m_cache.in.as<float>(), n, m_cache.out.as<float>(), m_stream));
     MRT_CUDA(cudaMemcpyAsync(rgb, m_cache.out.ptr, size_t(n) * 3 * sizeof(float), cudaMemcpyDeviceToHost, m_stream));
     uint32_t status = 0;
     MRT_CUDA(cudaMemcpyAsync(&status, m_cache.params.status, sizeof(status), cudaMemcpyDeviceToHost, m_stream));
@@ -1534,6 +1574,82 @@ mrtResult Engine::cacheTrain(const float* features, const float* targets, uint32
     return MRT_SUCCESS;
 }
 
+// Queries read the moving average of the parameters while averaging is on,
+// the live parameters otherwise.
+McacheParams Engine::inferenceParams() const {
+    McacheParams q = m_cache.params;
+    if (m_cache.emaDecay > 0.0f) {
+        q.grid = m_cache.emaGrid.as<float>();
+        q.mlp = m_cache.emaMlp.as<float>();
+    }
+    return q;
+}
+
+mrtResult Engine::resetAverage() {
+    MRT_CUDA(cudaMemcpyAsync(m_cache.emaGrid.ptr, m_cache.grid.ptr, mrtcu_rc_grid_floats() * sizeof(float),
+                             cudaMemcpyDeviceToDevice, m_stream));
+    MRT_CUDA(cudaMemcpyAsync(m_cache.emaMlp.ptr, m_cache.mlp.ptr, mrtcu_rc_mlp_floats() * sizeof(float),
+                             cudaMemcpyDeviceToDevice, m_stream));
+    return MRT_SUCCESS;
+}
+
+// Averaging of the weights queries read: decay in [0, 1); 0 switches it off
+// (queries read the live parameters). Switching it on starts the average at
+// the live parameters.
+mrtResult Engine::setCacheAveraging(float decay) {
+    MRT_TRY(checkAlive());
+    MRT_TRY(flushPending());
+    MRT_TRY(cacheStatus(0));
+    if (!(decay >= 0.0f && decay < 1.0f))
+        return fail(MRT_ERROR_INVALID_ARGUMENT, "radiance cache averaging: decay must be in [0, 1)");
+    MRT_TRY(guard(ensureCache()));
+    const bool wasOn = m_cache.emaDecay > 0.0f;
+    m_cache.emaDecay = decay;
+    m_cache.params.emaDecay = decay;
+    m_cache.params.emaGrid = decay > 0.0f ? m_cache.emaGrid.as<float>() : nullptr;
+    m_cache.params.emaMlp = decay > 0.0f ? m_cache.emaMlp.as<float>() : nullptr;
+    if (decay > 0.0f && !wasOn) MRT_TRY(resetAverage());
+    const cudaError_t e = cudaStreamSynchronize(m_stream);
+    if (e != cudaSuccess) return guard(fromCuda(e, "radiance cache averaging"));
+    return MRT_SUCCESS;
+}
+
+// One forward and backward pass of the training kernel over all n samples,
+// without the Adam step: the raw gradients of the mean loss, read back. The
+// grid gradient is cleared afterwards (the lazy Adam step treats nonzero
+// entries as touched), so later training is unaffected.
+mrtResult Engine::cacheGradients(const float* features, const float* targets, uint32_t n, float* gridOut,
+                                 float* mlpOut, float* loss) {
+    MRT_TRY(checkAlive());
+    MRT_TRY(cacheStatus(0));
+    MRT_TRY(guard(ensureCache()));
+    const size_t g = mrtcu_rc_grid_floats() * sizeof(float), w = mrtcu_rc_mlp_floats() * sizeof(float);
+    MRT_TRY(m_cache.in.ensure(std::max<size_t>(1, n) * 19 * sizeof(float)));
+    float* din = m_cache.in.as<float>();
+    MRT_CUDA(cudaMemsetAsync(m_cache.loss.ptr, 0, sizeof(float), m_stream));
+    MRT_CUDA(cudaMemsetAsync(m_cache.gMlp.ptr, 0, w, m_stream));
+    MRT_CUDA(cudaMemsetAsync(m_cache.gGrid.ptr, 0, g, m_stream));
+    if (n) {
+        MRT_CUDA(cudaMemcpyAsync(din, features, size_t(n) * 16 * sizeof(float), cudaMemcpyHostToDevice, m_stream));
+        MRT_CUDA(cudaMemcpyAsync(din + size_t(n) * 16, targets, size_t(n) * 3 * sizeof(float),
+                                 cudaMemcpyHostToDevice, m_stream));
+        MRT_CUDA(mrtcu_rc_gradients(&m_cache.params, din, din + size_t(n) * 16, n, m_cache.loss.as<float>(),
+                                    m_stream));
+    }
+    if (mlpOut) MRT_CUDA(cudaMemcpyAsync(mlpOut, m_cache.gMlp.ptr, w, cudaMemcpyDeviceToHost, m_stream));
+    if (gridOut) MRT_CUDA(cudaMemcpyAsync(gridOut, m_cache.gGrid.ptr, g, cudaMemcpyDeviceToHost, m_stream));
+    float l = 0.0f;
+    uint32_t status = 0;
+    MRT_CUDA(cudaMemcpyAsync(&l, m_cache.loss.ptr, sizeof(float), cudaMemcpyDeviceToHost, m_stream));
+    MRT_CUDA(cudaMemcpyAsync(&status, m_cache.params.status, sizeof(status), cudaMemcpyDeviceToHost, m_stream));
+    MRT_CUDA(cudaMemsetAsync(m_cache.gGrid.ptr, 0, g, m_stream));
+    const cudaError_t e = cudaStreamSynchronize(m_stream);
+    if (e != cudaSuccess) return guard(fromCuda(e, "radiance cache gradients"));
+    MRT_TRY(cacheStatus(status));
+    if (loss) *loss = l;
+    return MRT_SUCCESS;
+}
+
 mrtResult Engine::cacheParams(float* gridOut, float* mlpOut, const float* gridIn, const float* mlpIn) {
     MRT_TRY(checkAlive());
     MRT_TRY(guard(ensureCache()));
@@ -1548,6 +1664,7 @@ mrtResult Engine::cacheParams(float* gridOut, float* mlpOut, const float* gridIn
         for (DeviceBuffer* d : {&m_cache.gMlp, &m_cache.mMlp, &m_cache.vMlp})
             MRT_CUDA(cudaMemsetAsync(d->ptr, 0, w, m_stream));
         m_cache.params.step = 0;
+        MRT_TRY(resetAverage());
     }
     const cudaError_t e = cudaStreamSynchronize(m_stream);
     if (e != cudaSuccess) return guard(fromCuda(e, "radiance cache parameters"));
@@ -1623,7 +1740,7 @@ mrtResult Engine::cacheWave(const MrtFrameParams& p, uint32_t sampleBase, uint32
     const uint32_t nq = std::min(counts[0], K.qCap), nr = std::min(counts[1], K.rCap);
     const uint32_t slots = p.width * p.height * samples;
     MRT_CUDA(cudaEventRecord(ev[0], m_stream));
-    MRT_CUDA(mrtcu_rc_apply_queries(m_cache.params, K.qFeat, K.qBeta, nq, slots, m_cache.scratch.as<float>(),
+    MRT_CUDA(mrtcu_rc_apply_queries(inferenceParams(), K.qFeat, K.qBeta, nq, slots, m_cache.scratch.as<float>(),
                                     m_waveState.L, m_stream));
     MRT_CUDA(cudaEventRecord(ev[1], m_stream));
     MRT_CUDA(mrtcu_rc_record_targets(K.rPrefix, K.rBeta, nr, slots, m_waveState.L, m_cache.rTarget.as<float>(),

@@ -57,6 +57,7 @@ public:
     mrtResult readFramebuffer(mrtPixelFormat fmt, void* dst, size_t dstSize);
 
     mrtResult traceRays(const mrtxRay* rays, uint32_t n, mrtxHit* hits);
+    mrtResult traceRaysWavefront(const mrtxRay* rays, uint32_t n, mrtxHit* hits);
     mrtResult traceShadowRays(const mrtxRay* rays, uint32_t n, uint32_t* occluded);
     mrtResult readAccumulation(double* dst, size_t dstSize, uint32_t* spp);
     mrtResult getStats(mrtxStats* out) const;
@@ -71,6 +72,9 @@ public:
     mrtResult cacheQuery(const float* features, uint32_t n, float* rgb);
     mrtResult cacheTrain(const float* features, const float* targets, uint32_t n, uint32_t steps, float* loss);
     mrtResult cacheParams(float* gridOut, float* mlpOut, const float* gridIn, const float* mlpIn);
+    mrtResult cacheGradients(const float* features, const float* targets, uint32_t n, float* gridOut, float* mlpOut,
+                             float* loss);
+    mrtResult setCacheAveraging(float decay);
     mrtResult buildMeshBvhDevice(const V4f* pos, size_t nv, const uint32_t* idx, size_t nt, uint32_t maxLeaf,
                                  WideBvh& out);
     // Device build from device positions/indices into the builder's own
@@ -134,6 +138,7 @@ private:
     // radiance cache: parameters, gradients, Adam moments, query scratch
     struct RadianceCache {
         DeviceBuffer grid, mlp, gGrid, gMlp, mGrid, vGrid, mMlp, vMlp, in, out, loss, partial;
+        DeviceBuffer emaGrid, emaMlp;  // moving averages of the parameters, read by inference
         DeviceBuffer qFeat, qBeta, rFeat, rPrefix, rBeta, rTarget, counts, scratch;  // per-wave queries/records
         MrtCacheArgs args{};
         McacheParams params{};
@@ -145,6 +150,7 @@ private:
         bool failed = false;
         uint32_t trainingPaths = 0, stepsPerSample = 1, seed = 1, samplesPerUpdate = 4, trainingVertices = 0;
         float lr = 1e-2f;
+        float emaDecay = 0.99f;  // 0: inference reads the live parameters
         float lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
         void release();
     } m_cache;
@@ -152,6 +158,8 @@ private:
     void cacheBounds();
     mrtResult cacheWaveBuffers(uint32_t samples, uint32_t maxBounces);
     mrtResult cacheStatus(uint32_t status);
+    McacheParams inferenceParams() const;  // the parameters queries read (averaged or live)
+    mrtResult resetAverage();              // average := live parameters
     mrtResult cacheWave(const MrtFrameParams& p, uint32_t sampleBase, uint32_t samples, const cudaEvent_t* ev);
     MrtWaveState m_waveState{};
     uint32_t m_waveSamples = 0;  // samples per pixel one wave holds

@@ -18,7 +18,7 @@ import numpy as np
 import pytest
 
 from miniraytrace_b200 import abi
-from oracle.radiance_cache import encode, forward, forward_bf16, gradients_bf16
+from oracle.radiance_cache import bf16, encode, forward, forward_bf16, gradients_bf16
 
 pytestmark = pytest.mark.gpu
 
@@ -58,6 +58,7 @@ HI = np.array([3.0, 4.0, 2.5], np.float32)
 def engine(gpu):
     e = gpu.Engine(16, 16)
     e.set_radiance_cache(enabled=False, bounds=(LO, HI), learning_rate=LR)
+    e.set_cache_averaging(0.0)  # queries read the live weights (averaging has its own test)
     yield e
     e.close()
 
@@ -125,3 +126,103 @@ def test_training_fits_a_smooth_function(engine):
     want = np.stack([0.5 + 0.4 * np.sin(2 * held[:, 0]) * np.cos(3 * held[:, 2]), 0.3 + 0.2 * held[:, 4],
                      0.2 + 0.1 * held[:, 10]], 1)
     assert np.mean(np.abs(pred - want)) < 0.1
+
+
+def touched_grid_entries(F, grid):
+    """Flat indices of the grid floats some sample's corners reach (both
+    features of each corner entry), from the oracle's encoding."""
+    _, corners = encode(F, grid, LO, HI)
+    idx = np.unique(np.concatenate([i for lvl in corners for i, _ in lvl]))
+    return np.concatenate([2 * idx, 2 * idx + 1])
+
+
+@pytest.mark.parametrize("n", [1, 127, 129, 16384])
+def test_gradients_match_oracle_value_by_value(engine, n):
+    """The training kernels' raw gradients of one batch (before Adam) against
+    the oracle's gradients with the same BF16 roundings.
+
+    Tolerance: per MLP layer, 99.9% of the weights' gradients within 1e-2 of
+    that layer's largest |gradient| (FP32 sums in another order move the odd
+    activation or back-propagated value across a BF16 rounding boundary,
+    one BF16 step = 2^-8 relative), all within 5e-2 of it; the output
+    layer's unused rows exactly 0. Per hash-grid level the same bounds over
+    the entries the batch touches; every entry no sample reaches exactly 0.
+    The mean loss within 1e-2 relative (a single sample's output moves by
+    a BF16 step when one of its activations rounds the other way)."""
+    rng = np.random.default_rng(40 + n)
+    grid, mlp = random_params(rng)
+    engine.cache_params(grid, mlp)
+    F = random_features(rng, n, LO, HI)
+    targets = rng.uniform(0, 2, (n, 3)).astype(np.float32)
+    g_grid, g_mlp, loss = engine.cache_gradients(F, targets)
+    want_mlp, want_grid = gradients_bf16(F, targets.astype(np.float64), grid, mlp, LO, HI)
+
+    got_w = g_mlp.reshape(6, 64, 64).astype(np.float64)
+    want_w = want_mlp.reshape(6, 64, 64)
+    assert np.all(got_w[5][3:] == 0)
+    for layer in range(6):
+        rows = 3 if layer == 5 else 64
+        a, b = got_w[layer][:rows], want_w[layer][:rows]
+        scale = np.abs(b).max()
+        assert scale > 0, layer
+        close = np.abs(a - b) <= 1e-2 * scale
+        assert close.mean() >= 0.999, (n, layer, int((~close).sum()))
+        assert np.abs(a - b).max() <= 5e-2 * scale, (n, layer, np.abs(a - b).max() / scale)
+
+    touched = touched_grid_entries(F, grid)
+    untouched = np.ones(g_grid.size, bool)
+    untouched[touched] = False
+    assert np.all(g_grid[untouched] == 0), int(np.count_nonzero(g_grid[untouched]))
+    per_level = g_grid.size // 16
+    for level in range(16):
+        sel = touched[(touched >= level * per_level) & (touched < (level + 1) * per_level)]
+        a, b = g_grid[sel].astype(np.float64), want_grid[sel]
+        scale = np.abs(b).max()
+        if scale == 0:
+            assert np.all(a == 0), level
+            continue
+        close = np.abs(a - b) <= 1e-2 * scale
+        assert close.mean() >= 0.999, (n, level, int((~close).sum()))
+        assert np.abs(a - b).max() <= 5e-2 * scale, (n, level)
+
+    enc, _ = encode(F, grid, LO, HI)
+    W = mlp.reshape(6, 64, 64)
+    h = bf16(enc)
+    for layer in range(5):
+        h = bf16(np.maximum(h @ bf16(W[layer]).T, 0.0))
+    y = h @ bf16(W[5][:3]).T
+    want_loss = np.mean((y - targets) ** 2 / (y * y + 0.01))
+    assert abs(loss - want_loss) <= 1e-2 * want_loss, (loss, want_loss)
+
+    # nothing moved: the parameters are as written
+    grid1, mlp1 = engine.cache_params()
+    assert np.array_equal(grid1, grid) and np.array_equal(mlp1, mlp)
+
+
+def test_weight_average_follows_its_formula(engine):
+    """Averaging on: one Adam step moves the live weights; the average takes
+    them with weight 1 - d, d = min(decay, (1 + k) / (10 + k)) = 2/11 at the
+    first step (k = 1), entries the batch did not touch keep their value, and
+    queries read the average. Tolerance: queries as in
+    test_query_matches_numpy (the average itself is one FP32 blend)."""
+    rng = np.random.default_rng(6)
+    grid, mlp = random_params(rng)
+    engine.set_cache_averaging(0.9)
+    engine.cache_params(grid, mlp)  # restarts the average at these weights
+    F = random_features(rng, 512, LO, HI)
+    targets = rng.uniform(0, 2, (512, 3)).astype(np.float32)
+    engine.cache_train(F, targets, steps=1)
+    grid1, mlp1 = engine.cache_params()
+    d = np.float32(2.0 / 11.0)
+    want_grid = d * grid + (np.float32(1) - d) * grid1
+    want_mlp = d * mlp + (np.float32(1) - d) * mlp1
+    moved = grid1 != grid
+    want_grid[~moved] = grid[~moved]
+    Fq = random_features(rng, 1000, LO, HI)
+    out = engine.cache_query(Fq)
+    ref = forward_bf16(encode(Fq, want_grid, LO, HI)[0], want_mlp)
+    assert_bf16_close(out, ref)
+    live = forward_bf16(encode(Fq, grid1, LO, HI)[0], mlp1)
+    assert np.abs(out - live).max() > 1e-3  # it is not the live network
+    engine.set_cache_averaging(0.0)
+    assert_bf16_close(engine.cache_query(Fq), live)
