@@ -207,7 +207,8 @@ MRT_API mrtResult mrtxRadianceCacheParams(mrtEngine*, float* gridOut, float* mlp
  * query (rendering and mrtxRadianceCacheQuery) reads the average. The
  * online training's constant learning rate makes the live weights wander
  * from one step to the next; the average does not. decay in [0, 1); 0
- * switches averaging off (queries read the live weights). Default 0.99.
+ * switches averaging off (queries read the live weights); that is the
+ * default.
  * Writing parameters (mrtxRadianceCacheParams) restarts the average at
  * them. */
 MRT_API mrtResult mrtxSetRadianceCacheAveraging(mrtEngine*, float decay);

@@ -150,7 +150,7 @@ private:
         bool failed = false;
         uint32_t trainingPaths = 0, stepsPerSample = 1, seed = 1, samplesPerUpdate = 4, trainingVertices = 0;
         float lr = 1e-2f;
-        float emaDecay = 0.99f;  // 0: inference reads the live parameters
+        float emaDecay = 0.0f;  // 0: inference reads the live parameters (the default)
         float lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
         void release();
     } m_cache;

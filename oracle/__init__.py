@@ -2,7 +2,9 @@
 
 ctypes face of the CPU restatement of the MiniRaytrace shader math
 (liboracle.so, built by ``oracle/build_oracle.py``) and of the reference's own
-BVH builder compiled from its sources (``oracle/_ref/libref_bvh.so``).
+code compiled from its sources into ``oracle/_ref/``: the BVH builder
+(``libref_bvh.so``), the scene store's derived normals and tangents
+(``libref_scene.so``) and the environment-CDF loop (``libref_envcdf.so``).
 
 Only ``tests/``, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
 ``bench.py`` use this package, and only as the checker / the CPU baseline.
@@ -22,9 +24,13 @@ from miniraytrace_b200 import light_desc, material_desc, mesh_desc, texture_desc
 HERE = Path(__file__).resolve().parent
 LIB_PATH = HERE / "_build" / "liboracle.so"
 REF_BVH_PATH = HERE / "_ref" / "libref_bvh.so"
+REF_SCENE_PATH = HERE / "_ref" / "libref_scene.so"
+REF_ENVCDF_PATH = HERE / "_ref" / "libref_envcdf.so"
 
 _lib = None
 _ref = None
+_ref_scene = None
+_ref_envcdf = None
 
 NODE_DTYPE = np.dtype([("lo", "<f4", 3), ("leftOrPrim", "<u4"), ("hi", "<f4", 3), ("packed", "<u4")])
 
@@ -58,6 +64,7 @@ def load():
             "orc_readback_f32": (None, [vp, u32, u32, vp]), "orc_resolve_rgba8": (None, [vp, u32, f32, u32, vp]),
             "orc_pcg4d": (None, [vp, u32, vp]), "orc_stats": (None, [vp, vp]),
             "orc_diff_of_products": (None, [vp, u32, vp]),
+            "orc_mesh_attributes": (i32, [vp, u32, vp, u32, vp, vp, vp]),
             "orc_set_bruteforce": (None, [vp, i32]),
             "orc_set_all_leaf_instances": (None, [vp, i32]), "orc_unwalked_instances": (u32, [vp]),
         }
@@ -76,6 +83,74 @@ def diff_of_products(abcd):
     out = np.empty(x.shape[0], np.float32)
     load().orc_diff_of_products(x.ctypes.data, x.shape[0], out.ctypes.data)
     return out
+
+
+def _mesh_arrays(positions, indices, uvs):
+    pos = np.ascontiguousarray(np.asarray(positions, np.float32).reshape(-1, 3))
+    idx = np.ascontiguousarray(np.asarray(indices, np.uint32).reshape(-1))
+    uv = None if uvs is None else np.ascontiguousarray(np.asarray(uvs, np.float32).reshape(-1, 2))
+    return pos, idx, uv
+
+
+def _attributes(fn, positions, indices, uvs):
+    pos, idx, uv = _mesh_arrays(positions, indices, uvs)
+    n = np.zeros((pos.shape[0], 4), np.float32)
+    t = np.zeros((pos.shape[0], 4), np.float32)
+    k = fn(_p(pos), pos.shape[0], _p(idx), idx.size, _p(uv), _p(n), _p(t))
+    if k < 0:
+        raise ValueError("mesh rejected")
+    return n, (t if k else None)
+
+
+def mesh_attributes(positions, indices, uvs=None):
+    """The oracle's derived (normals, tangents or None) of a mesh given
+    without normals, 4 floats per vertex each."""
+    return _attributes(load().orc_mesh_attributes, positions, indices, uvs)
+
+
+def load_ref_scene():
+    """The reference's own scene store (compiled from its sources), or None."""
+    global _ref_scene
+    if _ref_scene is None and REF_SCENE_PATH.exists():
+        lib = C.CDLL(str(REF_SCENE_PATH))
+        lib.ref_mesh_attributes.restype = C.c_int
+        lib.ref_mesh_attributes.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p,
+                                            C.c_void_p]
+        _ref_scene = lib
+    return _ref_scene
+
+
+def ref_mesh_attributes(positions, indices, uvs=None):
+    """(normals, tangents or None) as the reference's Scene::addMesh derives
+    them (Scene.cpp:13-92), from its compiled sources."""
+    lib = load_ref_scene()
+    if lib is None:
+        raise RuntimeError("reference scene library not built (needs the reference checkout)")
+    return _attributes(lib.ref_mesh_attributes, positions, indices, uvs)
+
+
+def load_ref_envcdf():
+    """The reference's own environment-CDF loop (compiled), or None."""
+    global _ref_envcdf
+    if _ref_envcdf is None and REF_ENVCDF_PATH.exists():
+        lib = C.CDLL(str(REF_ENVCDF_PATH))
+        lib.ref_env_cdf.restype = None
+        lib.ref_env_cdf.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p]
+        _ref_envcdf = lib
+    return _ref_envcdf
+
+
+def ref_env_cdf(rgba):
+    """(cdf, integral) from the reference's Renderer.cpp:620-655 loop."""
+    lib = load_ref_envcdf()
+    if lib is None:
+        raise RuntimeError("reference env-CDF library not built (needs the reference checkout)")
+    px = np.ascontiguousarray(np.asarray(rgba, np.float32))
+    h, w = px.shape[:2]
+    cdf = np.empty(w * h + h, np.float32)
+    integ = C.c_float()
+    lib.ref_env_cdf(_p(px), w, h, _p(cdf), C.byref(integ))
+    return cdf, integ.value
 
 
 def load_ref_bvh():

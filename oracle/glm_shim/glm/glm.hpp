@@ -1,14 +1,19 @@
 // ORACLE -- test infrastructure only.
 //
 // A minimal stand-in for the subset of the GLM API that the reference's
-// core/include/mrt/MathTypes.hpp and core/src/accel/Bvh.cpp use, so that the
-// reference BVH builder compiles here (glm itself is not vendored in the
+// core/include/mrt/MathTypes.hpp, core/src/accel/Bvh.cpp,
+// core/src/scene/Scene.cpp and its environment-CDF loop use, so that those
+// reference sources compile here (glm itself is not vendored in the
 // reference checkout). Written from the GLSL/GLM public API: component-wise
 // vec2/vec3/vec4 arithmetic, scalar splats, operator[], min/max as
 // (b < a ? b : a) / (a < b ? b : a), and a column-major mat4. Only
-// component-wise operations reach the BVH build, so its results do not
-// depend on how this file associates multi-term sums (mat4 * vec4 below is
-// only compiled, never called by the build).
+// component-wise operations reach the BVH build. The geometric functions
+// follow the GLSL definitions with glm's evaluation: dot sums the products
+// left to right, cross is (y1 z2 - y2 z1, z1 x2 - z2 x1, x1 y2 - x2 y1),
+// length = sqrt(dot(v, v)) and normalize(v) = v * (1 / sqrt(dot(v, v)))
+// (glm's inversesqrt is 1 / sqrt); these are the only assumptions about
+// glm 1.0.1's arithmetic the scene-attribute pin rests on. mat4 * vec4 is
+// only compiled, never called by the code the pins run.
 #pragma once
 
 #include <cmath>
@@ -70,6 +75,24 @@ template <int N, class T> vec<N, T> operator*(const vec<N, T>& a, T s) {
     vec<N, T> r; for (uint32_t i = 0; i < N; ++i) r[i] = a[i] * s; return r;
 }
 template <int N, class T> vec<N, T>& operator+=(vec<N, T>& a, const vec<N, T>& b) { a = a + b; return a; }
+template <int N, class T> vec<N, T> operator/(const vec<N, T>& a, T s) {
+    vec<N, T> r; for (uint32_t i = 0; i < N; ++i) r[i] = a[i] / s; return r;
+}
+template <int N, class T> vec<N, T> operator-(const vec<N, T>& a) {
+    vec<N, T> r; for (uint32_t i = 0; i < N; ++i) r[i] = -a[i]; return r;
+}
+
+template <int N, class T> T dot(const vec<N, T>& a, const vec<N, T>& b) {
+    T s = a[0] * b[0];
+    for (uint32_t i = 1; i < N; ++i) s = s + a[i] * b[i];
+    return s;
+}
+template <class T> vec<3, T> cross(const vec<3, T>& a, const vec<3, T>& b) {
+    return vec<3, T>(a.y * b.z - b.y * a.z, a.z * b.x - b.z * a.x, a.x * b.y - b.x * a.y);
+}
+template <int N, class T> T length(const vec<N, T>& v) { return std::sqrt(dot(v, v)); }
+template <int N, class T> vec<N, T> normalize(const vec<N, T>& v) { return v * (T(1) / std::sqrt(dot(v, v))); }
+template <class T> constexpr T pi() { return T(3.14159265358979323846264338327950288); }
 
 template <int N, class T> vec<N, T> min(const vec<N, T>& a, const vec<N, T>& b) {
     vec<N, T> r; for (uint32_t i = 0; i < N; ++i) r[i] = (b[i] < a[i]) ? b[i] : a[i]; return r;

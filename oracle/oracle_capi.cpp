@@ -382,6 +382,33 @@ void orc_pcg4d(const uint32_t* in, uint32_t n, uint32_t* out) {
     }
 }
 
+// Derived attributes of one mesh as the oracle's scene store computes them
+// (normals when none are given, tangents when uvs are given; Scene.cpp:13-92
+// restated): normalsOut and tangentsOut receive 4 floats per vertex. Returns
+// the number of tangents written.
+int orc_mesh_attributes(const float* positions, uint32_t vertexCount, const uint32_t* indices, uint32_t indexCount,
+                        const float* uvs, float* normalsOut, float* tangentsOut) {
+    mrtMeshDesc d{};
+    d.structSize = sizeof(d);
+    d.vertexCount = vertexCount;
+    d.indexCount = indexCount;
+    d.positions = positions;
+    d.uvs = uvs;
+    d.indices = indices;
+    const MeshData m = copyMesh(d);
+    for (uint32_t i = 0; i < vertexCount; ++i) {
+        const V4<float>& n = m.normals[i];
+        normalsOut[4 * i] = n.x, normalsOut[4 * i + 1] = n.y, normalsOut[4 * i + 2] = n.z, normalsOut[4 * i + 3] = n.w;
+    }
+    if (tangentsOut)
+        for (size_t i = 0; i < m.tangents.size(); ++i) {
+            const V4<float>& t = m.tangents[i];
+            tangentsOut[4 * i] = t.x, tangentsOut[4 * i + 1] = t.y, tangentsOut[4 * i + 2] = t.z;
+            tangentsOut[4 * i + 3] = t.w;
+        }
+    return int(m.tangents.size());
+}
+
 // Kahan's a * b - c * d in single precision, as the watertight test's edge
 // fallback evaluates it (4 floats per entry in, 1 out).
 void orc_diff_of_products(const float* abcd, uint32_t n, float* out) {

@@ -236,3 +236,103 @@ def test_walk_modes_on_an_instanced_terrain(oracle_lib):
     assert np.allclose(every64, brute64, rtol=1e-12, atol=0)
     differ = ~np.all(faithful == brute, axis=-1)
     assert 0 < differ.sum() < 0.02 * differ.size
+
+
+# ---- pins against the reference's own scene store and env-CDF loop ---------
+# (oracle/build_oracle.py compiles core/src/scene/Scene.cpp and the CDF loop
+# of core/src/render/Renderer.cpp:620-655 from the reference sources into
+# oracle/_ref/; without the reference checkout these tests are skipped.)
+
+def attribute_meshes():
+    """Meshes that reach every branch of the reference's attribute code:
+    shared vertices, unused vertices (zero normal -> (0, 1, 0)), zero-area
+    triangles, degenerate uv triangles (|det| < 1e-12 skipped), tangents
+    parallel to the normal (the cross-product fallback), mirrored uvs
+    (negative handedness)."""
+    from miniraytrace_b200 import scenes
+    out = []
+    pos, idx, _, _ = scenes.heightfield(48)
+    out.append(("heightfield+uv", pos, idx, np.stack([pos[:, 0], pos[:, 2]], 1)))
+    ipos, iidx, _ = scenes.icosphere(2)
+    out.append(("icosphere", ipos, iidx, None))
+    r = np.random.default_rng(8)
+    soup = r.uniform(-1, 1, (300, 3)).astype(np.float32)
+    sidx = r.integers(0, 280, 600).astype(np.uint32)  # vertices 280..299 unused
+    sidx[:30] = np.repeat(sidx[:10], 3)                # zero-area triangles
+    uv = r.uniform(0, 1, (300, 2)).astype(np.float32)
+    uv[:40] = uv[0]                                    # degenerate uv triangles
+    uv[40:80, 0] *= -1                                 # mirrored
+    out.append(("soup", soup, sidx, uv))
+    flat = np.array([[0, 0, 0], [1, 0, 0], [0, 0, 1], [1, 0, 1]], np.float32)
+    fidx = np.array([0, 2, 1, 1, 2, 3], np.uint32)
+    fuv = np.array([[0, 0], [0, 0], [0, 1], [0, 1]], np.float32)  # u never changes: tangent fallback
+    out.append(("flat", flat, fidx, fuv))
+    return out
+
+
+def engine_attributes(tmp_path, pos, idx, uv):
+    import shutil
+    import subprocess
+    if shutil.which("g++") is None:
+        pytest.skip("needs g++")
+    root = Path(__file__).resolve().parents[1]
+    host = root / "miniraytrace_b200" / "csrc" / "host"
+    exe = tmp_path / "scene_attr_dump"
+    if not exe.exists():
+        subprocess.run(["g++", "-O2", "-std=c++17", "-ffp-contract=off", "-pthread", "-I", str(host), "-I",
+                        str(root / "include"), str(root / "tests" / "host" / "scene_attr_dump.cpp"),
+                        str(host / "scene.cpp"), "-o", str(exe)], check=True, capture_output=True)
+    pos = np.ascontiguousarray(pos, np.float32)
+    idx = np.ascontiguousarray(idx, np.uint32)
+    src, dst = tmp_path / "mesh.bin", tmp_path / "attr.bin"
+    with open(src, "wb") as f:
+        f.write(np.array([pos.shape[0], idx.size, 0 if uv is None else 1], np.uint32).tobytes())
+        f.write(pos.tobytes())
+        f.write(idx.tobytes())
+        if uv is not None:
+            f.write(np.ascontiguousarray(uv, np.float32).tobytes())
+    subprocess.run([str(exe), str(src), str(dst)], check=True)
+    a = np.fromfile(dst, np.float32).reshape(-1, 4)
+    nv = pos.shape[0]
+    return a[:nv], (a[nv:] if uv is not None else None)
+
+
+def test_mesh_attributes_equal_the_reference_scene_store(oracle_lib, tmp_path):
+    """Normals and tangents: the oracle's restatement and the engine's host
+    code (the attributes the GPU reads) equal, bit for bit, what the
+    reference's own Scene::addMesh computes (Scene.cpp:13-92)."""
+    if oracle_lib.load_ref_scene() is None:
+        pytest.skip("reference checkout absent: oracle/_ref/libref_scene.so not built")
+    for name, pos, idx, uv in attribute_meshes():
+        rn, rt = oracle_lib.ref_mesh_attributes(pos, idx, uv)
+        on, ot = oracle_lib.mesh_attributes(pos, idx, uv)
+        en, et = engine_attributes(tmp_path, pos, idx, uv)
+        assert np.array_equal(on, rn), name
+        assert np.array_equal(en[:, :3], rn[:, :3]), name
+        if uv is None:
+            assert rt is None and ot is None and et is None, name
+        else:
+            assert np.array_equal(ot, rt), name
+            assert np.array_equal(et, rt), name
+            if name == "soup":  # mirrored uvs give both handednesses
+                assert (rt[:, 3] == -1).any() and (rt[:, 3] == 1).any()
+
+
+def test_env_cdf_equals_the_reference_loop(oracle_lib):
+    """The oracle's CDF (which the device kernel matches bit for bit) equals
+    the reference's own loop compiled from Renderer.cpp: conditional rows,
+    marginal and integral, on maps with a sun peak, black rows, an all-black
+    map (integral clamped to 1e-8), one row, and odd sizes."""
+    if oracle_lib.load_ref_envcdf() is None:
+        pytest.skip("reference checkout absent: oracle/_ref/libref_envcdf.so not built")
+    from miniraytrace_b200 import scenes
+    maps = [scenes.procedural_sky(2048, 1024), scenes.procedural_sky(300, 77, sun_sigma_deg=3.0, sun_peak=500.0),
+            np.zeros((16, 8, 4), np.float32), scenes.procedural_sky(33, 1)]
+    holes = scenes.procedural_sky(128, 64)
+    holes[10:20] = 0.0
+    maps.append(holes)
+    for sky in maps:
+        cdf, integral = oracle_lib.env_cdf(sky)
+        rcdf, rintegral = oracle_lib.ref_env_cdf(sky)
+        assert np.array_equal(cdf, rcdf), sky.shape
+        assert np.float32(integral) == np.float32(rintegral), sky.shape
