@@ -12,6 +12,7 @@ and if no suitable GPU is present ``Engine()`` raises ``MrtError`` with
 from __future__ import annotations
 
 import ctypes as C
+import os
 from pathlib import Path
 
 import numpy as np
@@ -19,7 +20,8 @@ import numpy as np
 from . import abi
 from .abi import *  # noqa: F401,F403  (re-export enums and structs)
 
-_LIB_PATH = Path(__file__).resolve().parent / "libmrt.so"
+# MRT_LIBRARY names another build of the library (the autotuner's variants)
+_LIB_PATH = Path(os.environ.get("MRT_LIBRARY") or (Path(__file__).resolve().parent / "libmrt.so"))
 _lib = None
 
 

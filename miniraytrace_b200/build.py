@@ -6,11 +6,20 @@ The result, ``miniraytrace_b200/libmrt.so``, links the CUDA runtime statically
 and exports only the ``mrt*`` C ABI (every other symbol is hidden), so a
 caller needs nothing but the NVIDIA driver. Objects go to
 ``miniraytrace_b200/_build/`` and are rebuilt when their source or any header
-under ``csrc/`` or ``include/`` is newer.
+under ``csrc/`` or ``include/`` is newer, or when the kernels' tunable
+constants change.
+
+Tunable constants (thread-block sizes, register bounds, traversal
+scheduling thresholds) are preprocessor defines of the CUDA sources. Their
+values come from ``miniraytrace_b200/tuned.json``, written by the autotuner
+(``python -m miniraytrace_b200.autotune``); a define missing there keeps
+the default in the source. ``build(defines=..., lib=..., build_dir=...)``
+builds a variant elsewhere, which is how the autotuner measures candidates.
 """
 from __future__ import annotations
 
 import concurrent.futures as cf
+import json
 import os
 import shutil
 import subprocess
@@ -22,6 +31,10 @@ ROOT = PKG.parent
 CSRC = PKG / "csrc"
 BUILD = PKG / "_build"
 LIB = PKG / "libmrt.so"
+TUNED = PKG / "tuned.json"
+# Sources that read the tunable defines; a variant rebuilds only these and
+# links them with the shared objects of the main build directory.
+TUNED_SOURCES = {"pathtrace.cu"}
 
 CUDA_HOME = Path(os.environ.get("CUDA_HOME", "/usr/local/cuda"))
 NVCC = str(CUDA_HOME / "bin" / "nvcc")
@@ -70,20 +83,41 @@ def _run(cmd):
     return r
 
 
-def build(force: bool = False, verbose: bool = False) -> Path:
-    """Compile every kernel for sm_100a and link libmrt.so. Returns its path."""
+def tuned_defines() -> dict:
+    """The kernels' tunable constants chosen by the autotuner (name -> value)."""
+    if TUNED.exists():
+        return dict(json.loads(TUNED.read_text()).get("defines", {}))
+    return {}
+
+
+def build(force: bool = False, verbose: bool = False, defines: dict | None = None, lib: Path | None = None,
+          build_dir: Path | None = None) -> Path:
+    """Compile every kernel for sm_100a and link libmrt.so. Returns its path.
+    defines: the tunable constants (default: tuned.json); lib / build_dir:
+    where a variant goes (default: the package's libmrt.so and _build/)."""
+    if lib is None and os.environ.get("MRT_LIBRARY"):
+        return Path(os.environ["MRT_LIBRARY"])  # a variant built by its own build() call
     if not Path(NVCC).exists():
         raise RuntimeError(f"nvcc not found at {NVCC}")
+    defines = tuned_defines() if defines is None else dict(defines)
+    out = Path(lib) if lib else LIB
+    bdir = Path(build_dir) if build_dir else BUILD
+    bdir.mkdir(parents=True, exist_ok=True)
     BUILD.mkdir(exist_ok=True)
+    dflags = [f"-D{k}={v}" for k, v in sorted(defines.items())]
+    stamp = bdir / "defines.txt"
+    retune = not stamp.exists() or stamp.read_text() != " ".join(dflags)
     cu, cpp = _sources()
     hdr = _headers_mtime()
     jobs = []
     objs = []
     for src in cu:
-        obj = BUILD / (src.stem + ".cu.o")
+        tuned = src.name in TUNED_SOURCES
+        obj = (bdir if tuned else BUILD) / (src.stem + ".cu.o")
         objs.append(obj)
-        if force or _stale(obj, src, hdr):
-            jobs.append([NVCC, *NVCC_FLAGS, *NVCC_FILE_FLAGS.get(src.name, []), "-c", str(src), "-o", str(obj)])
+        if force or (tuned and retune) or _stale(obj, src, hdr):
+            jobs.append([NVCC, *NVCC_FLAGS, *(dflags if tuned else []), *NVCC_FILE_FLAGS.get(src.name, []), "-c",
+                         str(src), "-o", str(obj)])
     for src in cpp:
         obj = BUILD / (src.stem + ".o")
         objs.append(obj)
@@ -94,14 +128,15 @@ def build(force: bool = False, verbose: bool = False) -> Path:
             for r in ex.map(_run, jobs):
                 if verbose and r.stderr:
                     sys.stderr.write(r.stderr)
-    relink = force or bool(jobs) or not LIB.exists() or LIB.stat().st_mtime < max(o.stat().st_mtime for o in objs)
+    stamp.write_text(" ".join(dflags))
+    relink = force or bool(jobs) or not out.exists() or out.stat().st_mtime < max(o.stat().st_mtime for o in objs)
     if relink:
-        tmp = BUILD / "libmrt.so.tmp"
+        tmp = bdir / "libmrt.so.tmp"
         _run([NVCC, *ARCH, "-shared", "-cudart", "static", "-o", str(tmp), *map(str, objs),
               "-Xlinker", "--exclude-libs,ALL", "-Xlinker", "-z,defs",
               "-Xlinker", f"--version-script={CSRC / 'exports.map'}", "-lpthread", "-ldl", "-lrt"])
-        shutil.move(str(tmp), str(LIB))
-    return LIB
+        shutil.move(str(tmp), str(out))
+    return out
 
 
 if __name__ == "__main__":

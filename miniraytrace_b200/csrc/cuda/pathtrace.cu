@@ -176,9 +176,6 @@ enum { kExtendHead = 4, kShadowHead = 5 };
 // Threads per block of the traversal kernels and, when non-zero, the
 // minimum resident blocks per SM they are compiled for (which bounds their
 // registers; 0 leaves the register count to the compiler).
-#ifndef MRT_TRAV_THREADS
-#define MRT_TRAV_THREADS 128
-#endif
 #ifndef MRT_TRAV_MIN_BLOCKS
 #define MRT_TRAV_MIN_BLOCKS 7
 #endif
@@ -279,7 +276,11 @@ MRT_DEV void writeCacheFeatures(float* out, const Surface& s, float3 wo, const B
     f[3] = make_float4(bsdf.baseColor.z, 0.0f, 0.0f, 0.0f);
 }
 
-constexpr uint32_t kShadeBlock = 256;
+// Threads per block of the shade kernel.
+#ifndef MRT_SHADE_THREADS
+#define MRT_SHADE_THREADS 256
+#endif
+constexpr uint32_t kShadeBlock = MRT_SHADE_THREADS;
 
 // Appends to two lists at once, one atomic per list per block (a per-warp
 // atomic on the same counter serialised in L2: 4.2 M a bounce at 1080p x 64

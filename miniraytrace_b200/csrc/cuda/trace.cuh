@@ -459,13 +459,118 @@ MRT_DEV int travTriStep(const MrtFrameParams& P, WideTrav& T, TraversalCounters&
     return kTravRunning;
 }
 
+// Threads per block of the traversal kernels (a multiple of 32).
+#ifndef MRT_TRAV_THREADS
+#define MRT_TRAV_THREADS 128
+#endif
+
+// Warp-wide triangle phase: every pending (ray, triangle) pair of the warp
+// is tested, 32 pairs a round, one per lane, whichever lane owns the ray, so
+// lanes without triangles of their own (or without a ray) work too. Pairs
+// are numbered owner by owner in lane order and, within an owner, in
+// ascending triangle order; a lane finds the owner of its pair by a binary
+// search over the lanes' inclusive pair counts and takes the owner's ray
+// constants by shuffles. Closest hit: each hit is folded into its owner's
+// slot with a 64-bit shared-memory minimum of (t bits << 32 | triangle);
+// t > 0, so the bits order as the values, and the minimum is the nearest
+// hit with the lowest triangle index among equal t -- exactly the hit the
+// owner's own ascending scan with a shrinking tMax would keep, so results
+// are bit-identical to it. The winner's barycentrics follow through a
+// second slot written by the lane whose key equals the minimum. Any hit
+// (kAny): a warp-wide OR of the owners with a hit. Returns the lane's
+// kTrav* state; every pending lane ends with no triangles pending.
+template <bool kAny>
+MRT_DEV int travTriPhaseWarp(const MrtFrameParams& P, WideTrav& T, TraversalCounters& tc, bool pending) {
+    __shared__ unsigned long long sKey[MRT_TRAV_THREADS / 32][32];
+    __shared__ float2 sUV[MRT_TRAV_THREADS / 32][32];
+    const uint32_t full = 0xffffffffu;
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    const uint32_t bits = pending ? T.pendBits : 0u;
+    uint32_t incl = uint32_t(__popc(bits));
+#pragma unroll
+    for (uint32_t off = 1; off < 32; off <<= 1) {
+        const uint32_t v = __shfl_up_sync(full, incl, off);
+        if (lane >= off) incl += v;
+    }
+    const uint32_t total = __shfl_sync(full, incl, 31);
+    if (!kAny) sKey[warp][lane] = ~0ull;
+    __syncwarp();
+    const uint32_t kpack = uint32_t(T.sh.kx) | (uint32_t(T.sh.ky) << 2) | (uint32_t(T.sh.kz) << 4);
+    uint32_t occ = 0;  // kAny: bit o set when a pair of owner o hit
+    for (uint32_t first = 0; first < total; first += 32) {
+        const uint32_t k = first + lane;
+        // owner o: the first lane whose inclusive count exceeds k
+        uint32_t o = 0;
+#pragma unroll
+        for (uint32_t step = 16; step > 0; step >>= 1)
+            if (__shfl_sync(full, incl, o + step - 1) <= k) o += step;
+        const uint32_t ob = __shfl_sync(full, bits, o);
+        const uint32_t oi = __shfl_sync(full, incl, o);
+        const uint32_t obase = __shfl_sync(full, T.pendBase, o);
+        const uint32_t okp = __shfl_sync(full, kpack, o);
+        const float3 oo = f3(__shfl_sync(full, T.o.x, o), __shfl_sync(full, T.o.y, o), __shfl_sync(full, T.o.z, o));
+        Shear sh;
+        sh.kx = int(okp & 3u);
+        sh.ky = int((okp >> 2) & 3u);
+        sh.kz = int((okp >> 4) & 3u);
+        sh.sx = __shfl_sync(full, T.sh.sx, o);
+        sh.sy = __shfl_sync(full, T.sh.sy, o);
+        sh.sz = __shfl_sync(full, T.sh.sz, o);
+        const float otMax = __shfl_sync(full, T.tMax, o);
+        bool hit = false;
+        unsigned long long key = 0;
+        float u = 0.0f, v = 0.0f;
+        if (k < total) {
+            // the pair is bit number (k - first pair of o) among o's pending bits
+            const uint32_t nth = k - (oi - uint32_t(__popc(ob)));
+            const uint32_t tri = obase + __fns(ob, 0u, int(nth) + 1);
+            ++tc.tris;
+            if (tri >= P.triCount) {
+                tc.bad = true;
+            } else {
+                float t;
+                hit = hitTriangle(P.triVerts, tri, oo, sh, otMax, t, u, v);
+                if (hit) {
+                    if (kAny) {
+                        occ |= 1u << o;
+                    } else {
+                        key = (uint64_t(__float_as_uint(t)) << 32) | tri;
+                        atomicMin(&sKey[warp][o], key);
+                    }
+                }
+            }
+        }
+        if (!kAny) {
+            __syncwarp();
+            if (hit && sKey[warp][o] == key) sUV[warp][o] = make_float2(u, v);
+        }
+    }
+    __syncwarp();
+    if (!pending) return kTravRunning;
+    T.pendBits = 0;
+    if (kAny) return (__reduce_or_sync(full, occ) >> lane) & 1u ? kTravOccluded : kTravRunning;
+    const unsigned long long best = sKey[warp][lane];
+    if (best != ~0ull) {
+        const float t = __uint_as_float(uint32_t(best >> 32));
+        const float2 uv = sUV[warp][lane];
+        T.tMax = t;
+        T.hit.t = t;
+        T.hit.u = uv.x;
+        T.hit.v = uv.y;
+        T.hit.tri = uint32_t(best);
+        T.hit.inst = T.inst;
+    }
+    return kTravRunning;
+}
+
 // One warp-wide traversal step; every lane of the warp calls it, `active`
 // lanes advance their ray. Triangle tests are batched across the warp
 // (after Ylitie et al. 2017, section 4): a lane whose node test found leaf
-// triangles waits with them pending, and the warp runs a triangle phase once
-// at least MRT_TRI_PHASE_PCT percent of its active lanes have triangles
-// pending, or no lane has node work left; otherwise lanes without pending
-// triangles test one node each. Returns the lane's kTrav* state.
+// triangles waits with them pending, and the warp runs a triangle phase
+// (travTriPhaseWarp) once at least MRT_TRI_PHASE_PCT percent of its active
+// lanes have triangles pending, or no lane has node work left; otherwise
+// lanes without pending triangles test one node each. Returns the lane's
+// kTrav* state.
 #ifndef MRT_TRI_PHASE_PCT
 #define MRT_TRI_PHASE_PCT 25
 #endif
@@ -476,7 +581,7 @@ MRT_DEV int travWarpStep(const MrtFrameParams& P, WideTrav& T, WideStack& stack,
     const uint32_t pendLanes = __popc(__ballot_sync(0xffffffffu, pending));
     const uint32_t activeLanes = __popc(__ballot_sync(0xffffffffu, active));
     const bool triPhase = pendLanes * 100u >= activeLanes * MRT_TRI_PHASE_PCT || pendLanes == activeLanes;
-    if (triPhase) return pending ? travTriStep<kAny>(P, T, tc) : kTravRunning;
+    if (triPhase) return travTriPhaseWarp<kAny>(P, T, tc, pending);
     return active && !pending ? travNodeStep(P, T, stack, tc) : kTravRunning;
 }
 
