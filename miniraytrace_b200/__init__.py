@@ -340,6 +340,12 @@ class Engine:
         queries read (0 = queries read the live weights)."""
         _check(self.lib.mrtxSetRadianceCacheAveraging(self.h, float(decay)), "mrtxSetRadianceCacheAveraging")
 
+    def set_cache_schedule(self, lr_min: float, half_life_steps: float):
+        """mrtxSetRadianceCacheSchedule: the training rate halves every
+        half_life_steps Adam steps down to lr_min (0 = constant rate)."""
+        _check(self.lib.mrtxSetRadianceCacheSchedule(self.h, float(lr_min), float(half_life_steps)),
+               "mrtxSetRadianceCacheSchedule")
+
     def cache_gradients(self, features, targets):
         """mrtxRadianceCacheGradients: (grid gradient, MLP gradient, mean
         loss) of one batch, without an optimizer step."""

@@ -183,6 +183,7 @@ FUNCTIONS = [
     ("mrtxSetTraversalBudget", C.c_int, [C.c_void_p, C.c_uint32]),
     ("mrtxTraceRaysWavefront", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]),
     ("mrtxSetRadianceCacheAveraging", C.c_int, [C.c_void_p, C.c_float]),
+    ("mrtxSetRadianceCacheSchedule", C.c_int, [C.c_void_p, C.c_float, C.c_float]),
     ("mrtxRadianceCacheGradients", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p,
                                              C.c_void_p]),
     ("mrtxInjectAllocationFailure", C.c_int, [C.c_int32]),

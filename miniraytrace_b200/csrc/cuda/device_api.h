@@ -25,6 +25,11 @@ typedef struct McacheParams {
     float lo[3], invExtent[3];
     uint32_t step;
     float lr;
+    // Learning-rate schedule: step k (1-based) uses
+    // max(min(lrMin, lr), lr * 2^-((k - lrStart - 1) / lrHalfLife)), so the
+    // first step after a (re)start uses lr; lrHalfLife 0 keeps lr constant.
+    float lrMin, lrHalfLife;
+    uint32_t lrStart;
     uint32_t* status;        // device word: bit 0 set when a tensor-core wait gave up
 } McacheParams;
 

@@ -793,9 +793,13 @@ extern "C" cudaError_t mrtcu_rc_train(McacheParams* C, const float* features, co
         const float c1 = 1.0f / (1.0f - powf(b1, float(C->step))), c2 = 1.0f / (1.0f - powf(b2, float(C->step)));
         const float st = float(C->step);
         const float d = fminf(C->emaDecay, (1.0f + st) / (10.0f + st));
-        adamKernel<<<gridFor(gridN), 256, 0, stream>>>(C->grid, C->gGrid, C->mGrid, C->vGrid, gridN, C->lr, b1, b2,
+        float lr = C->lr;
+        if (C->lrHalfLife > 0.0f)
+            lr = fmaxf(fminf(C->lrMin, C->lr),
+                       C->lr * exp2f(-float(C->step - C->lrStart - 1u) / C->lrHalfLife));
+        adamKernel<<<gridFor(gridN), 256, 0, stream>>>(C->grid, C->gGrid, C->mGrid, C->vGrid, gridN, lr, b1, b2,
                                                        1e-10f, c1, c2, true, C->emaGrid, d);
-        adamKernel<<<gridFor(mlpN), 256, 0, stream>>>(C->mlp, C->gMlp, C->mMlp, C->vMlp, mlpN, C->lr, b1, b2,
+        adamKernel<<<gridFor(mlpN), 256, 0, stream>>>(C->mlp, C->gMlp, C->mMlp, C->vMlp, mlpN, lr, b1, b2,
                                                       1e-10f, c1, c2, false, C->emaMlp, d);
     }
     return cudaGetLastError();

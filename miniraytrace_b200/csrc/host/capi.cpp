@@ -349,6 +349,12 @@ MRT_API mrtResult mrtxRadianceCacheGradients(mrtEngine* e, const float* features
     return guarded([&] { return eng->cacheGradients(features, targets, count, gridGradOut, mlpGradOut, lossOut); });
 }
 
+MRT_API mrtResult mrtxSetRadianceCacheSchedule(mrtEngine* e, float lrMin, float halfLifeSteps) {
+    mrt::Engine* eng = unwrap(e);
+    if (!eng) return MRT_ERROR_INVALID_HANDLE;
+    return guarded([&] { return eng->setCacheSchedule(lrMin, halfLifeSteps); });
+}
+
 MRT_API mrtResult mrtxSetRadianceCacheAveraging(mrtEngine* e, float decay) {
     mrt::Engine* eng = unwrap(e);
     if (!eng) return MRT_ERROR_INVALID_HANDLE;

@@ -1506,6 +1506,9 @@ mrtResult Engine::ensureCache() {
     c.emaDecay = m_cache.emaDecay;
     c.step = 0;
     c.lr = m_cache.lr;
+    c.lrMin = m_cache.lrMin;
+    c.lrHalfLife = m_cache.lrHalfLife;
+    c.lrStart = 0;
     cacheBounds();
     MRT_CUDA(mrtcu_rc_init(c, m_cache.seed, m_stream));
     MRT_CUDA(cudaStreamSynchronize(m_stream));
@@ -1522,7 +1525,9 @@ mrtResult Engine::setRadianceCache(const mrtxRadianceCacheDesc& d) {
     m_cache.stepsPerSample = d.stepsPerSample ? d.stepsPerSample : 1u;
     m_cache.samplesPerUpdate = d.samplesPerUpdate ? std::min(d.samplesPerUpdate, 64u) : 4u;
     m_cache.trainingVertices = d.trainingVertices;
-    m_cache.lr = d.learningRate > 0.0f ? d.learningRate : 1e-2f;
+    const float lr = d.learningRate > 0.0f ? d.learningRate : 1e-2f;
+    const bool newRate = lr != m_cache.lr;
+    m_cache.lr = lr;
     m_cache.seed = d.seed;
     for (int a = 0; a < 3; ++a) {
         m_cache.lo[a] = d.boundsLo[a];
@@ -1531,6 +1536,7 @@ mrtResult Engine::setRadianceCache(const mrtxRadianceCacheDesc& d) {
     if (reinit) m_cache.release();
     MRT_TRY(guard(ensureCache()));
     m_cache.params.lr = m_cache.lr;
+    if (newRate) m_cache.params.lrStart = m_cache.params.step;  // the decay restarts from the new rate
     cacheBounds();
     if (bool(d.enabled) != m_cache.enabled) resetAccumulation();  // a different estimator
     m_cache.enabled = d.enabled != 0;
@@ -1571,6 +1577,24 @@ mrtResult Engine::cacheTrain(const float* features, const float* targets, uint32
     const cudaError_t e = cudaStreamSynchronize(m_stream);
     if (e != cudaSuccess) return guard(fromCuda(e, "radiance cache training"));
     if (loss) *loss = l;
+    return MRT_SUCCESS;
+}
+
+// Learning-rate decay of the online training: the rate halves every
+// halfLifeSteps Adam steps down to lrMin (halfLifeSteps 0: constant rate),
+// restarting from the full rate now.
+mrtResult Engine::setCacheSchedule(float lrMin, float halfLifeSteps) {
+    MRT_TRY(checkAlive());
+    MRT_TRY(flushPending());
+    MRT_TRY(cacheStatus(0));
+    if (!(lrMin >= 0.0f) || !(halfLifeSteps >= 0.0f))
+        return fail(MRT_ERROR_INVALID_ARGUMENT, "radiance cache schedule: lrMin and halfLifeSteps must be >= 0");
+    MRT_TRY(guard(ensureCache()));
+    m_cache.lrMin = lrMin;
+    m_cache.lrHalfLife = halfLifeSteps;
+    m_cache.params.lrMin = lrMin;
+    m_cache.params.lrHalfLife = halfLifeSteps;
+    m_cache.params.lrStart = m_cache.params.step;
     return MRT_SUCCESS;
 }
 
@@ -1664,6 +1688,7 @@ mrtResult Engine::cacheParams(float* gridOut, float* mlpOut, const float* gridIn
         for (DeviceBuffer* d : {&m_cache.gMlp, &m_cache.mMlp, &m_cache.vMlp})
             MRT_CUDA(cudaMemsetAsync(d->ptr, 0, w, m_stream));
         m_cache.params.step = 0;
+        m_cache.params.lrStart = 0;
         MRT_TRY(resetAverage());
     }
     const cudaError_t e = cudaStreamSynchronize(m_stream);

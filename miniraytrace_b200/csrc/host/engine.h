@@ -75,6 +75,7 @@ public:
     mrtResult cacheGradients(const float* features, const float* targets, uint32_t n, float* gridOut, float* mlpOut,
                              float* loss);
     mrtResult setCacheAveraging(float decay);
+    mrtResult setCacheSchedule(float lrMin, float halfLifeSteps);
     mrtResult buildMeshBvhDevice(const V4f* pos, size_t nv, const uint32_t* idx, size_t nt, uint32_t maxLeaf,
                                  WideBvh& out);
     // Device build from device positions/indices into the builder's own
@@ -150,7 +151,9 @@ private:
         bool failed = false;
         uint32_t trainingPaths = 0, stepsPerSample = 1, seed = 1, samplesPerUpdate = 4, trainingVertices = 0;
         float lr = 1e-2f;
-        float emaDecay = 0.0f;  // 0: inference reads the live parameters (the default)
+        float emaDecay = 0.99f;  // 0: inference reads the live parameters
+        // learning-rate decay: halves every lrHalfLife steps down to lrMin (0: constant)
+        float lrMin = 3e-4f, lrHalfLife = 48.0f;
         float lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
         void release();
     } m_cache;

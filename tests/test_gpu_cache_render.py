@@ -1,10 +1,11 @@
 """Rendering with the radiance cache (config 4's room at reduced sizes).
 Switching the cache on or off starts a new accumulation; with it off the
-path tracer is the plain one, bit for bit. With it on, the image is finite
-and opaque, its mean stays within 15 % of a converged plain image (the cache
-is biased, and its bias drifts as it trains), and at equal sample counts
-after a short training warm-up its
-relMSE against that image is well below the plain tracer's."""
+path tracer is the plain one, bit for bit. With it on (default training
+schedule: the learning rate halves every 48 Adam steps down to 3e-4, and
+queries read a moving average of the weights), after a training warm-up
+the image is finite and opaque, its mean stays within 3 % of a converged
+plain image for two cache seeds, and its relMSE against that image is at
+most half the plain tracer's at equal sample counts."""
 import numpy as np
 import pytest
 
@@ -40,17 +41,15 @@ def test_cache_toggle_keeps_the_plain_path(gpu):
     b.close()
 
 
-def test_cached_render_beats_plain_at_equal_samples(gpu):
-    # 320x180: about 1,800 training paths a sample. The cache is trained
-    # online with a constant learning rate, and its overall brightness drifts
-    # from one training round to the next (the gradient sums also use float
-    # atomics, so no two runs are alike). Mean of the cached image over the
-    # converged one, measured on a B200 (two seeds each): 64 warm-up samples
-    # 1.007 to 1.054; 256 samples 0.85 to 0.95; 1,024 samples 0.95 to 1.03;
-    # more training paths, a learning rate of 3e-3 or one training vertex
-    # stayed within 0.88 to 1.01. The bound on the mean (15 %) therefore only
-    # catches a gross error; the quality check is the relMSE, which stayed
-    # within 0.42 to 0.49 of the plain tracer's in every one of those runs.
+@pytest.mark.parametrize("seed", [1, 2])
+def test_cached_render_beats_plain_at_equal_samples(gpu, seed):
+    # 320x180: about 1,800 training paths a sample, one Adam step a sample.
+    # With a constant learning rate (1e-2) the cache's weights kept wandering
+    # and the cached image's mean over the converged one ranged 0.85 to 1.20
+    # between runs (four seeds, warm-ups of 64 and 256 samples); averaging
+    # the weights alone did not change that. Decaying the rate settled it:
+    # 0.995 to 1.003 with averaging (four seeds, 256-sample warm-up), relMSE
+    # 0.30 to 0.32 of the plain tracer's (B200 measurements).
     w, h, spp = 320, 180, 64
     s = scenes.room(w, h)
     ref = gpu.Engine(w, h)
@@ -66,14 +65,15 @@ def test_cached_render_beats_plain_at_equal_samples(gpu):
     plain.close()
     e = gpu.Engine(w, h)
     s.apply(e)
-    e.set_radiance_cache(enabled=True)
-    e.render_frames(64)        # training warm-up
+    e.set_radiance_cache(enabled=True, seed=seed)
+    e.render_frames(256)       # training warm-up
     e.set_sample_stream(0, 1)  # new accumulation, same trained cache
     e.render_frames(spp)
     X = e.read_framebuffer()[..., :3].astype(np.float64)
     e.close()
     err_cached = rel_mse(X, R)
-    print(f"cached/converged mean {X.mean() / R.mean():.4f}, relMSE cached {err_cached:.3e} plain {err_plain:.3e}")
+    print(f"seed {seed}: cached/converged mean {X.mean() / R.mean():.4f}, relMSE cached {err_cached:.3e} "
+          f"plain {err_plain:.3e}")
     assert np.isfinite(X).all()
-    assert abs(X.mean() / R.mean() - 1.0) < 0.15, (X.mean(), R.mean())
-    assert err_cached < 0.7 * err_plain, (err_cached, err_plain)
+    assert abs(X.mean() / R.mean() - 1.0) < 0.03, (X.mean(), R.mean())
+    assert err_cached < 0.5 * err_plain, (err_cached, err_plain)

@@ -92,12 +92,12 @@ def test_commit_and_render_recover_from_allocation_failures(gpu):
             try:
                 e.commit()
             except gpu.MrtError as err:
-                assert err.value.code == abi.MRT_ERROR_OUT_OF_MEMORY, err.value
+                assert err.code == abi.MRT_ERROR_OUT_OF_MEMORY, err
                 failed_commits += 1
             try:
                 e.render_frames(SPP)
             except gpu.MrtError as err:
-                assert err.value.code == abi.MRT_ERROR_OUT_OF_MEMORY, err.value
+                assert err.code == abi.MRT_ERROR_OUT_OF_MEMORY, err
                 failed_renders += 1
         finally:
             gpu.inject_allocation_failure(-1)

@@ -184,7 +184,7 @@ def test_wavefront_extend_kernel_at_config2_scale(gpu, oracle_lib):
     h1 = e.trace_rays(o1, d1, wavefront=True)
     # secondary rays from the primary hits, in all directions, mostly upward
     hit = h1["hit"] == 1
-    assert hit.mean() > 0.5
+    assert hit.mean() > 0.2  # the camera sees a third terrain, two thirds sky
     p = o1[hit] + h1["t"][hit][:, None] * d1[hit]
     k = p.shape[0]
     d2 = rng.normal(size=(k, 3)).astype(np.float32)
