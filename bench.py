@@ -66,6 +66,8 @@ def parse_args():
     ap.add_argument("--interactive-frames", type=int, default=48,
                     help="frames of the plug-in's loop (mrtCommitScene, mrtRenderFrame, RGBA32F readback every "
                          "frame) timed for e2e_interactive (0 = skip)")
+    ap.add_argument("--no-room", action="store_true",
+                    help="skip config 4's time to relMSE 1e-3 (cached vs plain) in the default line")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--spp", type=int, default=0, help="samples per pixel per step (0 = the workload's 64)")
@@ -239,7 +241,7 @@ def reference_arm(args):
 
 def ours_arm(args):
     import miniraytrace_b200 as mrt
-    from miniraytrace_b200 import replicas
+    from miniraytrace_b200 import replicas, scenes
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -390,6 +392,18 @@ def ours_arm(args):
             "loop": "mrtCommitScene + mrtRenderFrame (1 spp) + mrtReadFramebuffer(RGBA32F) into host memory, "
                     "per frame (the plug-in's render loop), wall-clock"}
 
+    # Config 4's time to relMSE 1e-3, cached vs plain (the second half of
+    # the headline metric), on the same GPU after the timed region.
+    room = None
+    if world == 1 and args.config == "terrain" and not args.no_room:
+        eng.close()
+        ref, ref_s = room_reference(mrt, scenes)
+        room = time_to_relmse(mrt, scenes, ref)
+        room["workload"] = ROOM_WORKLOAD
+        room["reference_render_s"] = ref_s
+        for arm in ("plain", "cached"):
+            room[arm].pop("curve_spp_ms_relmse", None)
+
     out = None
     if rank == 0:
         cpu = None
@@ -448,6 +462,7 @@ def ours_arm(args):
             "clocks": clocks,
             "e2e": e2e,
             "e2e_interactive": interactive,
+            "time_to_relmse_1e-3": room,
             "cpu_baseline": cpu,
         }
         print(json.dumps(out), flush=True)
@@ -541,15 +556,18 @@ def rel_mse(x, r):
     return float(np.mean(np.sum((x - r) ** 2 / (r * r + 1e-2), axis=-1)))
 
 
-def converge(engine, ref, target, chunk, limit):
+def converge(engine, ref, target, chunk, limit, windows=None):
     """Adds `chunk` samples at a time until the image is within relMSE
-    `target` of `ref` (or `limit` samples). Returns (spp, device seconds,
-    reached, curve of (spp, device ms, relMSE) at powers of two and at the
-    end). Device time is the engines' CUDA-event render time; the readback
-    and the relMSE between chunks are not counted."""
+    `target` of `ref` (or `limit` samples). With `windows` (a list of
+    (x0, y0, w, h)) the relMSE is taken over those windows' pixels, `ref`
+    holding them side by side in the same order. Returns (spp, device
+    seconds, reached, curve of (spp, device ms, relMSE) at powers of two and
+    at the end, cache counters, the image's mean over the reference's). Device
+    time is the engine's CUDA-event render time; the readback and the relMSE
+    between chunks are not counted."""
     spp, device_ms, curve = 0, 0.0, []
     cache = {"cacheQueryMs": 0.0, "cacheTrainMs": 0.0, "cacheQueries": 0, "cacheRecords": 0, "cacheSteps": 0}
-    err = float("inf")
+    err, X = float("inf"), None
     while err > target and spp < limit:
         engine.render_frames(chunk)
         spp += chunk
@@ -557,44 +575,79 @@ def converge(engine, ref, target, chunk, limit):
         device_ms += st["lastRenderMs"]
         for k in cache:
             cache[k] += st[k]
-        err = rel_mse(engine.read_framebuffer()[..., :3].astype(np.float64), ref)
+        img = engine.read_framebuffer()[..., :3]
+        X = (img if windows is None else
+             np.concatenate([img[y:y + h, x:x + w].reshape(-1, 3) for x, y, w, h in windows])).astype(np.float64)
+        err = rel_mse(X, ref)
         if spp & (spp - 1) == 0 or err <= target:
             curve.append((spp, round(device_ms, 1), err))
-    return spp, device_ms / 1e3, err <= target, curve, cache
+    return spp, device_ms / 1e3, err <= target, curve, cache, float(X.mean() / ref.mean())
 
 
 # FLOPs of one radiance-cache query: 5 hidden 64 x 64 layers and the 16 x 64
 # output layer as the tensor cores compute it, 2 FLOPs per multiply-add.
 CACHE_QUERY_FLOPS = 2 * (5 * 64 * 64 + 16 * 64)
 
+# Config 4's reference: 65,536 samples per pixel of the plain tracer, FP64
+# accumulated, over four 240 x 136 windows of the 1920 x 1080 frame centred
+# on its quadrants (130,560 pixels, a sixteenth of the frame; the whole frame
+# at that count would take about ten minutes). Each window is rendered by its
+# own engine through the exact sub-frustum of the frame's camera, so its
+# pixels estimate the same pixel integrals as the frame's.
+ROOM_REF_SPP = 65536
+ROOM_WINDOWS = [(360, 202, 240, 136), (1320, 202, 240, 136), (360, 742, 240, 136), (1320, 742, 240, 136)]
 
-def room_arm(args):
-    """Config 4 at 1920x1080, time to relMSE 1e-3, plain and radiance-cached.
-    The reference image is 16,384 spp of the plain tracer on a sample stream
-    disjoint from both measured runs. Each run starts from nothing (the
-    cached run from an untrained cache, so its training is timed) and adds
-    samples in chunks until the image is within relMSE 1e-3 of the
-    reference; its time is the summed device render time of those chunks."""
-    import torch
 
-    import miniraytrace_b200 as mrt
-    from miniraytrace_b200 import build as mrt_build
-    from miniraytrace_b200 import scenes
+def window_camera(cam, width, height, window):
+    """mrtSetCameraEx arguments of the sub-frustum of a look-at camera that
+    covers pixels [x0, x0 + w) x [y0, y0 + h) of a width x height frame
+    (reference Renderer.cpp:711-764: the frame spans [-tan * aspect, tan *
+    aspect] x [-tan, tan], rows top down)."""
+    x0, y0, w, h = window
+    th = float(np.tan(np.float32(cam["fov_y_deg"]) * np.float32(0.017453292519943295) * np.float32(0.5)))
+    r = th * width / height
+    lerp = lambda a, b, t: a * (1.0 - t) + b * t  # noqa: E731
+    pos = np.asarray(cam["position"], np.float64)
+    return dict(position=cam["position"], forward=tuple(np.asarray(cam["target"], np.float64) - pos), up=cam["up"],
+                left=lerp(-r, r, x0 / width), right=lerp(-r, r, (x0 + w) / width),
+                top=lerp(th, -th, y0 / height), bottom=lerp(th, -th, (y0 + h) / height))
 
-    if int(os.environ.get("RANK", "0")) != 0:
-        return 0
-    torch.cuda.set_device(0)
-    mrt_build.build()
-    W, H, REF_SPP, TARGET = 1920, 1080, 16384, 1e-3
+
+def room_reference(mrt, scenes, ref_spp=ROOM_REF_SPP, windows=ROOM_WINDOWS, chunk=1024):
+    """The reference pixels of the config-4 windows (float64, windows side by
+    side) and the device seconds it took; rendered as one mrtxRenderBatch of
+    the window engines per `chunk` samples, on a sample stream disjoint from
+    the measured runs."""
+    W, H = 1920, 1080
     s = scenes.room(W, H)
-    ref = mrt.Engine(W, H)
-    s.apply(ref)
-    ref.set_sample_stream(1 << 24, 1)  # samples disjoint from the measured runs'
-    ref.render_frames(REF_SPP)
-    R = ref.read_framebuffer()[..., :3].astype(np.float64)
-    ref.close()
-    sampler = ClockSampler(0)
-    sampler.start()
+    engines = []
+    for win in windows:
+        e = mrt.Engine(win[2], win[3])
+        s.apply(e)
+        e.set_render_settings(**dict(s.settings, width=win[2], height=win[3]))
+        e.set_camera_ex(**window_camera(s.camera, W, H, win))
+        e.set_sample_stream(1 << 24, 1)
+        e.commit()
+        engines.append(e)
+    import time as _t
+    t0 = _t.perf_counter()
+    for _ in range(ref_spp // chunk):
+        mrt.render_batch(engines, [chunk] * len(engines))
+    secs = _t.perf_counter() - t0
+    ref = np.concatenate([e.read_framebuffer()[..., :3].reshape(-1, 3) for e in engines]).astype(np.float64)
+    for e in engines:
+        e.close()
+    return ref, secs
+
+
+def time_to_relmse(mrt, scenes, ref, windows=ROOM_WINDOWS, target=1e-3):
+    """Config 4 at 1920x1080, plain and radiance-cached: each run starts from
+    nothing (the cached run from an untrained cache, so its training is
+    timed) and adds samples in chunks (64 plain, 16 cached) until the
+    windows' relMSE against the reference is at most `target`; its time is
+    the summed CUDA-event render time of those chunks."""
+    W, H = 1920, 1080
+    s = scenes.room(W, H)
     arms = {}
     for mode, chunk in (("plain", 64), ("cached", 16)):
         e = mrt.Engine(W, H)
@@ -602,9 +655,9 @@ def room_arm(args):
         e.commit()
         if mode == "cached":
             e.set_radiance_cache(enabled=True)
-        spp, secs, reached, curve, cache = converge(e, R, TARGET, chunk, REF_SPP // 4)
+        spp, secs, reached, curve, cache, mean = converge(e, ref, target, chunk, 4096, windows)
         arms[mode] = {"spp_to_target": spp if reached else None, "seconds": secs if reached else None,
-                      "ms_per_spp": secs * 1e3 / spp, "curve_spp_ms_relmse": curve}
+                      "ms_per_spp": secs * 1e3 / spp, "mean_over_reference": mean, "curve_spp_ms_relmse": curve}
         if mode == "cached" and cache["cacheQueryMs"] > 0:
             peak = measured_bf16_tflops()
             tflops = cache["cacheQueries"] * CACHE_QUERY_FLOPS / (cache["cacheQueryMs"] * 1e-3) / 1e12
@@ -616,19 +669,45 @@ def room_arm(args):
                 "training_steps": cache["cacheSteps"],
                 "share_of_render_time": (cache["cacheQueryMs"] + cache["cacheTrainMs"]) / (secs * 1e3)}
         e.close()
-    clocks = sampler.stop()
     plain_s, cached_s = arms["plain"]["seconds"], arms["cached"]["seconds"]
+    return {"target_relmse": target, "plain_s": plain_s, "cached_s": cached_s,
+            "plain_over_cached": plain_s / cached_s if plain_s and cached_s else None,
+            "cached_mean_over_reference": arms["cached"]["mean_over_reference"],
+            "plain": arms["plain"], "cached": arms["cached"]}
+
+
+ROOM_WORKLOAD = ("config 4: closed 20x4x10 room lit through one 2x2 window by the config-2 sky, config-2 heightfield "
+                 "as terrain (2,093,076 triangles), 1920x1080, depth 12; relMSE over four 240x136 windows against "
+                 f"{ROOM_REF_SPP} spp of the plain tracer (FP64 accumulation, independent sample stream); cache: "
+                 "hash grid 16 x 2^19 x 2 + 5 x 64 ReLU MLP, Adam lr 1e-2 halving every 48 steps down to 3e-4, "
+                 "moving-average weights for inference, a 32nd of the pixels as training paths, trained after "
+                 "every 4 samples")
+
+
+def room_arm(args):
+    """Config 4 at 1920x1080, time to relMSE 1e-3, plain and radiance-cached
+    (time_to_relmse), reported on its own."""
+    import torch
+
+    import miniraytrace_b200 as mrt
+    from miniraytrace_b200 import build as mrt_build
+    from miniraytrace_b200 import scenes
+
+    if int(os.environ.get("RANK", "0")) != 0:
+        return 0
+    torch.cuda.set_device(0)
+    mrt_build.build()
+    ref, ref_s = room_reference(mrt, scenes)
+    sampler = ClockSampler(0)
+    sampler.start()
+    res = time_to_relmse(mrt, scenes, ref)
+    clocks = sampler.stop()
     out = {
-        "metric": "time to relMSE 1e-3, radiance-cached (config 4)", "value": cached_s, "unit": "s",
+        "metric": "time to relMSE 1e-3, radiance-cached (config 4)", "value": res["cached_s"], "unit": "s",
         "higher_is_better": False, "n_gpus": 1, "dtype": "f32 (cache inference bf16)", "data": "synthetic",
-        "config": {"workload": "config 4: closed 20x4x10 room lit through one 2x2 window by the config-2 sky, "
-                               "config-2 heightfield as terrain (2,093,076 triangles), 1920x1080, depth 12",
-                   "reference": f"{REF_SPP} spp of the plain tracer, independent sample stream",
-                   "cache": "hash grid 16 x 2^19 x 2 + 5 x 64 ReLU MLP, Adam lr 1e-2, a 32nd of the pixels "
-                            "as training paths per sample, trained after every 4 samples",
-                   "chunk_spp": {"plain": 64, "cached": 16}},
-        "plain": arms["plain"], "cached": arms["cached"],
-        "plain_over_cached": plain_s / cached_s if plain_s and cached_s else None,
+        "config": {"workload": ROOM_WORKLOAD, "chunk_spp": {"plain": 64, "cached": 16},
+                   "reference_render_s": ref_s},
+        **{k: v for k, v in res.items()},
         "vs_baseline": None,
         "clocks": clocks,
     }
