@@ -13,47 +13,61 @@
 namespace {
 
 // Environment CDF (reference Renderer.cpp:620-655), bit-exact with the
-// reference's sequential double-precision sums: every row is accumulated
-// left to right by one thread (rows in parallel), the marginal and the
-// integral top to bottom by one thread. The map is streamed through shared
-// memory in 32-row x 128-column tiles so global loads and stores stay
-// coalesced; the dependent double-add chain of one row is the critical path
-// (a few tens of microseconds for a 4096 x 2048 map).
-constexpr int kCdfRows = 32;
+// reference's sequential double-precision sums. The conditional CDF of a row
+// is a prefix sum that must be taken left to right (its rounding is the
+// reference's), so each row's sum is one thread's dependent chain of double
+// adds; rows run in parallel, 8 to a block so that every SM holds a few
+// (a 1024-row map gives 128 blocks). A block's 128 threads stream the map
+// through shared memory in 8-row x 128-column tiles with coalesced 16-byte
+// loads, and each tile's loads are issued before the previous tile's sums
+// are taken, so HBM reads overlap the chains. The marginal CDF and the
+// integral are sequential over rows too (Renderer.cpp:642-655); the row
+// sums are staged through shared memory so that chain waits on no DRAM
+// load.
+constexpr int kCdfRows = 8;
 constexpr int kCdfCols = 128;
+
+__device__ __forceinline__ float texelLuminance(float4 p) {  // the reference's float expression
+    return __fadd_rn(__fadd_rn(__fmul_rn(0.2126f, p.x), __fmul_rn(0.7152f, p.y)), __fmul_rn(0.0722f, p.z));
+}
 
 __global__ void __launch_bounds__(kCdfCols) envCdfRowsKernel(const float4* __restrict__ texels,
                                                              const float* __restrict__ sinTheta, uint32_t w,
                                                              uint32_t h, float* __restrict__ cdf,
                                                              double* __restrict__ rowSums,
                                                              float* __restrict__ rowInv) {
-    __shared__ float tile[kCdfRows][kCdfCols + 1];
+    __shared__ float tile[2][kCdfRows][kCdfCols + 1];
     const uint32_t y0 = blockIdx.x * kCdfRows;
     const uint32_t rows = min(uint32_t(kCdfRows), h - y0);
     const uint32_t tid = threadIdx.x;
     double acc = 0.0;  // running row sum, owned by thread tid < rows
     const double s = tid < rows ? double(sinTheta[y0 + tid]) : 0.0;
-    for (uint32_t c0 = 0; c0 < w; c0 += kCdfCols) {
+    float next[kCdfRows];  // this thread's column of the next tile
+    auto fetch = [&](uint32_t c0) {
+#pragma unroll
+        for (int r = 0; r < kCdfRows; ++r)
+            if (uint32_t(r) < rows && c0 + tid < w) next[r] = texelLuminance(__ldg(texels + size_t(y0 + r) * w + c0 + tid));
+    };
+    fetch(0);
+    uint32_t buf = 0;
+    for (uint32_t c0 = 0; c0 < w; c0 += kCdfCols, buf ^= 1u) {
         const uint32_t cols = min(uint32_t(kCdfCols), w - c0);
-        for (uint32_t r = 0; r < rows; ++r) {
-            if (tid < cols) {
-                const float4 p = __ldg(texels + size_t(y0 + r) * w + c0 + tid);
-                // float luminance with the reference's operation order
-                tile[r][tid] =
-                    __fadd_rn(__fadd_rn(__fmul_rn(0.2126f, p.x), __fmul_rn(0.7152f, p.y)), __fmul_rn(0.0722f, p.z));
-            }
-        }
+#pragma unroll
+        for (int r = 0; r < kCdfRows; ++r)
+            if (uint32_t(r) < rows && tid < cols) tile[buf][r][tid] = next[r];
         __syncthreads();
+        if (c0 + kCdfCols < w) fetch(c0 + kCdfCols);  // in flight while the rows are summed
         if (tid < rows) {
+            float* row = tile[buf][tid];
+#pragma unroll 8
             for (uint32_t c = 0; c < cols; ++c) {
-                acc += double(tile[tid][c]) * s;
-                tile[tid][c] = float(acc);
+                acc = __dadd_rn(acc, __dmul_rn(double(row[c]), s));
+                row[c] = float(acc);
             }
         }
         __syncthreads();
         for (uint32_t r = 0; r < rows; ++r)
-            if (tid < cols) cdf[size_t(y0 + r) * w + c0 + tid] = tile[r][tid];
-        __syncthreads();
+            if (tid < cols) cdf[size_t(y0 + r) * w + c0 + tid] = tile[buf][r][tid];
     }
     if (tid < rows) {
         rowSums[y0 + tid] = acc;
@@ -69,25 +83,44 @@ __global__ void envCdfNormalizeKernel(float* __restrict__ cdf, const float* __re
         cdf[i] = __fmul_rn(cdf[i], rowInv[i / w]);
 }
 
-// Marginal CDF and integral, sequential over rows (Renderer.cpp:642-655).
-__global__ void envCdfMarginalKernel(const double* __restrict__ rowSums, uint32_t w, uint32_t h,
-                                     float* __restrict__ marginal, float* __restrict__ integral) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+// Marginal CDF and integral, sequential over rows (Renderer.cpp:642-655):
+// the block stages 4,096 row sums at a time in shared memory, then thread 0
+// runs the chains over them.
+constexpr uint32_t kMarginalChunk = 4096;
+__global__ void __launch_bounds__(1024) envCdfMarginalKernel(const double* __restrict__ rowSums, uint32_t w,
+                                                             uint32_t h, float* __restrict__ marginal,
+                                                             float* __restrict__ integral) {
+    __shared__ double sRow[kMarginalChunk];
     const float pi = 3.14159265358979323846f;
     const float dTheta = __fdiv_rn(pi, float(h));
     const float dPhi = __fdiv_rn(__fmul_rn(2.0f, pi), float(w));
-    double integ = 0.0, total = 0.0;
-    for (uint32_t y = 0; y < h; ++y) {
-        integ = __dadd_rn(integ, __dmul_rn(__dmul_rn(rowSums[y], double(dTheta)), double(dPhi)));
-        total = __dadd_rn(total, rowSums[y]);
+    double integ = 0.0, total = 0.0, run = 0.0;
+    for (int pass = 0; pass < 2; ++pass) {
+        for (uint32_t y0 = 0; y0 < h; y0 += kMarginalChunk) {
+            const uint32_t n = min(kMarginalChunk, h - y0);
+            __syncthreads();
+            for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) sRow[i] = rowSums[y0 + i];
+            __syncthreads();
+            if (threadIdx.x != 0) continue;
+            if (pass == 0) {
+#pragma unroll 8
+                for (uint32_t i = 0; i < n; ++i) {
+                    integ = __dadd_rn(integ, __dmul_rn(__dmul_rn(sRow[i], double(dTheta)), double(dPhi)));
+                    total = __dadd_rn(total, sRow[i]);
+                }
+            } else {
+#pragma unroll 8
+                for (uint32_t i = 0; i < n; ++i) {
+                    run = __dadd_rn(run, sRow[i]);
+                    marginal[y0 + i] = total > 0.0 ? float(__ddiv_rn(run, total)) : 0.0f;
+                }
+            }
+        }
     }
-    double run = 0.0;
-    for (uint32_t y = 0; y < h; ++y) {
-        run = __dadd_rn(run, rowSums[y]);
-        marginal[y] = total > 0.0 ? float(__ddiv_rn(run, total)) : 0.0f;
+    if (threadIdx.x == 0) {
+        const float f = float(integ);
+        *integral = f > 1e-8f ? f : 1e-8f;
     }
-    const float f = float(integ);
-    *integral = f > 1e-8f ? f : 1e-8f;
 }
 
 // Mean radiance per pixel. The reference divides by the host frame count
@@ -144,7 +177,7 @@ extern "C" cudaError_t mrtcu_env_cdf(const float4* texels, const float* sinTheta
     envCdfRowsKernel<<<(h + kCdfRows - 1) / kCdfRows, kCdfCols, 0, stream>>>(texels, sinTheta, w, h, cdf, rowSums,
                                                                               rowInv);
     envCdfNormalizeKernel<<<148 * 4, 256, 0, stream>>>(cdf, rowInv, w, h);
-    envCdfMarginalKernel<<<1, 32, 0, stream>>>(rowSums, w, h, cdf + size_t(w) * h, integral);
+    envCdfMarginalKernel<<<1, 1024, 0, stream>>>(rowSums, w, h, cdf + size_t(w) * h, integral);
     return cudaGetLastError();
 }
 
