@@ -98,7 +98,14 @@ MRT_DEV Bsdf makeBsdf(const MrtFrameParams& P, const Surface& s) {
 // Counter slots: closest rays, shadow rays, closest-hit node records fetched,
 // closest-hit triangle tests, surface hits, shadow node records, shadow
 // triangle tests. Added to ctr with one atomic per warp and counter.
+#ifdef MRT_TRAV_PROFILE
+// Slots 8..14 (a build with MRT_TRAV_PROFILE only): the extend kernel's
+// warp-step statistics (TraversalCounters).
+enum { kCtrClosest, kCtrShadow, kCtrExtNodes, kCtrExtTris, kCtrHits, kCtrShNodes, kCtrShTris, kCtrPad,
+       kCtrSteps, kCtrActive, kCtrTriSteps, kCtrTriPairs, kCtrTriRounds, kCtrNodeSteps, kCtrNodeLanes, kCtrCount };
+#else
 enum { kCtrClosest, kCtrShadow, kCtrExtNodes, kCtrExtTris, kCtrHits, kCtrShNodes, kCtrShTris, kCtrCount };
+#endif
 MRT_DEV void warpAddCounters(unsigned long long* ctr, const uint32_t (&c)[kCtrCount]) {
     if (ctr == nullptr) return;
 #pragma unroll
@@ -247,6 +254,15 @@ __global__ void MRT_TRAV_BOUNDS waveExtendKernel(MrtFrameParams P, MrtWaveState 
     if (tc.bad) atomicOr(P.errorFlags, 2u);
     c[kCtrExtNodes] = tc.nodes;
     c[kCtrExtTris] = tc.tris;
+#ifdef MRT_TRAV_PROFILE
+    c[kCtrSteps] = tc.steps;
+    c[kCtrActive] = tc.activeLanes;
+    c[kCtrTriSteps] = tc.triSteps;
+    c[kCtrTriPairs] = tc.triPairs;
+    c[kCtrTriRounds] = tc.triRounds;
+    c[kCtrNodeSteps] = tc.nodeSteps;
+    c[kCtrNodeLanes] = tc.nodeLanes;
+#endif
     warpAddCounters(P.rayCounters, c);
 }
 

@@ -181,6 +181,12 @@ MRT_DEV void refineHit(const MrtFrameParams& P, float3 o, float3 d, HitRecord& h
 struct TraversalCounters {
     uint32_t nodes = 0, tris = 0;
     bool bad = false;
+#ifdef MRT_TRAV_PROFILE
+    // Warp-step statistics, counted by lane 0 of each warp (a build with
+    // MRT_TRAV_PROFILE defined only): steps, lanes with a ray, triangle-phase
+    // steps, pairs and rounds, node-phase steps and lanes testing a node.
+    uint32_t steps = 0, activeLanes = 0, triSteps = 0, triPairs = 0, triRounds = 0, nodeSteps = 0, nodeLanes = 0;
+#endif
 };
 
 // Child-hit masks of one wide node.
@@ -581,6 +587,23 @@ MRT_DEV int travWarpStep(const MrtFrameParams& P, WideTrav& T, WideStack& stack,
     const uint32_t pendLanes = __popc(__ballot_sync(0xffffffffu, pending));
     const uint32_t activeLanes = __popc(__ballot_sync(0xffffffffu, active));
     const bool triPhase = pendLanes * 100u >= activeLanes * MRT_TRI_PHASE_PCT || pendLanes == activeLanes;
+#ifdef MRT_TRAV_PROFILE
+    {
+        const uint32_t pairs = __reduce_add_sync(0xffffffffu, pending ? uint32_t(__popc(T.pendBits)) : 0u);
+        if ((threadIdx.x & 31u) == 0) {
+            ++tc.steps;
+            tc.activeLanes += activeLanes;
+            if (triPhase) {
+                ++tc.triSteps;
+                tc.triPairs += pairs;
+                tc.triRounds += (pairs + 31u) / 32u;
+            } else {
+                ++tc.nodeSteps;
+                tc.nodeLanes += activeLanes - pendLanes;
+            }
+        }
+    }
+#endif
     if (triPhase) return travTriPhaseWarp<kAny>(P, T, tc, pending);
     return active && !pending ? travNodeStep(P, T, stack, tc) : kTravRunning;
 }

@@ -273,8 +273,8 @@ mrtResult Engine::init(const mrtEngineDesc& desc) {
     MRT_TRY(m_lights.ensure(sizeof(MrtLight)));
     MRT_TRY(m_flags.ensure(16));
     MRT_CUDA(cudaMemsetAsync(m_flags.ptr, 0, 16, m_stream));
-    MRT_TRY(m_rayCounters.ensure(64));
-    MRT_CUDA(cudaMemsetAsync(m_rayCounters.ptr, 0, 64, m_stream));
+    MRT_TRY(m_rayCounters.ensure(128));
+    MRT_CUDA(cudaMemsetAsync(m_rayCounters.ptr, 0, 128, m_stream));
     MRT_TRY(allocateFrame());
     MRT_CUDA(cudaStreamSynchronize(m_stream));
     m_stats.structSize = sizeof(mrtxStats);
@@ -1052,7 +1052,7 @@ mrtResult Engine::launchPending() {
     m_stats.extendLaunches = 0;
     MRT_TRY(guard(ensureWave(n)));
     const MrtFrameParams p = m_pendingParams;
-    MRT_CUDA(cudaMemsetAsync(m_rayCounters.ptr, 0, 64, m_stream));
+    MRT_CUDA(cudaMemsetAsync(m_rayCounters.ptr, 0, 128, m_stream));
     uint32_t launches = 0;
     // the cache mode renders waves of a few samples and trains after each
     const uint32_t waveCap = m_cache.enabled ? std::min(m_waveSamples, m_cache.samplesPerUpdate) : m_waveSamples;
@@ -1138,8 +1138,15 @@ mrtResult Engine::completePending() {
         resetAccumulation();
         return guard(fr);
     }
-    unsigned long long ctr[7];
+    unsigned long long ctr[16];
     MRT_CUDA(cudaMemcpy(ctr, m_rayCounters.ptr, sizeof(ctr), cudaMemcpyDeviceToHost));
+    // A build of the kernels with MRT_TRAV_PROFILE defined fills slots 8..14
+    // with the extend kernel's warp-step statistics; they are logged.
+    if (ctr[8])
+        log(LogLevel::Info, "extend warp steps " + std::to_string(ctr[8]) + " active lanes " + std::to_string(ctr[9]) +
+                                " triangle steps " + std::to_string(ctr[10]) + " pairs " + std::to_string(ctr[11]) +
+                                " rounds " + std::to_string(ctr[12]) + " node steps " + std::to_string(ctr[13]) +
+                                " node lanes " + std::to_string(ctr[14]));
     m_stats.raysClosest = ctr[0];
     m_stats.raysShadow = ctr[1];
     m_stats.nodeFetches = ctr[2];
