@@ -552,9 +552,12 @@ MRT_DEV int travTriPhaseWarp(const MrtFrameParams& P, WideTrav& T, TraversalCoun
         }
     }
     __syncwarp();
+    // every lane takes part in the reduction (a full-mask warp operation)
+    // before any lane leaves
+    const uint32_t occAll = kAny ? __reduce_or_sync(full, occ) : 0u;
     if (!pending) return kTravRunning;
     T.pendBits = 0;
-    if (kAny) return (__reduce_or_sync(full, occ) >> lane) & 1u ? kTravOccluded : kTravRunning;
+    if (kAny) return (occAll >> lane) & 1u ? kTravOccluded : kTravRunning;
     const unsigned long long best = sKey[warp][lane];
     if (best != ~0ull) {
         const float t = __uint_as_float(uint32_t(best >> 32));
