@@ -430,6 +430,13 @@ def ours_arm(args):
             "gpu_launches": launches,
             "kernel_ms_per_launch": float(np.mean(kernel_ms)),
             "step_ms": [round(x, 2) for x in step_ms],
+            # per step: the engine's own CUDA-event time of its kernels and
+            # the stage split, beside step_ms (events on the caller's stream
+            # around the synchronous render call, so host time is included):
+            # a slow step with an unchanged device time is host-side
+            "step_device_ms": [round(x, 2) for x in kernel_ms],
+            "step_stage_ms": [{k: round(cs[k], 2) for k in ("extendMs", "shadeMs", "shadowMs", "otherMs")}
+                              for cs in counters],
             "mrays_per_s": world * rays / launch_s / 1e6,
             "rays_per_path": rays / paths_per_step,
             "commit_ms": commit["commitMs"],
