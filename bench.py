@@ -687,7 +687,7 @@ def time_to_relmse(mrt, scenes, ref, windows=ROOM_WINDOWS, target=1e-3):
 ROOM_WORKLOAD = ("config 4: closed 20x4x10 room lit through one 2x2 window by the config-2 sky, config-2 heightfield "
                  "as terrain (2,093,076 triangles), 1920x1080, depth 12; relMSE over four 240x136 windows against "
                  f"{ROOM_REF_SPP} spp of the plain tracer (FP64 accumulation, independent sample stream); cache: "
-                 "hash grid 16 x 2^19 x 2 + 5 x 64 ReLU MLP, Adam lr 1e-2 halving every 48 steps down to 3e-4, "
+                 "hash grid 16 x 2^19 x 2 + 5 x 64 ReLU MLP, Adam lr 1e-2 halving every 96 steps down to 3e-4, "
                  "moving-average weights for inference, a 32nd of the pixels as training paths, trained after "
                  "every 4 samples")
 

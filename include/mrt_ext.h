@@ -225,7 +225,8 @@ MRT_API mrtResult mrtxSetRadianceCacheAveraging(mrtEngine*, float decay);
  * config-4 room: mean within 3% of the converged image, against 14% with
  * a constant rate). The schedule restarts from lr at this call, when the
  * learning rate changes, and when parameters are written. Defaults:
- * lrMin 3e-4, halfLifeSteps 48. */
+ * lrMin 3e-4, halfLifeSteps 96 (of 48, 96 and 192, the shortest time to
+ * relMSE 1e-3 on config 4 at 1080p). */
 MRT_API mrtResult mrtxSetRadianceCacheSchedule(mrtEngine*, float lrMin, float halfLifeSteps);
 
 /* The gradients the cache's training step computes for one batch, read

@@ -61,7 +61,7 @@ def measure(defines: dict, workdir: Path, steps: int, warmup: int) -> float:
     mrt_build.build(defines=defines, lib=lib, build_dir=bdir)
     env = dict(os.environ, MRT_LIBRARY=str(lib))
     cmd = [sys.executable, str(ROOT / "bench.py"), "--steps", str(steps), "--warmup", str(warmup),
-           "--no-cpu-baseline", "--e2e-steps", "0", "--interactive-frames", "0"]
+           "--no-cpu-baseline", "--e2e-steps", "0", "--interactive-frames", "0", "--no-room"]
     r = subprocess.run(cmd, capture_output=True, text=True, env=env, cwd=str(ROOT), timeout=900)
     if r.returncode != 0:
         raise RuntimeError(f"bench failed for {defines}:\n{r.stdout[-2000:]}\n{r.stderr[-2000:]}")

@@ -153,7 +153,7 @@ private:
         float lr = 1e-2f;
         float emaDecay = 0.99f;  // 0: inference reads the live parameters
         // learning-rate decay: halves every lrHalfLife steps down to lrMin (0: constant)
-        float lrMin = 3e-4f, lrHalfLife = 48.0f;
+        float lrMin = 3e-4f, lrHalfLife = 96.0f;
         float lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
         void release();
     } m_cache;

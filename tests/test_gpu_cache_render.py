@@ -1,7 +1,7 @@
 """Rendering with the radiance cache (config 4's room at reduced sizes).
 Switching the cache on or off starts a new accumulation; with it off the
 path tracer is the plain one, bit for bit. With it on (default training
-schedule: the learning rate halves every 48 Adam steps down to 3e-4, and
+schedule: the learning rate halves every 96 Adam steps down to 3e-4, and
 queries read a moving average of the weights), after a training warm-up
 the image is finite and opaque, its mean stays within 3 % of a converged
 plain image for two cache seeds, and its relMSE against that image is at
