@@ -60,7 +60,8 @@ def parse_args():
                          "room: time to relMSE 1e-3 on config 4, plain and radiance-cached; "
                          "cache: config 4 rendered with the radiance cache, 4 spp per step, reporting the "
                          "cache's inference and training kernels; large: config 5 (25.2 M triangles, 3840x2160, "
-                         "depth 16), 16 spp per step, no CPU baseline")
+                         "depth 16), 4 cameras in one batch, 16 spp per camera per step, then relMSE against "
+                         "time, cached vs plain, to 1024 spp (--no-room skips the curves)")
     ap.add_argument("--e2e-steps", type=int, default=4,
                     help="end-to-end steps averaged (wall-clock: host jitter of up to ~25 ms a step was seen)")
     ap.add_argument("--interactive-frames", type=int, default=48,
@@ -621,31 +622,35 @@ def window_camera(cam, width, height, window):
                 top=lerp(th, -th, y0 / height), bottom=lerp(th, -th, (y0 + h) / height))
 
 
-def room_reference(mrt, scenes, ref_spp=ROOM_REF_SPP, windows=ROOM_WINDOWS, chunk=1024):
-    """The reference pixels of the config-4 windows (float64, windows side by
-    side) and the device seconds it took; rendered as one mrtxRenderBatch of
-    the window engines per `chunk` samples, on a sample stream disjoint from
-    the measured runs."""
-    W, H = 1920, 1080
-    s = scenes.room(W, H)
+def window_reference(mrt, scene, width, height, windows, ref_spp, chunk=1024, camera=None):
+    """Reference pixels of `windows` of a width x height frame of `scene`
+    (float64, windows side by side) and the seconds they took: each window
+    rendered by its own engine through the sub-frustum of the frame's camera
+    (`camera`, default the scene's), all windows in one mrtxRenderBatch per
+    `chunk` samples, on a sample stream disjoint from the measured runs."""
+    cam = camera or scene.camera
     engines = []
     for win in windows:
         e = mrt.Engine(win[2], win[3])
-        s.apply(e)
-        e.set_render_settings(**dict(s.settings, width=win[2], height=win[3]))
-        e.set_camera_ex(**window_camera(s.camera, W, H, win))
+        scene.apply(e)
+        e.set_render_settings(**dict(scene.settings, width=win[2], height=win[3]))
+        e.set_camera_ex(**window_camera(cam, width, height, win))
         e.set_sample_stream(1 << 24, 1)
         e.commit()
         engines.append(e)
-    import time as _t
-    t0 = _t.perf_counter()
+    t0 = time.perf_counter()
     for _ in range(ref_spp // chunk):
         mrt.render_batch(engines, [chunk] * len(engines))
-    secs = _t.perf_counter() - t0
+    secs = time.perf_counter() - t0
     ref = np.concatenate([e.read_framebuffer()[..., :3].reshape(-1, 3) for e in engines]).astype(np.float64)
     for e in engines:
         e.close()
     return ref, secs
+
+
+def room_reference(mrt, scenes, ref_spp=ROOM_REF_SPP, windows=ROOM_WINDOWS, chunk=1024):
+    """The reference pixels of the config-4 windows (window_reference)."""
+    return window_reference(mrt, scenes.room(1920, 1080), 1920, 1080, windows, ref_spp, chunk)
 
 
 def time_to_relmse(mrt, scenes, ref, windows=ROOM_WINDOWS, target=1e-3):
@@ -723,6 +728,120 @@ def room_arm(args):
     return 0
 
 
+# Config 5's reference windows: four 240 x 136 windows of the 3840 x 2160
+# frame centred on its quadrants.
+LARGE_WINDOWS = [(840, 472, 240, 136), (2760, 472, 240, 136), (840, 1552, 240, 136), (2760, 1552, 240, 136)]
+
+
+def large_cameras(scene):
+    """Config 5's four cameras: the scene's, two moved half a unit across the
+    terrain's width, and one raised and pulled back, all looking down onto
+    the heightfield."""
+    c = scene.camera
+    p, t = np.asarray(c["position"]), np.asarray(c["target"])
+    cams = []
+    for dp, dt in (((0, 0, 0), (0, 0, 0)), ((-0.5, 0, 0), (-0.5, 0, 0)), ((0.5, 0, 0), (0.5, 0, 0)),
+                   ((0, 0.4, 0.3), (0, 0, 0))):
+        cams.append(dict(position=tuple(float(v) for v in p + dp), target=tuple(float(v) for v in t + dt),
+                         up=c["up"], fov_y_deg=c["fov_y_deg"]))
+    return cams
+
+
+def large_arm(args):
+    """Config 5: the 25,242,860-triangle scene at 3840x2160, depth 16, four
+    cameras per launch (one engine per camera, their waves issued together by
+    one mrtxRenderBatch), 16 of the 1024 spp per camera per step; then, on
+    camera 0, relMSE against device time for the plain and the
+    radiance-cached estimator up to 1024 spp, against a windowed 65,536-spp
+    reference (window_reference)."""
+    import torch
+
+    import miniraytrace_b200 as mrt
+    from miniraytrace_b200 import build as mrt_build
+    from miniraytrace_b200 import scenes
+
+    if int(os.environ.get("RANK", "0")) != 0:
+        return 0
+    torch.cuda.set_device(0)
+    mrt_build.build()
+    spp = args.spp or 16
+    scene = scenes.large(spp=spp)
+    W, H = scene.settings["width"], scene.settings["height"]
+    cams = large_cameras(scene)
+    engines = []
+    for cam in cams:
+        e = mrt.Engine(W, H)
+        scene.apply(e)
+        e.set_camera(**cam)
+        e.commit()
+        engines.append(e)
+    counts = [spp] * len(engines)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    for _ in range(args.warmup):
+        flush.fill_(1)
+        mrt.render_batch(engines, counts)
+    torch.cuda.synchronize()
+    sampler = ClockSampler(0)
+    sampler.start()
+    time.sleep(0.3)
+    step_ms, launches = [], 0
+    for k in range(args.steps):
+        flush.fill_(k & 0xFF)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        mrt.render_batch(engines, counts)
+        b.record()
+        torch.cuda.synchronize()
+        step_ms.append(a.elapsed_time(b))
+        launches += sum(e.stats()["kernelLaunches"] for e in engines)
+    clocks = sampler.stop()
+    st = engines[0].stats()
+    scene_mb = st["deviceBytes"] / 1e6
+    for e in engines:
+        e.close()
+    del flush
+    paths = len(engines) * W * H * spp
+    ms = float(np.mean(step_ms))
+    curves = None
+    if not args.no_room:
+        ref, ref_s = window_reference(mrt, scene, W, H, LARGE_WINDOWS, ROOM_REF_SPP, camera=cams[0])
+        curves = {"reference": f"{ROOM_REF_SPP} spp of the plain tracer over four 240x136 windows (FP64 "
+                               f"accumulation, independent sample stream)", "reference_render_s": ref_s}
+        for mode, chunk in (("plain", 64), ("cached", 16)):
+            e = mrt.Engine(W, H)
+            scene.apply(e)
+            e.set_camera(**cams[0])
+            e.commit()
+            if mode == "cached":
+                e.set_radiance_cache(enabled=True)
+            n, secs, reached, curve, _, mean = converge(e, ref, 1e-3, chunk, 1024, LARGE_WINDOWS)
+            if n < 1024:  # carry on to 1024 spp for the curve
+                more, more_s, _, curve2, _, mean = converge(e, ref, 0.0, chunk, 1024 - n, LARGE_WINDOWS)
+                curve += [(a + n, round(b + secs * 1e3, 1), c) for a, b, c in curve2]
+            e.close()
+            curves[mode] = {"seconds_to_relmse_1e-3": secs if reached else None,
+                            "spp_to_relmse_1e-3": n if reached else None, "mean_over_reference_at_1024": mean,
+                            "curve_spp_device_ms_relmse": curve}
+        ps, cs = curves["plain"]["seconds_to_relmse_1e-3"], curves["cached"]["seconds_to_relmse_1e-3"]
+        curves["plain_over_cached_to_1e-3"] = ps / cs if ps and cs else None
+    out = {
+        "metric": "Mpaths/s at 3840x2160, 4 cameras per launch (config 5)", "value": paths / (ms / 1e3) / 1e6,
+        "unit": "Mpaths/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"config 5: {scene.triangle_count:,} triangles (4096^2 fBm heightfield cropped to "
+                               f"19,999,980 triangles + 4,096 x 1280-triangle icosphere instances), 4096x2048 sky, "
+                               f"{W}x{H}, depth {scene.settings['max_bounces']}, 4 cameras, {spp} of 1024 spp per "
+                               "camera per step, one mrtxRenderBatch per step (one engine and scene copy per "
+                               "camera)", "scene_mb_per_engine": scene_mb,
+                   "l2": "a 256 MiB buffer is written between timed steps"},
+        "step_ms": [round(x, 2) for x in step_ms], "gpu_launches": launches, "clocks": clocks,
+        "relmse_over_time_camera0": curves,
+    }
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def cache_arm(args):
     """The config-4 room in the radiance-cache mode: W untimed steps, then K
     steps of 4 samples per pixel (one training round each). Reports the
@@ -791,6 +910,8 @@ def main():
         return room_arm(args)
     if args.config == "cache":
         return cache_arm(args)
+    if args.config == "large":
+        return large_arm(args)
     return ours_arm(args)
 
 
