@@ -806,7 +806,7 @@ extern "C" cudaError_t mrtcu_wave(const MrtFrameParams* p, const MrtWaveState* s
         n += 3;
         // plain mode: the fused tail, once few paths continue (the cache
         // mode's queries and training records come from the shade kernel)
-        if (MRT_TAIL_PATHS > 0 && !cache && b < p->maxBounces) {  // 0: no fused tail
+        if (!cache && b < p->maxBounces) {
             waveTailKernel<<<(MRT_TAIL_PATHS + 127) / 128, 128, 0, stream>>>(*p, *s, A, b, MRT_TAIL_PATHS);
             ++n;
         }
