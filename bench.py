@@ -333,8 +333,7 @@ def ours_arm(args):
     n_ext = max(1, c["extendLaunches"])
     per_ray = ncu_dram_bytes_per_ray(args.config)
     traffic = per_ray * c["raysClosest"] / n_ext if per_ray is not None else None
-    # rays of the wavefront kernels and of the fused tail kernel
-    rays = c["raysClosest"] + c["raysShadow"] + c["tailRaysClosest"] + c["tailRaysShadow"]
+    rays = c["raysClosest"] + c["raysShadow"]
 
     # end to end through the C ABI with host buffers (rank-local)
     e2e = None
@@ -437,13 +436,13 @@ def ours_arm(args):
             # around the synchronous render call, so host time is included):
             # a slow step with an unchanged device time is host-side
             "step_device_ms": [round(x, 2) for x in kernel_ms],
-            "step_stage_ms": [{k: round(cs[k], 2) for k in ("extendMs", "shadeMs", "shadowMs", "tailMs", "otherMs")}
+            "step_stage_ms": [{k: round(cs[k], 2) for k in ("extendMs", "shadeMs", "shadowMs", "otherMs")}
                               for cs in counters],
             "mrays_per_s": world * rays / launch_s / 1e6,
             "rays_per_path": rays / paths_per_step,
             "commit_ms": commit["commitMs"],
             "stage_ms_per_step": {"extend": c["extendMs"], "shade": c["shadeMs"], "shadow": c["shadowMs"],
-                                  "tail": c["tailMs"], "other": c["otherMs"]},
+                                  "other": c["otherMs"]},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "peak_source": peak_kind, "kernel": "waveExtendKernel (closest hit), all launches of a step",

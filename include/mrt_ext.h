@@ -100,11 +100,6 @@ typedef struct mrtxStats {
     float cacheQueryMs, cacheTrainMs;
     uint64_t cacheQueries, cacheRecords;
     uint32_t cacheSteps;
-    /* the fused tail of the last render call's waves (plain mode: once few
-     * paths continue, one kernel runs them to their end): its device time and
-     * the closest-hit and shadow rays it traced (not in the counts above) */
-    float tailMs;
-    uint64_t tailRaysClosest, tailRaysShadow;
 } mrtxStats;
 MRT_API mrtResult mrtxGetStats(mrtEngine*, mrtxStats* out);
 

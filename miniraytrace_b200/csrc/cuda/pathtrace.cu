@@ -98,18 +98,13 @@ MRT_DEV Bsdf makeBsdf(const MrtFrameParams& P, const Surface& s) {
 // Counter slots: closest rays, shadow rays, closest-hit node records fetched,
 // closest-hit triangle tests, surface hits, shadow node records, shadow
 // triangle tests. Added to ctr with one atomic per warp and counter.
-// Slots 7 and 8 count the closest-hit and shadow rays of the fused tail
-// kernel (its node and triangle counts are not added to the wavefront
-// kernels' slots 2, 3, 5, 6).
 #ifdef MRT_TRAV_PROFILE
-// Slots 9..15 (a build with MRT_TRAV_PROFILE only): the extend kernel's
+// Slots 8..14 (a build with MRT_TRAV_PROFILE only): the extend kernel's
 // warp-step statistics (TraversalCounters).
-enum { kCtrClosest, kCtrShadow, kCtrExtNodes, kCtrExtTris, kCtrHits, kCtrShNodes, kCtrShTris, kCtrTailClosest,
-       kCtrTailShadow, kCtrSteps, kCtrActive, kCtrTriSteps, kCtrTriPairs, kCtrTriRounds, kCtrNodeSteps,
-       kCtrNodeLanes, kCtrCount };
+enum { kCtrClosest, kCtrShadow, kCtrExtNodes, kCtrExtTris, kCtrHits, kCtrShNodes, kCtrShTris, kCtrPad,
+       kCtrSteps, kCtrActive, kCtrTriSteps, kCtrTriPairs, kCtrTriRounds, kCtrNodeSteps, kCtrNodeLanes, kCtrCount };
 #else
-enum { kCtrClosest, kCtrShadow, kCtrExtNodes, kCtrExtTris, kCtrHits, kCtrShNodes, kCtrShTris, kCtrTailClosest,
-       kCtrTailShadow, kCtrCount };
+enum { kCtrClosest, kCtrShadow, kCtrExtNodes, kCtrExtTris, kCtrHits, kCtrShNodes, kCtrShTris, kCtrCount };
 #endif
 MRT_DEV void warpAddCounters(unsigned long long* ctr, const uint32_t (&c)[kCtrCount]) {
     if (ctr == nullptr) return;
@@ -150,8 +145,6 @@ __global__ void __launch_bounds__(256) waveInitKernel(MrtFrameParams P, MrtWaveS
         S.counts[1] = 0;
         S.counts[2] = 0;
         S.counts[4] = 0;  // extend fetch counter (kExtendHead) of bounce 0
-        S.counts[6] = 0;  // the wave's tail is not fused yet (kTailDone)
-        S.counts[7] = 0;  // tail fetch counter (kTailHead)
     }
     if (slot >= A.slots) return;
     const uint32_t pixel = slot / A.samples;
@@ -178,10 +171,8 @@ __global__ void __launch_bounds__(256) waveInitKernel(MrtFrameParams P, MrtWaveS
 }
 
 // Queue fetch counters of the persistent traversal kernels, in the wave's
-// counts[] block (counts[0..1]: path queues, counts[2]: shadow queue);
-// kTailDone: 1 + the bounce after which the fused tail kernel finished the
-// wave's paths (0: not yet), kTailHead: the tail kernel's fetch counter.
-enum { kExtendHead = 4, kShadowHead = 5, kTailDone = 6, kTailHead = 7 };
+// counts[] block (counts[0..1]: path queues, counts[2]: shadow queue).
+enum { kExtendHead = 4, kShadowHead = 5 };
 
 // Lanes of a persistent traversal warp whose ray has finished take new rays
 // from the queue (one warp-aggregated atomic) once at least this many lanes
@@ -224,7 +215,6 @@ MRT_DEV uint32_t refillLane(uint32_t* head, uint32_t n, bool active, bool& drain
 // Persistent warps with lane refill; every lane of a warp stays in the loop
 // until the warp has no ray left.
 __global__ void MRT_TRAV_BOUNDS waveExtendKernel(MrtFrameParams P, MrtWaveState S, uint32_t cur) {
-    if (S.counts[kTailDone] != 0u) return;  // the tail kernel finished the wave's paths
     const uint32_t* __restrict__ q = S.queue[cur];
     const uint32_t n = S.counts[cur];
     if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -336,134 +326,9 @@ MRT_DEV void blockAppend2(uint32_t* ca, bool pa, uint32_t& ia, uint32_t* cb, boo
     __syncthreads();  // s is reused by the next call
 }
 
-// The shading of one path at its hit (pathtrace.comp:133-216): miss ->
-// environment with MIS; hit -> alpha pass-through, emission, one-light NEE
-// (the shadow ray and its contribution are returned), BSDF sample, Russian
-// roulette, next ray. The draws from the path's pcg4d stream happen in the
-// reference's order. `st` holds the path before the bounce and receives it
-// after; used by the wavefront's shade kernel and by the fused tail kernel,
-// so both evaluate the same operations.
-struct PathState {
-    float3 ro, rd, beta, L;
-    float prevBsdfPdf;  // pdf of the BSDF sample that made the ray (MIS on a miss)
-    uint32_t bounce;
-    uint32_t rngW;      // pcg4d counter
-};
-struct ShadeResult {
-    bool cont = false, shadow = false;
-    float3 shOrig = f3(0.0f), shDir = f3(0.0f), shContrib = f3(0.0f);
-    float shTMax = 0.0f;
-};
-template <bool kCache>
-MRT_DEV ShadeResult shadePath(const MrtFrameParams& P, const WaveArgs& A, const MrtCacheArgs& K, uint32_t slot,
-                              PathState& st, const HitRecord& hit, uint32_t (&c)[kCtrCount]) {
-    ShadeResult r;
-    bool cacheQuery = false;  // cache mode: the path stops here and takes the cache's prediction
-    const uint32_t pixel = slot / A.samples;
-    Rng rng{pixel % P.width, pixel / P.width, frameOf(P, A, slot), st.rngW};
-    const uint32_t bounce = st.bounce;
-    float3 ro = st.ro, rd = st.rd, beta = st.beta, L = st.L;
-    float prevBsdfPdf = st.prevBsdfPdf;
-    if (hit.tri == 0xffffffffu) {
-        const float3 env = envRadiance(P, rd);
-        if (maxComp(env) > 0.0f) {
-            float w = 1.0f;
-            if (bounce > 0u) w = balanceHeuristic(prevBsdfPdf, envPdf(P, rd) * envPickPdf(P));
-            L += beta * env * w;
-        }
-    } else {
-        c[kCtrHits]++;
-        const Surface s = makeSurface(P, rd, hit);
-        const MrtMaterial& mat = P.materials[s.mat];
-        const float opacity = mat.baseColorOpacity[3];
-        if (opacity < 1.0f && rng1(rng) >= opacity) {  // stochastic alpha pass-through
-            ro = s.pos + rd * MRT_EPS_RAY;
-            r.cont = bounce + 1u <= P.maxBounces;
-        } else {
-            float3 emission = f3p(mat.emissionRoughness);
-            if (mat.tex[4] >= 0) emission = emission * texRgb(P, mat.tex[4], s.uv);
-            if (maxComp(emission) > 0.0f && s.frontFace) L += beta * emission;
-            const Bsdf bsdf = makeBsdf(P, s);
-            if (kCache && bounce >= 1u) {
-                // A query (the cache stands for everything scattered
-                // from here on) or, on a training path's first
-                // vertices, a training record; its features are
-                // written out here.
-                // (Queries and records append in separate branches: a
-                // coalesced group then shares one list.)
-                cacheQuery = !cacheTrainingPath(K, pixel, frameOf(P, A, slot));
-                const float4 b4 = make_float4(beta.x, beta.y, beta.z, __uint_as_float(slot));
-                if (cacheQuery) {
-                    const uint32_t idx = coalescedAppend(K.qCount);
-                    if (idx < K.qCap) {
-                        writeCacheFeatures(K.qFeat + size_t(idx) * 16, s, -rd, bsdf);
-                        K.qBeta[idx] = b4;
-                    }
-                } else if (bounce <= K.recordBounces) {
-                    const uint32_t idx = coalescedAppend(K.rCount);
-                    if (idx < K.rCap) {
-                        writeCacheFeatures(K.rFeat + size_t(idx) * 16, s, -rd, bsdf);
-                        K.rPrefix[idx] = make_float4(L.x, L.y, L.z, __uint_as_float(slot));
-                        K.rBeta[idx] = b4;
-                    }
-                }
-            }
-            float3 Tn, Bn;
-            buildOnb(s.nShade, Tn, Bn);
-            const float3 nd = -rd;
-            float3 wo = f3(dot(nd, Tn), dot(nd, Bn), dot(nd, s.nShade));
-            if (wo.z < 1e-6f) wo.z = 1e-6f;
-            wo = normalize(wo);
-            const LightSample ls = cacheQuery ? LightSample{} : sampleOneLight(P, s.pos, rng);
-            if (!cacheQuery && ls.valid && ls.pdf > 1e-9f) {
-                const float3 wi = f3(dot(ls.wi, Tn), dot(ls.wi, Bn), dot(ls.wi, s.nShade));
-                float3 f;
-                float bsdfPdf;
-                bsdfEval(bsdf, wo, wi, f, bsdfPdf);
-                if (maxComp(f) > 0.0f) {
-                    const float w = ls.delta ? 1.0f : balanceHeuristic(ls.pdf, bsdfPdf);
-                    r.shadow = true;
-                    r.shOrig = s.pos + s.nGeom * (wi.z > 0.0f ? MRT_EPS_RAY : -MRT_EPS_RAY);
-                    r.shDir = ls.wi;
-                    r.shTMax = ls.dist - 2.0f * MRT_EPS_RAY;
-                    r.shContrib = beta * f * fabsf(wi.z) * ls.radiance * w / ls.pdf;
-                }
-            }
-            const BsdfSample bs = cacheQuery ? BsdfSample{} : bsdfSample(bsdf, wo, rng);
-            if (!cacheQuery && bs.valid) {
-                const float3 wiWorld = normalize(Tn * bs.wi.x + Bn * bs.wi.y + s.nShade * bs.wi.z);
-                beta *= bs.f * fabsf(bs.wi.z) / bs.pdf;
-                prevBsdfPdf = bs.pdf;
-                bool alive = true;
-                if (bounce >= 3u) {
-                    const float p = clampf(maxComp(beta), 0.05f, 0.95f);
-                    if (rng1(rng) >= p) alive = false;
-                    else beta /= p;
-                }
-                if (alive) {
-                    ro = s.pos + s.nGeom * (bs.wi.z > 0.0f ? MRT_EPS_RAY : -MRT_EPS_RAY);
-                    rd = wiWorld;
-                    r.cont = bounce + 1u <= P.maxBounces;
-                }
-            }
-        }
-    }
-    st.L = L;
-    if (r.cont) {
-        st.ro = ro;
-        st.rd = rd;
-        st.beta = beta;
-        st.prevBsdfPdf = prevBsdfPdf;
-        st.bounce = bounce + 1u;
-        st.rngW = rng.w;
-    }
-    return r;
-}
-
 template <bool kCache>
 __global__ void __launch_bounds__(kShadeBlock) waveShadeKernel(MrtFrameParams P, MrtWaveState S, WaveArgs A, uint32_t cur,
                                                        MrtCacheArgs K) {
-    if (S.counts[kTailDone] != 0u) return;  // the tail kernel finished the wave's paths
     const uint32_t* __restrict__ q = S.queue[cur];
     uint32_t* __restrict__ qn = S.queue[cur ^ 1u];
     const uint32_t n = S.counts[cur];
@@ -477,29 +342,112 @@ __global__ void __launch_bounds__(kShadeBlock) waveShadeKernel(MrtFrameParams P,
         uint32_t slot = 0;
         float3 shOrig = f3(0.0f), shDir = f3(0.0f), shContrib = f3(0.0f);
         float shTMax = 0.0f;
+        bool cacheQuery = false;  // cache mode: the path stops here and takes the cache's prediction
         if (valid) {
             slot = q[i];
             const float4 o4 = S.rayO[slot], d4 = S.rayD[slot], b4 = S.beta[slot], L4 = S.L[slot];
             const float4 h4 = S.hit[slot];
-            PathState st{f3(o4), f3(d4), f3(b4), f3(L4), o4.w, __float_as_uint(d4.w), __float_as_uint(b4.w)};
-            HitRecord hit;
-            hit.t = h4.x;
-            hit.u = h4.y;
-            hit.v = h4.z;
-            hit.tri = __float_as_uint(h4.w);
-            hit.inst = hit.tri != 0xffffffffu ? S.hitInst[slot] : 0u;
-            const ShadeResult r = shadePath<kCache>(P, A, K, slot, st, hit, c);
-            cont = r.cont;
-            shadow = r.shadow;
-            shOrig = r.shOrig;
-            shDir = r.shDir;
-            shTMax = r.shTMax;
-            shContrib = r.shContrib;
-            S.L[slot] = make_float4(st.L.x, st.L.y, st.L.z, 0.0f);
+            const uint32_t pixel = slot / A.samples;
+            Rng rng{pixel % P.width, pixel / P.width, frameOf(P, A, slot), __float_as_uint(b4.w)};
+            const uint32_t bounce = __float_as_uint(d4.w);
+            float3 ro = f3(o4), rd = f3(d4), beta = f3(b4), L = f3(L4);
+            float prevBsdfPdf = o4.w;
+            const uint32_t tri = __float_as_uint(h4.w);
+            if (tri == 0xffffffffu) {
+                const float3 env = envRadiance(P, rd);
+                if (maxComp(env) > 0.0f) {
+                    float w = 1.0f;
+                    if (bounce > 0u) w = balanceHeuristic(prevBsdfPdf, envPdf(P, rd) * envPickPdf(P));
+                    L += beta * env * w;
+                }
+            } else {
+                c[kCtrHits]++;
+                HitRecord hit;
+                hit.t = h4.x;
+                hit.u = h4.y;
+                hit.v = h4.z;
+                hit.tri = tri;
+                hit.inst = S.hitInst[slot];
+                const Surface s = makeSurface(P, rd, hit);
+                const MrtMaterial& mat = P.materials[s.mat];
+                const float opacity = mat.baseColorOpacity[3];
+                if (opacity < 1.0f && rng1(rng) >= opacity) {  // stochastic alpha pass-through
+                    ro = s.pos + rd * MRT_EPS_RAY;
+                    cont = bounce + 1u <= P.maxBounces;
+                } else {
+                    float3 emission = f3p(mat.emissionRoughness);
+                    if (mat.tex[4] >= 0) emission = emission * texRgb(P, mat.tex[4], s.uv);
+                    if (maxComp(emission) > 0.0f && s.frontFace) L += beta * emission;
+                    const Bsdf bsdf = makeBsdf(P, s);
+                    if (kCache && bounce >= 1u) {
+                        // A query (the cache stands for everything scattered
+                        // from here on) or, on a training path's first
+                        // vertices, a training record; its features are
+                        // written out here.
+                        // (Queries and records append in separate branches: a
+                        // coalesced group then shares one list.)
+                        cacheQuery = !cacheTrainingPath(K, pixel, frameOf(P, A, slot));
+                        const float4 b4 = make_float4(beta.x, beta.y, beta.z, __uint_as_float(slot));
+                        if (cacheQuery) {
+                            const uint32_t idx = coalescedAppend(K.qCount);
+                            if (idx < K.qCap) {
+                                writeCacheFeatures(K.qFeat + size_t(idx) * 16, s, -rd, bsdf);
+                                K.qBeta[idx] = b4;
+                            }
+                        } else if (bounce <= K.recordBounces) {
+                            const uint32_t idx = coalescedAppend(K.rCount);
+                            if (idx < K.rCap) {
+                                writeCacheFeatures(K.rFeat + size_t(idx) * 16, s, -rd, bsdf);
+                                K.rPrefix[idx] = make_float4(L.x, L.y, L.z, __uint_as_float(slot));
+                                K.rBeta[idx] = b4;
+                            }
+                        }
+                    }
+                    float3 Tn, Bn;
+                    buildOnb(s.nShade, Tn, Bn);
+                    const float3 nd = -rd;
+                    float3 wo = f3(dot(nd, Tn), dot(nd, Bn), dot(nd, s.nShade));
+                    if (wo.z < 1e-6f) wo.z = 1e-6f;
+                    wo = normalize(wo);
+                    const LightSample ls = cacheQuery ? LightSample{} : sampleOneLight(P, s.pos, rng);
+                    if (!cacheQuery && ls.valid && ls.pdf > 1e-9f) {
+                        const float3 wi = f3(dot(ls.wi, Tn), dot(ls.wi, Bn), dot(ls.wi, s.nShade));
+                        float3 f;
+                        float bsdfPdf;
+                        bsdfEval(bsdf, wo, wi, f, bsdfPdf);
+                        if (maxComp(f) > 0.0f) {
+                            const float w = ls.delta ? 1.0f : balanceHeuristic(ls.pdf, bsdfPdf);
+                            shadow = true;
+                            shOrig = s.pos + s.nGeom * (wi.z > 0.0f ? MRT_EPS_RAY : -MRT_EPS_RAY);
+                            shDir = ls.wi;
+                            shTMax = ls.dist - 2.0f * MRT_EPS_RAY;
+                            shContrib = beta * f * fabsf(wi.z) * ls.radiance * w / ls.pdf;
+                        }
+                    }
+                    const BsdfSample bs = cacheQuery ? BsdfSample{} : bsdfSample(bsdf, wo, rng);
+                    if (!cacheQuery && bs.valid) {
+                        const float3 wiWorld = normalize(Tn * bs.wi.x + Bn * bs.wi.y + s.nShade * bs.wi.z);
+                        beta *= bs.f * fabsf(bs.wi.z) / bs.pdf;
+                        prevBsdfPdf = bs.pdf;
+                        bool alive = true;
+                        if (bounce >= 3u) {
+                            const float p = clampf(maxComp(beta), 0.05f, 0.95f);
+                            if (rng1(rng) >= p) alive = false;
+                            else beta /= p;
+                        }
+                        if (alive) {
+                            ro = s.pos + s.nGeom * (bs.wi.z > 0.0f ? MRT_EPS_RAY : -MRT_EPS_RAY);
+                            rd = wiWorld;
+                            cont = bounce + 1u <= P.maxBounces;
+                        }
+                    }
+                }
+            }
+            S.L[slot] = make_float4(L.x, L.y, L.z, 0.0f);
             if (cont) {
-                S.rayO[slot] = make_float4(st.ro.x, st.ro.y, st.ro.z, st.prevBsdfPdf);
-                S.rayD[slot] = make_float4(st.rd.x, st.rd.y, st.rd.z, __uint_as_float(st.bounce));
-                S.beta[slot] = make_float4(st.beta.x, st.beta.y, st.beta.z, __uint_as_float(st.rngW));
+                S.rayO[slot] = make_float4(ro.x, ro.y, ro.z, prevBsdfPdf);
+                S.rayD[slot] = make_float4(rd.x, rd.y, rd.z, __uint_as_float(bounce + 1u));
+                S.beta[slot] = make_float4(beta.x, beta.y, beta.z, __uint_as_float(rng.w));
             }
         }
         uint32_t qi, si;
@@ -519,7 +467,6 @@ __global__ void __launch_bounds__(kShadeBlock) waveShadeKernel(MrtFrameParams P,
 // one shadow ray per bounce, so the update needs no atomics. Persistent
 // warps with lane refill, as the extend kernel.
 __global__ void MRT_TRAV_BOUNDS waveShadowKernel(MrtFrameParams P, MrtWaveState S) {
-    if (S.counts[kTailDone] != 0u) return;  // the tail kernel finished the wave's paths
     const uint32_t n = S.counts[2];
     if (blockIdx.x == 0 && threadIdx.x == 0) S.counts[kExtendHead] = 0;  // for the next bounce
     uint32_t c[kCtrCount] = {};
@@ -564,58 +511,6 @@ __global__ void MRT_TRAV_BOUNDS waveShadowKernel(MrtFrameParams P, MrtWaveState 
     warpAddCounters(P.rayCounters, c);
 }
 
-// Fused tail of a wave (plain mode). Late bounces hold few paths, and a
-// per-bounce launch then lasts as long as its slowest ray: on the 1080p
-// terrain a 1-spp frame spent half its time in bounces 4-12. Launched after
-// every bounce b's shadow kernel: once the queue of paths continuing to
-// bounce b + 1 holds at most `threshold` paths, each thread takes a path and
-// runs it to its end -- closest hit (the per-thread walk, whose hits equal
-// the wavefront kernel's), the same shadePath, the any-hit test of its
-// shadow ray -- so the remaining paths' latencies overlap instead of adding
-// up bounce by bounce. It records the bounce in counts[kTailDone]; the
-// later per-bounce kernels then return at once. A path's operations, draws
-// and radiance additions are those of the wavefront, in the same order.
-#ifndef MRT_TAIL_PATHS
-#define MRT_TAIL_PATHS 65536
-#endif
-__global__ void __launch_bounds__(128) waveTailKernel(MrtFrameParams P, MrtWaveState S, WaveArgs A, uint32_t b,
-                                                      uint32_t threshold) {
-    const uint32_t cur = (b & 1u) ^ 1u;  // the queue shade(b) filled
-    const uint32_t done = S.counts[kTailDone];
-    const uint32_t n = S.counts[cur];
-    // a tail fused after an earlier bounce, or too many paths left: nothing
-    // to do (this launch's own mark, b + 1, may already be visible)
-    if ((done != 0u && done != b + 1u) || (done == 0u && n > threshold)) return;
-    if (done == 0u && blockIdx.x == 0 && threadIdx.x == 0) S.counts[kTailDone] = b + 1u;
-    const uint32_t* __restrict__ q = S.queue[cur];
-    uint32_t c[kCtrCount] = {};
-    TraversalCounters tcClosest, tcShadow;
-    bool ok = true;
-    const MrtCacheArgs noCache{};
-    for (;;) {
-        const uint32_t i = atomicAdd(S.counts + kTailHead, 1u);
-        if (i >= n) break;
-        const uint32_t slot = q[i];
-        const float4 o4 = S.rayO[slot], d4 = S.rayD[slot], b4 = S.beta[slot], L4 = S.L[slot];
-        PathState st{f3(o4), f3(d4), f3(b4), f3(L4), o4.w, __float_as_uint(d4.w), __float_as_uint(b4.w)};
-        for (;;) {
-            HitRecord hit;
-            ok &= traceClosest(P, st.ro, st.rd, 1e30f, hit, tcClosest);
-            c[kCtrTailClosest]++;
-            const ShadeResult r = shadePath<false>(P, A, noCache, slot, st, hit, c);
-            if (r.shadow) {
-                c[kCtrTailShadow]++;
-                if (!traceAny(P, r.shOrig, r.shDir, r.shTMax, ok, tcShadow)) st.L += r.shContrib;
-            }
-            if (!r.cont) break;
-        }
-        S.L[slot] = make_float4(st.L.x, st.L.y, st.L.z, 0.0f);
-    }
-    if (!ok) atomicOr(P.errorFlags, 1u);
-    if (tcClosest.bad || tcShadow.bad) atomicOr(P.errorFlags, 2u);
-    warpAddCounters(P.rayCounters, c);
-}
-
 // Firefly clamp and NaN guard of every finished path (pathtrace.comp:219-225),
 // then the FP64 accumulation: per pixel, the wave's samples are added in
 // sample order (pathtrace.comp:227-228).
@@ -656,7 +551,6 @@ __global__ void queryToWaveKernel(const MrtQueryRay* __restrict__ rays, uint32_t
     if (i == 0) {
         S.counts[0] = n;
         S.counts[kExtendHead] = 0;
-        S.counts[kTailDone] = 0;
     }
     if (i >= n) return;
     const MrtQueryRay r = rays[i];
@@ -804,13 +698,6 @@ extern "C" cudaError_t mrtcu_wave(const MrtFrameParams* p, const MrtWaveState* s
         waveShadowKernel<<<gShadow, MRT_TRAV_THREADS, 0, stream>>>(*p, *s);
         if (ev) cudaEventRecord(ev[3], stream);
         n += 3;
-        // plain mode: the fused tail, once few paths continue (the cache
-        // mode's queries and training records come from the shade kernel)
-        if (!cache && b < p->maxBounces) {
-            waveTailKernel<<<(MRT_TAIL_PATHS + 127) / 128, 128, 0, stream>>>(*p, *s, A, b, MRT_TAIL_PATHS);
-            ++n;
-        }
-        if (ev) cudaEventRecord(ev[4], stream);
     }
     if (!cache) {  // the cache mode finalises after applying the cache (mrtcu_wave_finalize)
         waveFinalizeKernel<<<(pixels + 255) / 256, 256, 0, stream>>>(*p, *s, A);

@@ -1102,25 +1102,22 @@ mrtResult Engine::completePending() {
     MRT_CUDA(cudaEventElapsedTime(&ms, m_ev0, m_ev1));
     m_stats.lastRenderMs = ms;
     const size_t perWave = size_t(6) * bounces;
-    float ext = 0.0f, sha = 0.0f, shw = 0.0f, tail = 0.0f;
+    float ext = 0.0f, sha = 0.0f, shw = 0.0f;
     for (uint32_t w = 0; w < waves; ++w)
         for (uint32_t b = 0; b < bounces; ++b) {
             const cudaEvent_t* ev = m_stageEvents.data() + w * perWave + 6 * b;
-            float a = 0.0f, c = 0.0f, d = 0.0f, t = 0.0f;
+            float a = 0.0f, c = 0.0f, d = 0.0f;
             MRT_CUDA(cudaEventElapsedTime(&a, ev[0], ev[1]));
             MRT_CUDA(cudaEventElapsedTime(&c, ev[1], ev[2]));
             MRT_CUDA(cudaEventElapsedTime(&d, ev[2], ev[3]));
-            MRT_CUDA(cudaEventElapsedTime(&t, ev[3], ev[4]));
             ext += a;
             sha += c;
             shw += d;
-            tail += t;
         }
     m_stats.extendMs = ext;
     m_stats.shadeMs = sha;
     m_stats.shadowMs = shw;
-    m_stats.tailMs = tail;
-    m_stats.otherMs = ms - ext - sha - shw - tail;
+    m_stats.otherMs = ms - ext - sha - shw;
     m_stats.lastRenderSpp = n;
     m_stats.kernelLaunches = m_inFlightLaunches;
     m_stats.extendLaunches = waves * bounces;
@@ -1143,15 +1140,13 @@ mrtResult Engine::completePending() {
     }
     unsigned long long ctr[16];
     MRT_CUDA(cudaMemcpy(ctr, m_rayCounters.ptr, sizeof(ctr), cudaMemcpyDeviceToHost));
-    m_stats.tailRaysClosest = ctr[7];
-    m_stats.tailRaysShadow = ctr[8];
-    // A build of the kernels with MRT_TRAV_PROFILE defined fills slots 9..15
+    // A build of the kernels with MRT_TRAV_PROFILE defined fills slots 8..14
     // with the extend kernel's warp-step statistics; they are logged.
-    if (ctr[9])
-        log(LogLevel::Info, "extend warp steps " + std::to_string(ctr[9]) + " active lanes " + std::to_string(ctr[10]) +
-                                " triangle steps " + std::to_string(ctr[11]) + " pairs " + std::to_string(ctr[12]) +
-                                " rounds " + std::to_string(ctr[13]) + " node steps " + std::to_string(ctr[14]) +
-                                " node lanes " + std::to_string(ctr[15]));
+    if (ctr[8])
+        log(LogLevel::Info, "extend warp steps " + std::to_string(ctr[8]) + " active lanes " + std::to_string(ctr[9]) +
+                                " triangle steps " + std::to_string(ctr[10]) + " pairs " + std::to_string(ctr[11]) +
+                                " rounds " + std::to_string(ctr[12]) + " node steps " + std::to_string(ctr[13]) +
+                                " node lanes " + std::to_string(ctr[14]));
     m_stats.raysClosest = ctr[0];
     m_stats.raysShadow = ctr[1];
     m_stats.nodeFetches = ctr[2];
