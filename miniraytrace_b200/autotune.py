@@ -20,8 +20,11 @@ constant in turn every candidate value is built into its own directory
 (``build(defines=..., lib=...)``) and timed by ``bench.py`` in a child
 process that loads that build (``MRT_LIBRARY``); the best value is kept
 before the next constant is tried, and the sweep repeats for ``--rounds``.
-The objective is ``bench.py``'s ``value`` (Mpaths/s of the 1080p terrain
-workload, scene resident), the median of the child's timed steps. With
+The objective is Mpaths/s of the 1080p terrain workload (scene resident)
+over the median device time of the child's timed steps (``bench.py``'s
+``step_device_ms``: the engine's CUDA-event time of its kernels, free of the
+host jitter around the call); the starting point is measured once before
+the search and discarded, since a fresh GPU's first run reads low. With
 ``--write`` the winner goes to ``tuned.json``, which ``build()`` applies;
 every measurement is stored beside it.
 """
@@ -34,6 +37,8 @@ import subprocess
 import sys
 import tempfile
 from pathlib import Path
+
+import numpy as np
 
 from . import build as mrt_build
 
@@ -63,7 +68,10 @@ def measure(defines: dict, workdir: Path, steps: int, warmup: int) -> float:
         raise RuntimeError(f"bench failed for {defines}:\n{r.stdout[-2000:]}\n{r.stderr[-2000:]}")
     line = [ln for ln in r.stdout.splitlines() if ln.startswith("{")][-1]
     out = json.loads(line)
-    return float(out["value"])
+    # paths per second of device time: the engine's own CUDA-event time of
+    # its kernels per step (the step time around the call adds host jitter)
+    paths = out["config"]["width"] * out["config"]["height"] * out["config"]["spp_per_step"]
+    return paths / (float(np.median(out["step_device_ms"])) / 1e3) / 1e6
 
 
 def tune(rounds: int, steps: int, warmup: int, log=print) -> dict:
@@ -82,6 +90,7 @@ def tune(rounds: int, steps: int, warmup: int, log=print) -> dict:
                 log(json.dumps(results[-1]))
             return cache[key]
 
+        measure(current, work, steps, warmup)  # a first run on a fresh GPU reads low: discarded
         best = score(current)
         for _ in range(rounds):
             changed = False
@@ -96,7 +105,7 @@ def tune(rounds: int, steps: int, warmup: int, log=print) -> dict:
             if not changed:
                 break
     return {"defines": current, "mpaths_per_s": best, "measurements": results,
-            "objective": "bench.py value: Mpaths/s, 1920x1080 terrain (2,420,738 triangles), 64 spp per step, "
+            "objective": "Mpaths/s over the median device time per step, 1920x1080 terrain (2,420,738 triangles), 64 spp per step, "
                          f"{steps} timed steps after {warmup} warm-up steps"}
 
 

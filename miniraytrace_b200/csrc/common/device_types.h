@@ -196,6 +196,26 @@ typedef struct MrtWaveState {
     uint32_t pad;
 } MrtWaveState;
 
+// One job of a one-launch batch (several engines' waves rendered by the
+// same kernel launches): the job's frame parameters, its wave (pixels,
+// slots = pixels x samples, the first sample's index, samples per pixel),
+// and where its slots and pixels start in the batch's concatenated slot and
+// pixel ranges. A batch wave's slot s belongs to the last job whose
+// slotBase <= s; its local slot is s - slotBase.
+typedef struct MrtBatchJob {
+    MrtFrameParams params;
+    uint32_t pixels, slots, sampleBase, samples;
+    uint32_t slotBase, pixelBase;
+    uint32_t pad[2];
+} MrtBatchJob;
+
+typedef struct MrtBatchJobs {
+    const MrtBatchJob* jobs;  // device memory, `count` entries, slotBase ascending
+    uint32_t count;
+    uint32_t totalSlots, totalPixels;
+    uint32_t pad;
+} MrtBatchJobs;
+
 // One query ray of mrtxTraceRays (same layout as mrtxRay) and its hit.
 typedef struct MrtQueryRay {
     float origin[3];

@@ -46,6 +46,15 @@ extern "C" {
 cudaError_t mrtcu_wave(const MrtFrameParams* p, const MrtWaveState* s, uint32_t sampleBase, uint32_t samples,
                        uint32_t* launches, const cudaEvent_t* stageEvents, const MrtCacheArgs* cache,
                        cudaStream_t stream);
+// One-launch batch: the waves of `count` jobs (every job's scene and wave in
+// its MrtBatchJob; devJobs is the device copy of hostJobs, slot and pixel
+// bases ascending) rendered by one set of per-bounce kernel launches over
+// their concatenated slots (sum of slots <= s->capacity). `batch` carries
+// the ray counters and the error word of the whole batch; maxBounces is the
+// largest of the jobs' (each path stops at its own job's bound).
+cudaError_t mrtcu_wave_batch(const MrtFrameParams* batch, const MrtWaveState* s, const MrtBatchJob* devJobs,
+                             const MrtBatchJob* hostJobs, uint32_t count, uint32_t maxBounces, uint32_t* launches,
+                             const cudaEvent_t* stageEvents, cudaStream_t stream);
 // With a cache, mrtcu_wave leaves the wave unfinalised: the cache's
 // predictions are added to the paths, then this accumulates the wave.
 cudaError_t mrtcu_wave_finalize(const MrtFrameParams* p, const MrtWaveState* s, uint32_t sampleBase,

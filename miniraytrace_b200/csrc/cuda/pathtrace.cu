@@ -137,19 +137,41 @@ MRT_DEV uint32_t frameOf(const MrtFrameParams& P, const WaveArgs& A, uint32_t sl
     return P.streamOffset + (A.sampleBase + slot % A.samples) * P.streamStride;
 }
 
-// Camera rays of every slot of the wave (pathtrace.comp:101-130).
-__global__ void __launch_bounds__(256) waveInitKernel(MrtFrameParams P, MrtWaveState S, WaveArgs A) {
+// One-launch batch (kMulti kernels): the job a batch slot (or, with
+// `pixels`, a batch pixel) belongs to -- the last job whose base is at most
+// v (a binary search over at most a few dozen bases, L1-resident) -- and
+// that job's wave.
+MRT_DEV uint32_t batchJobOf(const MrtBatchJobs& B, uint32_t v, bool pixels) {
+    uint32_t lo = 0, hi = B.count;
+    while (hi - lo > 1u) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if ((pixels ? B.jobs[mid].pixelBase : B.jobs[mid].slotBase) <= v) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+MRT_DEV WaveArgs jobWave(const MrtBatchJob& J) { return WaveArgs{J.pixels, J.slots, J.sampleBase, J.samples}; }
+
+// Camera rays of every slot of the wave (pathtrace.comp:101-130). In a
+// one-launch batch every job's slots, each with its job's camera.
+template <bool kMulti>
+__global__ void __launch_bounds__(256) waveInitKernel(MrtFrameParams Pk, MrtWaveState S, WaveArgs Ak, MrtBatchJobs B) {
     const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t total = kMulti ? B.totalSlots : Ak.slots;
     if (slot == 0) {
-        S.counts[0] = A.slots;
+        S.counts[0] = total;
         S.counts[1] = 0;
         S.counts[2] = 0;
         S.counts[4] = 0;  // extend fetch counter (kExtendHead) of bounce 0
     }
-    if (slot >= A.slots) return;
-    const uint32_t pixel = slot / A.samples;
+    if (slot >= total) return;
+    const MrtBatchJob* J = kMulti ? B.jobs + batchJobOf(B, slot, false) : nullptr;
+    const MrtFrameParams& P = kMulti ? J->params : Pk;
+    const WaveArgs A = kMulti ? jobWave(*J) : Ak;
+    const uint32_t lslot = kMulti ? slot - J->slotBase : slot;
+    const uint32_t pixel = lslot / A.samples;
     const uint32_t px = pixel % P.width, py = pixel / P.width;
-    Rng rng{px, py, frameOf(P, A, slot), 0u};
+    Rng rng{px, py, frameOf(P, A, lslot), 0u};
     const float2 jitter = rng2(rng);
     const float u = (float(px) + jitter.x) / float(P.width);
     const float v = (float(py) + jitter.y) / float(P.height);
@@ -214,7 +236,8 @@ MRT_DEV uint32_t refillLane(uint32_t* head, uint32_t n, bool active, bool& drain
 // Closest hit of every queued ray (intersect.glsl:88-125 traceRay).
 // Persistent warps with lane refill; every lane of a warp stays in the loop
 // until the warp has no ray left.
-__global__ void MRT_TRAV_BOUNDS waveExtendKernel(MrtFrameParams P, MrtWaveState S, uint32_t cur) {
+template <bool kMulti>
+__global__ void MRT_TRAV_BOUNDS waveExtendKernel(MrtFrameParams Pk, MrtWaveState S, uint32_t cur, MrtBatchJobs B) {
     const uint32_t* __restrict__ q = S.queue[cur];
     const uint32_t n = S.counts[cur];
     if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -225,7 +248,7 @@ __global__ void MRT_TRAV_BOUNDS waveExtendKernel(MrtFrameParams P, MrtWaveState 
     uint32_t c[kCtrCount] = {};
     TraversalCounters tc;
     bool ok = true, active = false, drained = false;
-    uint32_t slot = 0;
+    uint32_t slot = 0, job = 0;  // job: the lane's ray's batch job (kMulti)
     WideTrav T;
     WideStack stack;
     for (;;) {
@@ -233,13 +256,15 @@ __global__ void MRT_TRAV_BOUNDS waveExtendKernel(MrtFrameParams P, MrtWaveState 
             const uint32_t i = refillLane(S.counts + kExtendHead, n, active, drained);
             if (i != 0xffffffffu) {
                 slot = q[i];
+                if (kMulti) job = batchJobOf(B, slot, false);
                 const float4 o = S.rayO[slot], d = S.rayD[slot];
-                travBegin(P, T, f3(o), f3(d), 1e30f);
+                travBegin(kMulti ? B.jobs[job].params : Pk, T, f3(o), f3(d), 1e30f);
                 active = true;
             }
         }
         if (!__any_sync(0xffffffffu, active)) break;
-        const int r = travWarpStep<false>(P, T, stack, tc, active);
+        const MrtFrameParams& P = kMulti ? B.jobs[job].params : Pk;
+        const int r = travWarpStep<false, kMulti>(P, T, stack, tc, active, B.jobs, job);
         if (active && r != kTravRunning) {
             HitRecord h = T.hit;
             if (h.tri != 0xffffffffu) refineHit(P, T.wo, T.wd, h);
@@ -250,8 +275,8 @@ __global__ void MRT_TRAV_BOUNDS waveExtendKernel(MrtFrameParams P, MrtWaveState 
             active = false;
         }
     }
-    if (!ok) atomicOr(P.errorFlags, 1u);
-    if (tc.bad) atomicOr(P.errorFlags, 2u);
+    if (!ok) atomicOr(Pk.errorFlags, 1u);
+    if (tc.bad) atomicOr(Pk.errorFlags, 2u);
     c[kCtrExtNodes] = tc.nodes;
     c[kCtrExtTris] = tc.tris;
 #ifdef MRT_TRAV_PROFILE
@@ -263,7 +288,7 @@ __global__ void MRT_TRAV_BOUNDS waveExtendKernel(MrtFrameParams P, MrtWaveState 
     c[kCtrNodeSteps] = tc.nodeSteps;
     c[kCtrNodeLanes] = tc.nodeLanes;
 #endif
-    warpAddCounters(P.rayCounters, c);
+    warpAddCounters(Pk.rayCounters, c);
 }
 
 // Shading of every queued path at its hit (pathtrace.comp:133-216): miss ->
@@ -326,9 +351,9 @@ MRT_DEV void blockAppend2(uint32_t* ca, bool pa, uint32_t& ia, uint32_t* cb, boo
     __syncthreads();  // s is reused by the next call
 }
 
-template <bool kCache>
-__global__ void __launch_bounds__(kShadeBlock) waveShadeKernel(MrtFrameParams P, MrtWaveState S, WaveArgs A, uint32_t cur,
-                                                       MrtCacheArgs K) {
+template <bool kCache, bool kMulti>
+__global__ void __launch_bounds__(kShadeBlock) waveShadeKernel(MrtFrameParams Pk, MrtWaveState S, WaveArgs Ak,
+                                                               uint32_t cur, MrtCacheArgs K, MrtBatchJobs B) {
     const uint32_t* __restrict__ q = S.queue[cur];
     uint32_t* __restrict__ qn = S.queue[cur ^ 1u];
     const uint32_t n = S.counts[cur];
@@ -345,10 +370,14 @@ __global__ void __launch_bounds__(kShadeBlock) waveShadeKernel(MrtFrameParams P,
         bool cacheQuery = false;  // cache mode: the path stops here and takes the cache's prediction
         if (valid) {
             slot = q[i];
+            const MrtBatchJob* J = kMulti ? B.jobs + batchJobOf(B, slot, false) : nullptr;
+            const MrtFrameParams& P = kMulti ? J->params : Pk;
+            const WaveArgs A = kMulti ? jobWave(*J) : Ak;
+            const uint32_t lslot = kMulti ? slot - J->slotBase : slot;  // the slot within its job's wave
             const float4 o4 = S.rayO[slot], d4 = S.rayD[slot], b4 = S.beta[slot], L4 = S.L[slot];
             const float4 h4 = S.hit[slot];
-            const uint32_t pixel = slot / A.samples;
-            Rng rng{pixel % P.width, pixel / P.width, frameOf(P, A, slot), __float_as_uint(b4.w)};
+            const uint32_t pixel = lslot / A.samples;
+            Rng rng{pixel % P.width, pixel / P.width, frameOf(P, A, lslot), __float_as_uint(b4.w)};
             const uint32_t bounce = __float_as_uint(d4.w);
             float3 ro = f3(o4), rd = f3(d4), beta = f3(b4), L = f3(L4);
             float prevBsdfPdf = o4.w;
@@ -386,7 +415,7 @@ __global__ void __launch_bounds__(kShadeBlock) waveShadeKernel(MrtFrameParams P,
                         // written out here.
                         // (Queries and records append in separate branches: a
                         // coalesced group then shares one list.)
-                        cacheQuery = !cacheTrainingPath(K, pixel, frameOf(P, A, slot));
+                        cacheQuery = !cacheTrainingPath(K, pixel, frameOf(P, A, lslot));
                         const float4 b4 = make_float4(beta.x, beta.y, beta.z, __uint_as_float(slot));
                         if (cacheQuery) {
                             const uint32_t idx = coalescedAppend(K.qCount);
@@ -459,20 +488,21 @@ __global__ void __launch_bounds__(kShadeBlock) waveShadeKernel(MrtFrameParams P,
             S.shC[si] = make_float4(shContrib.x, shContrib.y, shContrib.z, 0.0f);
         }
     }
-    warpAddCounters(P.rayCounters, c);
+    warpAddCounters(Pk.rayCounters, c);
 }
 
 // Any-hit test of every queued shadow ray; unoccluded rays add their NEE
 // contribution to their path (pathtrace.comp:192-195). A path has at most
 // one shadow ray per bounce, so the update needs no atomics. Persistent
 // warps with lane refill, as the extend kernel.
-__global__ void MRT_TRAV_BOUNDS waveShadowKernel(MrtFrameParams P, MrtWaveState S) {
+template <bool kMulti>
+__global__ void MRT_TRAV_BOUNDS waveShadowKernel(MrtFrameParams Pk, MrtWaveState S, MrtBatchJobs B) {
     const uint32_t n = S.counts[2];
     if (blockIdx.x == 0 && threadIdx.x == 0) S.counts[kExtendHead] = 0;  // for the next bounce
     uint32_t c[kCtrCount] = {};
     TraversalCounters tc;
     bool ok = true, active = false, drained = false;
-    uint32_t idx = 0;
+    uint32_t idx = 0, job = 0;  // job: the lane's ray's batch job (kMulti)
     WideTrav T;
     WideStack stack;
     for (;;) {
@@ -481,13 +511,15 @@ __global__ void MRT_TRAV_BOUNDS waveShadowKernel(MrtFrameParams P, MrtWaveState 
             if (i != 0xffffffffu) {
                 idx = i;
                 const float4 o = S.shO[i], d = S.shD[i];
-                travBegin(P, T, f3(o), f3(d), o.w);
+                if (kMulti) job = batchJobOf(B, __float_as_uint(d.w), false);
+                travBegin(kMulti ? B.jobs[job].params : Pk, T, f3(o), f3(d), o.w);
                 active = true;
                 c[kCtrShadow]++;
             }
         }
         if (!__any_sync(0xffffffffu, active)) break;
-        const int r = travWarpStep<true>(P, T, stack, tc, active);
+        const MrtFrameParams& P = kMulti ? B.jobs[job].params : Pk;
+        const int r = travWarpStep<true, kMulti>(P, T, stack, tc, active, B.jobs, job);
         if (active) {
             if (r != kTravRunning) {
                 ok &= T.ok;
@@ -504,22 +536,31 @@ __global__ void MRT_TRAV_BOUNDS waveShadowKernel(MrtFrameParams P, MrtWaveState 
             }
         }
     }
-    if (!ok) atomicOr(P.errorFlags, 1u);
-    if (tc.bad) atomicOr(P.errorFlags, 2u);
+    if (!ok) atomicOr(Pk.errorFlags, 1u);
+    if (tc.bad) atomicOr(Pk.errorFlags, 2u);
     c[kCtrShNodes] = tc.nodes;
     c[kCtrShTris] = tc.tris;
-    warpAddCounters(P.rayCounters, c);
+    warpAddCounters(Pk.rayCounters, c);
 }
 
 // Firefly clamp and NaN guard of every finished path (pathtrace.comp:219-225),
 // then the FP64 accumulation: per pixel, the wave's samples are added in
 // sample order (pathtrace.comp:227-228).
-__global__ void __launch_bounds__(256) waveFinalizeKernel(MrtFrameParams P, MrtWaveState S, WaveArgs A) {
-    const uint32_t pixel = blockIdx.x * blockDim.x + threadIdx.x;
-    if (pixel >= A.pixels) return;
+// In a one-launch batch every job's pixels, each into its job's
+// accumulation.
+template <bool kMulti>
+__global__ void __launch_bounds__(256) waveFinalizeKernel(MrtFrameParams Pk, MrtWaveState S, WaveArgs Ak,
+                                                          MrtBatchJobs B) {
+    const uint32_t gp = blockIdx.x * blockDim.x + threadIdx.x;
+    if (gp >= (kMulti ? B.totalPixels : Ak.pixels)) return;
+    const MrtBatchJob* J = kMulti ? B.jobs + batchJobOf(B, gp, true) : nullptr;
+    const MrtFrameParams& P = kMulti ? J->params : Pk;
+    const WaveArgs A = kMulti ? jobWave(*J) : Ak;
+    const uint32_t pixel = kMulti ? gp - J->pixelBase : gp;
+    const size_t slotBase = kMulti ? J->slotBase : 0u;
     double sx = 0.0, sy = 0.0, sz = 0.0;
     for (uint32_t s = 0; s < A.samples; ++s) {
-        const float4 l4 = S.L[size_t(pixel) * A.samples + s];
+        const float4 l4 = S.L[slotBase + size_t(pixel) * A.samples + s];
         float3 L = f3(l4);
         if (P.fireflyClamp > 0.0f) {
             const float m = maxComp(L);
@@ -642,6 +683,7 @@ int persistentBlocks(const void* kernel, int threads) {
 // wave of blocks). Computed once per device, on first use with it current.
 struct WaveGrids {
     int extend, shade, shadeCache, shadow;
+    int extendMulti, shadeMulti, shadowMulti;  // one-launch batch variants
 };
 
 const WaveGrids& waveGrids() {
@@ -652,13 +694,19 @@ const WaveGrids& waveGrids() {
     std::lock_guard<std::mutex> lock(mutex);
     auto it = grids.find(dev);
     if (it == grids.end())
-        it = grids.emplace(dev, WaveGrids{persistentBlocks(reinterpret_cast<const void*>(waveExtendKernel),
+        it = grids.emplace(dev, WaveGrids{persistentBlocks(reinterpret_cast<const void*>(waveExtendKernel<false>),
                                                            MRT_TRAV_THREADS),
-                                          persistentBlocks(reinterpret_cast<const void*>(waveShadeKernel<false>),
+                                          persistentBlocks(reinterpret_cast<const void*>(waveShadeKernel<false, false>),
                                                            kShadeBlock),
-                                          persistentBlocks(reinterpret_cast<const void*>(waveShadeKernel<true>),
+                                          persistentBlocks(reinterpret_cast<const void*>(waveShadeKernel<true, false>),
                                                            kShadeBlock),
-                                          persistentBlocks(reinterpret_cast<const void*>(waveShadowKernel),
+                                          persistentBlocks(reinterpret_cast<const void*>(waveShadowKernel<false>),
+                                                           MRT_TRAV_THREADS),
+                                          persistentBlocks(reinterpret_cast<const void*>(waveExtendKernel<true>),
+                                                           MRT_TRAV_THREADS),
+                                          persistentBlocks(reinterpret_cast<const void*>(waveShadeKernel<false, true>),
+                                                           kShadeBlock),
+                                          persistentBlocks(reinterpret_cast<const void*>(waveShadowKernel<true>),
                                                            MRT_TRAV_THREADS)})
                  .first;
     return it->second;
@@ -670,7 +718,7 @@ extern "C" cudaError_t mrtcu_wave_finalize(const MrtFrameParams* p, const MrtWav
     const uint32_t pixels = p->width * p->height;
     if (pixels == 0 || samples == 0) return cudaSuccess;
     WaveArgs A{pixels, pixels * samples, sampleBase, samples};
-    waveFinalizeKernel<<<(pixels + 255) / 256, 256, 0, stream>>>(*p, *s, A);
+    waveFinalizeKernel<false><<<(pixels + 255) / 256, 256, 0, stream>>>(*p, *s, A, MrtBatchJobs{});
     return cudaGetLastError();
 }
 
@@ -684,25 +732,66 @@ extern "C" cudaError_t mrtcu_wave(const MrtFrameParams* p, const MrtWaveState* s
     const int gExtend = g.extend, gShade = g.shade, gShadeCache = g.shadeCache, gShadow = g.shadow;
     WaveArgs A{pixels, pixels * samples, sampleBase, samples};
     uint32_t n = 0;
-    waveInitKernel<<<(A.slots + 255) / 256, 256, 0, stream>>>(*p, *s, A);
+    waveInitKernel<false><<<(A.slots + 255) / 256, 256, 0, stream>>>(*p, *s, A, MrtBatchJobs{});
     ++n;
     for (uint32_t b = 0; b <= p->maxBounces; ++b) {
         const uint32_t cur = b & 1u;
         const cudaEvent_t* ev = stageEvents ? stageEvents + 6 * b : nullptr;
         if (ev) cudaEventRecord(ev[0], stream);
-        waveExtendKernel<<<gExtend, MRT_TRAV_THREADS, 0, stream>>>(*p, *s, cur);
+        waveExtendKernel<false><<<gExtend, MRT_TRAV_THREADS, 0, stream>>>(*p, *s, cur, MrtBatchJobs{});
         if (ev) cudaEventRecord(ev[1], stream);
-        if (cache) waveShadeKernel<true><<<gShadeCache, kShadeBlock, 0, stream>>>(*p, *s, A, cur, *cache);
-        else waveShadeKernel<false><<<gShade, kShadeBlock, 0, stream>>>(*p, *s, A, cur, MrtCacheArgs{});
+        if (cache)
+            waveShadeKernel<true, false><<<gShadeCache, kShadeBlock, 0, stream>>>(*p, *s, A, cur, *cache,
+                                                                                   MrtBatchJobs{});
+        else
+            waveShadeKernel<false, false><<<gShade, kShadeBlock, 0, stream>>>(*p, *s, A, cur, MrtCacheArgs{},
+                                                                              MrtBatchJobs{});
         if (ev) cudaEventRecord(ev[2], stream);
-        waveShadowKernel<<<gShadow, MRT_TRAV_THREADS, 0, stream>>>(*p, *s);
+        waveShadowKernel<false><<<gShadow, MRT_TRAV_THREADS, 0, stream>>>(*p, *s, MrtBatchJobs{});
         if (ev) cudaEventRecord(ev[3], stream);
         n += 3;
     }
     if (!cache) {  // the cache mode finalises after applying the cache (mrtcu_wave_finalize)
-        waveFinalizeKernel<<<(pixels + 255) / 256, 256, 0, stream>>>(*p, *s, A);
+        waveFinalizeKernel<false><<<(pixels + 255) / 256, 256, 0, stream>>>(*p, *s, A, MrtBatchJobs{});
         ++n;
     }
+    if (launches) *launches += n;
+    return cudaGetLastError();
+}
+
+// One-launch batch: the waves of `count` jobs (devJobs: device copy of the
+// job table; the host copy gives the totals) rendered by one set of
+// per-bounce launches over the concatenated slots. `batch` carries the
+// batch's ray counters and error word (every job's own parameters carry
+// its scene). stageEvents as in mrtcu_wave.
+extern "C" cudaError_t mrtcu_wave_batch(const MrtFrameParams* batch, const MrtWaveState* s, const MrtBatchJob* devJobs,
+                                        const MrtBatchJob* hostJobs, uint32_t count, uint32_t maxBounces,
+                                        uint32_t* launches, const cudaEvent_t* stageEvents, cudaStream_t stream) {
+    if (count == 0) return cudaSuccess;
+    const MrtBatchJob& last = hostJobs[count - 1];
+    const uint32_t totalSlots = last.slotBase + last.slots, totalPixels = last.pixelBase + last.pixels;
+    if (totalSlots == 0) return cudaSuccess;
+    if (totalSlots > s->capacity) return cudaErrorInvalidValue;
+    const MrtBatchJobs B{devJobs, count, totalSlots, totalPixels, 0u};
+    const WaveGrids& g = waveGrids();
+    const WaveArgs none{0u, 0u, 0u, 1u};
+    uint32_t n = 0;
+    waveInitKernel<true><<<(totalSlots + 255) / 256, 256, 0, stream>>>(*batch, *s, none, B);
+    ++n;
+    for (uint32_t b = 0; b <= maxBounces; ++b) {
+        const uint32_t cur = b & 1u;
+        const cudaEvent_t* ev = stageEvents ? stageEvents + 6 * b : nullptr;
+        if (ev) cudaEventRecord(ev[0], stream);
+        waveExtendKernel<true><<<g.extendMulti, MRT_TRAV_THREADS, 0, stream>>>(*batch, *s, cur, B);
+        if (ev) cudaEventRecord(ev[1], stream);
+        waveShadeKernel<false, true><<<g.shadeMulti, kShadeBlock, 0, stream>>>(*batch, *s, none, cur, MrtCacheArgs{}, B);
+        if (ev) cudaEventRecord(ev[2], stream);
+        waveShadowKernel<true><<<g.shadowMulti, MRT_TRAV_THREADS, 0, stream>>>(*batch, *s, B);
+        if (ev) cudaEventRecord(ev[3], stream);
+        n += 3;
+    }
+    waveFinalizeKernel<true><<<(totalPixels + 255) / 256, 256, 0, stream>>>(*batch, *s, none, B);
+    ++n;
     if (launches) *launches += n;
     return cudaGetLastError();
 }
@@ -721,7 +810,7 @@ extern "C" cudaError_t mrtcu_trace_closest_wave(const MrtFrameParams* p, const M
     if (n > s->capacity) return cudaErrorInvalidValue;
     const WaveGrids& g = waveGrids();
     queryToWaveKernel<<<(n + 255) / 256, 256, 0, stream>>>(rays, n, *s);
-    waveExtendKernel<<<g.extend, MRT_TRAV_THREADS, 0, stream>>>(*p, *s, 0u);
+    waveExtendKernel<false><<<g.extend, MRT_TRAV_THREADS, 0, stream>>>(*p, *s, 0u, MrtBatchJobs{});
     waveToQueryKernel<<<(n + 255) / 256, 256, 0, stream>>>(*p, *s, n, hits);
     return cudaGetLastError();
 }

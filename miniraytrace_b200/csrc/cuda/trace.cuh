@@ -484,9 +484,13 @@ MRT_DEV int travTriStep(const MrtFrameParams& P, WideTrav& T, TraversalCounters&
 // are bit-identical to it. The winner's barycentrics follow through a
 // second slot written by the lane whose key equals the minimum. Any hit
 // (kAny): a warp-wide OR of the owners with a hit. Returns the lane's
-// kTrav* state; every pending lane ends with no triangles pending.
-template <bool kAny>
-MRT_DEV int travTriPhaseWarp(const MrtFrameParams& P, WideTrav& T, TraversalCounters& tc, bool pending) {
+// kTrav* state; every pending lane ends with no triangles pending. In a
+// one-launch batch (kMulti) lanes may walk different jobs' scenes: a
+// lane's `P` is its own job's parameters, and a pair's triangles are read
+// from its owner's job (jobs[owner's job]).
+template <bool kAny, bool kMulti = false>
+MRT_DEV int travTriPhaseWarp(const MrtFrameParams& P, WideTrav& T, TraversalCounters& tc, bool pending,
+                             const MrtBatchJob* jobs = nullptr, uint32_t job = 0u) {
     __shared__ unsigned long long sKey[MRT_TRAV_THREADS / 32][32];
     __shared__ float2 sUV[MRT_TRAV_THREADS / 32][32];
     const uint32_t full = 0xffffffffu;
@@ -523,6 +527,13 @@ MRT_DEV int travTriPhaseWarp(const MrtFrameParams& P, WideTrav& T, TraversalCoun
         sh.sy = __shfl_sync(full, T.sh.sy, o);
         sh.sz = __shfl_sync(full, T.sh.sz, o);
         const float otMax = __shfl_sync(full, T.tMax, o);
+        const float4* triVerts = P.triVerts;
+        uint32_t triCount = P.triCount;
+        if (kMulti) {
+            const MrtFrameParams& Po = jobs[__shfl_sync(full, job, o)].params;
+            triVerts = Po.triVerts;
+            triCount = Po.triCount;
+        }
         bool hit = false;
         unsigned long long key = 0;
         float u = 0.0f, v = 0.0f;
@@ -531,11 +542,11 @@ MRT_DEV int travTriPhaseWarp(const MrtFrameParams& P, WideTrav& T, TraversalCoun
             const uint32_t nth = k - (oi - uint32_t(__popc(ob)));
             const uint32_t tri = obase + __fns(ob, 0u, int(nth) + 1);
             ++tc.tris;
-            if (tri >= P.triCount) {
+            if (tri >= triCount) {
                 tc.bad = true;
             } else {
                 float t;
-                hit = hitTriangle(P.triVerts, tri, oo, sh, otMax, t, u, v);
+                hit = hitTriangle(triVerts, tri, oo, sh, otMax, t, u, v);
                 if (hit) {
                     if (kAny) {
                         occ |= 1u << o;
@@ -583,9 +594,9 @@ MRT_DEV int travTriPhaseWarp(const MrtFrameParams& P, WideTrav& T, TraversalCoun
 #ifndef MRT_TRI_PHASE_PCT
 #define MRT_TRI_PHASE_PCT 25
 #endif
-template <bool kAny>
+template <bool kAny, bool kMulti = false>
 MRT_DEV int travWarpStep(const MrtFrameParams& P, WideTrav& T, WideStack& stack, TraversalCounters& tc,
-                         bool active) {
+                         bool active, const MrtBatchJob* jobs = nullptr, uint32_t job = 0u) {
     const bool pending = active && T.pendBits != 0;
     const uint32_t pendLanes = __popc(__ballot_sync(0xffffffffu, pending));
     const uint32_t activeLanes = __popc(__ballot_sync(0xffffffffu, active));
@@ -607,7 +618,7 @@ MRT_DEV int travWarpStep(const MrtFrameParams& P, WideTrav& T, WideStack& stack,
         }
     }
 #endif
-    if (triPhase) return travTriPhaseWarp<kAny>(P, T, tc, pending);
+    if (triPhase) return travTriPhaseWarp<kAny, kMulti>(P, T, tc, pending, jobs, job);
     return active && !pending ? travNodeStep(P, T, stack, tc) : kTravRunning;
 }
 

@@ -351,12 +351,25 @@ mrtResult Engine::ensureWave(uint32_t samples) {
     if (m_waveSamples >= k) return MRT_SUCCESS;
     const uint64_t slots = pixels * k;
     if (slots > 0xffffffffull) return fail(MRT_ERROR_INVALID_ARGUMENT, "frame too large for one wave");
-    const size_t bytes = size_t(slots) * kWaveBytesPerSlot + 64;
     // growing frees the old allocation first: forget the carved pointers
     // before, so a failed allocation leaves no wave state that points into
     // freed memory (the next call allocates again)
     m_waveSamples = 0;
     m_waveState = MrtWaveState{};
+    MRT_TRY(carveWave(slots, m_waveState));
+    m_waveSamples = k;
+    return MRT_SUCCESS;
+}
+
+// A wave state of `slots` paths carved out of m_wave, grown as needed (when
+// it grows, this engine's own carved state is forgotten first; its next
+// ensureWave carves it again).
+mrtResult Engine::carveWave(uint64_t slots, MrtWaveState& w) {
+    const size_t bytes = size_t(slots) * kWaveBytesPerSlot + 64;
+    if (m_wave.bytes < bytes) {
+        m_waveSamples = 0;
+        m_waveState = MrtWaveState{};
+    }
     MRT_TRY(m_wave.ensure(bytes));
     char* base = static_cast<char*>(m_wave.ptr);
     auto carve = [&](size_t n) {
@@ -364,7 +377,6 @@ mrtResult Engine::ensureWave(uint32_t samples) {
         base += n;
         return p;
     };
-    MrtWaveState& w = m_waveState;
     w.rayO = reinterpret_cast<float4*>(carve(slots * 16));
     w.rayD = reinterpret_cast<float4*>(carve(slots * 16));
     w.beta = reinterpret_cast<float4*>(carve(slots * 16));
@@ -378,7 +390,6 @@ mrtResult Engine::ensureWave(uint32_t samples) {
     w.queue[1] = reinterpret_cast<uint32_t*>(carve(slots * 4));
     w.counts = reinterpret_cast<uint32_t*>(carve(64));
     w.capacity = uint32_t(slots);
-    m_waveSamples = k;
     return MRT_SUCCESS;
 }
 
@@ -1165,50 +1176,71 @@ mrtResult Engine::completePending() {
     return MRT_SUCCESS;
 }
 
-// mrtxRenderBatch: every engine commits, queues its samples and sizes its
-// wave state first (allocations would stall the other streams), then all
-// engines' waves are issued, each on its own stream, before any is waited
-// for, so jobs of uneven size overlap on the GPU.
+// mrtxRenderBatch: every engine commits and fixes its frame parameters
+// first. When all engines are on one GPU and none renders with the radiance
+// cache, their waves are rendered by one set of kernel launches
+// (renderBatchOneLaunch); otherwise every engine's waves are issued on its
+// own stream before any is waited for, so jobs of uneven size overlap.
 mrtResult Engine::renderBatch(Engine* const* engines, const uint32_t* spp, uint32_t count, mrtFrameInfo* infos) {
     const auto t0 = std::chrono::steady_clock::now();
+    // one set of launches when every engine is distinct, on one GPU and
+    // without the radiance cache (an engine listed twice keeps the stream
+    // path, where its earlier share is rendered before its later one)
+    bool oneLaunch = count >= 2;
+    for (uint32_t i = 0; i < count && oneLaunch; ++i) {
+        const Engine& e = *engines[i];
+        oneLaunch = !e.m_cache.enabled && e.m_device == engines[0]->m_device;
+        for (uint32_t j = 0; j < i && oneLaunch; ++j) oneLaunch = engines[j] != engines[i];
+    }
+    std::vector<uint32_t> n(count, 0u);
     for (uint32_t i = 0; i < count; ++i) {
         Engine& e = *engines[i];
         MRT_TRY(e.checkAlive());
         MRT_TRY(e.flushPending());  // samples queued earlier render first, in order
         MRT_TRY(e.commit(nullptr));
         const uint32_t done = e.m_frameIndex;
-        const uint32_t n = done < e.m_settings.sppLimit ? std::min(spp[i], e.m_settings.sppLimit - done) : 0u;
-        if (n > 0) {
+        n[i] = done < e.m_settings.sppLimit ? std::min(spp[i], e.m_settings.sppLimit - done) : 0u;
+        if (n[i] > 0) {
             e.fillParams(e.m_pendingParams);
-            e.m_pending = n;
             e.m_resolveExposure = std::exp2(e.m_settings.exposureEV);
             e.m_resolveTonemap = e.m_settings.tonemap;
-            MRT_TRY(e.guard(e.ensureWave(n)));
-        }
-    }
-    mrtResult launchError = MRT_SUCCESS;
-    uint32_t launched = 0;
-    for (; launched < count && launchError == MRT_SUCCESS; ++launched) {
-        Engine& e = *engines[launched];
-        launchError = e.checkAlive();
-        // at most kBatchWindow jobs run at once: job i waits on the GPU for
-        // job i - kBatchWindow, so a job fills its predecessor's last, short
-        // bounces without all jobs contending for SMs and L2
-        if (launchError == MRT_SUCCESS && launched >= kBatchWindow) {
-            Engine& prev = *engines[launched - kBatchWindow];
-            if (prev.m_inFlight) {
-                const cudaError_t we = cudaStreamWaitEvent(e.m_stream, prev.m_ev1, 0);
-                if (we != cudaSuccess) launchError = e.guard(fromCuda(we, "mrtxRenderBatch ordering"));
+            if (!oneLaunch) {
+                e.m_pending = n[i];
+                MRT_TRY(e.guard(e.ensureWave(n[i])));
             }
         }
-        if (launchError == MRT_SUCCESS) launchError = e.launchPending();
     }
-    mrtResult result = launchError;
-    for (uint32_t i = 0; i < launched; ++i) {  // every launched engine is completed, even after an error
+    mrtResult result = MRT_SUCCESS;
+    if (oneLaunch) {
+        result = renderBatchOneLaunch(engines, n.data(), count);
+    } else {
+        mrtResult launchError = MRT_SUCCESS;
+        uint32_t launched = 0;
+        for (; launched < count && launchError == MRT_SUCCESS; ++launched) {
+            Engine& e = *engines[launched];
+            launchError = e.checkAlive();
+            // at most kBatchWindow jobs run at once: job i waits on the GPU for
+            // job i - kBatchWindow, so a job fills its predecessor's last, short
+            // bounces without all jobs contending for SMs and L2
+            if (launchError == MRT_SUCCESS && launched >= kBatchWindow) {
+                Engine& prev = *engines[launched - kBatchWindow];
+                if (prev.m_inFlight) {
+                    const cudaError_t we = cudaStreamWaitEvent(e.m_stream, prev.m_ev1, 0);
+                    if (we != cudaSuccess) launchError = e.guard(fromCuda(we, "mrtxRenderBatch ordering"));
+                }
+            }
+            if (launchError == MRT_SUCCESS) launchError = e.launchPending();
+        }
+        result = launchError;
+        for (uint32_t i = 0; i < launched; ++i) {  // every launched engine is completed, even after an error
+            Engine& e = *engines[i];
+            mrtResult r = e.checkAlive();
+            if (r == MRT_SUCCESS) r = e.completePending();
+            if (result == MRT_SUCCESS) result = r;
+        }
+    }
+    for (uint32_t i = 0; i < count; ++i) {
         Engine& e = *engines[i];
-        mrtResult r = e.checkAlive();
-        if (r == MRT_SUCCESS) r = e.completePending();
-        if (result == MRT_SUCCESS) result = r;
         if (infos && infos[i].structSize >= sizeof(mrtFrameInfo)) {
             infos[i].spp = e.m_frameIndex + e.m_pending;
             infos[i].converged = e.m_frameIndex + e.m_pending >= e.m_settings.sppLimit ? 1 : 0;
@@ -1217,6 +1249,174 @@ mrtResult Engine::renderBatch(Engine* const* engines, const uint32_t* spp, uint3
         }
     }
     return result;
+}
+
+// One-launch batch: every engine's samples are split into the waves the
+// engine would render on its own (so each accumulation is bit for bit the
+// one it would get alone), and round r gathers every engine's r-th wave
+// into one batch wave, split further where it would exceed 2^28 paths. Each
+// batch runs as one set of per-bounce kernel launches over the
+// concatenated slots (mrtcu_wave_batch) on the first engine's stream, in
+// its wave buffer, with its ray counters and error word; the other engines
+// contribute their scenes and accumulation buffers. Statistics of every
+// engine are those of the whole batch (device time, stage times, rays).
+mrtResult Engine::renderBatchOneLaunch(Engine* const* engines, const uint32_t* n, uint32_t count) {
+    Engine& lead = *engines[0];
+    struct WaveJob {
+        uint32_t engine, sampleBase, samples;
+        uint64_t slots;
+    };
+    std::vector<std::vector<WaveJob>> waves(count);
+    size_t rounds = 0;
+    uint64_t largest = 0;
+    int active = -1;
+    for (uint32_t i = 0; i < count; ++i) {
+        if (n[i] == 0) continue;
+        Engine& e = *engines[i];
+        if (active < 0) active = int(i);
+        const uint64_t pixels = std::max<uint64_t>(1, uint64_t(e.m_settings.width) * e.m_settings.height);
+        const uint32_t k = uint32_t(std::max<uint64_t>(
+            1, std::min<uint64_t>(n[i], std::min<uint64_t>(64, e.m_maxWaveSlots / pixels))));
+        for (uint32_t done = 0; done < n[i]; done += k) {
+            const uint32_t s = std::min(k, n[i] - done);
+            waves[i].push_back(WaveJob{i, e.m_frameIndex + done, s, pixels * s});
+            largest = std::max<uint64_t>(largest, pixels * s);
+        }
+        rounds = std::max(rounds, waves[i].size());
+    }
+    if (active < 0) return MRT_SUCCESS;
+    // at most 2^28 paths a batch and half the device memory free now (the
+    // lead's wave buffer counted as free), but always room for the largest
+    // single wave
+    size_t freeBytes = 0, totalBytes = 0;
+    MRT_CUDA(cudaMemGetInfo(&freeBytes, &totalBytes));
+    const uint64_t budget = (uint64_t(freeBytes) + lead.m_wave.bytes) / 2 / kWaveBytesPerSlot;
+    const uint64_t cap = std::max<uint64_t>(largest, std::min<uint64_t>(uint64_t(1) << 28, budget));
+    if (largest > 0xffffffffull) return fail(MRT_ERROR_INVALID_ARGUMENT, "frame too large for one wave");
+    std::vector<std::vector<WaveJob>> batches;
+    uint64_t used = 0;
+    for (size_t r = 0; r < rounds; ++r) {
+        std::vector<WaveJob> cur;
+        uint64_t slots = 0;
+        for (uint32_t i = 0; i < count; ++i) {
+            if (r >= waves[i].size()) continue;
+            const WaveJob& w = waves[i][r];
+            if (!cur.empty() && slots + w.slots > cap) {
+                batches.push_back(cur);
+                used = std::max(used, slots);
+                cur.clear();
+                slots = 0;
+            }
+            cur.push_back(w);
+            slots += w.slots;
+        }
+        if (!cur.empty()) {
+            batches.push_back(cur);
+            used = std::max(used, slots);
+        }
+    }
+    MrtWaveState W{};
+    MRT_TRY(lead.guard(lead.carveWave(used, W)));
+    std::vector<MrtBatchJob> table;
+    std::vector<size_t> first;
+    std::vector<uint32_t> bounces;
+    for (const auto& batch : batches) {
+        first.push_back(table.size());
+        uint32_t slotBase = 0, pixelBase = 0, maxB = 0;
+        for (const WaveJob& w : batch) {
+            const Engine& e = *engines[w.engine];
+            MrtBatchJob j{};
+            j.params = e.m_pendingParams;
+            j.pixels = e.m_settings.width * e.m_settings.height;
+            j.samples = w.samples;
+            j.slots = uint32_t(w.slots);
+            j.sampleBase = w.sampleBase;
+            j.slotBase = slotBase;
+            j.pixelBase = pixelBase;
+            slotBase += j.slots;
+            pixelBase += j.pixels;
+            maxB = std::max(maxB, j.params.maxBounces);
+            table.push_back(j);
+        }
+        bounces.push_back(maxB);
+    }
+    MRT_TRY(lead.guard(lead.m_batchJobs.ensure(table.size() * sizeof(MrtBatchJob))));
+    MRT_CUDA(cudaMemcpyAsync(lead.m_batchJobs.ptr, table.data(), table.size() * sizeof(MrtBatchJob),
+                             cudaMemcpyHostToDevice, lead.m_stream));
+    MRT_CUDA(cudaMemsetAsync(lead.m_rayCounters.ptr, 0, 128, lead.m_stream));
+    MrtFrameParams bp = engines[active]->m_pendingParams;  // the batch's counters and error word
+    bp.rayCounters = lead.m_rayCounters.as<unsigned long long>();
+    bp.errorFlags = lead.m_flags.as<uint32_t>();
+    size_t events = 0;
+    for (uint32_t b : bounces) events += size_t(6) * (b + 1);
+    while (lead.m_stageEvents.size() < events) {
+        cudaEvent_t ev;
+        MRT_CUDA(cudaEventCreate(&ev));
+        lead.m_stageEvents.push_back(ev);
+    }
+    uint32_t launches = 0;
+    MRT_CUDA(cudaEventRecord(lead.m_ev0, lead.m_stream));
+    size_t ev = 0;
+    for (size_t b = 0; b < batches.size(); ++b) {
+        const cudaError_t le = mrtcu_wave_batch(&bp, &W, lead.m_batchJobs.as<MrtBatchJob>() + first[b],
+                                                table.data() + first[b], uint32_t(batches[b].size()), bounces[b],
+                                                &launches, lead.m_stageEvents.data() + ev, lead.m_stream);
+        if (le != cudaSuccess) return lead.guard(fromCuda(le, "one-launch batch"));
+        ev += size_t(6) * (bounces[b] + 1);
+    }
+    MRT_CUDA(cudaEventRecord(lead.m_ev1, lead.m_stream));
+    const cudaError_t se = cudaStreamSynchronize(lead.m_stream);
+    if (se != cudaSuccess) return lead.guard(fromCuda(se, "one-launch batch kernel"));
+    if (const mrtResult fr = lead.checkErrorFlags(); fr != MRT_SUCCESS) {
+        for (uint32_t i = 0; i < count; ++i) engines[i]->resetAccumulation();
+        return fr;
+    }
+    float ms = 0.0f, ext = 0.0f, sha = 0.0f, shw = 0.0f;
+    MRT_CUDA(cudaEventElapsedTime(&ms, lead.m_ev0, lead.m_ev1));
+    ev = 0;
+    for (uint32_t nb : bounces) {
+        for (uint32_t b = 0; b <= nb; ++b) {
+            const cudaEvent_t* e = lead.m_stageEvents.data() + ev + 6 * b;
+            float x = 0.0f, y = 0.0f, z = 0.0f;
+            MRT_CUDA(cudaEventElapsedTime(&x, e[0], e[1]));
+            MRT_CUDA(cudaEventElapsedTime(&y, e[1], e[2]));
+            MRT_CUDA(cudaEventElapsedTime(&z, e[2], e[3]));
+            ext += x;
+            sha += y;
+            shw += z;
+        }
+        ev += size_t(6) * (nb + 1);
+    }
+    unsigned long long ctr[16];
+    MRT_CUDA(cudaMemcpy(ctr, lead.m_rayCounters.ptr, sizeof(ctr), cudaMemcpyDeviceToHost));
+    for (uint32_t i = 0; i < count; ++i) {
+        if (n[i] == 0) continue;
+        Engine& e = *engines[i];
+        e.m_frameIndex += n[i];
+        mrtxStats& st = e.m_stats;
+        st.lastRenderMs = ms;
+        st.lastRenderSpp = n[i];
+        st.kernelLaunches = launches;
+        st.extendLaunches = 0;
+        for (uint32_t nb : bounces) st.extendLaunches += nb + 1;
+        st.extendMs = ext;
+        st.shadeMs = sha;
+        st.shadowMs = shw;
+        st.otherMs = ms - ext - sha - shw;
+        st.raysClosest = ctr[0];
+        st.raysShadow = ctr[1];
+        st.nodeFetches = ctr[2];
+        st.triTests = ctr[3];
+        st.surfaceHits = ctr[4];
+        st.shadowNodeFetches = ctr[5];
+        st.shadowTriTests = ctr[6];
+        st.nodeBytes = sizeof(MrtWideNode);
+        st.triBytes = 48;
+        st.cacheQueryMs = st.cacheTrainMs = 0.0f;
+        st.cacheQueries = st.cacheRecords = 0;
+        st.cacheSteps = 0;
+    }
+    return MRT_SUCCESS;
 }
 
 // Device -> pinned staging -> caller memory, in chunks so the host copy of

@@ -90,6 +90,9 @@ private:
     mrtResult guard(mrtResult r);  // records a device loss
     mrtResult allocateFrame();
     mrtResult ensureWave(uint32_t samples);
+    mrtResult carveWave(uint64_t slots, MrtWaveState& w);
+    // mrtxRenderBatch with every engine's waves in one set of launches
+    static mrtResult renderBatchOneLaunch(Engine* const* engines, const uint32_t* n, uint32_t count);
     uint32_t waveCapacitySamples() const;
     mrtResult launchPending();    // issues the queued samples' waves, no wait
     mrtResult completePending();  // waits for them, statistics, error flags
@@ -133,6 +136,7 @@ private:
     // device frame state
     DeviceBuffer m_accum, m_out32, m_out8, m_flags, m_rayCounters, m_queryRays, m_queryOut;
     DeviceBuffer m_wave;  // wavefront path state (one allocation, carved into MrtWaveState arrays)
+    DeviceBuffer m_batchJobs;  // job tables of a one-launch batch this engine leads
     DeviceBuffer m_bvhPos, m_bvhIdx, m_bvhScratch, m_bvhNodes, m_bvhPrims;  // device BVH builder
     DeviceBuffer m_packError;  // error word of the commit-time assembly kernels
 

@@ -15,7 +15,7 @@ def test_coordinate_descent_finds_the_fake_optimum(monkeypatch):
 
     def fake_measure(defines, workdir, steps, warmup):
         key = tuple(sorted(defines.items()))
-        assert key not in seen, "measured twice"
+        assert key not in seen or len(seen) == 1, "measured twice"  # the discarded first run repeats the start
         seen.append(key)
         return 1000.0 - sum(abs(defines[k] - v) / max(v, 1) for k, v in optimum.items())
 
