@@ -522,7 +522,8 @@ def batch_arm(args):
         torch.cuda.synchronize()
         step_ms.append(a.elapsed_time(b))
         completion.append([i["frameMs"] for i in infos])
-        launches += sum(e.stats()["kernelLaunches"] for e in engines)
+        # a one-launch batch reports its launches on every engine it rendered
+        launches += sum(st["kernelLaunches"] / max(1, st["batchJobs"]) for st in (e.stats() for e in engines))
     clocks = sampler.stop()
     # the same jobs one after another, for comparison
     seq_ms = []
@@ -550,7 +551,7 @@ def batch_arm(args):
                    "l2": "a 256 MiB buffer is written between timed steps"},
         "per_job_completion_ms": [float(np.mean([c[j] for c in completion])) for j in range(len(jobs))],
         "sequential_ms_per_step": float(np.mean(seq_ms)),
-        "gpu_launches": launches,
+        "gpu_launches": int(round(launches)),
         "clocks": clocks,
     }
     print(json.dumps(out), flush=True)
@@ -793,7 +794,8 @@ def large_arm(args):
         b.record()
         torch.cuda.synchronize()
         step_ms.append(a.elapsed_time(b))
-        launches += sum(e.stats()["kernelLaunches"] for e in engines)
+        # a one-launch batch reports its launches on every engine it rendered
+        launches += sum(st["kernelLaunches"] / max(1, st["batchJobs"]) for st in (e.stats() for e in engines))
     clocks = sampler.stop()
     st = engines[0].stats()
     scene_mb = st["deviceBytes"] / 1e6
@@ -834,7 +836,7 @@ def large_arm(args):
                                "camera per step, one mrtxRenderBatch per step (one engine and scene copy per "
                                "camera)", "scene_mb_per_engine": scene_mb,
                    "l2": "a 256 MiB buffer is written between timed steps"},
-        "step_ms": [round(x, 2) for x in step_ms], "gpu_launches": launches, "clocks": clocks,
+        "step_ms": [round(x, 2) for x in step_ms], "gpu_launches": int(round(launches)), "clocks": clocks,
         "relmse_over_time_camera0": curves,
     }
     print(json.dumps(out), flush=True)

@@ -100,7 +100,13 @@ typedef struct mrtxStats {
     float cacheQueryMs, cacheTrainMs;
     uint64_t cacheQueries, cacheRecords;
     uint32_t cacheSteps;
+    /* engines whose samples the last render call's launches rendered
+     * together: 1, or the job count of a one-launch mrtxRenderBatch (whose
+     * engines all report the batch's launches, times and counters) */
+    uint32_t batchJobs;
 } mrtxStats;
+/* out->structSize may be that of an earlier, shorter mrtxStats (fields are
+ * only appended; at least up to cacheSteps): the fields it covers are written. */
 MRT_API mrtResult mrtxGetStats(mrtEngine*, mrtxStats* out);
 
 /* Measured L2 read bandwidth (GB/s) of the engine's GPU: every SM re-reads a

@@ -132,7 +132,7 @@ class Stats(_Sized):
                 ("triBytes", C.c_uint32), ("extendMs", C.c_float), ("shadeMs", C.c_float), ("shadowMs", C.c_float),
                 ("otherMs", C.c_float), ("extendLaunches", C.c_uint32), ("cacheQueryMs", C.c_float),
                 ("cacheTrainMs", C.c_float), ("cacheQueries", C.c_uint64), ("cacheRecords", C.c_uint64),
-                ("cacheSteps", C.c_uint32)]
+                ("cacheSteps", C.c_uint32), ("batchJobs", C.c_uint32)]
 
 
 LOG_FN = C.CFUNCTYPE(None, C.c_int, C.c_char_p, C.c_void_p)

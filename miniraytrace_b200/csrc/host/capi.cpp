@@ -7,7 +7,9 @@
 // scene calls ignore bad handles, add-calls return MRT_INVALID_ID, and no C++
 // exception crosses the boundary (std::bad_alloc -> MRT_ERROR_OUT_OF_MEMORY,
 // anything else -> MRT_ERROR_UNKNOWN).
+#include <algorithm>
 #include <cmath>
+#include <cstddef>
 #include <cstring>
 #include <new>
 #include <string>
@@ -260,10 +262,20 @@ MRT_API mrtResult mrtxMeasureL2Bandwidth(mrtEngine* e, float* outGBs) {
 MRT_API mrtResult mrtxGetStats(mrtEngine* e, mrtxStats* out) {
     mrt::Engine* eng = unwrap(e);
     if (!eng) return MRT_ERROR_INVALID_HANDLE;
-    if (!validStruct(out)) return mrt::fail(MRT_ERROR_INVALID_ARGUMENT, "mrtxGetStats: bad mrtxStats");
+    // an older, shorter mrtxStats (fields are only ever appended) gets the
+    // fields it has
+    if (!out || out->structSize < offsetof(mrtxStats, batchJobs))
+        return mrt::fail(MRT_ERROR_INVALID_ARGUMENT, "mrtxGetStats: bad mrtxStats");
     return guarded([&] {
-        const mrtResult r = eng->flushPending();
-        return r != MRT_SUCCESS ? r : eng->getStats(out);
+        mrtResult r = eng->flushPending();
+        if (r != MRT_SUCCESS) return r;
+        mrtxStats full{};
+        r = eng->getStats(&full);
+        if (r != MRT_SUCCESS) return r;
+        const size_t size = std::min(out->structSize, sizeof(mrtxStats));
+        std::memcpy(reinterpret_cast<char*>(out) + sizeof(size_t), reinterpret_cast<const char*>(&full) + sizeof(size_t),
+                    size - sizeof(size_t));
+        return MRT_SUCCESS;
     });
 }
 

@@ -1145,6 +1145,7 @@ mrtResult Engine::completePending() {
     m_stats.cacheQueries = m_inFlightCache ? m_cacheQueries : 0;
     m_stats.cacheRecords = m_inFlightCache ? m_cacheRecords : 0;
     m_stats.cacheSteps = m_inFlightCache ? m_cacheSteps : 0;
+    m_stats.batchJobs = 1;
     if (const mrtResult fr = checkErrorFlags(); fr != MRT_SUCCESS) {
         resetAccumulation();
         return guard(fr);
@@ -1389,6 +1390,8 @@ mrtResult Engine::renderBatchOneLaunch(Engine* const* engines, const uint32_t* n
     }
     unsigned long long ctr[16];
     MRT_CUDA(cudaMemcpy(ctr, lead.m_rayCounters.ptr, sizeof(ctr), cudaMemcpyDeviceToHost));
+    uint32_t jobs = 0;
+    for (uint32_t i = 0; i < count; ++i) jobs += n[i] > 0 ? 1u : 0u;
     for (uint32_t i = 0; i < count; ++i) {
         if (n[i] == 0) continue;
         Engine& e = *engines[i];
@@ -1415,6 +1418,7 @@ mrtResult Engine::renderBatchOneLaunch(Engine* const* engines, const uint32_t* n
         st.cacheQueryMs = st.cacheTrainMs = 0.0f;
         st.cacheQueries = st.cacheRecords = 0;
         st.cacheSteps = 0;
+        st.batchJobs = jobs;
     }
     return MRT_SUCCESS;
 }

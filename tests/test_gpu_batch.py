@@ -26,6 +26,7 @@ def test_batch_of_uneven_jobs_equals_each_job_alone(gpu):
     stats = [e.stats() for e in engines]
     assert len({st["kernelLaunches"] for st in stats}) == 1
     assert len({st["lastRenderMs"] for st in stats}) == 1
+    assert all(st["batchJobs"] == len(jobs) for st in stats)
     batch_launches = stats[0]["kernelLaunches"]
     batched = []
     for e in engines:
@@ -38,7 +39,9 @@ def test_batch_of_uneven_jobs_equals_each_job_alone(gpu):
         s.apply(e)
         e.render_frames(s.spp)
         ref, m = e.read_accumulation()
-        alone_launches += e.stats()["kernelLaunches"]
+        st = e.stats()
+        assert st["batchJobs"] == 1
+        alone_launches += st["kernelLaunches"]
         e.close()
         assert n == m == s.spp, s.name
         assert np.array_equal(acc, ref), s.name
