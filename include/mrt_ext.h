@@ -91,7 +91,10 @@ typedef struct mrtxStats {
     uint64_t shadowTriTests;    /* ray/triangle tests of shadow rays */
     uint32_t nodeBytes;    /* bytes of one BVH node record */
     uint32_t triBytes;     /* bytes read by one ray/triangle test */
-    /* device time of the last render call per wavefront stage (CUDA events) */
+    /* device time of the last render call per wavefront stage (CUDA events);
+     * the shadow rays of a bounce are traced beside the next bounce's extend
+     * kernel, so shadowMs is the time they add past it (and the last
+     * bounce's shadow kernel); the four sum to lastRenderMs */
     float extendMs, shadeMs, shadowMs, otherMs;
     uint32_t extendLaunches; /* closest-hit (extend) kernel launches of the last render call */
     /* radiance-cache mode, last render call: device time of the cache's

@@ -191,7 +191,7 @@ typedef struct MrtWaveState {
     float4* shO;        // shadow ray origin.xyz, w = tMax
     float4* shD;        // shadow ray direction.xyz, w = bits(slot)
     float4* shC;        // contribution added when the shadow ray is unoccluded
-    uint32_t* counts;   // [0], [1] = queue lengths, [2] = shadow queue length
+    uint32_t* counts;   // [0..1] path queue lengths, [2..3] shadow queue lengths, [4..7] fetch heads
     uint32_t capacity;  // slots
     uint32_t pad;
 } MrtWaveState;

@@ -41,20 +41,29 @@ extern "C" {
 // samples) of every pixel (width * height * samples <= s->capacity slots);
 // sampleBase == 0 overwrites the accumulation, otherwise it adds. Adds the
 // number of kernels launched to *launches. stageEvents (may be NULL) holds 6
-// events per bounce; events 6b..6b+3 are recorded before extend, between
-// extend and shade, between shade and shadow, and after shadow of bounce b.
+// timing events per bounce: event 6b+0 before extend of bounce b, 6b+1 after
+// it, 6b+4 before shade (once bounce b-1's shadow rays are done), 6b+2 after
+// shade, 6b+3 after shadow. With a `side` stream and syncEvents (2 per
+// bounce, created with cudaEventDisableTiming) the shadow kernel of bounce b
+// runs on `side`, in parallel with the extend kernel of bounce b+1; all work
+// has joined `stream` again on return.
 cudaError_t mrtcu_wave(const MrtFrameParams* p, const MrtWaveState* s, uint32_t sampleBase, uint32_t samples,
-                       uint32_t* launches, const cudaEvent_t* stageEvents, const MrtCacheArgs* cache,
-                       cudaStream_t stream);
+                       uint32_t* launches, const cudaEvent_t* stageEvents, const cudaEvent_t* syncEvents,
+                       const MrtCacheArgs* cache, cudaStream_t stream, cudaStream_t side);
+// Whether mrtcu_wave runs the shadow kernels beside the next bounce's extend
+// when given a side stream (the build's MRT_SHADOW_OVERLAP, default 1).
+int mrtcu_shadow_overlap(void);
 // One-launch batch: the waves of `count` jobs (every job's scene and wave in
 // its MrtBatchJob; devJobs is the device copy of hostJobs, slot and pixel
 // bases ascending) rendered by one set of per-bounce kernel launches over
 // their concatenated slots (sum of slots <= s->capacity). `batch` carries
 // the ray counters and the error word of the whole batch; maxBounces is the
-// largest of the jobs' (each path stops at its own job's bound).
+// largest of the jobs' (each path stops at its own job's bound). Events and
+// the side stream as in mrtcu_wave.
 cudaError_t mrtcu_wave_batch(const MrtFrameParams* batch, const MrtWaveState* s, const MrtBatchJob* devJobs,
                              const MrtBatchJob* hostJobs, uint32_t count, uint32_t maxBounces, uint32_t* launches,
-                             const cudaEvent_t* stageEvents, cudaStream_t stream);
+                             const cudaEvent_t* stageEvents, const cudaEvent_t* syncEvents, cudaStream_t stream,
+                             cudaStream_t side);
 // With a cache, mrtcu_wave leaves the wave unfinalised: the cache's
 // predictions are added to the paths, then this accumulates the wave.
 cudaError_t mrtcu_wave_finalize(const MrtFrameParams* p, const MrtWaveState* s, uint32_t sampleBase,

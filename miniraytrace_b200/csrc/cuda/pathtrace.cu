@@ -125,6 +125,14 @@ MRT_DEV uint32_t coalescedAppend(uint32_t* count) {
     return g.shfl(base, 0) + g.thread_rank();
 }
 
+// The wave's counts[] block: [0..1] path queue lengths and [2..3] shadow
+// queue lengths, [4..5] and [6..7] the fetch heads of the extend and shadow
+// kernels, all indexed by bounce parity `cur`. The shadow rays of bounce b
+// are traced while the extend kernel of bounce b+1 runs (on another stream),
+// so the two never share a counter: extend(b) resets only counters that no
+// kernel of bounces b-1 and b still reads.
+enum { kShadowCount = 2, kExtendHead = 4, kShadowHead = 6 };
+
 // Slot layout of a wave: slot = pixel * samples + sample (sample-minor).
 struct WaveArgs {
     uint32_t pixels;      // W * H
@@ -161,8 +169,7 @@ __global__ void __launch_bounds__(256) waveInitKernel(MrtFrameParams Pk, MrtWave
     if (slot == 0) {
         S.counts[0] = total;
         S.counts[1] = 0;
-        S.counts[2] = 0;
-        S.counts[4] = 0;  // extend fetch counter (kExtendHead) of bounce 0
+        S.counts[kExtendHead] = 0;  // extend fetch counter of bounce 0
     }
     if (slot >= total) return;
     const MrtBatchJob* J = kMulti ? B.jobs + batchJobOf(B, slot, false) : nullptr;
@@ -192,9 +199,6 @@ __global__ void __launch_bounds__(256) waveInitKernel(MrtFrameParams Pk, MrtWave
     S.queue[0][slot] = slot;
 }
 
-// Queue fetch counters of the persistent traversal kernels, in the wave's
-// counts[] block (counts[0..1]: path queues, counts[2]: shadow queue).
-enum { kExtendHead = 4, kShadowHead = 5 };
 
 // Lanes of a persistent traversal warp whose ray has finished take new rays
 // from the queue (one warp-aggregated atomic) once at least this many lanes
@@ -241,9 +245,10 @@ __global__ void MRT_TRAV_BOUNDS waveExtendKernel(MrtFrameParams Pk, MrtWaveState
     const uint32_t* __restrict__ q = S.queue[cur];
     const uint32_t n = S.counts[cur];
     if (blockIdx.x == 0 && threadIdx.x == 0) {
-        S.counts[cur ^ 1u] = 0;  // next queue and shadow queue fill during shade
-        S.counts[2] = 0;
-        S.counts[kShadowHead] = 0;
+        S.counts[cur ^ 1u] = 0;  // next queue and this bounce's shadow queue fill during shade
+        S.counts[kShadowCount + cur] = 0;
+        S.counts[kShadowHead + cur] = 0;
+        S.counts[kExtendHead + (cur ^ 1u)] = 0;  // for the next bounce's extend
     }
     uint32_t c[kCtrCount] = {};
     TraversalCounters tc;
@@ -253,7 +258,7 @@ __global__ void MRT_TRAV_BOUNDS waveExtendKernel(MrtFrameParams Pk, MrtWaveState
     WideStack stack;
     for (;;) {
         if (!drained) {
-            const uint32_t i = refillLane(S.counts + kExtendHead, n, active, drained);
+            const uint32_t i = refillLane(S.counts + kExtendHead + cur, n, active, drained);
             if (i != 0xffffffffu) {
                 slot = q[i];
                 if (kMulti) job = batchJobOf(B, slot, false);
@@ -480,7 +485,7 @@ __global__ void __launch_bounds__(kShadeBlock) waveShadeKernel(MrtFrameParams Pk
             }
         }
         uint32_t qi, si;
-        blockAppend2(&S.counts[cur ^ 1u], cont, qi, &S.counts[2], shadow, si, sAppend);
+        blockAppend2(&S.counts[cur ^ 1u], cont, qi, &S.counts[kShadowCount + cur], shadow, si, sAppend);
         if (cont) qn[qi] = slot;
         if (shadow) {
             S.shO[si] = make_float4(shOrig.x, shOrig.y, shOrig.z, shTMax);
@@ -496,9 +501,8 @@ __global__ void __launch_bounds__(kShadeBlock) waveShadeKernel(MrtFrameParams Pk
 // one shadow ray per bounce, so the update needs no atomics. Persistent
 // warps with lane refill, as the extend kernel.
 template <bool kMulti>
-__global__ void MRT_TRAV_BOUNDS waveShadowKernel(MrtFrameParams Pk, MrtWaveState S, MrtBatchJobs B) {
-    const uint32_t n = S.counts[2];
-    if (blockIdx.x == 0 && threadIdx.x == 0) S.counts[kExtendHead] = 0;  // for the next bounce
+__global__ void MRT_TRAV_BOUNDS waveShadowKernel(MrtFrameParams Pk, MrtWaveState S, uint32_t cur, MrtBatchJobs B) {
+    const uint32_t n = S.counts[kShadowCount + cur];
     uint32_t c[kCtrCount] = {};
     TraversalCounters tc;
     bool ok = true, active = false, drained = false;
@@ -507,7 +511,7 @@ __global__ void MRT_TRAV_BOUNDS waveShadowKernel(MrtFrameParams Pk, MrtWaveState
     WideStack stack;
     for (;;) {
         if (!drained) {
-            const uint32_t i = refillLane(S.counts + kShadowHead, n, active, drained);
+            const uint32_t i = refillLane(S.counts + kShadowHead + cur, n, active, drained);
             if (i != 0xffffffffu) {
                 idx = i;
                 const float4 o = S.shO[i], d = S.shD[i];
@@ -713,6 +717,52 @@ const WaveGrids& waveGrids() {
 }
 }  // namespace
 
+// Stream order of a wave's bounces. Without a side stream (or without its
+// sync events) every kernel runs on `main` in order. With one, the shadow
+// kernel of bounce b runs on `side` after shade(b), in parallel with
+// extend(b+1) on `main`: the two persistent kernels fill each other's
+// draining tails, and shade(b+1) waits for both (the shadow kernel adds to
+// the paths' radiance, which shade(b+1) rewrites). The cross-stream waits
+// use `sync` (2 events per bounce, created without timing, the cheap kind
+// to wait on); the timing events `ev` (may be NULL; 6 per bounce) are only
+// recorded: [0] before extend, [1] after extend, [4] once the previous
+// bounce's shadow rays are done (before shade), [2] after shade, [3] after
+// shadow (on the stream that ran it), [5] unused.
+#ifndef MRT_SHADOW_OVERLAP
+#define MRT_SHADOW_OVERLAP 1
+#endif
+struct BounceStreams {
+    cudaStream_t main, side;
+    const cudaEvent_t* ev;
+    const cudaEvent_t* sync;
+    bool overlap() const { return MRT_SHADOW_OVERLAP && side != nullptr && sync != nullptr; }
+    void record(uint32_t b, int i, cudaStream_t s) const {
+        if (ev) cudaEventRecord(ev[6 * size_t(b) + i], s);
+    }
+    void beforeExtend(uint32_t b) const { record(b, 0, main); }
+    void beforeShade(uint32_t b) const {
+        record(b, 1, main);
+        if (overlap() && b > 0) cudaStreamWaitEvent(main, sync[2 * size_t(b - 1) + 1], 0);
+        record(b, 4, main);
+    }
+    cudaStream_t beforeShadow(uint32_t b) const {
+        record(b, 2, main);
+        if (!overlap()) return main;
+        cudaEventRecord(sync[2 * size_t(b)], main);
+        cudaStreamWaitEvent(side, sync[2 * size_t(b)], 0);
+        return side;
+    }
+    void afterShadow(uint32_t b) const {
+        record(b, 3, overlap() ? side : main);
+        if (overlap()) cudaEventRecord(sync[2 * size_t(b) + 1], side);
+    }
+    void join(uint32_t last) const {
+        if (overlap()) cudaStreamWaitEvent(main, sync[2 * size_t(last) + 1], 0);
+    }
+};
+
+extern "C" int mrtcu_shadow_overlap(void) { return MRT_SHADOW_OVERLAP; }
+
 extern "C" cudaError_t mrtcu_wave_finalize(const MrtFrameParams* p, const MrtWaveState* s, uint32_t sampleBase,
                                            uint32_t samples, cudaStream_t stream) {
     const uint32_t pixels = p->width * p->height;
@@ -724,7 +774,8 @@ extern "C" cudaError_t mrtcu_wave_finalize(const MrtFrameParams* p, const MrtWav
 
 extern "C" cudaError_t mrtcu_wave(const MrtFrameParams* p, const MrtWaveState* s, uint32_t sampleBase,
                                   uint32_t samples, uint32_t* launches, const cudaEvent_t* stageEvents,
-                                  const MrtCacheArgs* cache, cudaStream_t stream) {
+                                  const cudaEvent_t* syncEvents, const MrtCacheArgs* cache, cudaStream_t stream,
+                                  cudaStream_t side) {
     const uint32_t pixels = p->width * p->height;
     if (pixels == 0 || samples == 0) return cudaSuccess;
     if (uint64_t(pixels) * samples > s->capacity) return cudaErrorInvalidValue;
@@ -734,23 +785,23 @@ extern "C" cudaError_t mrtcu_wave(const MrtFrameParams* p, const MrtWaveState* s
     uint32_t n = 0;
     waveInitKernel<false><<<(A.slots + 255) / 256, 256, 0, stream>>>(*p, *s, A, MrtBatchJobs{});
     ++n;
+    const BounceStreams bs{stream, side, stageEvents, syncEvents};
     for (uint32_t b = 0; b <= p->maxBounces; ++b) {
         const uint32_t cur = b & 1u;
-        const cudaEvent_t* ev = stageEvents ? stageEvents + 6 * b : nullptr;
-        if (ev) cudaEventRecord(ev[0], stream);
+        bs.beforeExtend(b);
         waveExtendKernel<false><<<gExtend, MRT_TRAV_THREADS, 0, stream>>>(*p, *s, cur, MrtBatchJobs{});
-        if (ev) cudaEventRecord(ev[1], stream);
+        bs.beforeShade(b);
         if (cache)
             waveShadeKernel<true, false><<<gShadeCache, kShadeBlock, 0, stream>>>(*p, *s, A, cur, *cache,
                                                                                    MrtBatchJobs{});
         else
             waveShadeKernel<false, false><<<gShade, kShadeBlock, 0, stream>>>(*p, *s, A, cur, MrtCacheArgs{},
                                                                               MrtBatchJobs{});
-        if (ev) cudaEventRecord(ev[2], stream);
-        waveShadowKernel<false><<<gShadow, MRT_TRAV_THREADS, 0, stream>>>(*p, *s, MrtBatchJobs{});
-        if (ev) cudaEventRecord(ev[3], stream);
+        waveShadowKernel<false><<<gShadow, MRT_TRAV_THREADS, 0, bs.beforeShadow(b)>>>(*p, *s, cur, MrtBatchJobs{});
+        bs.afterShadow(b);
         n += 3;
     }
+    bs.join(p->maxBounces);
     if (!cache) {  // the cache mode finalises after applying the cache (mrtcu_wave_finalize)
         waveFinalizeKernel<false><<<(pixels + 255) / 256, 256, 0, stream>>>(*p, *s, A, MrtBatchJobs{});
         ++n;
@@ -766,7 +817,8 @@ extern "C" cudaError_t mrtcu_wave(const MrtFrameParams* p, const MrtWaveState* s
 // its scene). stageEvents as in mrtcu_wave.
 extern "C" cudaError_t mrtcu_wave_batch(const MrtFrameParams* batch, const MrtWaveState* s, const MrtBatchJob* devJobs,
                                         const MrtBatchJob* hostJobs, uint32_t count, uint32_t maxBounces,
-                                        uint32_t* launches, const cudaEvent_t* stageEvents, cudaStream_t stream) {
+                                        uint32_t* launches, const cudaEvent_t* stageEvents,
+                                        const cudaEvent_t* syncEvents, cudaStream_t stream, cudaStream_t side) {
     if (count == 0) return cudaSuccess;
     const MrtBatchJob& last = hostJobs[count - 1];
     const uint32_t totalSlots = last.slotBase + last.slots, totalPixels = last.pixelBase + last.pixels;
@@ -778,18 +830,18 @@ extern "C" cudaError_t mrtcu_wave_batch(const MrtFrameParams* batch, const MrtWa
     uint32_t n = 0;
     waveInitKernel<true><<<(totalSlots + 255) / 256, 256, 0, stream>>>(*batch, *s, none, B);
     ++n;
+    const BounceStreams bs{stream, side, stageEvents, syncEvents};
     for (uint32_t b = 0; b <= maxBounces; ++b) {
         const uint32_t cur = b & 1u;
-        const cudaEvent_t* ev = stageEvents ? stageEvents + 6 * b : nullptr;
-        if (ev) cudaEventRecord(ev[0], stream);
+        bs.beforeExtend(b);
         waveExtendKernel<true><<<g.extendMulti, MRT_TRAV_THREADS, 0, stream>>>(*batch, *s, cur, B);
-        if (ev) cudaEventRecord(ev[1], stream);
+        bs.beforeShade(b);
         waveShadeKernel<false, true><<<g.shadeMulti, kShadeBlock, 0, stream>>>(*batch, *s, none, cur, MrtCacheArgs{}, B);
-        if (ev) cudaEventRecord(ev[2], stream);
-        waveShadowKernel<true><<<g.shadowMulti, MRT_TRAV_THREADS, 0, stream>>>(*batch, *s, B);
-        if (ev) cudaEventRecord(ev[3], stream);
+        waveShadowKernel<true><<<g.shadowMulti, MRT_TRAV_THREADS, 0, bs.beforeShadow(b)>>>(*batch, *s, cur, B);
+        bs.afterShadow(b);
         n += 3;
     }
+    bs.join(maxBounces);
     waveFinalizeKernel<true><<<(totalPixels + 255) / 256, 256, 0, stream>>>(*batch, *s, none, B);
     ++n;
     if (launches) *launches += n;

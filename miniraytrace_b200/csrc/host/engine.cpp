@@ -234,6 +234,7 @@ mrtResult Engine::init(const mrtEngineDesc& desc) {
                                                std::to_string(prop.minor) +
                                                ") cannot run this library's kernels, which are compiled for sm_100a only.");
     MRT_CUDA(cudaStreamCreateWithFlags(&m_stream, cudaStreamNonBlocking));
+    MRT_CUDA(cudaStreamCreateWithFlags(&m_side, cudaStreamNonBlocking));
     MRT_CUDA(cudaEventCreate(&m_ev0));
     MRT_CUDA(cudaEventCreate(&m_ev1));
     m_copyEvents.resize(16);
@@ -285,13 +286,14 @@ Engine::~Engine() {
     if (m_stream) {
         cudaSetDevice(m_device);
         cudaStreamSynchronize(m_stream);
+        if (m_side) cudaStreamSynchronize(m_side);
     }
     DeviceBuffer* bufs[] = {&m_nodes,     &m_triVerts, &m_triIndex,   &m_normals,      &m_uvs,        &m_tangents,
                             &m_instances, &m_materials, &m_lights,     &m_envTexels,    &m_envCdf,     &m_envSin,
                             &m_envRowSums, &m_envIntegral, &m_texTable, &m_accum,       &m_out32,      &m_out8,
                             &m_flags,     &m_rayCounters, &m_queryRays, &m_queryOut, &m_wave,
                             &m_bvhPos,    &m_bvhIdx,    &m_bvhScratch, &m_bvhNodes,    &m_bvhPrims,
-                            &m_packError};
+                            &m_packError, &m_srgbLut, &m_batchJobs};
     for (DeviceBuffer* b : bufs) b->release();
     for (auto& [id, b] : m_blas) b.release();
     m_cache.release();
@@ -304,10 +306,13 @@ Engine::~Engine() {
         if (ev) cudaEventDestroy(ev);
     for (auto& ev : m_stageEvents)
         if (ev) cudaEventDestroy(ev);
+    for (auto& ev : m_syncEvents)
+        if (ev) cudaEventDestroy(ev);
     for (auto& ev : m_cacheEvents)
         if (ev) cudaEventDestroy(ev);
     if (m_ev0) cudaEventDestroy(m_ev0);
     if (m_ev1) cudaEventDestroy(m_ev1);
+    if (m_side) cudaStreamDestroy(m_side);
     if (m_stream) cudaStreamDestroy(m_stream);
 }
 
@@ -1070,11 +1075,7 @@ mrtResult Engine::launchPending() {
     if (m_cache.enabled) MRT_TRY(guard(cacheWaveBuffers(waveCap, p.maxBounces)));
     const uint32_t waves = (n + waveCap - 1) / waveCap;
     const size_t perWave = size_t(6) * (p.maxBounces + 1);
-    while (m_stageEvents.size() < waves * perWave) {
-        cudaEvent_t ev;
-        MRT_CUDA(cudaEventCreate(&ev));
-        m_stageEvents.push_back(ev);
-    }
+    MRT_TRY(ensureEvents(waves * perWave));
     while (m_cache.enabled && m_cacheEvents.size() < size_t(3) * waves) {
         cudaEvent_t ev;
         MRT_CUDA(cudaEventCreate(&ev));
@@ -1089,7 +1090,8 @@ mrtResult Engine::launchPending() {
         if (m_cache.enabled) MRT_CUDA(cudaMemsetAsync(m_cache.counts.ptr, 0, 8, m_stream));
         const cudaError_t le = mrtcu_wave(&p, &m_waveState, m_frameIndex + done, k, &launches,
                                           m_stageEvents.data() + wave * perWave,
-                                          m_cache.enabled ? &m_cache.args : nullptr, m_stream);
+                                          m_syncEvents.data() + wave * perWave / 3,
+                                          m_cache.enabled ? &m_cache.args : nullptr, m_stream, m_side);
         if (le != cudaSuccess) return guard(fromCuda(le, "path tracing launch"));
         if (m_cache.enabled) MRT_TRY(guard(cacheWave(p, m_frameIndex + done, k, m_cacheEvents.data() + 3 * wave)));
         done += k;
@@ -1100,6 +1102,44 @@ mrtResult Engine::launchPending() {
     m_inFlightBounces = p.maxBounces + 1;
     m_inFlightLaunches = launches;
     m_inFlightCache = m_cache.enabled;
+    return MRT_SUCCESS;
+}
+
+// At least `stage` timing events (6 per bounce of a render call) and a
+// third as many sync events without timing (2 per bounce).
+mrtResult Engine::ensureEvents(size_t stage) {
+    while (m_stageEvents.size() < stage) {
+        cudaEvent_t ev;
+        MRT_CUDA(cudaEventCreate(&ev));
+        m_stageEvents.push_back(ev);
+    }
+    while (m_syncEvents.size() < stage / 3) {
+        cudaEvent_t ev;
+        MRT_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        m_syncEvents.push_back(ev);
+    }
+    return MRT_SUCCESS;
+}
+
+// Device time per wavefront stage of one wave from its stage events (the
+// launch order of mrtcu_wave): extend and shade are their kernels' spans on
+// the main stream. The shadow stage is the time the shadow kernels add to
+// the wave: where they run beside the next bounce's extend kernel, the wait
+// of the main stream for them once extend is done, plus the last bounce's
+// shadow kernel; in serial order, their spans.
+static mrtResult addStageTimes(const cudaEvent_t* ev, uint32_t bounces, float& ext, float& sha, float& shw) {
+    const bool overlap = mrtcu_shadow_overlap() != 0;
+    for (uint32_t b = 0; b < bounces; ++b) {
+        const cudaEvent_t* e = ev + 6 * size_t(b);
+        float x = 0.0f, y = 0.0f, z = 0.0f, wait = 0.0f;
+        MRT_CUDA(cudaEventElapsedTime(&x, e[0], e[1]));
+        MRT_CUDA(cudaEventElapsedTime(&wait, e[1], e[4]));
+        MRT_CUDA(cudaEventElapsedTime(&y, e[4], e[2]));
+        if (!overlap || b + 1 == bounces) MRT_CUDA(cudaEventElapsedTime(&z, e[2], e[3]));
+        ext += x;
+        sha += y;
+        shw += z + wait;
+    }
     return MRT_SUCCESS;
 }
 
@@ -1115,16 +1155,7 @@ mrtResult Engine::completePending() {
     const size_t perWave = size_t(6) * bounces;
     float ext = 0.0f, sha = 0.0f, shw = 0.0f;
     for (uint32_t w = 0; w < waves; ++w)
-        for (uint32_t b = 0; b < bounces; ++b) {
-            const cudaEvent_t* ev = m_stageEvents.data() + w * perWave + 6 * b;
-            float a = 0.0f, c = 0.0f, d = 0.0f;
-            MRT_CUDA(cudaEventElapsedTime(&a, ev[0], ev[1]));
-            MRT_CUDA(cudaEventElapsedTime(&c, ev[1], ev[2]));
-            MRT_CUDA(cudaEventElapsedTime(&d, ev[2], ev[3]));
-            ext += a;
-            sha += c;
-            shw += d;
-        }
+        MRT_TRY(addStageTimes(m_stageEvents.data() + w * perWave, bounces, ext, sha, shw));
     m_stats.extendMs = ext;
     m_stats.shadeMs = sha;
     m_stats.shadowMs = shw;
@@ -1350,18 +1381,15 @@ mrtResult Engine::renderBatchOneLaunch(Engine* const* engines, const uint32_t* n
     bp.errorFlags = lead.m_flags.as<uint32_t>();
     size_t events = 0;
     for (uint32_t b : bounces) events += size_t(6) * (b + 1);
-    while (lead.m_stageEvents.size() < events) {
-        cudaEvent_t ev;
-        MRT_CUDA(cudaEventCreate(&ev));
-        lead.m_stageEvents.push_back(ev);
-    }
+    MRT_TRY(lead.ensureEvents(events));
     uint32_t launches = 0;
     MRT_CUDA(cudaEventRecord(lead.m_ev0, lead.m_stream));
     size_t ev = 0;
     for (size_t b = 0; b < batches.size(); ++b) {
         const cudaError_t le = mrtcu_wave_batch(&bp, &W, lead.m_batchJobs.as<MrtBatchJob>() + first[b],
                                                 table.data() + first[b], uint32_t(batches[b].size()), bounces[b],
-                                                &launches, lead.m_stageEvents.data() + ev, lead.m_stream);
+                                                &launches, lead.m_stageEvents.data() + ev,
+                                                lead.m_syncEvents.data() + ev / 3, lead.m_stream, lead.m_side);
         if (le != cudaSuccess) return lead.guard(fromCuda(le, "one-launch batch"));
         ev += size_t(6) * (bounces[b] + 1);
     }
@@ -1376,16 +1404,7 @@ mrtResult Engine::renderBatchOneLaunch(Engine* const* engines, const uint32_t* n
     MRT_CUDA(cudaEventElapsedTime(&ms, lead.m_ev0, lead.m_ev1));
     ev = 0;
     for (uint32_t nb : bounces) {
-        for (uint32_t b = 0; b <= nb; ++b) {
-            const cudaEvent_t* e = lead.m_stageEvents.data() + ev + 6 * b;
-            float x = 0.0f, y = 0.0f, z = 0.0f;
-            MRT_CUDA(cudaEventElapsedTime(&x, e[0], e[1]));
-            MRT_CUDA(cudaEventElapsedTime(&y, e[1], e[2]));
-            MRT_CUDA(cudaEventElapsedTime(&z, e[2], e[3]));
-            ext += x;
-            sha += y;
-            shw += z;
-        }
+        MRT_TRY(addStageTimes(lead.m_stageEvents.data() + ev, nb + 1, ext, sha, shw));
         ev += size_t(6) * (nb + 1);
     }
     unsigned long long ctr[16];

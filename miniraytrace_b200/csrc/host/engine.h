@@ -91,6 +91,7 @@ private:
     mrtResult allocateFrame();
     mrtResult ensureWave(uint32_t samples);
     mrtResult carveWave(uint64_t slots, MrtWaveState& w);
+    mrtResult ensureEvents(size_t stage);
     // mrtxRenderBatch with every engine's waves in one set of launches
     static mrtResult renderBatchOneLaunch(Engine* const* engines, const uint32_t* n, uint32_t count);
     uint32_t waveCapacitySamples() const;
@@ -111,6 +112,8 @@ private:
 
     int m_device = 0;
     cudaStream_t m_stream = nullptr;
+    cudaStream_t m_side = nullptr;  // shadow kernels beside the next bounce's extend
+    std::vector<cudaEvent_t> m_syncEvents;  // 2 per bounce of a render call, without timing
     cudaEvent_t m_ev0 = nullptr, m_ev1 = nullptr;
     std::vector<cudaEvent_t> m_copyEvents;
     std::vector<cudaEvent_t> m_stageEvents;  // 6 per bounce per wave of one render call
