@@ -14,7 +14,9 @@ The tunable constants are preprocessor defines of the CUDA sources:
   takes new rays from the queue;
 - ``MRT_SHADE_THREADS``: threads per block of the shade kernel;
 - ``MRT_SHADOW_OVERLAP``: 1 runs a bounce's shadow kernel on a second stream
-  beside the next bounce's extend kernel, 0 runs every kernel in order.
+  beside the next bounce's extend kernel, 0 runs every kernel in order;
+- ``MRT_SHARED_STACK``: traversal stack entries per thread held in shared
+  memory (the rest in local memory; 0: all in local memory).
 
 The search is coordinate descent from the current values
 (``miniraytrace_b200/tuned.json``, else the sources' defaults): for each
@@ -48,13 +50,14 @@ PKG = Path(__file__).resolve().parent
 ROOT = PKG.parent
 
 DEFAULTS = {"MRT_TRAV_MIN_BLOCKS": 7, "MRT_TRI_PHASE_PCT": 25, "MRT_REFILL_IDLE": 8, "MRT_SHADE_THREADS": 256,
-            "MRT_SHADOW_OVERLAP": 1}
+            "MRT_SHADOW_OVERLAP": 1, "MRT_SHARED_STACK": 8}
 SPACE = {
     "MRT_TRAV_MIN_BLOCKS": [6, 7, 8],
     "MRT_TRI_PHASE_PCT": [12, 25, 50, 75],
     "MRT_REFILL_IDLE": [4, 8, 16],
     "MRT_SHADE_THREADS": [128, 256, 512],
     "MRT_SHADOW_OVERLAP": [0, 1],
+    "MRT_SHARED_STACK": [0, 8, 16],
 }
 
 

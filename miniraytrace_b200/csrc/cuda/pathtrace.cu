@@ -255,7 +255,7 @@ __global__ void MRT_TRAV_BOUNDS waveExtendKernel(MrtFrameParams Pk, MrtWaveState
     bool ok = true, active = false, drained = false;
     uint32_t slot = 0, job = 0;  // job: the lane's ray's batch job (kMulti)
     WideTrav T;
-    WideStack stack;
+    SplitStack stack;
     for (;;) {
         if (!drained) {
             const uint32_t i = refillLane(S.counts + kExtendHead + cur, n, active, drained);
@@ -508,7 +508,7 @@ __global__ void MRT_TRAV_BOUNDS waveShadowKernel(MrtFrameParams Pk, MrtWaveState
     bool ok = true, active = false, drained = false;
     uint32_t idx = 0, job = 0;  // job: the lane's ray's batch job (kMulti)
     WideTrav T;
-    WideStack stack;
+    SplitStack stack;
     for (;;) {
         if (!drained) {
             const uint32_t i = refillLane(S.counts + kShadowHead + cur, n, active, drained);

@@ -317,6 +317,16 @@ MRT_DEV uint32_t childIndex(uint32_t childBase, uint32_t imask, uint32_t b, uint
 // Traversal stack entries (node groups), shared by the TLAS and the BLAS
 // being walked.
 #define MRT_WIDE_STACK 48
+// Threads per block of the traversal kernels (a multiple of 32).
+#ifndef MRT_TRAV_THREADS
+#define MRT_TRAV_THREADS 128
+#endif
+// Stack entries of a traversal-kernel thread held in shared memory: the
+// bottom ones, which hold nearly every walk (the TLAS and one BLAS of an
+// 8-wide tree seldom need more); deeper entries go to local memory.
+#ifndef MRT_SHARED_STACK
+#define MRT_SHARED_STACK 8
+#endif
 
 // Traversal state of one ray, advanced one step at a time (travWarpStep), so a
 // persistent warp can start a new ray in a lane whose ray has finished while
@@ -341,9 +351,37 @@ struct WideTrav {
     bool ok;            // cleared on a stack overflow or an exhausted visit budget
 };
 // The stack of node groups lives apart from WideTrav (an array the walk
-// indexes dynamically sits in local memory; kept separate, the scalar state
-// stays in registers).
-typedef uint2 WideStack[MRT_WIDE_STACK];
+// indexes dynamically cannot live in registers; kept separate, the scalar
+// state stays in registers). Two forms with the same get/set:
+// A one-ray-per-thread walk (trace queries): all entries in local memory.
+struct LocalStack {
+    uint2 e[MRT_WIDE_STACK];
+    MRT_DEV uint2 get(int i) const { return e[i]; }
+    MRT_DEV void set(int i, uint2 v) { e[i] = v; }
+};
+// A persistent traversal kernel's thread (blocks of MRT_TRAV_THREADS):
+// entries below MRT_SHARED_STACK in the block's shared array, entry i of
+// thread t at [i][t] (a warp's 8-byte entries at one depth fill two
+// conflict-free wavefronts; at mixed depths the bank is still that of t),
+// the rest in local memory. MRT_SHARED_STACK 0 keeps all in local memory.
+#if MRT_SHARED_STACK > 0
+MRT_DEV uint2 (&travSharedStack())[MRT_SHARED_STACK][MRT_TRAV_THREADS] {
+    __shared__ uint2 s[MRT_SHARED_STACK][MRT_TRAV_THREADS];
+    return s;
+}
+struct SplitStack {
+    uint2 deep[MRT_WIDE_STACK - MRT_SHARED_STACK];
+    MRT_DEV uint2 get(int i) const {
+        return i < MRT_SHARED_STACK ? travSharedStack()[i][threadIdx.x] : deep[i - MRT_SHARED_STACK];
+    }
+    MRT_DEV void set(int i, uint2 v) {
+        if (i < MRT_SHARED_STACK) travSharedStack()[i][threadIdx.x] = v;
+        else deep[i - MRT_SHARED_STACK] = v;
+    }
+};
+#else
+typedef LocalStack SplitStack;
+#endif
 
 MRT_DEV void travBegin(const MrtFrameParams& P, WideTrav& T, float3 o, float3 d, float tMax) {
     T.wo = o;
@@ -372,11 +410,15 @@ MRT_DEV void travBegin(const MrtFrameParams& P, WideTrav& T, float3 o, float3 d,
 enum { kTravRunning = 0, kTravDone = 1, kTravOccluded = 2 };
 
 // Node step of one lane with no triangles pending: bookkeeping (instance
-// entry, return to the TLAS, stack pops) until one node has been tested.
-// The BLAS leaf hits of that node become the lane's pending triangles; TLAS
-// leaf hits (instances) stay in the group and are entered on the next step.
-// Returns kTravDone when the walk is over.
-MRT_DEV int travNodeStep(const MrtFrameParams& P, WideTrav& T, WideStack& stack, TraversalCounters& tc) {
+// entry, return to the TLAS, stack pops) until the lane has a node to test,
+// then one node test. The BLAS leaf hits of that node become the lane's
+// pending triangles; TLAS leaf hits (instances) stay in the group and are
+// entered on the next step. Returns kTravDone when the walk is over.
+// The node test sits after the bookkeeping loop, not inside it: lanes that
+// pop first and lanes whose group still holds a child meet before the test,
+// so a warp runs it once per step rather than once per loop trip.
+template <class Stack>
+MRT_DEV int travNodeStep(const MrtFrameParams& P, WideTrav& T, Stack& stack, TraversalCounters& tc) {
     for (;;) {
         if (T.g.primBits) {  // instances (BLAS leaf hits never stay in the group)
             const uint32_t b = uint32_t(__ffs(T.g.primBits) - 1);
@@ -398,26 +440,7 @@ MRT_DEV int travNodeStep(const MrtFrameParams& P, WideTrav& T, WideStack& stack,
             T.g = WideGroup{in->blasRoot, 0u, 0x80000000u, 0u};
             continue;
         }
-        if (T.g.nodeBits & 0xff000000u) {
-            if (++T.visits > P.maxVisits) {
-                T.ok = false;
-                return kTravDone;
-            }
-            const uint32_t b = 31u - uint32_t(__clz(T.g.nodeBits & 0xff000000u));
-            const uint32_t rest = T.g.nodeBits & ~(1u << b);
-            const uint32_t child = childIndex(T.g.childBase, T.g.nodeBits & 0xffu, b, T.oct);
-            if (rest & 0xff000000u) {
-                if (T.sp < MRT_WIDE_STACK) stack[T.sp++] = make_uint2(T.g.childBase, rest);
-                else T.ok = false;
-            }
-            T.g = intersectWide(P, child, T.o, T.inv, T.oct, T.tMax, tc);
-            if (T.blasBase >= 0 && T.g.primBits) {
-                T.pendBase = T.g.primBase;
-                T.pendBits = T.g.primBits;
-                T.g.primBits = 0;
-            }
-            return kTravRunning;
-        }
+        if (T.g.nodeBits & 0xff000000u) break;
         if (T.sp == T.blasBase) {  // BLAS finished: resume the parked TLAS group
             T.g = T.parked;
             T.blasBase = -1;
@@ -427,11 +450,29 @@ MRT_DEV int travNodeStep(const MrtFrameParams& P, WideTrav& T, WideStack& stack,
             continue;
         }
         if (T.sp == 0) return kTravDone;
-        const uint2 e = stack[--T.sp];
+        const uint2 e = stack.get(--T.sp);
         T.g.childBase = e.x;
         T.g.nodeBits = e.y;
         T.g.primBits = 0;
     }
+    if (++T.visits > P.maxVisits) {
+        T.ok = false;
+        return kTravDone;
+    }
+    const uint32_t b = 31u - uint32_t(__clz(T.g.nodeBits & 0xff000000u));
+    const uint32_t rest = T.g.nodeBits & ~(1u << b);
+    const uint32_t child = childIndex(T.g.childBase, T.g.nodeBits & 0xffu, b, T.oct);
+    if (rest & 0xff000000u) {
+        if (T.sp < MRT_WIDE_STACK) stack.set(T.sp++, make_uint2(T.g.childBase, rest));
+        else T.ok = false;
+    }
+    T.g = intersectWide(P, child, T.o, T.inv, T.oct, T.tMax, tc);
+    if (T.blasBase >= 0 && T.g.primBits) {
+        T.pendBase = T.g.primBase;
+        T.pendBits = T.g.primBits;
+        T.g.primBits = 0;
+    }
+    return kTravRunning;
 }
 
 // Triangle step: the lane's pending triangles. kAny: kTravOccluded at the
@@ -464,11 +505,6 @@ MRT_DEV int travTriStep(const MrtFrameParams& P, WideTrav& T, TraversalCounters&
     }
     return kTravRunning;
 }
-
-// Threads per block of the traversal kernels (a multiple of 32).
-#ifndef MRT_TRAV_THREADS
-#define MRT_TRAV_THREADS 128
-#endif
 
 // Warp-wide triangle phase: every pending (ray, triangle) pair of the warp
 // is tested, 32 pairs a round, one per lane, whichever lane owns the ray, so
@@ -594,8 +630,8 @@ MRT_DEV int travTriPhaseWarp(const MrtFrameParams& P, WideTrav& T, TraversalCoun
 #ifndef MRT_TRI_PHASE_PCT
 #define MRT_TRI_PHASE_PCT 25
 #endif
-template <bool kAny, bool kMulti = false>
-MRT_DEV int travWarpStep(const MrtFrameParams& P, WideTrav& T, WideStack& stack, TraversalCounters& tc,
+template <bool kAny, bool kMulti = false, class Stack>
+MRT_DEV int travWarpStep(const MrtFrameParams& P, WideTrav& T, Stack& stack, TraversalCounters& tc,
                          bool active, const MrtBatchJob* jobs = nullptr, uint32_t job = 0u) {
     const bool pending = active && T.pendBits != 0;
     const uint32_t pendLanes = __popc(__ballot_sync(0xffffffffu, pending));
@@ -624,7 +660,7 @@ MRT_DEV int travWarpStep(const MrtFrameParams& P, WideTrav& T, WideStack& stack,
 
 // The same walk for one ray on its own (trace queries).
 template <bool kAny>
-MRT_DEV int travRun(const MrtFrameParams& P, WideTrav& T, WideStack& stack, TraversalCounters& tc) {
+MRT_DEV int travRun(const MrtFrameParams& P, WideTrav& T, LocalStack& stack, TraversalCounters& tc) {
     for (;;) {
         const int r = T.pendBits ? travTriStep<kAny>(P, T, tc) : travNodeStep(P, T, stack, tc);
         if (r != kTravRunning) return r;
@@ -635,7 +671,7 @@ MRT_DEV int travRun(const MrtFrameParams& P, WideTrav& T, WideStack& stack, Trav
 // with the reference's arithmetic. Returns false on a traversal error.
 MRT_DEV bool traceClosest(const MrtFrameParams& P, float3 o, float3 d, float tMax, HitRecord& hit, TraversalCounters& tc) {
     WideTrav T;
-    WideStack stack;
+    LocalStack stack;
     travBegin(P, T, o, d, tMax);
     travRun<false>(P, T, stack, tc);
     hit = T.hit;
@@ -646,7 +682,7 @@ MRT_DEV bool traceClosest(const MrtFrameParams& P, float3 o, float3 d, float tMa
 // Any hit in (1e-4, tMax) (reference intersect.glsl:128-178).
 MRT_DEV bool traceAny(const MrtFrameParams& P, float3 o, float3 d, float tMax, bool& ok, TraversalCounters& tc) {
     WideTrav T;
-    WideStack stack;
+    LocalStack stack;
     travBegin(P, T, o, d, tMax);
     const int r = travRun<true>(P, T, stack, tc);
     ok &= T.ok;
