@@ -275,6 +275,42 @@ MRT_API mrtResult mrtxBuildMeshBvh(mrtEngine* engine, const float* positions, ui
                                    uint32_t maxLeafPrims, void* nodesOut, uint32_t nodeCapacity,
                                    uint32_t* primOrderOut, uint32_t* nodeCountOut);
 
+/* Opt-in denoiser of the display image, in place of the reference's
+ * optional OIDN filter (core/src/post/Denoiser.cpp:10-112, scheduled by
+ * Renderer.cpp:845-884; the reference built without OIDN never denoises,
+ * and neither does this library until a call enables it): an edge-avoiding
+ * a-trous wavelet filter (Dammertz et al. 2010) on the GPU, guided by the
+ * first-hit albedo, shading normal and distance (the reference's AOVs),
+ * computed by a pass of `guideSamples` jittered camera rays per pixel once
+ * per accumulation. With `enabled` and the render setting `denoise` on, the
+ * RGBA8_SRGB read shows the denoised image from `minSpp` samples on,
+ * re-denoised when the sample count has doubled since (the reference's
+ * schedule: 8, 16, 32, ... up to sppLimit), and frame infos report
+ * denoised = 1; RGBA32F_LINEAR reads stay the raw mean, as in the
+ * reference. Fields of zero take the defaults in brackets. */
+typedef struct mrtxDenoiserDesc {
+    size_t structSize;
+    int32_t enabled;        /* 0: off (the default) */
+    uint32_t iterations;    /* filter passes, tap spacing 1, 2, 4, ... [5], at most 10 */
+    uint32_t guideSamples;  /* camera rays per pixel of the guide pass [4] */
+    uint32_t minSpp;        /* first denoised display at this many samples [8] */
+    float sigmaColor;       /* colour weight [0.5] (on colour / (1 + luminance)) */
+    float normalPower;      /* normal weight exponent [64] */
+    float sigmaAlbedo;      /* albedo weight [0.1] */
+    float sigmaDepth;       /* distance weight, relative to distance and spacing [0.1] */
+} mrtxDenoiserDesc;
+MRT_API mrtResult mrtxSetDenoiser(mrtEngine*, const mrtxDenoiserDesc*);
+/* The denoised linear image of the samples rendered so far (RGBA32F, alpha
+ * 1, rows top down; bytes >= width * height * 16), filtered now with the
+ * current parameters. MRT_ERROR_INVALID_ARGUMENT while the denoiser is off. */
+MRT_API mrtResult mrtxReadDenoised(mrtEngine*, float* rgba, size_t bytes);
+/* The denoiser's guides (each width * height RGBA32F; bytes of each buffer
+ * >= width * height * 16): mean first-hit albedo (alpha 1), and mean shading
+ * normal (not renormalised) with the mean distance to the first hit in
+ * alpha (0 where every guide ray missed). Computed if stale. Either pointer
+ * may be NULL. */
+MRT_API mrtResult mrtxReadDenoiserGuides(mrtEngine*, float* albedo, float* normalDepth, size_t bytes);
+
 /* Largest map height mrtxBuildEnvCdfNoAlloc accepts. */
 #define MRTX_ENV_CDF_NOALLOC_MAX_HEIGHT 8192u
 

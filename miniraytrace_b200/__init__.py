@@ -358,6 +358,27 @@ class Engine:
                                                    C.byref(loss)), "mrtxRadianceCacheGradients")
         return g, w, loss.value
 
+    def set_denoiser(self, enabled=True, iterations=0, guide_samples=0, min_spp=0, sigma_color=0.0,
+                     normal_power=0.0, sigma_albedo=0.0, sigma_depth=0.0):
+        """mrtxSetDenoiser (zeros take the library's defaults)."""
+        d = abi.DenoiserDesc(enabled=1 if enabled else 0, iterations=iterations, guideSamples=guide_samples,
+                             minSpp=min_spp, sigmaColor=sigma_color, normalPower=normal_power,
+                             sigmaAlbedo=sigma_albedo, sigmaDepth=sigma_depth)
+        _check(self.lib.mrtxSetDenoiser(self.h, C.byref(d)), "mrtxSetDenoiser")
+
+    def read_denoised(self):
+        """mrtxReadDenoised: the denoised linear image (H x W x 4 float32)."""
+        a = np.empty((self.height, self.width, 4), np.float32)
+        _check(self.lib.mrtxReadDenoised(self.h, _ptr(a), a.nbytes), "mrtxReadDenoised")
+        return a
+
+    def read_denoiser_guides(self):
+        """mrtxReadDenoiserGuides: (albedo, normal + distance), H x W x 4 float32 each."""
+        al = np.empty((self.height, self.width, 4), np.float32)
+        nd = np.empty((self.height, self.width, 4), np.float32)
+        _check(self.lib.mrtxReadDenoiserGuides(self.h, _ptr(al), _ptr(nd), al.nbytes), "mrtxReadDenoiserGuides")
+        return al, nd
+
     def cache_params(self, grid=None, mlp=None):
         """Returns (grid, mlp) as read, then writes the given arrays."""
         g = np.empty(abi.CACHE_GRID_FLOATS, np.float32)

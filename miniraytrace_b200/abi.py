@@ -105,6 +105,12 @@ class RadianceCacheDesc(_Sized):
                 ("trainingVertices", C.c_uint32)]
 
 
+class DenoiserDesc(_Sized):
+    _fields_ = [("structSize", C.c_size_t), ("enabled", C.c_int32), ("iterations", C.c_uint32),
+                ("guideSamples", C.c_uint32), ("minSpp", C.c_uint32), ("sigmaColor", C.c_float),
+                ("normalPower", C.c_float), ("sigmaAlbedo", C.c_float), ("sigmaDepth", C.c_float)]
+
+
 class CommitStats(_Sized):
     _fields_ = [("structSize", C.c_size_t), ("blasRebuilt", C.c_uint32), ("tlasRebuilt", C.c_int32),
                 ("commitMs", C.c_float)]
@@ -191,6 +197,9 @@ FUNCTIONS = [
     ("mrtxBuildWideBvh", C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p,
                                    C.POINTER(C.c_uint32)]),
     ("mrtxSetRadianceCache", C.c_int, [C.c_void_p, C.POINTER(RadianceCacheDesc)]),
+    ("mrtxSetDenoiser", C.c_int, [C.c_void_p, C.POINTER(DenoiserDesc)]),
+    ("mrtxReadDenoised", C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t]),
+    ("mrtxReadDenoiserGuides", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t]),
     ("mrtxRadianceCacheQuery", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]),
     ("mrtxRadianceCacheTrain", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32,
                                          C.POINTER(C.c_float)]),

@@ -106,6 +106,23 @@ cudaError_t mrtcu_l2_read_probe(const void* buf, size_t count, uint32_t reps, ui
 cudaError_t mrtcu_readback_rgba32f(const double* accum, size_t npix, uint32_t spp, float4* out,
                                    cudaStream_t stream);
 
+// Opt-in denoiser (denoise.cu): parameters of the a-trous filter.
+typedef struct MrtDenoiseParams {
+    uint32_t width, height, iterations;
+    float sigmaColor, normalPower, sigmaAlbedo, sigmaDepth, albedoFloor;
+} MrtDenoiseParams;
+// Denoiser guides of every pixel: mean first-hit albedo (a = 1) and shading
+// normal with the mean distance to that hit (w; 0 when no ray hit), over
+// `samples` jittered camera rays drawing from frame indices streamBase...
+cudaError_t mrtcu_denoise_guides(const MrtFrameParams* p, uint32_t samples, uint32_t streamBase, float4* albedo,
+                                 float4* normalDepth, cudaStream_t stream);
+// The denoised linear image of the FP64 accumulation (RGBA32F, a = 1);
+// work holds 3 x width x height float4.
+cudaError_t mrtcu_denoise(const double* accum, const float4* albedo, const float4* normalDepth,
+                          const MrtDenoiseParams* d, float4* work, float4* out, cudaStream_t stream);
+// RGBA8 resolve of a linear image (the denoised one), as mrtcu_resolve_rgba8.
+cudaError_t mrtcu_resolve_rgba8_linear(const float4* color, size_t npix, float exposure, uint32_t tonemap,
+                                       uchar4* out, cudaStream_t stream);
 // RGBA8 resolve (reference resolve.comp:24-56): mean = sum / count,
 // exposure, optional ACES, sRGB encode, UNORM8 store, alpha 255.
 cudaError_t mrtcu_resolve_rgba8(const double* accum, size_t npix, float exposure, uint32_t tonemap,

@@ -164,6 +164,23 @@ __global__ void resolveKernel(const double2* __restrict__ accum, size_t npix, fl
     out[i] = make_uchar4(o[0], o[1], o[2], 255);
 }
 
+// The same resolve of a linear image (resolve.comp:44-46, the denoised branch).
+__global__ void resolveLinearKernel(const float4* __restrict__ color, size_t npix, float exposure, uint32_t tonemap,
+                                    uchar4* __restrict__ out) {
+    const size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= npix) return;
+    const float4 c4 = color[i];
+    const float c[3] = {c4.x, c4.y, c4.z};
+    unsigned char o[3];
+    for (int k = 0; k < 3; ++k) {
+        float v = c[k] * exposure;
+        if (tonemap == 1u) v = acesTonemap(v);
+        v = linearToSrgb(fminf(fmaxf(v, 0.0f), 1e4f));
+        o[k] = toUnorm8(v);
+    }
+    out[i] = make_uchar4(o[0], o[1], o[2], 255);
+}
+
 __global__ void addKernel(double* __restrict__ dst, const double* __restrict__ src, size_t n) {
     for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
         dst[i] += src[i];
@@ -296,5 +313,12 @@ extern "C" cudaError_t mrtcu_resolve_rgba8(const double* accum, size_t npix, flo
 extern "C" cudaError_t mrtcu_add_f64(double* dst, const double* src, size_t n, cudaStream_t stream) {
     if (n == 0) return cudaSuccess;
     addKernel<<<148 * 8, 256, 0, stream>>>(dst, src, n);
+    return cudaGetLastError();
+}
+
+extern "C" cudaError_t mrtcu_resolve_rgba8_linear(const float4* color, size_t npix, float exposure, uint32_t tonemap,
+                                                  uchar4* out, cudaStream_t stream) {
+    if (npix == 0) return cudaSuccess;
+    resolveLinearKernel<<<unsigned((npix + 255) / 256), 256, 0, stream>>>(color, npix, exposure, tonemap, out);
     return cudaGetLastError();
 }

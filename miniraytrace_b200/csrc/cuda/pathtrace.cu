@@ -12,8 +12,9 @@
 //   - accumulation is FP64 (double4 per pixel: r, g, b, count), the wave's
 //     samples summed per pixel in sample order;
 //   - traversal is the watertight two-level walk of trace.cuh;
-//   - the first-hit AOV buffers of the reference are not produced (they only
-//     feed an optional OIDN denoiser and are not readable through the ABI).
+//   - the first-hit AOV buffers of the reference (which only feed its
+//     optional OIDN denoiser) are not accumulated by the path tracer; the
+//     opt-in denoiser computes its guides in a pass of its own (aovKernel).
 #include <cooperative_groups.h>
 #include <map>
 #include <mutex>
@@ -160,6 +161,22 @@ MRT_DEV uint32_t batchJobOf(const MrtBatchJobs& B, uint32_t v, bool pixels) {
 }
 MRT_DEV WaveArgs jobWave(const MrtBatchJob& J) { return WaveArgs{J.pixels, J.slots, J.sampleBase, J.samples}; }
 
+// The camera ray through pixel (px, py) at sub-pixel offset `jitter`
+// (pathtrace.comp:101-123: perspective or orthographic, asymmetric frustum).
+MRT_DEV void cameraRay(const MrtFrameParams& P, uint32_t px, uint32_t py, float2 jitter, float3& ro, float3& rd) {
+    const float u = (float(px) + jitter.x) / float(P.width);
+    const float v = (float(py) + jitter.y) / float(P.height);
+    const float sx = mixf(P.frustum[0], P.frustum[1], u);
+    const float sy = mixf(P.frustum[3], P.frustum[2], v);  // top..bottom: rows go down
+    if (P.flags & MRT_FLAG_ORTHO) {
+        ro = f3p(P.camPos) + sx * f3p(P.camRight) + sy * f3p(P.camUp);
+        rd = f3p(P.camForward);
+    } else {
+        ro = f3p(P.camPos);
+        rd = normalize(f3p(P.camForward) + sx * f3p(P.camRight) + sy * f3p(P.camUp));
+    }
+}
+
 // Camera rays of every slot of the wave (pathtrace.comp:101-130). In a
 // one-launch batch every job's slots, each with its job's camera.
 template <bool kMulti>
@@ -179,19 +196,8 @@ __global__ void __launch_bounds__(256) waveInitKernel(MrtFrameParams Pk, MrtWave
     const uint32_t pixel = lslot / A.samples;
     const uint32_t px = pixel % P.width, py = pixel / P.width;
     Rng rng{px, py, frameOf(P, A, lslot), 0u};
-    const float2 jitter = rng2(rng);
-    const float u = (float(px) + jitter.x) / float(P.width);
-    const float v = (float(py) + jitter.y) / float(P.height);
-    const float sx = mixf(P.frustum[0], P.frustum[1], u);
-    const float sy = mixf(P.frustum[3], P.frustum[2], v);  // top..bottom: rows go down
     float3 ro, rd;
-    if (P.flags & MRT_FLAG_ORTHO) {
-        ro = f3p(P.camPos) + sx * f3p(P.camRight) + sy * f3p(P.camUp);
-        rd = f3p(P.camForward);
-    } else {
-        ro = f3p(P.camPos);
-        rd = normalize(f3p(P.camForward) + sx * f3p(P.camRight) + sy * f3p(P.camUp));
-    }
+    cameraRay(P, px, py, rng2(rng), ro, rd);
     S.rayO[slot] = make_float4(ro.x, ro.y, ro.z, 0.0f);
     S.rayD[slot] = make_float4(rd.x, rd.y, rd.z, __uint_as_float(0u));
     S.beta[slot] = make_float4(1.0f, 1.0f, 1.0f, __uint_as_float(rng.w));
@@ -669,6 +675,57 @@ __global__ void traceAnyKernel(MrtFrameParams P, const MrtQueryRay* __restrict__
     if (tc.bad) atomicOr(P.errorFlags, 2u);
 }
 
+// Denoiser guides: the reference's first-hit AOVs (pathtrace.comp:130-167,
+// 230-233) -- at the first surface a camera ray does not pass through
+// (stochastic alpha as in the path tracer), the albedo (base colour times
+// its texture) and the shading normal -- averaged over `samples` jittered
+// camera rays per pixel (a miss adds zero, as in the reference), plus the
+// mean distance travelled to that surface over the rays that found one (0
+// when none did) in normalDepth.w. The rays draw from frame indices
+// streamBase, streamBase + 1, ..., a stream apart from the renders'.
+__global__ void __launch_bounds__(128) aovKernel(MrtFrameParams P, uint32_t samples, uint32_t streamBase,
+                                                 float4* __restrict__ albedo, float4* __restrict__ normalDepth) {
+    const uint32_t pixel = blockIdx.x * blockDim.x + threadIdx.x;
+    if (pixel >= P.width * P.height) return;
+    const uint32_t px = pixel % P.width, py = pixel / P.width;
+    float3 alb = f3(0.0f), nrm = f3(0.0f);
+    float depth = 0.0f;
+    uint32_t found = 0;
+    TraversalCounters tc;
+    bool ok = true;
+    for (uint32_t k = 0; k < samples; ++k) {
+        Rng rng{px, py, streamBase + k, 0u};
+        float3 ro, rd;
+        cameraRay(P, px, py, rng2(rng), ro, rd);
+        float travelled = 0.0f;
+        for (uint32_t layer = 0; layer <= P.maxBounces; ++layer) {  // the path tracer's bound on pass-throughs
+            HitRecord hit;
+            ok &= traceClosest(P, ro, rd, 1e30f, hit, tc);
+            if (hit.tri == 0xffffffffu) break;
+            const Surface s = makeSurface(P, rd, hit);
+            const MrtMaterial& m = P.materials[s.mat];
+            travelled += hit.t;
+            const float opacity = m.baseColorOpacity[3];
+            if (opacity < 1.0f && rng1(rng) >= opacity) {
+                ro = s.pos + rd * MRT_EPS_RAY;
+                continue;
+            }
+            float3 a = f3p(m.baseColorOpacity);
+            if (m.tex[0] >= 0) a = a * texRgb(P, m.tex[0], s.uv);
+            alb += a;
+            nrm += s.nShade;
+            depth += travelled;
+            ++found;
+            break;
+        }
+    }
+    if (!ok) atomicOr(P.errorFlags, 1u);
+    if (tc.bad) atomicOr(P.errorFlags, 2u);
+    const float inv = 1.0f / float(samples);
+    albedo[pixel] = make_float4(alb.x * inv, alb.y * inv, alb.z * inv, 1.0f);
+    normalDepth[pixel] = make_float4(nrm.x * inv, nrm.y * inv, nrm.z * inv, found ? depth / float(found) : 0.0f);
+}
+
 }  // namespace
 
 namespace {
@@ -871,5 +928,13 @@ extern "C" cudaError_t mrtcu_trace_any(const MrtFrameParams* p, const MrtQueryRa
                                        uint32_t* occluded, cudaStream_t stream) {
     if (n == 0) return cudaSuccess;
     traceAnyKernel<<<(n + 127) / 128, 128, 0, stream>>>(*p, rays, n, occluded);
+    return cudaGetLastError();
+}
+
+extern "C" cudaError_t mrtcu_denoise_guides(const MrtFrameParams* p, uint32_t samples, uint32_t streamBase,
+                                            float4* albedo, float4* normalDepth, cudaStream_t stream) {
+    const uint32_t pixels = p->width * p->height;
+    if (pixels == 0 || samples == 0) return cudaSuccess;
+    aovKernel<<<(pixels + 127) / 128, 128, 0, stream>>>(*p, samples, streamBase, albedo, normalDepth);
     return cudaGetLastError();
 }

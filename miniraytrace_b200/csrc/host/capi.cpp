@@ -367,6 +367,25 @@ MRT_API mrtResult mrtxSetRadianceCacheSchedule(mrtEngine* e, float lrMin, float 
     return guarded([&] { return eng->setCacheSchedule(lrMin, halfLifeSteps); });
 }
 
+MRT_API mrtResult mrtxSetDenoiser(mrtEngine* e, const mrtxDenoiserDesc* d) {
+    mrt::Engine* eng = unwrap(e);
+    if (!eng) return MRT_ERROR_INVALID_HANDLE;
+    if (!validStruct(d)) return mrt::fail(MRT_ERROR_INVALID_ARGUMENT, "mrtxSetDenoiser: bad mrtxDenoiserDesc");
+    return guarded([&] { return eng->setDenoiser(*d); });
+}
+
+MRT_API mrtResult mrtxReadDenoised(mrtEngine* e, float* rgba, size_t bytes) {
+    mrt::Engine* eng = unwrap(e);
+    if (!eng) return MRT_ERROR_INVALID_HANDLE;
+    return guarded([&] { return eng->readDenoised(rgba, bytes); });
+}
+
+MRT_API mrtResult mrtxReadDenoiserGuides(mrtEngine* e, float* albedo, float* normalDepth, size_t bytes) {
+    mrt::Engine* eng = unwrap(e);
+    if (!eng) return MRT_ERROR_INVALID_HANDLE;
+    return guarded([&] { return eng->readDenoiserGuides(albedo, normalDepth, bytes); });
+}
+
 MRT_API mrtResult mrtxSetRadianceCacheAveraging(mrtEngine* e, float decay) {
     mrt::Engine* eng = unwrap(e);
     if (!eng) return MRT_ERROR_INVALID_HANDLE;

@@ -297,6 +297,7 @@ Engine::~Engine() {
     for (DeviceBuffer* b : bufs) b->release();
     for (auto& [id, b] : m_blas) b.release();
     m_cache.release();
+    m_denoiser.release();
     for (auto& t : m_texData) t.release();
     if (m_pinned) cudaFreeHost(m_pinned);
     if (m_stage) cudaFreeHost(m_stage);
@@ -417,6 +418,11 @@ mrtResult Engine::setSettings(const Settings& s) {
 void Engine::resetAccumulation() {
     m_frameIndex = 0;
     m_pending = 0;  // queued samples would be discarded by the reset anyway
+    // the reference's reset of its denoiser state (Renderer.cpp:766-769)
+    m_denoiser.guidesValid = false;
+    m_denoiser.useDenoised = false;
+    m_denoiser.nextAt = m_denoiser.minSpp;
+    m_denoiser.denoisedSpp = 0;
 }
 
 mrtResult Engine::setSampleStream(uint32_t offset, uint32_t stride) {
@@ -1030,7 +1036,7 @@ mrtResult Engine::renderFrames(uint32_t count, mrtFrameInfo* info, bool defer) {
     if (info && info->structSize >= sizeof(mrtFrameInfo)) {
         info->spp = m_frameIndex + m_pending;
         info->converged = m_frameIndex + m_pending >= m_settings.sppLimit ? 1 : 0;
-        info->denoised = 0;
+        info->denoised = denoiserActive() && m_denoiser.useDenoised ? 1 : 0;
         // A call that rendered reports its wall time, as the reference times
         // its render call (Renderer.cpp:774, 837-841). A queued frame has not
         // been rendered yet: it reports the device time of one sample of the
@@ -1276,7 +1282,7 @@ mrtResult Engine::renderBatch(Engine* const* engines, const uint32_t* spp, uint3
         if (infos && infos[i].structSize >= sizeof(mrtFrameInfo)) {
             infos[i].spp = e.m_frameIndex + e.m_pending;
             infos[i].converged = e.m_frameIndex + e.m_pending >= e.m_settings.sppLimit ? 1 : 0;
-            infos[i].denoised = 0;
+            infos[i].denoised = e.denoiserActive() && e.m_denoiser.useDenoised ? 1 : 0;
             infos[i].frameMs = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
         }
     }
@@ -1481,14 +1487,124 @@ mrtResult Engine::readFramebuffer(mrtPixelFormat fmt, void* dst, size_t dstSize)
     const size_t pixels = size_t(m_settings.width) * m_settings.height;
     if (fmt == MRT_PIXEL_RGBA8_SRGB) {
         if (dstSize < pixels * 4) return fail(MRT_ERROR_INVALID_ARGUMENT, "dst too small for RGBA8 readback");
-        MRT_CUDA(mrtcu_resolve_rgba8(m_accum.as<double>(), pixels, m_resolveExposure, m_resolveTonemap,
-                                     m_out8.as<uchar4>(), m_stream));
+        // the denoised display image (reference Renderer.cpp:845-884 with
+        // resolve.comp:44-46): first at minSpp samples, then again once the
+        // count has doubled
+        if (denoiserActive() && m_frameIndex >= m_denoiser.nextAt && m_frameIndex != m_denoiser.denoisedSpp) {
+            MRT_TRY(runDenoise());
+            m_denoiser.useDenoised = true;
+            m_denoiser.nextAt = std::min(m_frameIndex * 2, m_settings.sppLimit);
+        }
+        if (denoiserActive() && m_denoiser.useDenoised)
+            MRT_CUDA(mrtcu_resolve_rgba8_linear(m_denoiser.out.as<float4>(), pixels, m_resolveExposure,
+                                                m_resolveTonemap, m_out8.as<uchar4>(), m_stream));
+        else
+            MRT_CUDA(mrtcu_resolve_rgba8(m_accum.as<double>(), pixels, m_resolveExposure, m_resolveTonemap,
+                                         m_out8.as<uchar4>(), m_stream));
         return guard(download(dst, m_out8.ptr, pixels * 4));
     }
     if (fmt != MRT_PIXEL_RGBA32F_LINEAR) return fail(MRT_ERROR_INVALID_ARGUMENT, "unknown pixel format");
     if (dstSize < pixels * 16) return fail(MRT_ERROR_INVALID_ARGUMENT, "dst too small for RGBA32F readback");
     MRT_CUDA(mrtcu_readback_rgba32f(m_accum.as<double>(), pixels, m_frameIndex, m_out32.as<float4>(), m_stream));
     return guard(download(dst, m_out32.ptr, pixels * 16));
+}
+
+// ---------------------------------------------------------------- denoiser --
+
+void Engine::DenoiserState::release() {
+    albedo.release();
+    normalDepth.release();
+    work.release();
+    out.release();
+}
+
+mrtResult Engine::setDenoiser(const mrtxDenoiserDesc& d) {
+    MRT_TRY(checkAlive());
+    MRT_TRY(flushPending());
+    if (d.iterations > 10) return fail(MRT_ERROR_INVALID_ARGUMENT, "denoiser iterations must be at most 10");
+    const float weights[4] = {d.sigmaColor, d.normalPower, d.sigmaAlbedo, d.sigmaDepth};
+    for (float v : weights)
+        if (!(v >= 0.0f) || !std::isfinite(v)) return fail(MRT_ERROR_INVALID_ARGUMENT, "denoiser weights must be >= 0");
+    DenoiserState& D = m_denoiser;
+    D.enabled = d.enabled != 0;
+    D.params.iterations = d.iterations ? d.iterations : 5u;
+    D.params.sigmaColor = d.sigmaColor > 0.0f ? d.sigmaColor : 0.5f;
+    D.params.normalPower = d.normalPower > 0.0f ? d.normalPower : 64.0f;
+    D.params.sigmaAlbedo = d.sigmaAlbedo > 0.0f ? d.sigmaAlbedo : 0.1f;
+    D.params.sigmaDepth = d.sigmaDepth > 0.0f ? d.sigmaDepth : 0.1f;
+    const uint32_t samples = d.guideSamples ? d.guideSamples : 4u;
+    if (samples != D.guideSamples) D.guidesValid = false;
+    D.guideSamples = samples;
+    D.minSpp = d.minSpp ? d.minSpp : 8u;
+    // new parameters apply from the next display read
+    D.useDenoised = false;
+    D.nextAt = D.minSpp;
+    D.denoisedSpp = 0;
+    if (!D.enabled) {
+        D.release();
+        D.guidesValid = false;
+    }
+    return MRT_SUCCESS;
+}
+
+// The guides of the samples rendered so far: computed with the frame
+// parameters those samples were rendered with (after the first render; the
+// current ones before), on a sample stream of their own.
+mrtResult Engine::ensureGuides() {
+    DenoiserState& D = m_denoiser;
+    const size_t pixels = size_t(m_settings.width) * m_settings.height;
+    MRT_TRY(guard(D.albedo.ensure(pixels * 16)));
+    MRT_TRY(guard(D.normalDepth.ensure(pixels * 16)));
+    if (D.guidesValid) return MRT_SUCCESS;
+    MrtFrameParams p;
+    if (m_frameIndex > 0) {
+        p = m_pendingParams;
+    } else {
+        MRT_TRY(commit(nullptr));
+        fillParams(p);
+    }
+    MRT_CUDA(mrtcu_denoise_guides(&p, D.guideSamples, 0xC0000000u, D.albedo.as<float4>(),
+                                  D.normalDepth.as<float4>(), m_stream));
+    const cudaError_t se = cudaStreamSynchronize(m_stream);
+    if (se != cudaSuccess) return guard(fromCuda(se, "denoiser guide kernel"));
+    MRT_TRY(guard(checkErrorFlags()));
+    D.guidesValid = true;
+    return MRT_SUCCESS;
+}
+
+mrtResult Engine::runDenoise() {
+    DenoiserState& D = m_denoiser;
+    const size_t pixels = size_t(m_settings.width) * m_settings.height;
+    MRT_TRY(ensureGuides());
+    MRT_TRY(guard(D.work.ensure(pixels * 48)));
+    MRT_TRY(guard(D.out.ensure(pixels * 16)));
+    D.params.width = m_settings.width;
+    D.params.height = m_settings.height;
+    MRT_CUDA(mrtcu_denoise(m_accum.as<double>(), D.albedo.as<float4>(), D.normalDepth.as<float4>(), &D.params,
+                           D.work.as<float4>(), D.out.as<float4>(), m_stream));
+    D.denoisedSpp = m_frameIndex;
+    return MRT_SUCCESS;
+}
+
+mrtResult Engine::readDenoised(float* rgba, size_t bytes) {
+    MRT_TRY(checkAlive());
+    MRT_TRY(flushPending());
+    if (!m_denoiser.enabled) return fail(MRT_ERROR_INVALID_ARGUMENT, "the denoiser is off (mrtxSetDenoiser)");
+    const size_t pixels = size_t(m_settings.width) * m_settings.height;
+    if (!rgba || bytes < pixels * 16) return fail(MRT_ERROR_INVALID_ARGUMENT, "dst too small for the denoised image");
+    MRT_TRY(runDenoise());
+    return guard(download(rgba, m_denoiser.out.ptr, pixels * 16));
+}
+
+mrtResult Engine::readDenoiserGuides(float* albedo, float* normalDepth, size_t bytes) {
+    MRT_TRY(checkAlive());
+    MRT_TRY(flushPending());
+    const size_t pixels = size_t(m_settings.width) * m_settings.height;
+    if (bytes < pixels * 16) return fail(MRT_ERROR_INVALID_ARGUMENT, "dst too small for the denoiser guides");
+    MRT_TRY(ensureGuides());
+    if (albedo) MRT_TRY(guard(download(albedo, m_denoiser.albedo.ptr, pixels * 16)));
+    if (normalDepth) MRT_TRY(guard(download(normalDepth, m_denoiser.normalDepth.ptr, pixels * 16)));
+    return MRT_SUCCESS;
 }
 
 // ---------------------------------------------------------------- queries --

@@ -76,6 +76,9 @@ public:
                              float* loss);
     mrtResult setCacheAveraging(float decay);
     mrtResult setCacheSchedule(float lrMin, float halfLifeSteps);
+    mrtResult setDenoiser(const mrtxDenoiserDesc& d);
+    mrtResult readDenoised(float* rgba, size_t bytes);
+    mrtResult readDenoiserGuides(float* albedo, float* normalDepth, size_t bytes);
     mrtResult buildMeshBvhDevice(const V4f* pos, size_t nv, const uint32_t* idx, size_t nt, uint32_t maxLeaf,
                                  WideBvh& out);
     // Device build from device positions/indices into the builder's own
@@ -164,6 +167,20 @@ private:
         float lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
         void release();
     } m_cache;
+    // Opt-in denoiser (mrtxSetDenoiser): guides once per accumulation, the
+    // filtered image re-made on the reference's doubling schedule.
+    struct DenoiserState {
+        bool enabled = false;
+        MrtDenoiseParams params{0, 0, 5, 0.5f, 64.0f, 0.1f, 0.1f, 0.01f};
+        uint32_t guideSamples = 4, minSpp = 8;
+        DeviceBuffer albedo, normalDepth, work, out;
+        bool guidesValid = false, useDenoised = false;
+        uint32_t nextAt = 8, denoisedSpp = 0;
+        void release();
+    } m_denoiser;
+    bool denoiserActive() const { return m_denoiser.enabled && m_settings.denoise; }
+    mrtResult ensureGuides();
+    mrtResult runDenoise();
     mrtResult ensureCache();
     void cacheBounds();
     mrtResult cacheWaveBuffers(uint32_t samples, uint32_t maxBounces);

@@ -51,7 +51,7 @@ def test_reference_abi_function_set(mrt_lib):
 
 STRUCTS = ["mrtEngineDesc", "mrtMeshDesc", "mrtMaterialDesc", "mrtTextureDesc", "mrtLightDesc", "mrtCameraDesc",
            "mrtCameraDescEx", "mrtRenderSettings", "mrtFrameInfo", "mrtCommitStats", "mrtxRay", "mrtxHit",
-           "mrtxStats", "mrtxRadianceCacheDesc"]
+           "mrtxStats", "mrtxRadianceCacheDesc", "mrtxDenoiserDesc"]
 
 
 def test_ctypes_layouts_match_c(mrt_lib):
@@ -60,7 +60,8 @@ def test_ctypes_layouts_match_c(mrt_lib):
           "mrtTextureDesc": abi.TextureDesc, "mrtLightDesc": abi.LightDesc, "mrtCameraDesc": abi.CameraDesc,
           "mrtCameraDescEx": abi.CameraDescEx, "mrtRenderSettings": abi.RenderSettings,
           "mrtFrameInfo": abi.FrameInfo, "mrtCommitStats": abi.CommitStats, "mrtxRay": abi.Ray,
-          "mrtxHit": abi.Hit, "mrtxStats": abi.Stats, "mrtxRadianceCacheDesc": abi.RadianceCacheDesc}
+          "mrtxHit": abi.Hit, "mrtxStats": abi.Stats, "mrtxRadianceCacheDesc": abi.RadianceCacheDesc,
+          "mrtxDenoiserDesc": abi.DenoiserDesc}
     src = '#include <stdio.h>\n#include <stddef.h>\n#include "mrt_ext.h"\nint main(void){\n'
     for s in STRUCTS:
         src += f'printf("{s} %zu\\n", sizeof({s}));\n'
