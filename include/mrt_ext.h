@@ -294,7 +294,8 @@ typedef struct mrtxDenoiserDesc {
     uint32_t iterations;    /* filter passes, tap spacing 1, 2, 4, ... [5], at most 10 */
     uint32_t guideSamples;  /* camera rays per pixel of the guide pass [4] */
     uint32_t minSpp;        /* first denoised display at this many samples [8] */
-    float sigmaColor;       /* colour weight [0.5] (on colour / (1 + luminance)) */
+    float sigmaColor;       /* colour weight at 1 sample per pixel [1.0], on log(1 + colour);
+                               divided by sqrt(samples) as the noise falls */
     float normalPower;      /* normal weight exponent [64] */
     float sigmaAlbedo;      /* albedo weight [0.1] */
     float sigmaDepth;       /* distance weight, relative to distance and spacing [0.1] */

@@ -10,7 +10,8 @@
 // floored), so texture detail is not blurred, then multiplies the albedo
 // back. Pass i (i = 0 .. iterations-1) takes the 5 x 5 B3-spline taps
 // (1/16, 1/4, 3/8, 1/4, 1/16) at spacing 2^i, each weighted by
-//   colour:  exp(-|c_p - c_q|^2 / (sigmaColor^2 2^-i)),  c = colour / (1 + luminance)
+//   colour:  exp(-|c_p - c_q|^2 / (s^2 2^-i)),  c = log(1 + colour) per channel,
+//            s = sigmaColor / sqrt(samples) (the noise falls as 1/sqrt(samples))
 //   normal:  max(0, n_p . n_q)^normalPower
 //   albedo:  exp(-|a_p - a_q|^2 / sigmaAlbedo^2)
 //   depth:   exp(-|z_p - z_q| / (sigmaDepth z_p 2^i))
@@ -26,15 +27,18 @@ namespace {
 
 constexpr int kTile = 16;
 
-__device__ float lum(float3 c) { return 0.2126f * c.x + 0.7152f * c.y + 0.0722f * c.z; }
 __device__ float3 f3of(float4 v) { return make_float3(v.x, v.y, v.z); }
 __device__ float dist2(float3 a, float3 b) {
     const float x = a.x - b.x, y = a.y - b.y, z = a.z - b.z;
     return x * x + y * y + z * z;
 }
-__device__ float3 compress(float3 c) {
-    const float s = 1.0f / (1.0f + fmaxf(lum(c), 0.0f));
-    return make_float3(c.x * s, c.y * s, c.z * s);
+// The colour the weights compare: log(1 + colour), the demodulated value
+// times the floored albedo (a log keeps bright and dim pixels apart at any
+// exposure).
+__device__ float3 logColour(float3 irr, float3 al, float floorA) {
+    return make_float3(__logf(1.0f + fmaxf(irr.x * fmaxf(al.x, floorA), 0.0f)),
+                       __logf(1.0f + fmaxf(irr.y * fmaxf(al.y, floorA), 0.0f)),
+                       __logf(1.0f + fmaxf(irr.z * fmaxf(al.z, floorA), 0.0f)));
 }
 
 // Mean colour of the FP64 accumulation divided by the albedo guide, and the
@@ -64,7 +68,7 @@ __global__ void __launch_bounds__(kTile * kTile) atrousKernel(const float4* __re
     if (x >= w || y >= h) return;
     const float kB3[3] = {0.375f, 0.25f, 0.0625f};
     const size_t p = size_t(y) * w + x;
-    const float3 cp = f3of(in[p]), ccp = compress(cp), ap = f3of(albedo[p]);
+    const float3 ap = f3of(albedo[p]), ccp = logColour(f3of(in[p]), ap, d.albedoFloor);
     const float4 np = unitNormal[p];
     const bool hitP = np.w > 0.0f;
     const float invAlbedo2 = 1.0f / (d.sigmaAlbedo * d.sigmaAlbedo);
@@ -78,13 +82,14 @@ __global__ void __launch_bounds__(kTile * kTile) atrousKernel(const float4* __re
             const int xx = x + dx * step;
             if (xx < 0 || xx >= w) continue;
             const size_t q = size_t(yy) * w + xx;
-            const float3 cq = f3of(in[q]);
             const float4 nq = unitNormal[q];
             if ((nq.w > 0.0f) != hitP) continue;
-            float wgt = kB3[dx < 0 ? -dx : dx] * kB3[dy < 0 ? -dy : dy] * __expf(-dist2(ccp, compress(cq)) * invColor2);
+            const float3 cq = f3of(in[q]), aq = f3of(albedo[q]);
+            float wgt = kB3[dx < 0 ? -dx : dx] * kB3[dy < 0 ? -dy : dy] *
+                        __expf(-dist2(ccp, logColour(cq, aq, d.albedoFloor)) * invColor2);
             if (hitP) {
                 const float nd = fmaxf(np.x * nq.x + np.y * nq.y + np.z * nq.z, 0.0f);
-                wgt *= __powf(nd, d.normalPower) * __expf(-dist2(ap, f3of(albedo[q])) * invAlbedo2) *
+                wgt *= __powf(nd, d.normalPower) * __expf(-dist2(ap, aq) * invAlbedo2) *
                        __expf(-fabsf(np.w - nq.w) * invDepth);
             }
             sum.x += wgt * cq.x;
@@ -120,7 +125,8 @@ extern "C" cudaError_t mrtcu_denoise(const double* accum, const float4* albedo, 
                                                  d->albedoFloor, src, unitNormal);
     const dim3 grid((d->width + kTile - 1) / kTile, (d->height + kTile - 1) / kTile), block(kTile, kTile);
     for (uint32_t i = 0; i < d->iterations; ++i) {
-        const float sigma2 = d->sigmaColor * d->sigmaColor * ldexpf(1.0f, -int(i));
+        const float noise2 = d->sigmaColor * d->sigmaColor / float(d->samples > 0 ? d->samples : 1);
+        const float sigma2 = noise2 * ldexpf(1.0f, -int(i));
         atrousKernel<<<grid, block, 0, stream>>>(src, dst, albedo, unitNormal, *d, 1 << i, 1.0f / sigma2);
         float4* t = src;
         src = dst;

@@ -108,7 +108,7 @@ cudaError_t mrtcu_readback_rgba32f(const double* accum, size_t npix, uint32_t sp
 
 // Opt-in denoiser (denoise.cu): parameters of the a-trous filter.
 typedef struct MrtDenoiseParams {
-    uint32_t width, height, iterations;
+    uint32_t width, height, iterations, samples;  // samples: per pixel in the accumulation
     float sigmaColor, normalPower, sigmaAlbedo, sigmaDepth, albedoFloor;
 } MrtDenoiseParams;
 // Denoiser guides of every pixel: mean first-hit albedo (a = 1) and shading

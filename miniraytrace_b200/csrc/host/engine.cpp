@@ -1528,7 +1528,7 @@ mrtResult Engine::setDenoiser(const mrtxDenoiserDesc& d) {
     DenoiserState& D = m_denoiser;
     D.enabled = d.enabled != 0;
     D.params.iterations = d.iterations ? d.iterations : 5u;
-    D.params.sigmaColor = d.sigmaColor > 0.0f ? d.sigmaColor : 0.5f;
+    D.params.sigmaColor = d.sigmaColor > 0.0f ? d.sigmaColor : 1.0f;
     D.params.normalPower = d.normalPower > 0.0f ? d.normalPower : 64.0f;
     D.params.sigmaAlbedo = d.sigmaAlbedo > 0.0f ? d.sigmaAlbedo : 0.1f;
     D.params.sigmaDepth = d.sigmaDepth > 0.0f ? d.sigmaDepth : 0.1f;
@@ -1580,6 +1580,7 @@ mrtResult Engine::runDenoise() {
     MRT_TRY(guard(D.out.ensure(pixels * 16)));
     D.params.width = m_settings.width;
     D.params.height = m_settings.height;
+    D.params.samples = m_frameIndex;
     MRT_CUDA(mrtcu_denoise(m_accum.as<double>(), D.albedo.as<float4>(), D.normalDepth.as<float4>(), &D.params,
                            D.work.as<float4>(), D.out.as<float4>(), m_stream));
     D.denoisedSpp = m_frameIndex;

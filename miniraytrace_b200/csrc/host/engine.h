@@ -171,7 +171,7 @@ private:
     // filtered image re-made on the reference's doubling schedule.
     struct DenoiserState {
         bool enabled = false;
-        MrtDenoiseParams params{0, 0, 5, 0.5f, 64.0f, 0.1f, 0.1f, 0.01f};
+        MrtDenoiseParams params{0, 0, 5, 0, 1.0f, 64.0f, 0.1f, 0.1f, 0.01f};
         uint32_t guideSamples = 4, minSpp = 8;
         DeviceBuffer albedo, normalDepth, work, out;
         bool guidesValid = false, useDenoised = false;

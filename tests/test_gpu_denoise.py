@@ -21,8 +21,8 @@ pytestmark = pytest.mark.gpu
 B3 = np.array([0.375, 0.25, 0.0625], np.float32)
 
 
-def denoise_numpy(mean, albedo, normal_depth, iterations=5, sigma_color=0.5, normal_power=64.0, sigma_albedo=0.1,
-                  sigma_depth=0.1, floor=0.01):
+def denoise_numpy(mean, albedo, normal_depth, samples, iterations=5, sigma_color=1.0, normal_power=64.0,
+                  sigma_albedo=0.1, sigma_depth=0.1, floor=0.01):
     """The a-trous passes of csrc/cuda/denoise.cu in float32 numpy."""
     h, w = mean.shape[:2]
     al = albedo[..., :3].astype(np.float32)
@@ -33,17 +33,12 @@ def denoise_numpy(mean, albedo, normal_depth, iterations=5, sigma_color=0.5, nor
     un = np.where(ln > 0, n / np.where(ln > 0, ln, 1), 0).astype(np.float32)
     z = normal_depth[..., 3].astype(np.float32)
     hit = z > 0
-    lum_w = np.array([0.2126, 0.7152, 0.0722], np.float32)
-
-    def compress(c):
-        return c / (1.0 + np.maximum((c * lum_w).sum(-1, keepdims=True), 0.0))
-
     src = irr
     ys, xs = np.mgrid[0:h, 0:w]
     for i in range(iterations):
         step = 1 << i
-        inv_c2 = np.float32(1.0 / (sigma_color * sigma_color * 2.0 ** -i))
-        cc = compress(src)
+        inv_c2 = np.float32(1.0 / (sigma_color * sigma_color / samples * 2.0 ** -i))
+        cc = np.log1p(np.maximum(src * alf, 0.0)).astype(np.float32)
         inv_d = np.where(hit, 1.0 / (sigma_depth * np.where(hit, z, 1) * step), 0).astype(np.float32)
         acc = np.zeros_like(src)
         wsum = np.zeros((h, w), np.float32)
@@ -111,7 +106,7 @@ def test_filter_matches_numpy_restatement(gpu):
     mean = acc[..., :3] / acc[..., 3:4]
     albedo, nd = e.read_denoiser_guides()
     got = e.read_denoised()
-    want = denoise_numpy(mean, albedo, nd)
+    want = denoise_numpy(mean, albedo, nd, 16)
     assert np.all(got[..., 3] == 1.0)
     peak = float(np.abs(want).max())
     err = np.abs(got[..., :3] - want)
