@@ -50,7 +50,7 @@ PKG = Path(__file__).resolve().parent
 ROOT = PKG.parent
 
 DEFAULTS = {"MRT_TRAV_MIN_BLOCKS": 7, "MRT_TRI_PHASE_PCT": 25, "MRT_REFILL_IDLE": 8, "MRT_SHADE_THREADS": 256,
-            "MRT_SHADOW_OVERLAP": 1, "MRT_SHARED_STACK": 8}
+            "MRT_SHADOW_OVERLAP": 1, "MRT_SHARED_STACK": 0}
 SPACE = {
     "MRT_TRAV_MIN_BLOCKS": [6, 7, 8],
     "MRT_TRI_PHASE_PCT": [12, 25, 50, 75],
