@@ -456,7 +456,7 @@ def ours_arm(args):
                          "note": "algorithmic bytes = node records x %d B + triangle tests x %d B + rays x %d B of "
                                  "queue/ray/hit I/O, counted in the timed launches; most node and triangle reads "
                                  "are served by L1/L2, so frac is against HBM but the data path is on-chip; "
-                                 "traffic = ncu DRAM bytes per closest-hit ray (1-spp capture of the same scene) "
+                                 "traffic = ncu DRAM bytes per closest-hit ray (bounces 0-2 of a 4-spp step of the same scene) "
                                  "x rays per step / launches per step"
                                  % (c["nodeBytes"], c["triBytes"], RAY_IO_BYTES)},
             "roofline_l2": {"bound": "l2", "achieved": achieved, "peak": l2_gbs, "unit": "GB/s",
@@ -465,7 +465,7 @@ def ours_arm(args):
                             "peak_source": "measured in this process (mrtxMeasureL2Bandwidth): every SM re-reads a "
                                            "32 MiB buffer with L2-only loads, 32 passes, CUDA events",
                             "note": "the extend kernel is bound by instruction issue (ncu, bounce 1 of a 4-spp frame: "
-                                    "80% of issue slots busy, 10.0 threads per warp instruction), not by L2"},
+                                    "79% of issue slots busy, ALU pipe 66%, 12.7 threads per warp instruction), not by L2"},
             "rays_closest_per_step": c["raysClosest"],
             "per_ray": {"closest_nodes": c["nodeFetches"] / max(1, c["raysClosest"]),
                         "closest_tris": c["triTests"] / max(1, c["raysClosest"]),
