@@ -124,6 +124,7 @@ typedef struct MrtCacheArgs {
     uint32_t rCap;
     uint32_t trainStride;
     uint32_t recordBounces;  // training paths record their vertices 1..recordBounces
+    float spreadC;           // path-spread threshold c of the query vertex (a_n > c a_0)
 } MrtCacheArgs;
 
 // Everything one path-tracing launch reads; passed by value as the kernel

@@ -392,6 +392,7 @@ __global__ void __launch_bounds__(kShadeBlock) waveShadeKernel(MrtFrameParams Pk
             const uint32_t bounce = __float_as_uint(d4.w);
             float3 ro = f3(o4), rd = f3(d4), beta = f3(b4), L = f3(L4);
             float prevBsdfPdf = o4.w;
+            float spread = L4.w;  // cache mode: what is left of the path's spread budget
             const uint32_t tri = __float_as_uint(h4.w);
             if (tri == 0xffffffffu) {
                 const float3 env = envRadiance(P, rd);
@@ -419,6 +420,20 @@ __global__ void __launch_bounds__(kShadeBlock) waveShadeKernel(MrtFrameParams Pk
                     if (mat.tex[4] >= 0) emission = emission * texRgb(P, mat.tex[4], s.uv);
                     if (maxComp(emission) > 0.0f && s.frontFace) L += beta * emission;
                     const Bsdf bsdf = makeBsdf(P, s);
+                    if (kCache) {
+                        // Path spread (Mueller et al. 2021, "Real-time Neural
+                        // Radiance Caching", section 3.4): the camera vertex
+                        // sets the budget sqrt(c a0), a0 = t^2 / (4 pi cos);
+                        // every later vertex spends t / sqrt(p cos) of it, p
+                        // the solid-angle pdf of the bounce that reached it.
+                        // A path is queried at the first vertex past bounce 0
+                        // with the budget spent, so sharp reflections and
+                        // refractions carry on to the surfaces they show
+                        // instead of showing the cache's smooth prediction.
+                        const float cosHit = fmaxf(fabsf(dot(rd, s.nGeom)), 1e-4f);
+                        if (bounce == 0u) spread = h4.x * sqrtf(K.spreadC * 0.0795774715f / cosHit);  // 1 / (4 pi)
+                        else spread -= h4.x * rsqrtf(fmaxf(prevBsdfPdf * cosHit, 1e-30f));
+                    }
                     if (kCache && bounce >= 1u) {
                         // A query (the cache stands for everything scattered
                         // from here on) or, on a training path's first
@@ -426,7 +441,8 @@ __global__ void __launch_bounds__(kShadeBlock) waveShadeKernel(MrtFrameParams Pk
                         // written out here.
                         // (Queries and records append in separate branches: a
                         // coalesced group then shares one list.)
-                        cacheQuery = !cacheTrainingPath(K, pixel, frameOf(P, A, lslot));
+                        const bool training = cacheTrainingPath(K, pixel, frameOf(P, A, lslot));
+                        cacheQuery = !training && spread <= 0.0f;
                         const float4 b4 = make_float4(beta.x, beta.y, beta.z, __uint_as_float(slot));
                         if (cacheQuery) {
                             const uint32_t idx = coalescedAppend(K.qCount);
@@ -434,7 +450,7 @@ __global__ void __launch_bounds__(kShadeBlock) waveShadeKernel(MrtFrameParams Pk
                                 writeCacheFeatures(K.qFeat + size_t(idx) * 16, s, -rd, bsdf);
                                 K.qBeta[idx] = b4;
                             }
-                        } else if (bounce <= K.recordBounces) {
+                        } else if (training && bounce <= K.recordBounces) {
                             const uint32_t idx = coalescedAppend(K.rCount);
                             if (idx < K.rCap) {
                                 writeCacheFeatures(K.rFeat + size_t(idx) * 16, s, -rd, bsdf);
@@ -483,7 +499,7 @@ __global__ void __launch_bounds__(kShadeBlock) waveShadeKernel(MrtFrameParams Pk
                     }
                 }
             }
-            S.L[slot] = make_float4(L.x, L.y, L.z, 0.0f);
+            S.L[slot] = make_float4(L.x, L.y, L.z, kCache ? spread : 0.0f);
             if (cont) {
                 S.rayO[slot] = make_float4(ro.x, ro.y, ro.z, prevBsdfPdf);
                 S.rayD[slot] = make_float4(rd.x, rd.y, rd.z, __uint_as_float(bounce + 1u));

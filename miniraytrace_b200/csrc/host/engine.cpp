@@ -2095,6 +2095,7 @@ mrtResult Engine::cacheWaveBuffers(uint32_t samples, uint32_t maxBounces) {
     K.rCap = uint32_t(r);
     K.trainStride = stride;
     K.recordBounces = vertices;
+    K.spreadC = 0.01f;  // the neural radiance caching paper's c
     cacheBounds();
     return MRT_SUCCESS;
 }
