@@ -13,6 +13,8 @@ The tunable constants are preprocessor defines of the CUDA sources:
 - ``MRT_REFILL_IDLE``: idle lanes of a persistent traversal warp before it
   takes new rays from the queue;
 - ``MRT_SHADE_THREADS``: threads per block of the shade kernel;
+- ``MRT_SHADE_MIN_BLOCKS``: resident blocks per SM the shade kernel is
+  compiled for (a register bound; 0: none, about 100 registers);
 - ``MRT_SHADOW_OVERLAP``: 1 runs a bounce's shadow kernel on a second stream
   beside the next bounce's extend kernel, 0 runs every kernel in order;
 - ``MRT_SHARED_STACK``: traversal stack entries per thread held in shared
@@ -50,7 +52,7 @@ PKG = Path(__file__).resolve().parent
 ROOT = PKG.parent
 
 DEFAULTS = {"MRT_TRAV_MIN_BLOCKS": 7, "MRT_TRI_PHASE_PCT": 25, "MRT_REFILL_IDLE": 8, "MRT_SHADE_THREADS": 256,
-            "MRT_SHADOW_OVERLAP": 1, "MRT_SHARED_STACK": 0}
+            "MRT_SHADOW_OVERLAP": 1, "MRT_SHARED_STACK": 0, "MRT_SHADE_MIN_BLOCKS": 0}
 SPACE = {
     "MRT_TRAV_MIN_BLOCKS": [6, 7, 8],
     "MRT_TRI_PHASE_PCT": [12, 25, 50, 75],
@@ -58,6 +60,7 @@ SPACE = {
     "MRT_SHADE_THREADS": [128, 256, 512],
     "MRT_SHADOW_OVERLAP": [0, 1],
     "MRT_SHARED_STACK": [0, 8, 16],
+    "MRT_SHADE_MIN_BLOCKS": [0, 2, 3],
 }
 
 

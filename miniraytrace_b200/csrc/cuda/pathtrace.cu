@@ -328,11 +328,21 @@ MRT_DEV void writeCacheFeatures(float* out, const Surface& s, float3 wo, const B
     f[3] = make_float4(bsdf.baseColor.z, 0.0f, 0.0f, 0.0f);
 }
 
-// Threads per block of the shade kernel.
+// Threads per block of the shade kernel and, when non-zero, the minimum
+// resident blocks per SM it is compiled for (a register bound; 0 leaves the
+// register count, about 100, to the compiler).
 #ifndef MRT_SHADE_THREADS
 #define MRT_SHADE_THREADS 256
 #endif
+#ifndef MRT_SHADE_MIN_BLOCKS
+#define MRT_SHADE_MIN_BLOCKS 0
+#endif
 constexpr uint32_t kShadeBlock = MRT_SHADE_THREADS;
+#if MRT_SHADE_MIN_BLOCKS > 0
+#define MRT_SHADE_BOUNDS __launch_bounds__(kShadeBlock, MRT_SHADE_MIN_BLOCKS)
+#else
+#define MRT_SHADE_BOUNDS __launch_bounds__(kShadeBlock)
+#endif
 
 // Appends to two lists at once, one atomic per list per block (a per-warp
 // atomic on the same counter serialised in L2: 4.2 M a bounce at 1080p x 64
@@ -363,7 +373,7 @@ MRT_DEV void blockAppend2(uint32_t* ca, bool pa, uint32_t& ia, uint32_t* cb, boo
 }
 
 template <bool kCache, bool kMulti>
-__global__ void __launch_bounds__(kShadeBlock) waveShadeKernel(MrtFrameParams Pk, MrtWaveState S, WaveArgs Ak,
+__global__ void MRT_SHADE_BOUNDS waveShadeKernel(MrtFrameParams Pk, MrtWaveState S, WaveArgs Ak,
                                                                uint32_t cur, MrtCacheArgs K, MrtBatchJobs B) {
     const uint32_t* __restrict__ q = S.queue[cur];
     uint32_t* __restrict__ qn = S.queue[cur ^ 1u];

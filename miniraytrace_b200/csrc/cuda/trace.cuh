@@ -634,13 +634,19 @@ MRT_DEV int travTriPhaseWarp(const MrtFrameParams& P, WideTrav& T, TraversalCoun
 #ifndef MRT_TRI_PHASE_PCT
 #define MRT_TRI_PHASE_PCT 25
 #endif
+// The same threshold for any-hit (shadow) walks, which end at their first
+// hit and so may prefer another balance of node and triangle work.
+#ifndef MRT_TRI_PHASE_PCT_ANY
+#define MRT_TRI_PHASE_PCT_ANY MRT_TRI_PHASE_PCT
+#endif
 template <bool kAny, bool kMulti = false, class Stack>
 MRT_DEV int travWarpStep(const MrtFrameParams& P, WideTrav& T, Stack& stack, TraversalCounters& tc,
                          bool active, const MrtBatchJob* jobs = nullptr, uint32_t job = 0u) {
     const bool pending = active && T.pendBits != 0;
     const uint32_t pendLanes = __popc(__ballot_sync(0xffffffffu, pending));
     const uint32_t activeLanes = __popc(__ballot_sync(0xffffffffu, active));
-    const bool triPhase = pendLanes * 100u >= activeLanes * MRT_TRI_PHASE_PCT || pendLanes == activeLanes;
+    const uint32_t pct = kAny ? MRT_TRI_PHASE_PCT_ANY : MRT_TRI_PHASE_PCT;
+    const bool triPhase = pendLanes * 100u >= activeLanes * pct || pendLanes == activeLanes;
 #ifdef MRT_TRAV_PROFILE
     {
         const uint32_t pairs = __reduce_add_sync(0xffffffffu, pending ? uint32_t(__popc(T.pendBits)) : 0u);

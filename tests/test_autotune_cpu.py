@@ -11,7 +11,7 @@ from miniraytrace_b200 import autotune, build
 
 def test_coordinate_descent_finds_the_fake_optimum(monkeypatch):
     optimum = {"MRT_TRAV_MIN_BLOCKS": 6, "MRT_TRI_PHASE_PCT": 50, "MRT_REFILL_IDLE": 8, "MRT_SHADE_THREADS": 512,
-               "MRT_SHADOW_OVERLAP": 0, "MRT_SHARED_STACK": 16}
+               "MRT_SHADOW_OVERLAP": 0, "MRT_SHARED_STACK": 16, "MRT_SHADE_MIN_BLOCKS": 2}
     seen = []
 
     def fake_measure(defines, workdir, steps, warmup):
