@@ -500,6 +500,44 @@ struct Carve {
 
 }  // namespace
 
+// The builder's stable LSD radix sort for other callers: `passes` 8-bit
+// passes (even, so the sorted pairs end in keysA / valsA) over n pairs.
+// scratch holds mrtcu_sort_pairs_scratch_words(n) words. n is limited so the
+// digit histogram (256 words a 2,048-pair tile) scans in two levels.
+extern "C" uint32_t mrtcu_sort_pairs_max(void) { return uint32_t(kScanSegment) * kScanSegment / 256u * kSortTile; }
+
+extern "C" size_t mrtcu_sort_pairs_scratch_words(uint32_t n) {
+    const size_t tiles = (size_t(n) + kSortTile - 1) / kSortTile, len = 256 * tiles;
+    return len + (len + kScanSegment - 1) / kScanSegment;
+}
+
+extern "C" cudaError_t mrtcu_sort_pairs(uint32_t* keysA, uint32_t* valsA, uint32_t* keysB, uint32_t* valsB,
+                                        uint32_t n, uint32_t passes, uint32_t* scratch, cudaStream_t stream) {
+    if (n <= 1) return cudaSuccess;
+    if ((passes & 1u) || passes > 4u || n > mrtcu_sort_pairs_max()) return cudaErrorInvalidValue;
+    const uint32_t tiles = (n + kSortTile - 1) / kSortTile;
+    uint32_t* hist = scratch;
+    uint32_t* segSums = scratch + size_t(256) * tiles;
+    for (uint32_t pass = 0; pass < passes; ++pass) {
+        const int shift = 8 * int(pass);
+        uint32_t* kIn = pass & 1 ? keysB : keysA;
+        uint32_t* vIn = pass & 1 ? valsB : valsA;
+        uint32_t* kOut = pass & 1 ? keysA : keysB;
+        uint32_t* vOut = pass & 1 ? valsA : valsB;
+        sortHistKernel<<<tiles, kSortThreads, 0, stream>>>(kIn, n, shift, hist, tiles);
+        const uint32_t len = 256u * tiles, segments = (len + kScanSegment - 1) / kScanSegment;
+        if (segments == 1) {
+            scanSegmentsKernel<<<1, kScanThreads, 0, stream>>>(hist, len, nullptr);
+        } else {
+            scanSegmentsKernel<<<segments, kScanThreads, 0, stream>>>(hist, len, segSums);
+            scanSegmentsKernel<<<1, kScanThreads, 0, stream>>>(segSums, segments, nullptr);
+            addSegmentOffsetsKernel<<<segments, kScanThreads, 0, stream>>>(hist, len, segSums);
+        }
+        sortScatterKernel<<<tiles, kSortThreads, 0, stream>>>(kIn, vIn, kOut, vOut, n, shift, hist, tiles);
+    }
+    return cudaGetLastError();
+}
+
 extern "C" size_t mrtcu_wide_bvh_scratch_bytes(uint32_t triCount) {
     const size_t n = triCount > 0 ? triCount : 1;
     const size_t tiles = (n + kSortTile - 1) / kSortTile;

@@ -165,9 +165,19 @@ cudaError_t mrtcu_rc_init(McacheParams C, uint32_t seed, cudaStream_t stream);
 cudaError_t mrtcu_rc_query(McacheParams C, const float* features, uint32_t n, float* out3, cudaStream_t stream);
 // Cache mode of a wave: predictions for n queries added to the paths'
 // radiance (scratch3: 3 floats per query), and training targets of n
-// records (3 floats each).
+// records (3 floats each). With sortScratch (mrtcu_rc_sort_scratch_words(n)
+// words) the queries are evaluated in Morton order of their positions.
+size_t mrtcu_rc_sort_scratch_words(uint32_t n);
 cudaError_t mrtcu_rc_apply_queries(McacheParams C, const float* qFeat, const float4* qBeta, uint32_t n,
-                                   uint32_t slots, float* scratch3, float4* L, cudaStream_t stream);
+                                   uint32_t slots, float* scratch3, float4* L, uint32_t* sortScratch,
+                                   cudaStream_t stream);
+// The BVH builder's stable LSD radix sort of (key, value) pairs: `passes`
+// 8-bit passes (even; sorted pairs end in keysA / valsA), n at most
+// mrtcu_sort_pairs_max(), scratch of mrtcu_sort_pairs_scratch_words(n) words.
+uint32_t mrtcu_sort_pairs_max(void);
+size_t mrtcu_sort_pairs_scratch_words(uint32_t n);
+cudaError_t mrtcu_sort_pairs(uint32_t* keysA, uint32_t* valsA, uint32_t* keysB, uint32_t* valsB, uint32_t n,
+                             uint32_t passes, uint32_t* scratch, cudaStream_t stream);
 cudaError_t mrtcu_rc_record_targets(const float4* prefix, const float4* beta, uint32_t n, uint32_t slots,
                                     const float4* L, float* targets, cudaStream_t stream);
 cudaError_t mrtcu_rc_train(McacheParams* C, const float* features, const float* targets, uint32_t n, uint32_t steps,

@@ -305,9 +305,13 @@ __device__ __forceinline__ void groupSync(uint32_t id) { asm volatile("bar.sync 
 // columns [64 h, 64 h + 64), and walks tiles blockIdx.x * kGroups + h,
 // stepping by gridDim.x * kGroups. (Warp w of the CTA reaches tensor-memory
 // lanes 32 (w % 4) .. 32 (w % 4) + 31, so every group covers all 128 lanes.)
+// With `order`, row i of the walk is query order[i] (its features read and
+// its prediction written there): queries sorted by position share the hash
+// grid's cells, so a warp's corner gathers hit the same lines.
 __global__ void __launch_bounds__(kTile* kQueryGroups, 3) tcQueryKernel(McacheParams C, const float* __restrict__ features,
                                                                      uint32_t n, float* __restrict__ out3,
-                                                                     bool clampOut) {
+                                                                     bool clampOut,
+                                                                     const uint32_t* __restrict__ order) {
     extern __shared__ __align__(1024) uint8_t smem[];
     uint8_t* sW = smem;  // W0..W4 (8 KiB each), W5 (2 KiB)
     uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kWAllBytes + kQueryGroups * kABytes);
@@ -339,8 +343,9 @@ __global__ void __launch_bounds__(kTile* kQueryGroups, 3) tcQueryKernel(McachePa
     bool ok = true;
     for (uint32_t tile = blockIdx.x * kQueryGroups + h; ok && size_t(tile) * kTile < n;
          tile += gridDim.x * kQueryGroups) {
-        const uint32_t q = tile * kTile + r;
-        const bool valid = q < n;
+        const uint32_t row = tile * kTile + r;
+        const bool valid = row < n;
+        const uint32_t q = valid && order ? order[row] : row;
         float f[16];
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
@@ -702,6 +707,31 @@ __global__ void recordTargetsKernel(const float4* __restrict__ prefix, const flo
     }
 }
 
+// 30-bit Morton code of each query's position in the cache's bounds (10
+// bits an axis) and its index: the keys that order a wave's queries.
+__device__ uint32_t spread3(uint32_t v) {  // 10 bits to every third of 30
+    v &= 0x3ffu;
+    v = (v | (v << 16)) & 0x030000ffu;
+    v = (v | (v << 8)) & 0x0300f00fu;
+    v = (v | (v << 4)) & 0x030c30c3u;
+    v = (v | (v << 2)) & 0x09249249u;
+    return v;
+}
+__global__ void queryKeysKernel(McacheParams C, const float* __restrict__ features, uint32_t n,
+                                uint32_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float4 f = reinterpret_cast<const float4*>(features)[size_t(i) * 4];
+        const float pos[3] = {f.x, f.y, f.z};
+        uint32_t q[3];
+        for (int a = 0; a < 3; ++a) {
+            const float u = fminf(fmaxf((pos[a] - C.lo[a]) * C.invExtent[a], 0.0f), 1.0f);
+            q[a] = uint32_t(u * 1023.0f);
+        }
+        keys[i] = spread3(q[0]) | (spread3(q[1]) << 1) | (spread3(q[2]) << 2);
+        vals[i] = i;
+    }
+}
+
 size_t smemQuery() { return kWAllBytes + kQueryGroups * kABytes + 8 * kQueryGroups + 16; }
 
 unsigned gridFor(size_t n) {
@@ -742,7 +772,7 @@ extern "C" cudaError_t mrtcu_rc_init(McacheParams C, uint32_t seed, cudaStream_t
 }
 
 static cudaError_t launchQuery(const McacheParams& C, const float* features, uint32_t n, float* out3, bool clampOut,
-                               cudaStream_t stream) {
+                               cudaStream_t stream, const uint32_t* order = nullptr) {
     if (n == 0) return cudaSuccess;
     cudaError_t e = cudaFuncSetAttribute(tcQueryKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smemQuery()));
     if (e != cudaSuccess) return e;
@@ -755,7 +785,7 @@ static cudaError_t launchQuery(const McacheParams& C, const float* features, uin
     const uint32_t groups = (n + kTile - 1) / kTile;
     const uint32_t want = (groups + kQueryGroups - 1) / kQueryGroups;
     const uint32_t ctas = want < uint32_t(sms) * 3u ? want : uint32_t(sms) * 3u;
-    tcQueryKernel<<<ctas, kTile * kQueryGroups, smemQuery(), stream>>>(C, features, n, out3, clampOut);
+    tcQueryKernel<<<ctas, kTile * kQueryGroups, smemQuery(), stream>>>(C, features, n, out3, clampOut, order);
     return cudaGetLastError();
 }
 
@@ -828,10 +858,27 @@ extern "C" cudaError_t mrtcu_rc_gradients(McacheParams* C, const float* features
     return cudaGetLastError();
 }
 
+extern "C" size_t mrtcu_rc_sort_scratch_words(uint32_t n) { return size_t(4) * n + mrtcu_sort_pairs_scratch_words(n); }
+
 extern "C" cudaError_t mrtcu_rc_apply_queries(McacheParams C, const float* qFeat, const float4* qBeta, uint32_t n,
-                                              uint32_t slots, float* scratch3, float4* L, cudaStream_t stream) {
+                                              uint32_t slots, float* scratch3, float4* L, uint32_t* sortScratch,
+                                              cudaStream_t stream) {
     if (n == 0) return cudaSuccess;
-    const cudaError_t e = launchQuery(C, qFeat, n, scratch3, kRenderClamp, stream);
+    // queries in Morton order of their positions (when a sort scratch is
+    // given and n is within the sort's limit); predictions land at each
+    // query's own index either way
+    const uint32_t* order = nullptr;
+    if (sortScratch && n <= mrtcu_sort_pairs_max()) {
+        uint32_t* keysA = sortScratch;
+        uint32_t* valsA = keysA + n;
+        uint32_t* keysB = valsA + n;
+        uint32_t* valsB = keysB + n;
+        queryKeysKernel<<<gridFor(n), 256, 0, stream>>>(C, qFeat, n, keysA, valsA);
+        const cudaError_t se = mrtcu_sort_pairs(keysA, valsA, keysB, valsB, n, 4u, valsB + n, stream);
+        if (se != cudaSuccess) return se;
+        order = valsA;
+    }
+    const cudaError_t e = launchQuery(C, qFeat, n, scratch3, kRenderClamp, stream, order);
     if (e != cudaSuccess) return e;
     applyQueriesKernel<<<gridFor(n), 256, 0, stream>>>(scratch3, qBeta, n, slots, L);
     return cudaGetLastError();

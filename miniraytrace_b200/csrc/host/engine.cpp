@@ -1805,7 +1805,7 @@ mrtResult Engine::buildMeshBvhDevice(const V4f* pos, size_t nv, const uint32_t* 
 
 void Engine::RadianceCache::release() {
     for (DeviceBuffer* d : {&grid, &mlp, &gGrid, &gMlp, &mGrid, &vGrid, &mMlp, &vMlp, &in, &out, &loss, &partial, &qFeat,
-                            &qBeta, &rFeat, &rPrefix, &rBeta, &rTarget, &counts, &scratch, &emaGrid, &emaMlp})
+                            &qBeta, &rFeat, &rPrefix, &rBeta, &rTarget, &counts, &scratch, &sortScratch, &emaGrid, &emaMlp})
         d->release();
     allocated = false;
 }
@@ -2078,6 +2078,7 @@ mrtResult Engine::cacheWaveBuffers(uint32_t samples, uint32_t maxBounces) {
     MRT_TRY(m_cache.qFeat.ensure(q * 16 * sizeof(float)));
     MRT_TRY(m_cache.qBeta.ensure(q * sizeof(float4)));
     MRT_TRY(m_cache.scratch.ensure(q * 3 * sizeof(float)));
+    MRT_TRY(m_cache.sortScratch.ensure(mrtcu_rc_sort_scratch_words(uint32_t(q)) * sizeof(uint32_t)));
     MRT_TRY(m_cache.rFeat.ensure(r * 16 * sizeof(float)));
     MRT_TRY(m_cache.rPrefix.ensure(r * sizeof(float4)));
     MRT_TRY(m_cache.rBeta.ensure(r * sizeof(float4)));
@@ -2114,7 +2115,7 @@ mrtResult Engine::cacheWave(const MrtFrameParams& p, uint32_t sampleBase, uint32
     const uint32_t slots = p.width * p.height * samples;
     MRT_CUDA(cudaEventRecord(ev[0], m_stream));
     MRT_CUDA(mrtcu_rc_apply_queries(inferenceParams(), K.qFeat, K.qBeta, nq, slots, m_cache.scratch.as<float>(),
-                                    m_waveState.L, m_stream));
+                                    m_waveState.L, m_cache.sortScratch.as<uint32_t>(), m_stream));
     MRT_CUDA(cudaEventRecord(ev[1], m_stream));
     MRT_CUDA(mrtcu_rc_record_targets(K.rPrefix, K.rBeta, nr, slots, m_waveState.L, m_cache.rTarget.as<float>(),
                                      m_stream));

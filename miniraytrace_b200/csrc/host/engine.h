@@ -151,6 +151,7 @@ private:
         DeviceBuffer grid, mlp, gGrid, gMlp, mGrid, vGrid, mMlp, vMlp, in, out, loss, partial;
         DeviceBuffer emaGrid, emaMlp;  // moving averages of the parameters, read by inference
         DeviceBuffer qFeat, qBeta, rFeat, rPrefix, rBeta, rTarget, counts, scratch;  // per-wave queries/records
+        DeviceBuffer sortScratch;  // Morton keys and order of a wave's queries
         MrtCacheArgs args{};
         McacheParams params{};
         bool allocated = false, enabled = false;
