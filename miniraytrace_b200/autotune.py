@@ -55,8 +55,8 @@ DEFAULTS = {"MRT_TRAV_MIN_BLOCKS": 7, "MRT_TRI_PHASE_PCT": 25, "MRT_REFILL_IDLE"
             "MRT_SHADOW_OVERLAP": 1, "MRT_SHARED_STACK": 0, "MRT_SHADE_MIN_BLOCKS": 0}
 SPACE = {
     "MRT_TRAV_MIN_BLOCKS": [6, 7, 8],
-    "MRT_TRI_PHASE_PCT": [12, 25, 50, 75],
-    "MRT_REFILL_IDLE": [4, 8, 16],
+    "MRT_TRI_PHASE_PCT": [6, 9, 12, 18, 25, 50, 75],
+    "MRT_REFILL_IDLE": [4, 6, 8, 10, 12, 16],
     "MRT_SHADE_THREADS": [128, 256, 512],
     "MRT_SHADOW_OVERLAP": [0, 1],
     "MRT_SHARED_STACK": [0, 8, 16],
