@@ -107,6 +107,11 @@ typedef struct mrtxStats {
      * together: 1, or the job count of a one-launch mrtxRenderBatch (whose
      * engines all report the batch's launches, times and counters) */
     uint32_t batchJobs;
+    /* last commit that rebuilt geometry or instances: mesh BVHs built on the
+     * GPU, and 1 if the instance tree (TLAS) was built there
+     * (mrtxSetBvhBuildThresholds) */
+    uint32_t commitDeviceBlas;
+    uint32_t commitDeviceTlas;
 } mrtxStats;
 /* out->structSize may be that of an earlier, shorter mrtxStats (fields are
  * only appended; at least up to cacheSteps): the fields it covers are written. */
@@ -140,6 +145,21 @@ MRT_API mrtResult mrtxSetSampleStream(mrtEngine*, uint32_t offset, uint32_t stri
  * empties (intersect.glsl:48-125) and every device error aborts the process
  * (core/src/gpu/GpuContext.hpp:22-31). */
 MRT_API mrtResult mrtxSetTraversalBudget(mrtEngine*, uint32_t maxVisits);
+
+/* Where the acceleration structures are built. A mesh of at least
+ * minTriangles triangles gets its BVH built on the engine's GPU (Morton
+ * codes, radix sort, LBVH topology, SAH-optimal collapse to 8-wide nodes),
+ * smaller meshes on host threads (binned SAH, the same collapse); an instance
+ * set of at least minInstances instances gets its TLAS built on the GPU by the
+ * same builder, a smaller one on the host. 0 selects the default (16384
+ * triangles, 2048 instances); 1 builds everything on the GPU and 0xFFFFFFFF
+ * everything on the host. Either site gives a valid tree over the same
+ * primitives, so closest hits and images do not depend on the choice; the
+ * host's SAH tree is slightly cheaper to trace, the GPU's is built in
+ * milliseconds. Takes effect at the next commit that rebuilds a mesh or the
+ * instances. The reference builds every BVH on the CPU
+ * (core/src/render/Renderer.cpp:342-368, 448-508). */
+MRT_API mrtResult mrtxSetBvhBuildThresholds(mrtEngine*, uint32_t minTriangles, uint32_t minInstances);
 
 /* Test hook for allocation failures: after this call the next
  * `succeedFirst` device or pinned-host allocations of the library succeed
@@ -258,9 +278,9 @@ MRT_API mrtResult mrtxBuildWideBvh(const float* aabbs, uint32_t count, uint32_t 
                                    uint32_t nodeCapacity, uint32_t* primOrderOut, uint32_t* nodeCountOut);
 
 /* Builders of mrtxBuildMeshBvh. */
-#define MRTX_BVH_HOST_SAH 0u     /* binned-SAH binary tree on the host (meshes below 65536 triangles) */
+#define MRTX_BVH_HOST_SAH 0u     /* binned-SAH binary tree on the host (by default meshes below 16384 triangles) */
 #define MRTX_BVH_HOST_LBVH 1u    /* Morton-code LBVH on the host: the device builder's reference */
-#define MRTX_BVH_DEVICE_LBVH 2u  /* the same LBVH built on the engine's GPU (meshes of 65536+ triangles) */
+#define MRTX_BVH_DEVICE_LBVH 2u  /* the same LBVH built on the engine's GPU (by default meshes of 16384+ triangles) */
 
 /* The 8-wide BVH the engine builds for a triangle mesh (positions: 3 floats
  * per vertex; indices: 3 per triangle, each < vertexCount), from the chosen

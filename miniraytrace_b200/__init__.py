@@ -397,6 +397,13 @@ class Engine:
         gives up and the call fails (0 = the default, 2^22)."""
         _check(self.lib.mrtxSetTraversalBudget(self.h, max_visits), "mrtxSetTraversalBudget")
 
+    def set_bvh_build_thresholds(self, min_triangles: int = 0, min_instances: int = 0):
+        """mrtxSetBvhBuildThresholds: meshes of at least min_triangles
+        triangles and instance sets of at least min_instances instances get
+        their BVH built on the GPU, smaller ones on the host (0 = default;
+        1 = always on the GPU; 0xFFFFFFFF = always on the host)."""
+        _check(self.lib.mrtxSetBvhBuildThresholds(self.h, min_triangles, min_instances), "mrtxSetBvhBuildThresholds")
+
     def copy_accumulation_device(self, dev_ptr: int, nbytes: int, accumulate: bool):
         _check(self.lib.mrtxCopyAccumulationDevice(self.h, C.c_void_p(dev_ptr), nbytes, 1 if accumulate else 0),
                "mrtxCopyAccumulationDevice")

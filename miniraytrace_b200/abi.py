@@ -138,7 +138,8 @@ class Stats(_Sized):
                 ("triBytes", C.c_uint32), ("extendMs", C.c_float), ("shadeMs", C.c_float), ("shadowMs", C.c_float),
                 ("otherMs", C.c_float), ("extendLaunches", C.c_uint32), ("cacheQueryMs", C.c_float),
                 ("cacheTrainMs", C.c_float), ("cacheQueries", C.c_uint64), ("cacheRecords", C.c_uint64),
-                ("cacheSteps", C.c_uint32), ("batchJobs", C.c_uint32)]
+                ("cacheSteps", C.c_uint32), ("batchJobs", C.c_uint32), ("commitDeviceBlas", C.c_uint32),
+                ("commitDeviceTlas", C.c_uint32)]
 
 
 LOG_FN = C.CFUNCTYPE(None, C.c_int, C.c_char_p, C.c_void_p)
@@ -187,6 +188,7 @@ FUNCTIONS = [
                                   C.POINTER(C.c_float)]),
     ("mrtxSetSampleStream", C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32]),
     ("mrtxSetTraversalBudget", C.c_int, [C.c_void_p, C.c_uint32]),
+    ("mrtxSetBvhBuildThresholds", C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32]),
     ("mrtxTraceRaysWavefront", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]),
     ("mrtxSetRadianceCacheAveraging", C.c_int, [C.c_void_p, C.c_float]),
     ("mrtxSetRadianceCacheSchedule", C.c_int, [C.c_void_p, C.c_float, C.c_float]),

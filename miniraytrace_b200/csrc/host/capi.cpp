@@ -298,6 +298,12 @@ MRT_API mrtResult mrtxSetTraversalBudget(mrtEngine* e, uint32_t maxVisits) {
     return guarded([&] { return eng->setTraversalBudget(maxVisits); });
 }
 
+MRT_API mrtResult mrtxSetBvhBuildThresholds(mrtEngine* e, uint32_t minTriangles, uint32_t minInstances) {
+    mrt::Engine* eng = unwrap(e);
+    if (!eng) return MRT_ERROR_INVALID_HANDLE;
+    return guarded([&] { return eng->setBvhBuildThresholds(minTriangles, minInstances); });
+}
+
 MRT_API mrtResult mrtxInjectAllocationFailure(int32_t succeedFirst) {
     mrt::setAllocationFailureInjection(succeedFirst);
     return MRT_SUCCESS;

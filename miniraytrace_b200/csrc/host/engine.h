@@ -65,6 +65,7 @@ public:
     mrtResult buildEnvCdf(const float* rgba, uint32_t w, uint32_t h, float* cdf, float* integral);
     mrtResult setSampleStream(uint32_t offset, uint32_t stride);
     mrtResult setTraversalBudget(uint32_t maxVisits);
+    mrtResult setBvhBuildThresholds(uint32_t minTriangles, uint32_t minInstances);
     mrtResult copyAccumulationDevice(void* dev, size_t bytes, bool accumulate);
     // 8-wide BVH of one triangle mesh built on this engine's GPU (LBVH
     // topology, SAH-optimal collapse), read back into `out`.
@@ -105,6 +106,7 @@ private:
     mrtResult packMaterials();
     mrtResult packGeometry(uint32_t& rebuilt);
     mrtResult packInstances();
+    mrtResult buildTlasOnDevice(const std::vector<Box3>& boxes, std::vector<uint32_t>& order, uint32_t& count);
     mrtResult packLights();
     mrtResult packEnvironment();
     mrtResult uploadTextures();
@@ -137,6 +139,8 @@ private:
     DeviceBuffer m_texTable;
     DeviceBuffer m_srgbLut;  // 256 floats: sRGB decode of k / 255
     uint32_t m_maxVisits = 0;  // traversal visit budget (0: the kernels' default)
+    // smallest mesh (triangles) and instance set whose BVH is built on the GPU
+    uint32_t m_deviceMinTriangles = 0, m_deviceMinInstances = 0;
     DeviceBuffer m_texData[MRT_MAX_TEXTURES];
     std::vector<uint32_t> m_texGeneration;
     // device frame state

@@ -280,3 +280,45 @@ def test_instance_tree_has_one_instance_per_leaf():
         per_leaf = [ref[1] for nd in nodes for _, kind, ref in children(nd) if kind == "leaf"]
         assert per_leaf and all(n == 1 for n in per_leaf)
         assert sorted(subtree_prims(nodes, order, 0)) == list(range(len(b)))
+
+
+def boxes_as_triangles(boxes):
+    """The engine's input to the device builder for an instance tree: each
+    box (lo, hi) becomes the degenerate triangle (lo, hi, lo)."""
+    b = np.asarray(boxes, np.float32)
+    pos = np.empty((2 * len(b), 3), np.float32)
+    pos[0::2], pos[1::2] = b[:, :3], b[:, 3:]
+    k = np.arange(len(b), dtype=np.uint32)
+    return pos, np.stack([2 * k, 2 * k + 1, 2 * k], 1)
+
+
+def test_instance_boxes_through_the_mesh_builder():
+    """The TLAS the device builds (mrtxSetBvhBuildThresholds): instance boxes
+    fed to the mesh builder as degenerate triangles. Checked here on its host
+    reference (the LBVH the device build equals node for node): every
+    triangle's box is exactly its instance's box, every instance sits in a
+    leaf of its own, also for nested and equal boxes, and every quantised
+    child box holds the instance boxes below it."""
+    rng = np.random.default_rng(5)
+    c = rng.uniform(-5, 5, (2500, 3))
+    r = rng.exponential(1.0, (2500, 1)) * rng.uniform(0.2, 1.0, (2500, 3))
+    boxes = np.concatenate([c - r, c + r], 1).astype(np.float32)
+    boxes[100:120] = boxes[0]
+    boxes[120:140, :3] = boxes[0, :3] - 1.0
+    boxes[120:140, 3:] = boxes[0, 3:] + 1.0
+    for b in (boxes[:1], boxes[:2], boxes[:3], boxes):
+        pos, idx = boxes_as_triangles(b)
+        tri = pos[idx]
+        assert np.array_equal(np.concatenate([tri.min(1), tri.max(1)], 1), b)
+        nodes, order = mrt.build_mesh_bvh(pos, idx, builder=1, max_leaf_prims=1)
+        assert sorted(order.tolist()) == list(range(len(b)))
+        per_leaf = [ref[1] for nd in nodes for _, kind, ref in children(nd) if kind == "leaf"]
+        assert per_leaf and all(n == 1 for n in per_leaf)
+        assert sorted(subtree_prims(nodes, order, 0)) == list(range(len(b)))
+        for ni, nd in enumerate(nodes):
+            s, k = grid(nd)
+            for slot, kind, ref in children(nd):
+                prims = subtree_prims(nodes, order, ref) if kind == "node" else order[ref[0]:ref[0] + ref[1]].tolist()
+                pb = b[prims].astype(np.float64)
+                assert (k + nd["qlo"][:, slot] <= pb[:, :3] / s).all(), (ni, slot)
+                assert (k + nd["qhi"][:, slot] >= pb[:, 3:] / s).all(), (ni, slot)
