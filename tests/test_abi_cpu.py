@@ -127,6 +127,8 @@ def test_null_and_short_struct_handling(mrt_lib):
     assert lib.mrtxReadAccumulation(None, None, 0, None) == abi.MRT_ERROR_INVALID_HANDLE
     assert lib.mrtxMeasureL2Bandwidth(None, None) == abi.MRT_ERROR_INVALID_HANDLE
     assert lib.mrtxGetStats(None, None) == abi.MRT_ERROR_INVALID_HANDLE
+    assert lib.mrtxSetBvhBuildThresholds(None, 1, 1) == abi.MRT_ERROR_INVALID_HANDLE
+    assert lib.mrtxSetTraversalBudget(None, 1) == abi.MRT_ERROR_INVALID_HANDLE
     assert lib.mrtGetLastErrorMessage() is not None
 
 
