@@ -19,6 +19,7 @@ builds a variant elsewhere, which is how the autotuner measures candidates.
 from __future__ import annotations
 
 import concurrent.futures as cf
+import fcntl
 import json
 import os
 import shutil
@@ -104,6 +105,18 @@ def build(force: bool = False, verbose: bool = False, defines: dict | None = Non
     bdir = Path(build_dir) if build_dir else BUILD
     bdir.mkdir(parents=True, exist_ok=True)
     BUILD.mkdir(exist_ok=True)
+    # one build at a time: the ranks of a multi-GPU run (and parallel test
+    # workers) call build() together; the first compiles, the others wait
+    # for its lock and then find every object fresh
+    with open(BUILD / ".build.lock", "w") as lock:
+        fcntl.flock(lock, fcntl.LOCK_EX)
+        try:
+            return _build_locked(force, verbose, defines, out, bdir)
+        finally:
+            fcntl.flock(lock, fcntl.LOCK_UN)
+
+
+def _build_locked(force, verbose, defines, out, bdir) -> Path:
     dflags = [f"-D{k}={v}" for k, v in sorted(defines.items())]
     stamp = bdir / "defines.txt"
     retune = not stamp.exists() or stamp.read_text() != " ".join(dflags)
