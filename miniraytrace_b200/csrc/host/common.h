@@ -4,6 +4,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <cstdint>
 #include <string>
@@ -38,6 +39,19 @@ bool isStickyCudaError(cudaError_t e);
 // set back to -1. allocationFailureInjected() is asked at each allocation.
 void setAllocationFailureInjection(int64_t succeedFirst);
 bool allocationFailureInjected();
+
+// A named range on the host timeline for profilers (NVTX, header-only;
+// without a tool attached a push or pop is one pointer test). The engine
+// marks commits, render calls and readbacks, so that for example
+// `ncu --nvtx --nvtx-include "mrt render/"` profiles only the kernels a
+// render call launches.
+class TraceRange {
+public:
+    explicit TraceRange(const char* name) { nvtxRangePushA(name); }
+    ~TraceRange() { nvtxRangePop(); }
+    TraceRange(const TraceRange&) = delete;
+    TraceRange& operator=(const TraceRange&) = delete;
+};
 
 }  // namespace mrt
 

@@ -466,6 +466,7 @@ mrtResult Engine::commit(mrtCommitStats* stats) {
 
 // reference Renderer.cpp:290-320
 mrtResult Engine::sync(mrtCommitStats* stats) {
+    const TraceRange range("mrt commit");
     const auto t0 = std::chrono::steady_clock::now();
     const uint32_t dirty = m_scene.dirty();
     if (dirty == DirtyNone) {
@@ -625,6 +626,7 @@ mrtResult Engine::buildBlasOnDevice(Blas& b) {
 // small ones on host threads (concurrently); the global arrays are then
 // assembled on the device (node rebase, triangle gather, attribute copies).
 mrtResult Engine::packGeometry(uint32_t& rebuilt) {
+    const TraceRange range("mrt commit: meshes");
     auto& meshes = m_scene.meshes();
     for (auto it = m_blas.begin(); it != m_blas.end();) {
         if (meshes.count(it->first)) {
@@ -735,6 +737,7 @@ mrtResult Engine::packGeometry(uint32_t& rebuilt) {
 // reference Renderer.cpp:448-508: TLAS over instance world bounds (leaf size
 // 1), instances stored in TLAS leaf order, TLAS nodes after the BLAS nodes.
 mrtResult Engine::packInstances() {
+    const TraceRange range("mrt commit: instances");
     std::vector<const InstanceData*> flat;
     std::vector<uint32_t> ids;
     std::vector<Box3> boxes;
@@ -893,6 +896,7 @@ mrtResult Engine::packLights() {
 // Environment map upload + CDF on the device (reference Renderer.cpp:605-662
 // builds it on the CPU).
 mrtResult Engine::packEnvironment() {
+    const TraceRange range("mrt commit: environment");
     m_hasEnv = m_scene.hasEnvironment();
     if (!m_hasEnv) {
         m_envW = m_envH = 0;
@@ -1138,6 +1142,7 @@ mrtResult Engine::flushPending() {
 // without waiting (completePending waits and collects the statistics).
 mrtResult Engine::launchPending() {
     if (m_pending == 0 || m_inFlight != 0) return MRT_SUCCESS;
+    const TraceRange range("mrt render");
     const uint32_t n = m_pending;
     m_pending = 0;
     m_stats.kernelLaunches = 0;
@@ -1221,6 +1226,7 @@ static mrtResult addStageTimes(const cudaEvent_t* ev, uint32_t bounces, float& e
 
 mrtResult Engine::completePending() {
     if (m_inFlight == 0) return MRT_SUCCESS;
+    const TraceRange range("mrt render: wait");
     const uint32_t n = m_inFlight, waves = m_inFlightWaves, bounces = m_inFlightBounces;
     m_inFlight = 0;
     const cudaError_t se = cudaStreamSynchronize(m_stream);
@@ -1290,6 +1296,7 @@ mrtResult Engine::completePending() {
 // (renderBatchOneLaunch); otherwise every engine's waves are issued on its
 // own stream before any is waited for, so jobs of uneven size overlap.
 mrtResult Engine::renderBatch(Engine* const* engines, const uint32_t* spp, uint32_t count, mrtFrameInfo* infos) {
+    const TraceRange range("mrt render batch");
     const auto t0 = std::chrono::steady_clock::now();
     // one set of launches when every engine is distinct, on one GPU and
     // without the radiance cache (an engine listed twice keeps the stream
@@ -1554,6 +1561,7 @@ mrtResult Engine::download(void* dst, const void* src, size_t bytes) {
 mrtResult Engine::readFramebuffer(mrtPixelFormat fmt, void* dst, size_t dstSize) {
     MRT_TRY(checkAlive());
     MRT_TRY(flushPending());
+    const TraceRange range("mrt readback");
     const size_t pixels = size_t(m_settings.width) * m_settings.height;
     if (fmt == MRT_PIXEL_RGBA8_SRGB) {
         if (dstSize < pixels * 4) return fail(MRT_ERROR_INVALID_ARGUMENT, "dst too small for RGBA8 readback");
