@@ -78,33 +78,45 @@ void buildRange(Ctx& c, uint32_t nodeId, uint32_t b, uint32_t e) {
         const float ext = cb.hi[a] - cb.lo[a];
         scale[a] = ext > 1e-20f ? kBins * (1.0f - 1e-6f) / ext : 0.0f;
     }
-    for (int a = 0; a < 3; ++a) {
-        if (scale[a] == 0.0f) continue;
-        Bounds bins[kBins];
-        uint32_t cnt[kBins] = {};
-        for (uint32_t i = b; i < e; ++i) {
-            const uint32_t p = c.idx[i];
+    // all three axes binned in one pass over the range
+    Bounds bins[3][kBins];
+    uint32_t cnt[3][kBins] = {};
+    for (uint32_t i = b; i < e; ++i) {
+        const uint32_t p = c.idx[i];
+        for (int a = 0; a < 3; ++a) {
+            if (scale[a] == 0.0f) continue;
             int k = int(scale[a] * (c.cent[3 * p + a] - cb.lo[a]));
             k = std::min(std::max(k, 0), kBins - 1);
-            bins[k].grow(c.boxes[p].lo, c.boxes[p].hi);
-            cnt[k]++;
+            bins[a][k].grow(c.boxes[p].lo, c.boxes[p].hi);
+            cnt[a][k]++;
         }
+    }
+    for (int a = 0; a < 3; ++a) {
+        if (scale[a] == 0.0f) continue;
+        // An empty bin changes neither bound nor count: the right-hand
+        // areas carry over it, and a split after it costs exactly what the
+        // split before it costs, which the strict comparison below keeps.
         float rArea[kBins];
         uint32_t rCnt[kBins];
         Bounds acc;
         uint32_t s = 0;
+        float area = 0.0f;
         for (int k = kBins - 1; k > 0; --k) {
-            acc.grow(bins[k]);
-            s += cnt[k];
-            rArea[k] = acc.area();
+            if (cnt[a][k]) {
+                acc.grow(bins[a][k]);
+                s += cnt[a][k];
+                area = acc.area();
+            }
+            rArea[k] = area;
             rCnt[k] = s;
         }
         Bounds lacc;
         uint32_t ls = 0;
         for (int k = 0; k < kBins - 1; ++k) {
-            lacc.grow(bins[k]);
-            ls += cnt[k];
-            if (ls == 0 || rCnt[k + 1] == 0) continue;
+            if (!cnt[a][k]) continue;
+            lacc.grow(bins[a][k]);
+            ls += cnt[a][k];
+            if (rCnt[k + 1] == 0) continue;
             const float cost = lacc.area() * ls + rArea[k + 1] * rCnt[k + 1];
             if (cost < bestCost) {
                 bestCost = cost;

@@ -322,3 +322,43 @@ def test_instance_boxes_through_the_mesh_builder():
                 pb = b[prims].astype(np.float64)
                 assert (k + nd["qlo"][:, slot] <= pb[:, :3] / s).all(), (ni, slot)
                 assert (k + nd["qhi"][:, slot] >= pb[:, 3:] / s).all(), (ni, slot)
+
+
+def test_host_builder_trees_are_unchanged():
+    """The host's binned-SAH builder and the 8-wide collapse, pinned by a
+    hash of their output on seeded inputs (boxes with nested and equal
+    members, a triangle soup, a heightfield): a change of the host trees,
+    which the measured traversal costs were taken with, shows up here."""
+    import hashlib
+
+    def boxes(n, seed):
+        rng = np.random.default_rng(seed)
+        c = rng.uniform(-5, 5, (n, 3))
+        r = rng.exponential(1.0, (n, 1)) * rng.uniform(0.2, 1.0, (n, 3))
+        b = np.concatenate([c - r, c + r], 1).astype(np.float32)
+        if n > 40:
+            b[10:20] = b[0]
+            b[20:30, :3] = b[0, :3] - 1
+            b[20:30, 3:] = b[0, 3:] + 1
+        return b
+
+    def digest(nodes, order):
+        return hashlib.sha256(nodes.tobytes() + order.tobytes()).hexdigest()[:16]
+
+    expected = {
+        "boxes1_leaf1": "c1d5f41ce809fa25", "boxes1_leaf3": "c1d5f41ce809fa25",
+        "boxes2_leaf1": "69fd58385c8c5ec6", "boxes2_leaf3": "df927126a9dfd8b7",
+        "boxes3_leaf1": "ece8ff83899983f7", "boxes3_leaf3": "0d92900593e276ae",
+        "boxes7_leaf1": "3d63154ff7b29788", "boxes7_leaf3": "3d63154ff7b29788",
+        "boxes100_leaf1": "8cb71f891b5ecf8c", "boxes100_leaf3": "062ce40d7f642c5f",
+        "boxes1000_leaf1": "a61b148f69d79feb", "boxes1000_leaf3": "0e7ed9077243481d",
+        "boxes5000_leaf1": "2b0c017692ffb5b4", "boxes5000_leaf3": "930b0d8062c56333",
+        "soup3000": "ff09c97e70e2a48a", "hf40": "f8bea9d16356041f",
+    }
+    got = {}
+    for n in (1, 2, 3, 7, 100, 1000, 5000):
+        for leaf in (1, 3):
+            got[f"boxes{n}_leaf{leaf}"] = digest(*mrt.build_wide_bvh(boxes(n, n), leaf))
+    for name, (p, i) in {"soup3000": soup_mesh(3000, 4), "hf40": heightfield_mesh(40, 3)}.items():
+        got[name] = digest(*mrt.build_mesh_bvh(p, i, 0))
+    assert got == expected
