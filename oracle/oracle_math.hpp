@@ -124,7 +124,10 @@ struct M4 {
 // columns c0, c1, c2 of R, the rows of R^-1 are (c1 x c2, c2 x c0, c0 x c1)
 // divided by det = c0 . (c1 x c2); the translation becomes -R^-1 t. The
 // reference uses glm::inverse (Renderer.cpp:475), whose rounding is not
-// restated here; both are exact for identity and translate/scale transforms.
+// restated here; both are exact for identity, translations and
+// power-of-two scales. For other scales s this formula's entries
+// s^2 * (1 / s^3) are within 2 ulp of 1/s, and glm's may round differently:
+// parity with the reference's inverse is unpinned there.
 template <class T>
 M4<T> inverse(const M4<T>& a) {
     const V3<T> c0(a.m[0][0], a.m[0][1], a.m[0][2]);
