@@ -547,3 +547,56 @@ def test_l2_bandwidth_probe(gpu):
     assert e.stats()["deviceBytes"] == base
     e.close()
 
+
+
+def test_managed_smoke_and_engine_lifecycle_cycles(gpu):
+    """The reference's managed smoke test (rhino/MiniRaytrace.Smoke/
+    Program.cs:33-130) through the C ABI: an emissive triangle at 64x64 and
+    4 spp (commit rebuilds exactly one BLAS, spp 4, a non-black RGBA8 image,
+    RGBA32F alpha 1), then 30 engine lifecycles on worker threads as its
+    render sessions run them (created on the render thread, a few frames of
+    an empty scene read back, destroyed). Every cycle completes, and the
+    device memory the process holds returns to its level after the first."""
+    import threading
+
+    import torch
+
+    e = gpu.Engine(64, 64)
+    m = e.add_mesh(np.array([[-0.6, -0.6, 0], [0.6, -0.6, 0], [0, 0.6, 0]], np.float32),
+                   np.array([0, 1, 2], np.uint32))
+    mat = e.add_material(base_color=(1.0, 0.2, 0.1), emission=(2.0, 0.4, 0.2))
+    assert e.add_instance(m, None, mat) != 0
+    e.set_camera(position=(0, 0, 3), target=(0, 0, 0))
+    e.set_render_settings(width=64, height=64, spp_limit=4, denoise=False)
+    assert e.commit()["blasRebuilt"] == 1
+    info = None
+    for _ in range(4):
+        info = e.render_frame()
+    assert info["spp"] == 4
+    rgba8 = e.read_framebuffer(abi.MRT_PIXEL_RGBA8_SRGB)
+    assert (rgba8[..., :3] > 10).any()
+    assert (e.read_framebuffer(abi.MRT_PIXEL_RGBA32F_LINEAR)[..., 3] == 1.0).all()
+    e.close()
+
+    def cycle(out):
+        try:
+            s = gpu.Engine(48, 48)
+            s.set_render_settings(width=48, height=48, denoise=False)
+            for _ in range(3):
+                s.commit()
+                s.render_frame()
+                img = s.read_framebuffer(abi.MRT_PIXEL_RGBA32F_LINEAR)
+            s.close()
+            out.append(bool(np.isfinite(img).all() and (img[..., 3] == 1.0).all()))
+        except Exception as ex:  # reported below
+            out.append(ex)
+
+    free = []
+    for i in range(30):
+        out = []
+        t = threading.Thread(target=cycle, args=(out,))
+        t.start()
+        t.join(timeout=60)
+        assert not t.is_alive() and out == [True], (i, out)
+        free.append(torch.cuda.mem_get_info()[0])
+    assert free[0] - min(free[1:]) < 64 << 20, [f >> 20 for f in free]
