@@ -86,7 +86,7 @@ def test_room_65536spp_relmse_against_fp64_oracle(gpu, oracle_lib):
 
 
 def test_time_to_relmse_reference_against_fp64_oracle(gpu, oracle_lib):
-    """The reference bench.py judges config 4's time to relMSE 1e-3 against:
+    """The reference image bench.py measures config 4's time to relMSE 1e-3 against:
     65,536 spp of the plain tracer (FP64 accumulation) over four 240x136
     windows of the 1920x1080 frame, each rendered through the exact
     sub-frustum of the frame's camera by its own engine. On a fixed random
