@@ -336,3 +336,51 @@ def test_env_cdf_equals_the_reference_loop(oracle_lib):
         rcdf, rintegral = oracle_lib.ref_env_cdf(sky)
         assert np.array_equal(cdf, rcdf), sky.shape
         assert np.float32(integral) == np.float32(rintegral), sky.shape
+
+
+def bvh2_depth(nodes):
+    """Levels of a BVH2 (root = 1). The reference's walks (intersect.glsl:
+    48-125) pop a node and push both children of an internal one, so a walk
+    holds at most `depth` stack entries."""
+    left = nodes["leftOrPrim"]
+    count = nodes["packed"] >> 2
+    best, stack = 0, [(0, 1)]
+    while stack:
+        n, d = stack.pop()
+        best = max(best, d)
+        if count[n] == 0:
+            stack += [(int(left[n]), d + 1), (int(left[n]) + 1, d + 1)]
+    return best
+
+
+def test_reference_stacks_hold_the_terrain_trees(oracle_lib):
+    """The reference walks a BLAS with a fixed 32-entry stack and the TLAS
+    with a 16-entry one, without overflow checks (intersect.glsl:51, 96, 132,
+    154), while the oracle restating the walks uses 64 entries. On the
+    terrain workload the reference builder's trees (4 triangles a BLAS leaf,
+    1 instance a TLAS leaf, Renderer.cpp:342-368, 448-508) are shallow enough
+    that the reference's stacks never overflow, so the two walks are the
+    same: 2,093,058-triangle heightfield and 1,280-triangle icosphere BLASes
+    (at most 32 levels), 257-instance TLAS (at most 16). (The largest
+    workload's trees, measured once: 19,999,980-triangle heightfield depth
+    25; 4,097-instance TLAS depth 16, which fills the reference's TLAS stack
+    exactly.)"""
+    from miniraytrace_b200 import scenes
+    s = scenes.terrain(64, 36, sky=(64, 32))
+    bounds = []
+    for m in s.meshes:
+        a = tri_aabbs(m.positions[m.indices.reshape(-1, 3)])
+        depth = bvh2_depth(oracle_lib.bvh_build(a, 4)[0])
+        assert depth <= 32, (len(a), depth)
+        bounds.append((a[:, :3].min(0), a[:, 3:].max(0)))
+    boxes = []
+    for mi, xf, _ in s.instances:
+        lo, hi = bounds[mi]
+        if xf is not None:
+            c = np.array([[x, y, z] for x in (lo[0], hi[0]) for y in (lo[1], hi[1]) for z in (lo[2], hi[2])])
+            w = c @ xf[:, :3].T.astype(np.float64) + xf[:, 3]
+            lo, hi = w.min(0), w.max(0)
+        boxes.append(np.concatenate([lo, hi]))
+    assert len(boxes) == 257
+    depth = bvh2_depth(oracle_lib.bvh_build(np.array(boxes, np.float32), 1)[0])
+    assert depth <= 16, depth
